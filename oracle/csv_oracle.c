@@ -1,0 +1,599 @@
+/* csv_oracle.c -- CPU restatement of the reference brick codec.
+ *
+ * TEST INFRASTRUCTURE ONLY (the oracle).  Loaded by tests/, by
+ * __graft_entry__.smoke() and by bench.py's CPU-baseline leg, as the checker.
+ * The product library never links or calls it.
+ *
+ * Each function cites the reference lines it restates.  Reference paths are
+ * relative to the reference project root.  Parity of this restatement is
+ * pinned in tests/test_oracle.py against the reference sources compiled as
+ * oracle/_ref/libcsvref.so (encode bytes, full-resolution decode, majority
+ * vote, rANS model) and against the shipped compressed_dataset.csbd.
+ */
+#include "csv_oracle.h"
+
+#include <stdlib.h>
+#include <string.h>
+
+#define EMPTY_LABEL UINT64_MAX /* types.hpp:19 */
+#define RANS_L (1u << 23)      /* types.hpp:24-28 */
+#define TOT_BITS 12u
+#define TOT (1u << TOT_BITS)
+
+enum { OP_RP = 0, OP_RX, OP_RY, OP_RZ, OP_PA, OP_P0, OP_PD }; /* types.hpp:162-171 */
+
+void or_free(void* p) { free(p); }
+
+/* ---------------------------------------------------------------- Morton */
+/* utils.cpp:4-21: 10 bits per axis, x in bit 0. */
+static uint32_t spread3(uint32_t v) {
+    uint32_t r = 0;
+    for (int i = 0; i < 10; ++i) r |= ((v >> i) & 1u) << (3 * i);
+    return r;
+}
+uint32_t or_morton3(uint32_t x, uint32_t y, uint32_t z) {
+    return spread3(x) | (spread3(y) << 1) | (spread3(z) << 2);
+}
+/* utils.cpp:24-43 */
+void or_demorton3(uint32_t m, uint32_t* x, uint32_t* y, uint32_t* z) {
+    uint32_t a = 0, b = 0, c = 0;
+    for (int i = 0; i < 10; ++i) {
+        a |= ((m >> (3 * i)) & 1u) << i;
+        b |= ((m >> (3 * i + 1)) & 1u) << i;
+        c |= ((m >> (3 * i + 2)) & 1u) << i;
+    }
+    *x = a; *y = b; *z = c;
+}
+
+/* ------------------------------------------------------------- majority */
+/* majorityVote8 (brick.hpp:24-37): std::max_element over a
+ * std::unordered_map<uint64_t,int> filled in child order 0..7.  With GNU
+ * libstdc++ the map has 13 buckets for up to 8 keys and the identity hash, so
+ * key k sits in bucket k % 13.  A key whose bucket is empty is linked at the
+ * front of the iteration list; a key whose bucket is occupied is linked just
+ * before that bucket's first key.  Iteration therefore visits bucket groups
+ * newest-group-first and, inside a group, newest-key-first; max_element keeps
+ * the first maximal count.  Equivalently: among keys with the maximal count,
+ * the winner maximises (first-insertion index of its bucket group, its own
+ * insertion index). */
+uint64_t or_majority8(const uint64_t* v) {
+    uint64_t key[8];
+    int cnt[8], grp[8], n = 0;
+    for (int i = 0; i < 8; ++i) {
+        int j;
+        for (j = 0; j < n; ++j)
+            if (key[j] == v[i]) break;
+        if (j < n) { cnt[j]++; continue; }
+        key[n] = v[i];
+        cnt[n] = 1;
+        grp[n] = n;
+        for (int k = 0; k < n; ++k)
+            if (key[k] % 13u == v[i] % 13u) { grp[n] = grp[k]; break; }
+        n++;
+    }
+    int best = 0;
+    for (int j = 1; j < n; ++j) {
+        if (cnt[j] > cnt[best] ||
+            (cnt[j] == cnt[best] && (grp[j] > grp[best] || (grp[j] == grp[best] && j > best))))
+            best = j;
+    }
+    return key[best];
+}
+
+/* -------------------------------------------------------------- pyramid */
+/* splitGridIntoBricks (brick.hpp:133-195): brick (bx,by,bz) voxel (dx,dy,dz)
+ * reads vol[gx + W*(gy + H*gz)], 0 outside the volume, stored at Morton
+ * index of (dx,dy,dz).  Brick::buildLevel (brick.hpp:92-123): parent m has
+ * children 8m..8m+7 (utils.cpp:45-68); constant = all 8 children equal the
+ * majority and are constant themselves; leaves are constant (brick.hpp:188).
+ * Levels are stored coarse-first here: level l at offset (8^l-1)/7. */
+static uint32_t levels_of(uint32_t b) {
+    uint32_t L = 0;
+    while ((1u << L) < b) L++;
+    return L + 1; /* std::bit_width(b), brick.hpp:50 */
+}
+static size_t level_off(uint32_t l) { return (((size_t)1 << (3 * l)) - 1) / 7; }
+
+static void cut_brick(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b,
+                      size_t bx, size_t by, size_t bz, uint64_t* leaf) {
+    for (uint32_t dz = 0; dz < b; ++dz)
+        for (uint32_t dy = 0; dy < b; ++dy)
+            for (uint32_t dx = 0; dx < b; ++dx) {
+                size_t gx = bx * b + dx, gy = by * b + dy, gz = bz * b + dz;
+                uint64_t lab = 0;
+                if (gx < W && gy < H && gz < D) lab = vol[gx + W * (gy + H * gz)];
+                leaf[or_morton3(dx, dy, dz)] = lab;
+            }
+}
+
+static void build_pyramid(uint32_t b, uint64_t* lab, uint8_t* cst) {
+    uint32_t L = levels_of(b);
+    size_t nleaf = (size_t)b * b * b;
+    memset(cst + level_off(L - 1), 1, nleaf);
+    for (int l = (int)L - 2; l >= 0; --l) {
+        size_t nn = (size_t)1 << (3 * l);
+        uint64_t* P = lab + level_off(l);
+        uint8_t* PC = cst + level_off(l);
+        const uint64_t* C = lab + level_off(l + 1);
+        const uint8_t* CC = cst + level_off(l + 1);
+        for (size_t m = 0; m < nn; ++m) {
+            uint64_t maj = or_majority8(C + 8 * m);
+            int same = 1;
+            for (int c = 0; c < 8; ++c) same &= (C[8 * m + c] == maj) && CC[8 * m + c];
+            P[m] = maj;
+            PC[m] = (uint8_t)same;
+        }
+    }
+}
+
+int or_pyramid(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b, uint32_t brick_index,
+               uint64_t* labels, uint8_t* constant) {
+    size_t nbx = (W + b - 1) / b, nby = (H + b - 1) / b, nbz = (D + b - 1) / b;
+    if (brick_index >= nbx * nby * nbz) return -1;
+    /* split order: bx outer, bz inner (brick.hpp:152-154) */
+    size_t bz = brick_index % nbz, by = (brick_index / nbz) % nby, bx = brick_index / (nbz * nby);
+    uint32_t L = levels_of(b);
+    cut_brick(vol, W, H, D, b, bx, by, bz, labels + level_off(L - 1));
+    build_pyramid(b, labels, constant);
+    return 0;
+}
+
+/* ------------------------------------------------------------ encoding */
+typedef struct { uint8_t* p; size_t n, cap; } buf_t;
+static void bput(buf_t* b, const void* src, size_t n) {
+    if (b->n + n > b->cap) {
+        size_t c = b->cap ? b->cap : 1024;
+        while (c < b->n + n) c *= 2;
+        b->p = (uint8_t*)realloc(b->p, c);
+        b->cap = c;
+    }
+    memcpy(b->p + b->n, src, n);
+    b->n += n;
+}
+static void bput32(buf_t* b, uint32_t v) { bput(b, &v, 4); }
+
+typedef struct {
+    uint64_t* pal; uint32_t np, pcap;
+    uint8_t* nib;  uint32_t nn, ncap; /* one nibble per byte while building */
+} enc_t;
+
+static void push_nib(enc_t* e, uint8_t v) {
+    if (e->nn == e->ncap) { e->ncap = e->ncap ? 2 * e->ncap : 4096; e->nib = (uint8_t*)realloc(e->nib, e->ncap); }
+    e->nib[e->nn++] = v & 15;
+}
+static void push_pal(enc_t* e, uint64_t v) {
+    if (e->np == e->pcap) { e->pcap = e->pcap ? 2 * e->pcap : 64; e->pal = (uint64_t*)realloc(e->pal, 8 * e->pcap); }
+    e->pal[e->np++] = v;
+}
+
+/* bestOperation (brickEncoding.hpp:188-318) for child `n` (Morton) at coarse
+ * level lc = l+1 with parent level l. */
+static int best_op(const uint64_t* lab, uint32_t lc, uint32_t n, uint64_t parent_label, enc_t* e, uint8_t* delta) {
+    const uint64_t* C = lab + level_off(lc);
+    const uint64_t* P = lab + level_off(lc - 1);
+    uint64_t L = C[n];
+    if (parent_label == L) return OP_RP; /* :202-203 */
+    uint32_t x, y, z;
+    or_demorton3(n, &x, &y, &z);
+    int size = 1 << lc;
+    for (int axis = 0; axis < 3; ++axis) { /* X, Y, Z order: :277-282 */
+        int c[3] = {(int)x, (int)y, (int)z};
+        c[axis] += (c[axis] & 1) ? 1 : -1; /* outside the sibling block: :224-240 */
+        if (c[axis] < 0 || c[axis] >= size) continue; /* :244-246 */
+        uint32_t nm = or_morton3((uint32_t)c[0], (uint32_t)c[1], (uint32_t)c[2]);
+        if (nm < n) {
+            if (C[nm] == L) return OP_RX + axis; /* :256-261 */
+        } else {
+            /* neighbor's parent (:265-272); levelIndex = lc > 0 always here */
+            if (P[or_morton3((uint32_t)c[0] >> 1, (uint32_t)c[1] >> 1, (uint32_t)c[2] >> 1)] == L)
+                return OP_RX + axis;
+        }
+    }
+    /* palette reverse find (:288-317) */
+    for (int64_t i = (int64_t)e->np - 1; i >= 0; --i) {
+        if (e->pal[i] == L) {
+            uint32_t last = e->np - 1;
+            if ((uint32_t)i == last) return OP_P0;
+            uint32_t dist = last - (uint32_t)i - 1;
+            if (dist <= 15) { *delta = (uint8_t)dist; return OP_PD; }
+            return OP_PA;
+        }
+    }
+    return OP_PA;
+}
+
+/* encodeBrick (brickEncoding.hpp:348-447) + packOperationsToNibbles
+ * (brickEncoding.cpp:11-91): nibbles in emission order. */
+static void encode_brick(uint32_t b, const uint64_t* lab, const uint8_t* cst, enc_t* e) {
+    uint32_t L = levels_of(b);
+    e->np = 0; e->nn = 0;
+    push_pal(e, lab[0]);
+    push_nib(e, (uint8_t)((OP_PA << 1) | (cst[0] ? 1 : 0))); /* root: :360-367 */
+    for (uint32_t l = 0; l + 1 < L; ++l) {
+        size_t nn = (size_t)1 << (3 * l);
+        const uint64_t* P = lab + level_off(l);
+        const uint8_t* PC = cst + level_off(l);
+        const uint8_t* CC = cst + level_off(l + 1);
+        const uint64_t* C = lab + level_off(l + 1);
+        for (size_t m = 0; m < nn; ++m) {
+            if (PC[m]) continue; /* :386 */
+            for (uint32_t c = 0; c < 8; ++c) {
+                uint32_t n = (uint32_t)(8 * m + c); /* child Morton = 8m + c (utils.cpp:45-68) */
+                uint8_t delta = 0;
+                int op = best_op(lab, l + 1, n, P[m], e, &delta);
+                if (op == OP_PA) push_pal(e, C[n]); /* :423 */
+                push_nib(e, (uint8_t)((op << 1) | (CC[n] ? 1 : 0)));
+                if (op == OP_PD) push_nib(e, delta);
+            }
+        }
+    }
+}
+
+/* buildRansModel (brickEncoding.cpp:146-200). */
+void or_build_model(const uint64_t* raw16, uint32_t* freq, uint32_t* cum) {
+    uint64_t raw_sum = 0, norm = 0;
+    for (int i = 0; i < 16; ++i) {
+        uint32_t f = (uint32_t)raw16[i]; /* size_t -> uint32_t as in :157 */
+        if (f == 0) f = 1;
+        freq[i] = f;
+        raw_sum += f;
+    }
+    for (int i = 0; i < 16; ++i) {
+        uint64_t s = ((uint64_t)freq[i] * TOT) / raw_sum;
+        if (s == 0) s = 1;
+        freq[i] = (uint32_t)s;
+        norm += s;
+    }
+    while (norm < TOT) { freq[0]++; norm++; }
+    while (norm > TOT) {
+        int largest = 0;
+        for (int i = 1; i < 16; ++i)
+            if (freq[i] > freq[largest]) largest = i;
+        if (freq[largest] > 1) { freq[largest]--; norm--; } else break;
+    }
+    uint32_t acc = 0;
+    for (int i = 0; i < 16; ++i) { cum[i] = acc; acc += freq[i]; }
+    cum[16] = acc;
+}
+
+/* rANS over the packed bytes: ransEncodeSymbol (brickEncoding.cpp:202-219)
+ * applied to all 2*bytes nibbles (pad included) in reverse, then ransFlush
+ * (brickEncoding.hpp:452-464) little-endian.  Bytes are in emission order. */
+static void rans_encode(const uint8_t* nib, uint32_t nn, const uint32_t* freq, const uint32_t* cum, buf_t* out) {
+    uint32_t nsym2 = (nn + 1) & ~1u; /* pad nibble (0) when odd */
+    uint32_t x = RANS_L;
+    for (int64_t i = (int64_t)nsym2 - 1; i >= 0; --i) {
+        uint8_t s = (uint32_t)i < nn ? nib[i] : 0;
+        uint32_t f = freq[s], st = cum[s];
+        while (x >= ((RANS_L >> TOT_BITS) << 8) * f) {
+            uint8_t byte = (uint8_t)(x & 0xff);
+            bput(out, &byte, 1);
+            x >>= 8;
+        }
+        x = ((x / f) * TOT) + (x % f) + st;
+    }
+    for (int i = 0; i < 4; ++i) {
+        uint8_t byte = (uint8_t)(x & 0xff);
+        bput(out, &byte, 1);
+        x >>= 8;
+    }
+}
+
+/* compressDataset (brickEncoding.hpp:466-531) + saveDatasetToFile
+ * (fileIO.cpp:15-99). */
+int or_encode(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b, uint8_t** out, size_t* out_len) {
+    if (b < 2 || (b & (b - 1)) || b > 1024) return -1;
+    size_t nbx = (W + b - 1) / b, nby = (H + b - 1) / b, nbz = (D + b - 1) / b;
+    size_t nb = nbx * nby * nbz;
+    uint32_t L = levels_of(b);
+    size_t ntot = level_off(L);
+    uint64_t* lab = (uint64_t*)malloc(ntot * 8);
+    uint8_t* cst = (uint8_t*)malloc(ntot);
+    enc_t e = {0};
+    uint64_t hist[16] = {0};
+    /* per brick: palette, nibbles, nsym, ID */
+    uint64_t** pals = (uint64_t**)calloc(nb, sizeof(void*));
+    uint32_t* npal = (uint32_t*)calloc(nb, 4);
+    uint8_t** nibs = (uint8_t**)calloc(nb, sizeof(void*));
+    uint32_t* nnib = (uint32_t*)calloc(nb, 4);
+    uint32_t* ids = (uint32_t*)calloc(nb, 4);
+    size_t i = 0;
+    for (size_t bx = 0; bx < nbx; ++bx)
+        for (size_t by = 0; by < nby; ++by)
+            for (size_t bz = 0; bz < nbz; ++bz, ++i) {
+                cut_brick(vol, W, H, D, b, bx, by, bz, lab + level_off(L - 1));
+                build_pyramid(b, lab, cst);
+                encode_brick(b, lab, cst, &e);
+                ids[i] = or_morton3((uint32_t)bx, (uint32_t)by, (uint32_t)bz);
+                pals[i] = (uint64_t*)malloc(8 * (size_t)e.np);
+                memcpy(pals[i], e.pal, 8 * (size_t)e.np);
+                npal[i] = e.np;
+                nibs[i] = (uint8_t*)malloc(e.nn + 1);
+                memcpy(nibs[i], e.nib, e.nn);
+                nnib[i] = e.nn;
+                if (i % 512 == 0) { /* brickEncoding.hpp:482, brickEncoding.cpp:131-143 */
+                    for (uint32_t k = 0; k < e.nn; ++k) hist[e.nib[k]]++;
+                    if (e.nn & 1) hist[0]++; /* the pad nibble of the last byte */
+                }
+            }
+    uint32_t freq[16], cum[17];
+    or_build_model(hist, freq, cum);
+    buf_t o = {0};
+    bput32(&o, 0x43534244u);
+    bput32(&o, 1);
+    bput32(&o, (uint32_t)nb);
+    bput32(&o, b); /* the reference stores BRICK_SIZE (fileIO.cpp:28); see DESIGN */
+    bput32(&o, 16);
+    bput32(&o, TOT);
+    bput(&o, freq, 64);
+    bput(&o, cum, 64);
+    buf_t r = {0};
+    for (i = 0; i < nb; ++i) {
+        r.n = 0;
+        rans_encode(nibs[i], nnib[i], freq, cum, &r);
+        bput32(&o, ids[i]);
+        bput32(&o, npal[i]);
+        bput(&o, pals[i], 8 * (size_t)npal[i]);
+        bput32(&o, (uint32_t)r.n);
+        bput(&o, r.p, r.n);
+        bput32(&o, nnib[i]);
+        free(pals[i]);
+        free(nibs[i]);
+    }
+    free(r.p);
+    free(pals); free(npal); free(nibs); free(nnib); free(ids);
+    free(e.pal); free(e.nib); free(lab); free(cst);
+    *out = o.p;
+    *out_len = o.n;
+    return 0;
+}
+
+/* ------------------------------------------------------------- decoding */
+/* findSymbol (brickDecoding.cpp:126-135) with the loaded 16-entry table. */
+static uint32_t find_sym(uint32_t x, const uint32_t* cum16) {
+    uint32_t s = 0;
+    while (s + 1 < 16 && x >= cum16[s + 1]) ++s;
+    return s;
+}
+
+/* decodeRansStream + ransDecodeSymbol (brickDecoding.cpp:137-188). */
+int or_rans_decode(const uint32_t* freq, const uint32_t* cum, uint32_t total_freq, const uint8_t* enc,
+                   uint32_t E, uint32_t nsym, uint8_t* nib_out) {
+    if (E < 4 || total_freq != TOT) return -1;
+    uint32_t pos = E;
+    uint32_t x = ((uint32_t)enc[E - 1] << 24) | ((uint32_t)enc[E - 2] << 16) | ((uint32_t)enc[E - 3] << 8) | enc[E - 4];
+    pos -= 4;
+    for (uint32_t i = 0; i < nsym; ++i) {
+        uint32_t v = x % TOT;
+        uint32_t s = find_sym(v, cum);
+        x = freq[s] * (x / TOT) + (v - cum[s]);
+        while (x < RANS_L && pos > 0) x = (x << 8) | enc[--pos];
+        if (i & 1) nib_out[i >> 1] |= (uint8_t)(s & 15);
+        else nib_out[i >> 1] = (uint8_t)((s & 15) << 4);
+    }
+    return 0;
+}
+
+/* decode.wgsl:344-509 in label space (the RGBA transfer function of
+ * decode.wgsl:135-172 is not applied), which equals brickDecoding.hpp:174-242
+ * at full resolution.  Slot of node m at level l is m << 3(t-l)
+ * (coarseNodeToOutputIndex, decode.wgsl:239-245: scaling every coordinate by
+ * 2^k shifts the Morton code by 3k).  Differences from the reference, each a
+ * defined outcome where the reference has none:
+ *   - root stop bit set (the brick is one label): fill with palette[0]; the
+ *     C++ decoder throws and the WGSL decoder leaves 8^t-1 voxels EMPTY.
+ *   - a palette index past the palette is clamped to P-1 as decode.wgsl:472-485
+ *     does (status bit 2); reading past the stream is skipped as
+ *     decode.wgsl:449 does (status bit 1); op code 7 yields label 0 as
+ *     decode.wgsl:487-489 does (status bit 4).
+ * Returns the status bits (0 = clean). */
+int or_decode_brick(const uint64_t* palette, uint32_t P, const uint8_t* nib, uint32_t nib_bytes,
+                    uint32_t b, uint32_t t, uint64_t* out) {
+    uint32_t L = levels_of(b);
+    if (t >= L || P == 0) return 8;
+    size_t nout = (size_t)1 << (3 * t);
+    for (size_t k = 0; k < nout; ++k) out[k] = EMPTY_LABEL;
+    out[0] = palette[0];
+    int status = 0;
+    if (nib_bytes > 0 && (nib[0] >> 4) & 1) {
+        for (size_t k = 0; k < nout; ++k) out[k] = palette[0];
+        return 0;
+    }
+    uint32_t pos = 0, hi_next = 0, ip = 0;
+#define RDNIB(v)                                                              \
+    do {                                                                      \
+        uint8_t by_ = nib[pos];                                               \
+        if (hi_next) { v = by_ >> 4; hi_next = 0; }                           \
+        else { v = by_ & 15; hi_next = 1; pos++; }                            \
+    } while (0)
+    for (uint32_t l = 0; l < t; ++l) {
+        size_t nn = (size_t)1 << (3 * l);
+        uint32_t sh_p = 3 * (t - l), sh_c = 3 * (t - l - 1);
+        for (size_t m = 0; m < nn; ++m) {
+            size_t i = m << sh_p;
+            size_t last = (8 * m + 7) << sh_c;
+            if (out[last] != EMPTY_LABEL) continue;
+            uint64_t parent = out[i];
+            for (uint32_t c = 0; c < 8; ++c) {
+                uint32_t n = (uint32_t)(8 * m + c);
+                size_t j = (size_t)n << sh_c;
+                if (pos >= nib_bytes) { status |= 1; continue; }
+                uint32_t v, d = 0;
+                RDNIB(v);
+                uint32_t code = v >> 1, stop = v & 1;
+                if (code == OP_PD) {
+                    if (pos >= nib_bytes) { status |= 1; d = 0; }
+                    else RDNIB(d);
+                }
+                uint64_t val;
+                if (code == OP_RP) {
+                    val = parent;
+                } else if (code <= OP_RZ) {
+                    /* getNeighborValue (decode.wgsl:247-306) */
+                    uint32_t x, y, z;
+                    or_demorton3(n, &x, &y, &z);
+                    int cc[3] = {(int)x, (int)y, (int)z};
+                    int a = (int)code - 1;
+                    cc[a] += (cc[a] & 1) ? 1 : -1;
+                    int maxc = (1 << (l + 1)) - 1;
+                    if (cc[0] < 0 || cc[1] < 0 || cc[2] < 0 || cc[0] > maxc || cc[1] > maxc || cc[2] > maxc) {
+                        val = out[(size_t)or_morton3(x >> 1, y >> 1, z >> 1) << sh_p];
+                    } else {
+                        uint32_t nm = or_morton3((uint32_t)cc[0], (uint32_t)cc[1], (uint32_t)cc[2]);
+                        if (nm < n) val = out[(size_t)nm << sh_c];
+                        else val = out[(size_t)or_morton3((uint32_t)cc[0] >> 1, (uint32_t)cc[1] >> 1, (uint32_t)cc[2] >> 1) << sh_p];
+                    }
+                } else if (code == OP_PA) {
+                    ip += 1;
+                    uint32_t k = ip >= P ? (status |= 2, P - 1) : ip;
+                    val = palette[k];
+                } else if (code == OP_P0) {
+                    uint32_t k = ip >= P ? (status |= 2, P - 1) : ip;
+                    val = palette[k];
+                } else if (code == OP_PD) {
+                    uint32_t k = ip - d - 1;
+                    if (k >= P) { status |= 2; k = P - 1; }
+                    val = palette[k];
+                } else {
+                    status |= 4;
+                    val = 0;
+                }
+                out[j] = val;
+                if (stop) {
+                    size_t cnt = (size_t)1 << sh_c;
+                    for (size_t q = 0; q < cnt; ++q) out[j + q] = val;
+                }
+            }
+        }
+    }
+#undef RDNIB
+    return status;
+}
+
+/* ----------------------------------------------------------- .csbd read */
+typedef struct {
+    uint32_t nb, b, total;
+    uint32_t freq[16], cum[16];
+    size_t* off; /* byte offset of each brick record */
+} img_t;
+
+static int parse_image(const uint8_t* img, size_t len, img_t* I) {
+    /* layout: fileIO.cpp:25-96 */
+    if (len < 152) return -1;
+    uint32_t h[6];
+    memcpy(h, img, 24);
+    if (h[0] != 0x43534244u || h[4] != 16) return -1;
+    I->nb = h[2]; I->b = h[3]; I->total = h[5];
+    memcpy(I->freq, img + 24, 64);
+    memcpy(I->cum, img + 88, 64);
+    I->off = (size_t*)malloc(sizeof(size_t) * (I->nb + 1));
+    size_t o = 152;
+    for (uint32_t i = 0; i < I->nb; ++i) {
+        I->off[i] = o;
+        uint32_t P, E;
+        if (o + 8 > len) { free(I->off); return -1; }
+        memcpy(&P, img + o + 4, 4);
+        o += 8 + 8 * (size_t)P;
+        if (o + 4 > len) { free(I->off); return -1; }
+        memcpy(&E, img + o, 4);
+        o += 4 + E + 4;
+        if (o > len) { free(I->off); return -1; }
+    }
+    I->off[I->nb] = o;
+    return 0;
+}
+
+int or_decode_image(const uint8_t* img, size_t len, uint32_t t, uint64_t* out, uint32_t* status) {
+    img_t I;
+    if (parse_image(img, len, &I)) return -1;
+    size_t per = (size_t)1 << (3 * t);
+    for (uint32_t i = 0; i < I.nb; ++i) {
+        size_t o = I.off[i];
+        uint32_t P, E, ns;
+        memcpy(&P, img + o + 4, 4);
+        const uint64_t* pal = (const uint64_t*)(const void*)(img + o + 8); /* may be unaligned: copy */
+        uint64_t* palc = (uint64_t*)malloc(8 * (size_t)(P ? P : 1));
+        memcpy(palc, pal, 8 * (size_t)P);
+        o += 8 + 8 * (size_t)P;
+        memcpy(&E, img + o, 4);
+        const uint8_t* enc = img + o + 4;
+        memcpy(&ns, img + o + 4 + E, 4);
+        uint32_t nbytes = (ns + 1) / 2;
+        uint8_t* nib = (uint8_t*)calloc(nbytes + 1, 1);
+        int st = 0;
+        if (or_rans_decode(I.freq, I.cum, I.total, enc, E, ns, nib)) st = 16;
+        else st = or_decode_brick(palc, P, nib, nbytes, I.b, t, out + per * i);
+        if (status) status[i] = (uint32_t)st;
+        free(nib);
+        free(palc);
+    }
+    free(I.off);
+    return (int)I.nb;
+}
+
+/* ------------------------------------------------------------ seek index */
+/* The project's sidecar (no reference counterpart): replaying the decoder's
+ * serial rANS pass, record (state, byte position, nibble index, palette
+ * index) before every ops_per_ckpt-th op, the op count, and the first op of
+ * each level.  Level l+1 holds 8 ops per level-l op with stop bit 0 (8 ops for
+ * level 1 unless the root's stop bit is set); this is the decoder's skip rule
+ * (decode.wgsl:430-433) stated through stop bits. */
+int or_seek_index(const uint32_t* freq, const uint32_t* cum, const uint8_t* enc, uint32_t E, uint32_t nsym,
+                  uint32_t P, uint32_t b, uint32_t S, uint32_t* n_ops, uint32_t* level_start,
+                  uint32_t* ckpt, uint32_t max_ckpt, uint32_t* n_ckpt) {
+    (void)P;
+    uint32_t L = levels_of(b);
+    for (int k = 0; k < 8; ++k) level_start[k] = 0;
+    *n_ops = 0; *n_ckpt = 0;
+    if (E < 4 || nsym == 0) return -1;
+    uint32_t pos = E - 4;
+    uint32_t x = ((uint32_t)enc[E - 1] << 24) | ((uint32_t)enc[E - 2] << 16) | ((uint32_t)enc[E - 3] << 8) | enc[E - 4];
+    uint32_t sym_i = 0;
+#define DEC(outv)                                                     \
+    do {                                                              \
+        uint32_t v_ = x % TOT, s_ = find_sym(v_, cum);                \
+        x = freq[s_] * (x / TOT) + (v_ - cum[s_]);                    \
+        while (x < RANS_L && pos > 0) x = (x << 8) | enc[--pos];      \
+        outv = s_;                                                    \
+        sym_i++;                                                      \
+    } while (0)
+    uint32_t root;
+    DEC(root);
+    if (root & 1) return 0; /* one-label brick: no ops */
+    uint32_t ops = 0, ip = 0, need = 8, lvl = 0, active_next = 0, done_in_level = 0;
+    int status = 0;
+    level_start[0] = 0;
+    while (lvl + 1 < L && need > 0) {
+        if (ops % S == 0) {
+            if (*n_ckpt < max_ckpt) {
+                uint32_t* c = ckpt + 4 * (*n_ckpt);
+                c[0] = x; c[1] = pos; c[2] = sym_i; c[3] = ip;
+            }
+            (*n_ckpt)++;
+        }
+        if (sym_i >= nsym) { status = 1; break; }
+        uint32_t v;
+        DEC(v);
+        uint32_t code = v >> 1, stop = v & 1;
+        if (code == OP_PD) {
+            if (sym_i >= nsym) { status = 1; ops++; break; }
+            uint32_t d;
+            DEC(d);
+            (void)d;
+        }
+        if (code == OP_PA) ip++;
+        if (!stop) active_next++;
+        ops++;
+        if (++done_in_level == need) {
+            lvl++;
+            level_start[lvl] = ops;
+            need = 8 * active_next;
+            active_next = 0;
+            done_in_level = 0;
+        }
+    }
+#undef DEC
+    for (uint32_t k = lvl + 1; k < 8; ++k) level_start[k] = ops;
+    *n_ops = ops;
+    return status;
+}

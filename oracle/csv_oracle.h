@@ -1,0 +1,53 @@
+/* csv_oracle.h -- CPU restatement of the reference codec, TEST INFRASTRUCTURE ONLY.
+ *
+ * This is the oracle: a plain-C restatement of the reference algorithm for the
+ * compressed-segmentation brick codec (encoder/CSVEncoder/src, web/shaders/
+ * decode.wgsl, web/shaders/rayTrace.wgsl, web/scripts/camera.js).  It is
+ * pinned against the reference sources compiled as oracle/_ref/libcsvref.so
+ * and against the reference's shipped compressed_dataset.csbd (decode-only
+ * golden).  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+ * leg may load it, and only as the checker; the product never links it.
+ */
+#ifndef CSV_ORACLE_H
+#define CSV_ORACLE_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+uint32_t or_morton3(uint32_t x, uint32_t y, uint32_t z);
+void or_demorton3(uint32_t m, uint32_t* x, uint32_t* y, uint32_t* z);
+uint64_t or_majority8(const uint64_t* labels);
+void or_build_model(const uint64_t* raw16, uint32_t* freq16, uint32_t* cum17);
+
+/* Whole-volume encode to a .csbd v1 image (malloc'd; free with or_free). */
+int or_encode(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b,
+              uint8_t** out, size_t* out_len);
+/* Coarse-first pyramid of brick `brick_index` (split order): level l holds 8^l
+ * nodes in Morton order at offset (8^l - 1)/7. */
+int or_pyramid(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b, uint32_t brick_index,
+               uint64_t* labels, uint8_t* constant);
+
+/* rANS stage of one brick: repacked nibble bytes, ceil(nsym/2) of them. */
+int or_rans_decode(const uint32_t* freq16, const uint32_t* cum16, uint32_t total_freq,
+                   const uint8_t* enc, uint32_t enc_len, uint32_t nsym, uint8_t* nib_out);
+/* Label-space decode of one brick at target LOD t (2^t voxels per axis). */
+int or_decode_brick(const uint64_t* palette, uint32_t P, const uint8_t* nib, uint32_t nib_bytes,
+                    uint32_t b, uint32_t t, uint64_t* out);
+/* Whole image: every brick at LOD t, brick i (file order) at out + i*8^t. */
+int or_decode_image(const uint8_t* img, size_t len, uint32_t t, uint64_t* out, uint32_t* status);
+
+/* Seek index of one brick (the project's sidecar format; see csv.h). */
+int or_seek_index(const uint32_t* freq16, const uint32_t* cum16, const uint8_t* enc, uint32_t enc_len,
+                  uint32_t nsym, uint32_t P, uint32_t b, uint32_t ops_per_ckpt,
+                  uint32_t* n_ops, uint32_t* level_start /* [8] */, uint32_t* ckpt /* 4 per */,
+                  uint32_t max_ckpt, uint32_t* n_ckpt);
+
+void or_free(void* p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

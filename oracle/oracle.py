@@ -1,0 +1,249 @@
+"""ctypes loader for the CPU checkers.  TEST INFRASTRUCTURE ONLY.
+
+``Oracle``     -> oracle/libcsvoracle.so, this project's C restatement of the
+                  reference codec (oracle/csv_oracle.c).
+``Reference``  -> oracle/_ref/libcsvref.so, the unmodified reference encoder /
+                  decoder sources compiled by ``make -C oracle ref``.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference arm
+import this module, and only to check or to time the CPU reference.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "libcsvoracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libcsvref.so")
+REF_SRC = "/root/reference/encoder/CSVEncoder/src"
+
+_u8p = C.POINTER(C.c_uint8)
+_u32p = C.POINTER(C.c_uint32)
+_u64p = C.POINTER(C.c_uint64)
+
+
+def _ptr(a: np.ndarray, t):
+    return a.ctypes.data_as(t)
+
+
+def build(ref: bool | None = None) -> None:
+    """Compile the restatement, and the reference library when its sources exist."""
+    subprocess.run(["make", "-s", "-C", HERE, "libcsvoracle.so"], check=True)
+    if ref is None:
+        ref = os.path.isdir(REF_SRC)
+    if ref:
+        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+
+
+class Oracle:
+    def __init__(self, path: str = ORACLE_SO):
+        if not os.path.exists(path):
+            build(ref=False)
+        L = C.CDLL(path)
+        L.or_morton3.restype = C.c_uint32
+        L.or_morton3.argtypes = [C.c_uint32] * 3
+        L.or_majority8.restype = C.c_uint64
+        L.or_majority8.argtypes = [_u64p]
+        L.or_build_model.argtypes = [_u64p, _u32p, _u32p]
+        L.or_encode.argtypes = [_u64p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_uint32,
+                                C.POINTER(_u8p), C.POINTER(C.c_size_t)]
+        L.or_pyramid.argtypes = [_u64p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_uint32, C.c_uint32,
+                                 _u64p, _u8p]
+        L.or_rans_decode.argtypes = [_u32p, _u32p, C.c_uint32, _u8p, C.c_uint32, C.c_uint32, _u8p]
+        L.or_decode_brick.argtypes = [_u64p, C.c_uint32, _u8p, C.c_uint32, C.c_uint32, C.c_uint32, _u64p]
+        L.or_decode_image.argtypes = [_u8p, C.c_size_t, C.c_uint32, _u64p, _u32p]
+        L.or_seek_index.argtypes = [_u32p, _u32p, _u8p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                    C.c_uint32, _u32p, _u32p, _u32p, C.c_uint32, _u32p]
+        L.or_free.argtypes = [C.c_void_p]
+        self.lib = L
+
+    def morton3(self, x, y, z) -> int:
+        return self.lib.or_morton3(x, y, z)
+
+    def majority8(self, labels) -> int:
+        a = np.ascontiguousarray(labels, dtype=np.uint64)
+        return int(self.lib.or_majority8(_ptr(a, _u64p)))
+
+    def build_model(self, raw16):
+        raw = np.ascontiguousarray(raw16, dtype=np.uint64)
+        f = np.zeros(16, np.uint32)
+        c = np.zeros(17, np.uint32)
+        self.lib.or_build_model(_ptr(raw, _u64p), _ptr(f, _u32p), _ptr(c, _u32p))
+        return f, c
+
+    def encode(self, vol: np.ndarray, brick: int) -> bytes:
+        """vol has shape (D, H, W) in C order, i.e. x fastest."""
+        v = np.ascontiguousarray(vol, dtype=np.uint64)
+        D, H, W = v.shape
+        out = _u8p()
+        n = C.c_size_t()
+        rc = self.lib.or_encode(_ptr(v, _u64p), W, H, D, brick, C.byref(out), C.byref(n))
+        if rc:
+            raise RuntimeError("oracle encode failed")
+        data = C.string_at(out, n.value)
+        self.lib.or_free(out)
+        return data
+
+    def pyramid(self, vol: np.ndarray, brick: int, index: int):
+        v = np.ascontiguousarray(vol, dtype=np.uint64)
+        D, H, W = v.shape
+        levels = brick.bit_length()
+        tot = ((1 << (3 * levels)) - 1) // 7
+        lab = np.zeros(tot, np.uint64)
+        cst = np.zeros(tot, np.uint8)
+        rc = self.lib.or_pyramid(_ptr(v, _u64p), W, H, D, brick, index, _ptr(lab, _u64p), _ptr(cst, _u8p))
+        if rc:
+            raise RuntimeError("oracle pyramid failed")
+        out = []
+        for l in range(levels):
+            o = ((1 << (3 * l)) - 1) // 7
+            out.append((lab[o:o + (1 << (3 * l))], cst[o:o + (1 << (3 * l))]))
+        return out
+
+    def decode_image(self, img: bytes, lod: int):
+        a = np.frombuffer(img, np.uint8)
+        nb = int(np.frombuffer(img[8:12], np.uint32)[0])
+        out = np.zeros(nb * (1 << (3 * lod)), np.uint64)
+        st = np.zeros(nb, np.uint32)
+        rc = self.lib.or_decode_image(_ptr(a, _u8p), len(img), lod, _ptr(out, _u64p), _ptr(st, _u32p))
+        if rc < 0:
+            raise RuntimeError("oracle decode failed")
+        return out.reshape(nb, -1), st
+
+    def rans_decode(self, freq, cum16, enc: bytes, nsym: int) -> bytes:
+        f = np.ascontiguousarray(freq, np.uint32)
+        c = np.ascontiguousarray(cum16, np.uint32)
+        e = np.frombuffer(enc, np.uint8)
+        out = np.zeros((nsym + 1) // 2, np.uint8)
+        rc = self.lib.or_rans_decode(_ptr(f, _u32p), _ptr(c, _u32p), 4096, _ptr(e, _u8p), len(enc), nsym,
+                                     _ptr(out, _u8p))
+        if rc:
+            raise RuntimeError("oracle rans failed")
+        return out.tobytes()
+
+    def decode_brick(self, palette, nib: bytes, brick: int, lod: int):
+        p = np.ascontiguousarray(palette, np.uint64)
+        n = np.frombuffer(nib, np.uint8) if len(nib) else np.zeros(1, np.uint8)
+        out = np.zeros(1 << (3 * lod), np.uint64)
+        st = self.lib.or_decode_brick(_ptr(p, _u64p), len(p), _ptr(n, _u8p), len(nib), brick, lod,
+                                      _ptr(out, _u64p))
+        return out, st
+
+    def seek_index(self, freq, cum16, enc: bytes, nsym: int, P: int, brick: int, S: int):
+        f = np.ascontiguousarray(freq, np.uint32)
+        c = np.ascontiguousarray(cum16, np.uint32)
+        e = np.frombuffer(enc, np.uint8)
+        nops = np.zeros(1, np.uint32)
+        ls = np.zeros(8, np.uint32)
+        maxc = nsym // S + 2
+        ck = np.zeros(4 * maxc, np.uint32)
+        nck = np.zeros(1, np.uint32)
+        st = self.lib.or_seek_index(_ptr(f, _u32p), _ptr(c, _u32p), _ptr(e, _u8p), len(enc), nsym, P, brick, S,
+                                    _ptr(nops, _u32p), _ptr(ls, _u32p), _ptr(ck, _u32p), maxc, _ptr(nck, _u32p))
+        return int(nops[0]), ls, ck[:4 * int(nck[0])].reshape(-1, 4), st
+
+
+class Reference:
+    """The reference sources compiled here (oracle/_ref/libcsvref.so)."""
+
+    def __init__(self, path: str = REF_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        L = C.CDLL(path)
+        L.ref_last_error.restype = C.c_char_p
+        L.ref_free.argtypes = [C.c_void_p]
+        L.ref_encode.argtypes = [_u64p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_int, C.POINTER(_u8p),
+                                 C.POINTER(C.c_size_t), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                 C.POINTER(C.c_double)]
+        L.ref_decode_brick_full.argtypes = [_u8p, C.c_size_t, C.c_uint32, _u64p]
+        L.ref_decode_all_full.argtypes = [_u8p, C.c_size_t, _u64p, _u32p, C.c_uint32, C.POINTER(C.c_double),
+                                          C.POINTER(C.c_double)]
+        L.ref_rans_decode.argtypes = [_u8p, C.c_size_t, C.c_uint32, _u8p, C.POINTER(C.c_size_t)]
+        L.ref_majority8.restype = C.c_uint64
+        L.ref_majority8.argtypes = [_u64p]
+        L.ref_build_model.argtypes = [_u64p, _u32p, _u32p]
+        L.ref_build_pyramid64.argtypes = [_u64p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_uint32, _u64p, _u8p]
+        self.lib = L
+
+    def error(self) -> str:
+        return self.lib.ref_last_error().decode()
+
+    def encode(self, vol: np.ndarray, brick: int, timings: bool = False):
+        v = np.ascontiguousarray(vol, dtype=np.uint64)
+        D, H, W = v.shape
+        out = _u8p()
+        n = C.c_size_t()
+        t = [C.c_double(), C.c_double(), C.c_double()]
+        rc = self.lib.ref_encode(_ptr(v, _u64p), W, H, D, brick, C.byref(out), C.byref(n),
+                                 C.byref(t[0]), C.byref(t[1]), C.byref(t[2]))
+        if rc:
+            raise RuntimeError("reference encode failed: " + self.error())
+        data = C.string_at(out, n.value)
+        self.lib.ref_free(out)
+        if timings:
+            return data, {"split_ms": t[0].value, "compress_ms": t[1].value, "save_ms": t[2].value}
+        return data
+
+    def decode_brick_full(self, img: bytes, index: int, brick: int):
+        a = np.frombuffer(img, np.uint8)
+        out = np.zeros(brick ** 3, np.uint64)
+        rc = self.lib.ref_decode_brick_full(_ptr(a, _u8p), len(img), index, _ptr(out, _u64p))
+        if rc:
+            raise RuntimeError(self.error())
+        return out
+
+    def decode_all_full(self, img: bytes, brick: int, max_bricks: int = 0, keep: bool = True):
+        a = np.frombuffer(img, np.uint8)
+        nb = int(np.frombuffer(img[8:12], np.uint32)[0])
+        if max_bricks:
+            nb = min(nb, max_bricks)
+        out = np.zeros(nb * brick ** 3, np.uint64) if keep else None
+        st = np.zeros(nb, np.uint32)
+        tr, tp = C.c_double(), C.c_double()
+        n = self.lib.ref_decode_all_full(_ptr(a, _u8p), len(img), _ptr(out, _u64p) if keep else None,
+                                         _ptr(st, _u32p), max_bricks, C.byref(tr), C.byref(tp))
+        if n < 0:
+            raise RuntimeError(self.error())
+        return (out.reshape(nb, -1) if keep else None), st, {"rans_ms": tr.value, "replay_ms": tp.value}
+
+    def rans_decode(self, img: bytes, index: int, nsym: int) -> bytes:
+        a = np.frombuffer(img, np.uint8)
+        out = np.zeros((nsym + 1) // 2 + 1, np.uint8)
+        n = C.c_size_t()
+        rc = self.lib.ref_rans_decode(_ptr(a, _u8p), len(img), index, _ptr(out, _u8p), C.byref(n))
+        if rc:
+            raise RuntimeError(self.error())
+        return out[:n.value].tobytes()
+
+    def majority8(self, labels) -> int:
+        a = np.ascontiguousarray(labels, dtype=np.uint64)
+        return int(self.lib.ref_majority8(_ptr(a, _u64p)))
+
+    def build_model(self, raw16):
+        raw = np.ascontiguousarray(raw16, dtype=np.uint64)
+        f = np.zeros(16, np.uint32)
+        c = np.zeros(17, np.uint32)
+        self.lib.ref_build_model(_ptr(raw, _u64p), _ptr(f, _u32p), _ptr(c, _u32p))
+        return f, c
+
+    def pyramid64(self, vol: np.ndarray, index: int):
+        v = np.ascontiguousarray(vol, dtype=np.uint64)
+        D, H, W = v.shape
+        tot = sum(8 ** l for l in range(7))
+        lab = np.zeros(tot, np.uint64)
+        cst = np.zeros(tot, np.uint8)
+        n = self.lib.ref_build_pyramid64(_ptr(v, _u64p), W, H, D, index, _ptr(lab, _u64p), _ptr(cst, _u8p))
+        if n < 0:
+            raise RuntimeError("pyramid failed")
+        # finest-first in the reference; return coarse-first like Oracle.pyramid
+        out = []
+        o = 0
+        for l in range(6, -1, -1):
+            cnt = 8 ** l
+            out.append((lab[o:o + cnt], cst[o:o + cnt]))
+            o += cnt
+        return out[::-1]
