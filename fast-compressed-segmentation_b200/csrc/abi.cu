@@ -1,0 +1,364 @@
+// abi.cu -- the C ABI (include/csv.h): contexts, .csbd staging, and launches.
+//
+// Host-side work here is parsing and bookkeeping only; every codec step runs
+// in the sm_100a kernels of decode.cu / encode.cu.  There is no CPU decode or
+// encode path: without a usable CUDA device every call fails with CSV_ECUDA.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "csv_internal.h"
+
+using namespace csv;
+
+struct csv_ctx {
+    int device = 0;
+    std::string err;
+    DecodeScratch scr;
+    uint32_t scr_b = 0;
+    EncoderState* enc = nullptr;
+};
+
+struct csv_dataset {
+    csv_ctx* ctx = nullptr;
+    DeviceDataset d;
+};
+
+namespace {
+
+int fail(csv_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+int cuda_fail(csv_ctx* ctx, cudaError_t e, const char* where) {
+    return fail(ctx, CSV_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+uint32_t rd32(const uint8_t* p) {
+    uint32_t v;
+    memcpy(&v, p, 4);
+    return v;
+}
+
+// Host view of a .csbd v1 image (fileIO.cpp:25-96, datasetLoader.js:39-146).
+struct ImageView {
+    uint32_t nb = 0, b = 0, total = 0;
+    uint32_t freq[16], cum[16];
+    struct Rec {
+        size_t pal_at, enc_at;
+        uint32_t id, P, E, nsym;
+    };
+    std::vector<Rec> recs;
+};
+
+int parse_image(csv_ctx* ctx, const uint8_t* img, size_t len, ImageView& v) {
+    if (!img || len < kHeaderBytes) return fail(ctx, CSV_EFORMAT, "image shorter than the 152-byte header");
+    if (rd32(img) != kMagic) return fail(ctx, CSV_EFORMAT, "Invalid file format (bad magic)");
+    if (rd32(img + 4) != 1) return fail(ctx, CSV_EFORMAT, "unsupported .csbd version");
+    v.nb = rd32(img + 8);
+    v.b = rd32(img + 12);
+    if (v.b < 2 || v.b > 64 || (v.b & (v.b - 1)))
+        return fail(ctx, CSV_EFORMAT, "brick size must be a power of two in [2, 64]");
+    if (rd32(img + 16) != 16) return fail(ctx, CSV_EFORMAT, "symbol count must be 16");
+    v.total = rd32(img + 20);
+    if (v.total != kTot) return fail(ctx, CSV_EFORMAT, "total frequency must be 4096");
+    for (int i = 0; i < 16; ++i) {
+        v.freq[i] = rd32(img + 24 + 4 * i);
+        v.cum[i] = rd32(img + 88 + 4 * i);
+        if (v.freq[i] > kTot || v.cum[i] >= kTot) return fail(ctx, CSV_EFORMAT, "rANS model entry out of range");
+    }
+    v.recs.resize(v.nb);
+    size_t o = kHeaderBytes;
+    for (uint32_t i = 0; i < v.nb; ++i) {
+        ImageView::Rec& r = v.recs[i];
+        if (o + 8 > len) return fail(ctx, CSV_EFORMAT, "truncated brick header");
+        r.id = rd32(img + o);
+        r.P = rd32(img + o + 4);
+        if (r.P == 0 || r.P > kMaxPalette) return fail(ctx, CSV_EFORMAT, "palette size out of range");
+        r.pal_at = o + 8;
+        o += 8 + 8ull * r.P;
+        if (o + 4 > len) return fail(ctx, CSV_EFORMAT, "truncated palette");
+        r.E = rd32(img + o);
+        r.enc_at = o + 4;
+        o += 4 + (size_t)r.E;
+        if (o + 4 > len) return fail(ctx, CSV_EFORMAT, "truncated stream");
+        r.nsym = rd32(img + o);
+        o += 4;
+    }
+    return CSV_OK;
+}
+
+void free_dataset(DeviceDataset& d) {
+    cudaFree(d.d_bricks);
+    cudaFree(d.d_pal);
+    cudaFree(d.d_enc);
+    cudaFree(d.d_ck);
+    cudaFree(d.d_lut);
+    free(d.h_ids);
+    d = DeviceDataset();
+}
+
+constexpr uint32_t kOpsPerCheckpoint = 512;
+
+int stage_dataset(csv_ctx* ctx, const uint8_t* img, const ImageView& v, DeviceDataset& d, cudaStream_t st) {
+    d.device = ctx->device;
+    d.nb = v.nb;
+    d.b = v.b;
+    d.L = levels_of(v.b);
+    d.S = kOpsPerCheckpoint;
+    d.total = v.total;
+    memcpy(d.freq, v.freq, sizeof d.freq);
+    memcpy(d.cum, v.cum, sizeof d.cum);
+    std::vector<BrickDesc> desc(v.nb);
+    uint64_t pal_n = 0, enc_n = 0, ck_n = 0;
+    d.h_ids = (uint32_t*)malloc(sizeof(uint32_t) * std::max<uint32_t>(1, v.nb));
+    for (uint32_t i = 0; i < v.nb; ++i) {
+        const auto& r = v.recs[i];
+        BrickDesc& b = desc[i];
+        memset(&b, 0, sizeof b);
+        b.pal_off = pal_n;
+        b.enc_off = enc_n;
+        b.P = r.P;
+        b.E = r.E;
+        b.nsym = r.nsym;
+        b.id = r.id;
+        b.ck_off = (uint32_t)ck_n;
+        b.ck_cap = (r.nsym + d.S - 1) / d.S + 1;
+        b.flags = BF_NOINDEX;
+        d.h_ids[i] = r.id;
+        pal_n += r.P;
+        enc_n += (r.E + 15) & ~15ull;
+        ck_n += b.ck_cap;
+        d.max_nsym = std::max(d.max_nsym, r.nsym);
+    }
+    if (ck_n > 0xFFFFFFFFull) return fail(ctx, CSV_ERANGE, "dataset too large for the seek index");
+    d.stream_bytes = 0;
+    for (auto& r : v.recs) d.stream_bytes += r.E;
+    d.palette_entries = pal_n;
+    d.ck_entries = ck_n;
+    std::vector<uint64_t> pal(std::max<uint64_t>(1, pal_n));
+    std::vector<uint8_t> enc(std::max<uint64_t>(16, enc_n), 0);
+    for (uint32_t i = 0; i < v.nb; ++i) {
+        const auto& r = v.recs[i];
+        memcpy(pal.data() + desc[i].pal_off, img + r.pal_at, 8ull * r.P);
+        memcpy(enc.data() + desc[i].enc_off, img + r.enc_at, r.E);
+    }
+    uint32_t lut[kTot];
+    build_lut(v.freq, v.cum, lut);
+    cudaError_t e;
+    if ((e = cudaMalloc(&d.d_bricks, sizeof(BrickDesc) * std::max<uint32_t>(1, v.nb))) != cudaSuccess ||
+        (e = cudaMalloc(&d.d_pal, 8 * pal.size())) != cudaSuccess ||
+        (e = cudaMalloc(&d.d_enc, enc.size())) != cudaSuccess ||
+        (e = cudaMalloc(&d.d_ck, sizeof(Checkpoint) * std::max<uint64_t>(1, ck_n))) != cudaSuccess ||
+        (e = cudaMalloc(&d.d_lut, sizeof lut)) != cudaSuccess)
+        return fail(ctx, CSV_ENOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
+    if ((e = cudaMemcpyAsync(d.d_bricks, desc.data(), sizeof(BrickDesc) * v.nb, cudaMemcpyHostToDevice, st)) !=
+            cudaSuccess ||
+        (e = cudaMemcpyAsync(d.d_pal, pal.data(), 8 * pal.size(), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(d.d_enc, enc.data(), enc.size(), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(d.d_lut, lut, sizeof lut, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return cuda_fail(ctx, e, "staging copy");
+    // the host vectors go out of scope: finish the copies first
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "staging copy");
+    return CSV_OK;
+}
+
+int ensure_scratch(csv_ctx* ctx, uint32_t b) {
+    if (ctx->scr.base && ctx->scr_b >= b) return CSV_OK;
+    size_t per = decode_scratch_per_cta(b);
+    uint32_t ctas = decode_grid(ctx->device, 0xFFFFFFFFu);
+    cudaFree(ctx->scr.base);
+    ctx->scr.base = nullptr;
+    cudaError_t e = cudaMalloc(&ctx->scr.base, per * ctas);
+    if (e != cudaSuccess) return fail(ctx, CSV_ENOMEM, std::string("decode scratch: ") + cudaGetErrorString(e));
+    if (!ctx->scr.d_queue) {
+        e = cudaMalloc(&ctx->scr.d_queue, 64);
+        if (e != cudaSuccess) return fail(ctx, CSV_ENOMEM, "decode queue");
+    }
+    ctx->scr.per_cta = per;
+    ctx->scr.ctas = ctas;
+    ctx->scr_b = b;
+    return CSV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int csv_abi_version(void) { return CSV_ABI_VERSION; }
+
+void csv_free(void* p) { free(p); }
+
+int csv_create(int device, csv_ctx** out) {
+    if (!out) return CSV_EINVAL;
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || device < 0 || device >= n) return CSV_ECUDA;
+    csv_ctx* c = new (std::nothrow) csv_ctx();
+    if (!c) return CSV_ENOMEM;
+    c->device = device;
+    DeviceGuard g(device);
+    if ((e = cudaFree(nullptr)) != cudaSuccess) {
+        delete c;
+        return CSV_ECUDA;
+    }
+    *out = c;
+    return CSV_OK;
+}
+
+void csv_destroy(csv_ctx* ctx) {
+    if (!ctx) return;
+    DeviceGuard g(ctx->device);
+    cudaFree(ctx->scr.base);
+    cudaFree(ctx->scr.d_queue);
+    encoder_state_free(ctx->enc);
+    delete ctx;
+}
+
+const char* csv_last_error(const csv_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int csv_open(csv_ctx* ctx, const uint8_t* image, size_t len, csv_dataset** out) {
+    if (!ctx || !out) return CSV_EINVAL;
+    *out = nullptr;
+    DeviceGuard g(ctx->device);
+    ImageView v;
+    int rc = parse_image(ctx, image, len, v);
+    if (rc) return rc;
+    csv_dataset* ds = new (std::nothrow) csv_dataset();
+    if (!ds) return fail(ctx, CSV_ENOMEM, "host allocation");
+    ds->ctx = ctx;
+    cudaStream_t st = 0;
+    rc = stage_dataset(ctx, image, v, ds->d, st);
+    if (rc == CSV_OK) {
+        cudaError_t e = launch_build_index(ds->d, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "seek index");
+    }
+    if (rc) {
+        free_dataset(ds->d);
+        delete ds;
+        return rc;
+    }
+    *out = ds;
+    return CSV_OK;
+}
+
+int csv_dataset_info_get(const csv_dataset* ds, csv_dataset_info* info) {
+    if (!ds || !info) return CSV_EINVAL;
+    info->num_bricks = ds->d.nb;
+    info->brick_size = ds->d.b;
+    info->levels = ds->d.L;
+    info->ops_per_checkpoint = ds->d.S;
+    info->stream_bytes = ds->d.stream_bytes;
+    info->palette_entries = ds->d.palette_entries;
+    memcpy(info->freq, ds->d.freq, sizeof info->freq);
+    memcpy(info->cum, ds->d.cum, sizeof info->cum);
+    return CSV_OK;
+}
+
+int csv_dataset_ids(const csv_dataset* ds, uint32_t* ids, uint32_t n) {
+    if (!ds || !ids || n < ds->d.nb) return CSV_EINVAL;
+    memcpy(ids, ds->d.h_ids, sizeof(uint32_t) * ds->d.nb);
+    return CSV_OK;
+}
+
+void csv_close(csv_dataset* ds) {
+    if (!ds) return;
+    DeviceGuard g(ds->d.device);
+    free_dataset(ds->d);
+    delete ds;
+}
+
+int csv_decode_batch(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_reqs, uint32_t n, uint64_t* d_out,
+                     uint32_t* d_status, void* stream) {
+    if (!ctx || !ds) return CSV_EINVAL;
+    if (n == 0) return CSV_OK;
+    if (!d_reqs || !d_out || !d_status) return fail(ctx, CSV_EINVAL, "null request, output or status pointer");
+    DeviceGuard g(ctx->device);
+    int rc = ensure_scratch(ctx, ds->d.b);
+    if (rc) return rc;
+    cudaError_t e = launch_decode(ds->d, d_reqs, n, d_out, d_status, ctx->scr, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "decode launch");
+    return CSV_OK;
+}
+
+int csv_decode_image(csv_ctx* ctx, const uint8_t* image, size_t len, uint32_t lod, uint64_t* out, uint32_t* status) {
+    if (!ctx || !out) return CSV_EINVAL;
+    DeviceGuard g(ctx->device);
+    csv_dataset* ds = nullptr;
+    int rc = csv_open(ctx, image, len, &ds);
+    if (rc) return rc;
+    if (lod >= ds->d.L) {
+        csv_close(ds);
+        return fail(ctx, CSV_EINVAL, "lod beyond log2(brick size)");
+    }
+    uint32_t nb = ds->d.nb;
+    uint64_t per = 1ull << (3 * lod);
+    std::vector<csv_request> reqs(nb);
+    for (uint32_t i = 0; i < nb; ++i) reqs[i] = csv_request{i, lod, per * i};
+    csv_request* d_reqs = nullptr;
+    uint64_t* d_out = nullptr;
+    uint32_t* d_st = nullptr;
+    cudaError_t e;
+    cudaStream_t st = 0;
+    if ((e = cudaMalloc(&d_reqs, sizeof(csv_request) * std::max<uint32_t>(1, nb))) != cudaSuccess ||
+        (e = cudaMalloc(&d_out, 8 * per * std::max<uint32_t>(1, nb))) != cudaSuccess ||
+        (e = cudaMalloc(&d_st, 4 * std::max<uint32_t>(1, nb))) != cudaSuccess) {
+        rc = fail(ctx, CSV_ENOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
+    } else if ((e = cudaMemcpyAsync(d_reqs, reqs.data(), sizeof(csv_request) * nb, cudaMemcpyHostToDevice, st)) !=
+               cudaSuccess) {
+        rc = cuda_fail(ctx, e, "request copy");
+    } else {
+        rc = csv_decode_batch(ctx, ds, d_reqs, nb, d_out, d_st, st);
+        if (rc == CSV_OK) {
+            std::vector<uint32_t> hst(nb);
+            if ((e = cudaMemcpyAsync(out, d_out, 8 * per * nb, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+                (e = cudaMemcpyAsync(hst.data(), d_st, 4 * nb, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+                (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+                rc = cuda_fail(ctx, e, "decode");
+            } else {
+                if (status) memcpy(status, hst.data(), 4 * nb);
+                for (uint32_t i = 0; i < nb && rc == CSV_OK; ++i)
+                    if (hst[i]) rc = fail(ctx, CSV_EBRICK, "brick " + std::to_string(i) + " status " +
+                                                               std::to_string(hst[i]));
+            }
+        }
+    }
+    cudaFree(d_reqs);
+    cudaFree(d_out);
+    cudaFree(d_st);
+    csv_close(ds);
+    return rc;
+}
+
+int csv_synth_volume(csv_ctx* ctx, uint64_t* d_volume, uint32_t W, uint32_t H, uint32_t D, int kind, uint32_t n_cells,
+                     uint32_t n_tubes, float r_min, float r_max, float zero_frac, uint64_t seed, void* stream) {
+    if (!ctx || !d_volume || kind < 0 || kind > 2) return CSV_EINVAL;
+    DeviceGuard g(ctx->device);
+    cudaError_t e = synth_volume(d_volume, W, H, D, kind, n_cells, n_tubes, r_min, r_max, zero_frac, seed,
+                                 (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "synth");
+    return CSV_OK;
+}
+
+}  // extern "C"

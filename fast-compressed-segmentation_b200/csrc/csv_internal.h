@@ -1,0 +1,101 @@
+// csv_internal.h -- shared device/host definitions of the B200 CSV codec.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/csv.h"
+
+namespace csv {
+
+// Codec constants (types.hpp:18-28).
+constexpr uint32_t kRansL = 1u << 23;     // RANS_LIMIT / RANS_INIT
+constexpr uint32_t kTotBits = 12;         // LOG_TOTAL_FREQ
+constexpr uint32_t kTot = 1u << kTotBits; // RANS_TOTAL
+constexpr uint32_t kMagic = 0x43534244u;  // fileIO.cpp:25
+constexpr uint32_t kHeaderBytes = 152;    // 16 B header + 136 B model (fileIO.cpp:25-49)
+
+// Op codes (types.hpp:162-171) and nibble layout (op << 1 | stop, brickEncoding.cpp:66-67).
+enum : uint32_t { OP_RP = 0, OP_RX = 1, OP_RY = 2, OP_RZ = 3, OP_PA = 4, OP_P0 = 5, OP_PD = 6 };
+
+// Brick descriptor flags.
+constexpr uint32_t BF_UNIFORM = 1u;   // root stop bit set: the whole brick is palette[0]
+constexpr uint32_t BF_TRUNCATED = 2u; // the stream ends inside the level structure
+constexpr uint32_t BF_NOINDEX = 4u;   // no seek index (not built)
+
+// Per-brick device descriptor, file order.
+struct BrickDesc {
+    uint64_t pal_off;        // first palette entry in the palette pool
+    uint64_t enc_off;        // first byte of the rANS stream in the stream pool (16-byte aligned)
+    uint32_t P, E, nsym, id; // palette size, stream bytes, nibble count, Morton brick ID
+    uint32_t ck_off, ck_cap; // seek checkpoints: first entry and capacity
+    uint32_t n_ops, flags;   // ops after the root nibble; BF_* flags
+    uint32_t level_start[8]; // level_start[l] = first op whose node is on level l+1
+};
+static_assert(sizeof(BrickDesc) == 80, "BrickDesc layout");
+
+// One seek checkpoint: decoder state before an op (see csv_oracle.c:or_seek_index).
+struct Checkpoint {
+    uint32_t state, pos, sym, ip;
+};
+
+// Decoded-op record (4 bytes): code | stop << 3 | palette index << 8.
+constexpr uint32_t REC_PIDX_SHIFT = 8;
+constexpr uint32_t PIDX_LABEL0 = 0xFFFFFFu; // "label 0" (op code 7, decode.wgsl:487-489)
+constexpr uint32_t kMaxPalette = 0xFFFFFEu;
+
+// Node info word: inactive -> palette index; active -> ACT | rank among active nodes of its level.
+constexpr uint32_t NI_ACT = 0x80000000u;
+
+inline uint32_t levels_of(uint32_t b) {
+    uint32_t L = 0;
+    while ((1u << L) < b) ++L;
+    return L + 1;
+}
+// Ops after the root nibble in the fullest brick: sum_{l=1}^{L-1} 8^l.
+inline uint64_t max_ops_of(uint32_t b) {
+    uint32_t L = levels_of(b);
+    return ((1ull << (3 * L)) - 8) / 7;
+}
+
+// Device-resident dataset.
+struct DeviceDataset {
+    int device = 0;
+    uint32_t nb = 0, b = 0, L = 0, S = 0;
+    uint32_t freq[16] = {}, cum[16] = {}, total = 0;
+    uint64_t stream_bytes = 0, palette_entries = 0, ck_entries = 0;
+    uint32_t max_nsym = 0;
+    BrickDesc* d_bricks = nullptr;
+    uint64_t* d_pal = nullptr;
+    uint8_t* d_enc = nullptr;
+    Checkpoint* d_ck = nullptr;
+    uint32_t* d_lut = nullptr; // 4096 packed entries: sym | freq << 4 | start << 17
+    uint32_t* h_ids = nullptr;
+};
+
+// Launch helpers implemented in decode.cu.
+cudaError_t build_lut(const uint32_t* freq, const uint32_t* cum, uint32_t* h_lut);
+cudaError_t launch_build_index(DeviceDataset& ds, cudaStream_t st);
+
+struct DecodeScratch {
+    uint8_t* base = nullptr;
+    size_t per_cta = 0;
+    uint32_t ctas = 0;
+    uint32_t* d_queue = nullptr;
+};
+size_t decode_scratch_per_cta(uint32_t b);
+uint32_t decode_grid(int device, uint32_t n);
+cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, uint32_t n, uint64_t* d_out,
+                          uint32_t* d_status, const DecodeScratch& scr, cudaStream_t st);
+
+// Encoder state owned by a context (encode.cu).
+struct EncoderState;
+void encoder_state_free(EncoderState* s);
+
+cudaError_t synth_volume(uint64_t* d_vol, uint32_t W, uint32_t H, uint32_t D, int kind, uint32_t n_cells,
+                         uint32_t n_tubes, float r_min, float r_max, float zero_frac, uint64_t seed,
+                         cudaStream_t st);
+
+}  // namespace csv

@@ -1,0 +1,506 @@
+// decode.cu -- sm_100a brick decoder: seek-index build and the batched decode kernel.
+//
+// Reference behaviour restated here (paths relative to the reference root):
+//   rANS          brickDecoding.cpp:126-188 (== web/scripts/decode.js:36-104)
+//   op parsing    brickDecoding.cpp:20-59, decode.wgsl:87-127
+//   replay        brickDecoding.hpp:174-242 (full resolution), decode.wgsl:344-509 (any LOD)
+//   neighbors     brickDecoding.cpp:77-124, decode.wgsl:247-306
+//
+// The reference replays every op of a brick in one serial chain (one leader
+// thread per workgroup in decode.wgsl).  Here a brick is decoded by a whole
+// CTA:
+//   1. rANS: the brick's op stream is cut at seek checkpoints (decoder state
+//      every S ops, built once per dataset); each thread decodes one segment
+//      and writes one 4-byte record per op (code, stop, resolved palette index).
+//   2. levels, coarse to fine: node values are palette indices.  A node of
+//      level l+1 whose parent is inactive (stop-filled) takes the parent's
+//      value; otherwise its op gives it: Rp -> parent, Pa/P0/Pd -> palette
+//      index, Rx/Ry/Rz -> the neighbour outside the sibling block.  A neighbour
+//      on the +1 side is later in Morton order, so the reference reads its
+//      parent (known, previous level).  A neighbour on the -1 side is earlier,
+//      on the same level; its local index has one more 1-bit than the node's,
+//      so such chains are at most three hops long and are resolved on the fly
+//      without any ordering between threads.
+//   3. the last level is written straight to HBM, 8 children (64 bytes) per
+//      parent, with streaming 16-byte stores.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "csv_internal.h"
+
+namespace csv {
+
+constexpr int kDecThreads = 256;
+constexpr uint32_t kSmemLevels = 5;    // levels 0..4 (<= 4096 nodes) keep node info in shared memory
+constexpr uint32_t kSmemNodes = 4681;  // sum_{l<5} 8^l
+constexpr uint32_t kPalCache = 1024;   // palettes up to this size are copied to shared memory
+constexpr uint32_t REC_MISSING = OP_RP | 8u;
+
+__host__ __device__ constexpr uint32_t lvl_off(uint32_t l) { return ((1u << (3 * l)) - 1) / 7; }
+
+struct DecShared {
+    uint32_t lut[kTot];
+    uint32_t ni[kSmemNodes];
+    uint32_t av[kSmemNodes];
+    uint32_t base[4096];
+    uint64_t pal[kPalCache];
+    uint32_t warp_sums[kDecThreads / 32];
+    BrickDesc br;
+    csv_request req;
+    uint32_t work, status, nact_next, pad;
+};
+
+// ------------------------------------------------------------------ LUT
+// findSymbol (brickDecoding.cpp:126-135) over the loaded 16-entry cumulative
+// table, tabulated for all x in [0, 4096): symbol | freq << 4 | start << 17.
+cudaError_t build_lut(const uint32_t* freq, const uint32_t* cum, uint32_t* h_lut) {
+    for (uint32_t x = 0; x < kTot; ++x) {
+        uint32_t s = 0;
+        while (s + 1 < 16 && x >= cum[s + 1]) ++s;
+        h_lut[x] = s | (freq[s] << 4) | (cum[s] << 17);
+    }
+    return cudaSuccess;
+}
+
+// One rANS decode step (ransDecodeSymbol, brickDecoding.cpp:137-151), totalFreq
+// 4096 so % and / are a mask and a shift.
+__device__ __forceinline__ uint32_t rans_step(uint32_t& x, uint32_t& pos, const uint8_t* __restrict__ enc,
+                                              const uint32_t* __restrict__ lut) {
+    uint32_t v = x & (kTot - 1);
+    uint32_t e = lut[v];
+    uint32_t f = (e >> 4) & 0x1FFFu, st = e >> 17;
+    x = f * (x >> kTotBits) + v - st;
+    while (x < kRansL && pos > 0) x = (x << 8) | __ldg(enc + (--pos));
+    return e & 15u;
+}
+
+// -------------------------------------------------------------- seek index
+// One thread per brick: the decoder's serial pass, recording a checkpoint
+// before every S-th op and the first op of every level.  Level l+1 has 8 ops
+// per op of level l with stop bit 0; level 1 has 8 unless the root's stop bit
+// is set (then the brick is one label).
+__global__ void __launch_bounds__(128) build_index_kernel(BrickDesc* __restrict__ bricks, uint32_t nb,
+                                                          const uint8_t* __restrict__ enc_pool,
+                                                          const uint32_t* __restrict__ g_lut,
+                                                          Checkpoint* __restrict__ ck, uint32_t L, uint32_t S) {
+    __shared__ uint32_t lut[kTot];
+    for (uint32_t i = threadIdx.x; i < kTot; i += blockDim.x) lut[i] = g_lut[i];
+    __syncthreads();
+    uint32_t bi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (bi >= nb) return;
+    BrickDesc br = bricks[bi];
+    uint32_t ls[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) ls[k] = 0;
+    uint32_t flags = 0, ops = 0, n_ck = 0;
+    if (br.E < 4 || br.nsym == 0) {
+        flags = BF_TRUNCATED;
+    } else {
+        const uint8_t* enc = enc_pool + br.enc_off;
+        uint32_t pos = br.E - 4;
+        uint32_t x = ((uint32_t)enc[br.E - 1] << 24) | ((uint32_t)enc[br.E - 2] << 16) |
+                     ((uint32_t)enc[br.E - 3] << 8) | enc[br.E - 4];
+        uint32_t sym = 1;
+        uint32_t root = rans_step(x, pos, enc, lut);
+        if (root & 1u) {
+            flags = BF_UNIFORM;
+        } else {
+            uint32_t ip = 0, need = 8, lvl = 0, act = 0, done = 0;
+            while (lvl + 1 < L && need > 0) {
+                if (ops % S == 0) {
+                    if (n_ck < br.ck_cap) ck[br.ck_off + n_ck] = Checkpoint{x, pos, sym, ip};
+                    ++n_ck;
+                }
+                if (sym >= br.nsym) { flags |= BF_TRUNCATED; break; }
+                uint32_t v = rans_step(x, pos, enc, lut);
+                ++sym;
+                uint32_t code = v >> 1;
+                if (code == OP_PD) {
+                    if (sym >= br.nsym) { flags |= BF_TRUNCATED; ++ops; break; }
+                    rans_step(x, pos, enc, lut);
+                    ++sym;
+                }
+                if (code == OP_PA) ++ip;
+                if (!(v & 1u)) ++act;
+                ++ops;
+                if (++done == need) {
+                    ++lvl;
+                    ls[lvl] = ops;
+                    need = 8 * act;
+                    act = 0;
+                    done = 0;
+                }
+            }
+            for (uint32_t k = lvl + 1; k < 8; ++k) ls[k] = ops;
+            if (n_ck > br.ck_cap) flags |= BF_TRUNCATED;
+        }
+    }
+    BrickDesc& o = bricks[bi];
+    o.n_ops = ops;
+    o.flags = flags;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) o.level_start[k] = ls[k];
+}
+
+cudaError_t launch_build_index(DeviceDataset& ds, cudaStream_t st) {
+    if (ds.nb == 0) return cudaSuccess;
+    uint32_t blocks = (ds.nb + 127) / 128;
+    build_index_kernel<<<blocks, 128, 0, st>>>(ds.d_bricks, ds.nb, ds.d_enc, ds.d_lut, ds.d_ck, ds.L, ds.S);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ decode kernel
+struct DecodeArgs {
+    const BrickDesc* bricks;
+    const uint64_t* pal;
+    const uint8_t* enc;
+    const Checkpoint* ck;
+    const uint32_t* lut;
+    const csv_request* reqs;
+    uint64_t* out;
+    uint32_t* status;
+    uint8_t* scratch;
+    uint64_t scratch_per_cta;
+    uint32_t* queue;
+    uint32_t nb, L, S, n;
+};
+
+__device__ __forceinline__ void st_cs_v2(uint64_t* p, uint64_t a, uint64_t b) {
+    asm volatile("st.global.cs.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(a), "l"(b) : "memory");
+}
+
+// Writes `cnt` copies of `v` at out[0..cnt) (out 8-byte aligned).
+__device__ void fill_labels(uint64_t* out, uint64_t cnt, uint64_t v) {
+    uint64_t start = 0;
+    if (((uintptr_t)out & 15) && cnt) {
+        if (threadIdx.x == 0) out[0] = v;
+        start = 1;
+    }
+    uint64_t pairs = (cnt - start) / 2;
+    for (uint64_t i = threadIdx.x; i < pairs; i += blockDim.x) st_cs_v2(out + start + 2 * i, v, v);
+    if (((cnt - start) & 1) && threadIdx.x == 0) out[cnt - 1] = v;
+}
+
+struct LevelView {
+    const uint32_t* ni;  // node info of the parent level
+    const uint32_t* av;  // active values of the parent level
+    const uint32_t* rec; // op records of the brick
+    uint32_t o;          // first op of the child level
+    uint32_t n_rec;      // records available
+};
+
+__device__ __forceinline__ uint32_t get_rec(const LevelView& v, uint32_t idx) {
+    return idx < v.n_rec ? v.rec[idx] : REC_MISSING;
+}
+__device__ __forceinline__ uint32_t node_value(const LevelView& v, uint32_t p) {
+    uint32_t i = v.ni[p];
+    return (i & NI_ACT) ? v.av[i & ~NI_ACT] : i;
+}
+
+// Value (palette index) of node n on level lc whose op record is `rec`; the
+// parent of n is active.  Follows getNeighborValue (brickDecoding.cpp:77-124,
+// decode.wgsl:247-306) with the output array replaced by node values: the -1
+// neighbour is read as a node of the same level, the +1 neighbour through its
+// parent.  A neighbour outside the brick reads the reference's "parent slot",
+// which for child c > 0 already holds child 0's value (slot aliasing of
+// coarseNodeToOutputIndex); malformed streams only.  Morton indices strictly
+// decrease along a chain, so it terminates; the iteration cap only guards
+// against a corrupt seek index.
+__device__ uint32_t resolve(const LevelView& v, uint32_t rec, uint32_t n, uint32_t lc, uint32_t& st) {
+    const uint32_t lvlmask = (lc >= 10) ? 0x3FFFFFFFu : ((1u << (3 * lc)) - 1u);
+#pragma unroll 1
+    for (int hop = 0; hop < 4096; ++hop) {
+        uint32_t code = rec & 7u;
+        if (code >= OP_PA) return rec >> REC_PIDX_SHIFT;
+        if (code == OP_RP) return node_value(v, n >> 3);
+        uint32_t a = code - 1;
+        uint32_t m = (0x09249249u << a) & lvlmask;
+        uint32_t bit = 1u << a;
+        bool oob;
+        uint32_t N;
+        if (n & bit) {
+            oob = (n & m) == m;
+            N = (((n | ~m) + bit) & m) | (n & ~m);
+            if (!oob) return node_value(v, N >> 3);
+        } else {
+            oob = (n & m) == 0;
+            N = (((n & m) - bit) & m) | (n & ~m);
+            if (!oob) {
+                uint32_t q = v.ni[N >> 3];
+                if (!(q & NI_ACT)) return q;
+                rec = get_rec(v, v.o + 8 * (q & ~NI_ACT) + (N & 7u));
+                n = N;
+                continue;
+            }
+        }
+        // outside the brick: the parent slot
+        if ((n & 7u) == 0) return node_value(v, n >> 3);
+        uint32_t q = v.ni[n >> 3];
+        rec = get_rec(v, v.o + 8 * (q & ~NI_ACT));
+        n &= ~7u;
+    }
+    st |= CSV_BRICK_BADOP;
+    return 0;
+}
+
+__device__ __forceinline__ uint64_t label_of(const uint64_t* pal, uint32_t pidx) {
+    return pidx == PIDX_LABEL0 ? 0ull : pal[pidx];
+}
+
+// Block-wide exclusive scan of a[0..n) in place (n <= blockDim * 16); returns the total.
+__device__ uint32_t block_exclusive_scan(uint32_t* a, uint32_t n, uint32_t* warp_sums) {
+    const uint32_t T = blockDim.x, tid = threadIdx.x;
+    const uint32_t per = (n + T - 1) / T;
+    const uint32_t b0 = min(n, tid * per), b1 = min(n, b0 + per);
+    uint32_t s = 0;
+    for (uint32_t i = b0; i < b1; ++i) s += a[i];
+    uint32_t lane = tid & 31, w = tid >> 5;
+    uint32_t inc = s;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, inc, d);
+        if (lane >= (uint32_t)d) inc += y;
+    }
+    if (lane == 31) warp_sums[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        uint32_t nw = T / 32;
+        uint32_t ws = lane < nw ? warp_sums[lane] : 0;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, ws, d);
+            if (lane >= (uint32_t)d) ws += y;
+        }
+        if (lane < nw) warp_sums[lane] = ws;
+    }
+    __syncthreads();
+    uint32_t run = inc - s + (w ? warp_sums[w - 1] : 0);
+    for (uint32_t i = b0; i < b1; ++i) {
+        uint32_t t = a[i];
+        a[i] = run;
+        run += t;
+    }
+    uint32_t total = warp_sums[T / 32 - 1];
+    __syncthreads();
+    return total;
+}
+
+__global__ void __launch_bounds__(kDecThreads) decode_kernel(DecodeArgs A) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    DecShared& S = *reinterpret_cast<DecShared*>(smem_raw);
+    const uint32_t tid = threadIdx.x;
+
+    for (uint32_t i = tid; i < kTot; i += blockDim.x) S.lut[i] = A.lut[i];
+
+    uint8_t* scr = A.scratch + (uint64_t)blockIdx.x * A.scratch_per_cta;
+    uint32_t* recs = reinterpret_cast<uint32_t*>(scr);
+    const uint64_t max_ops = ((1ull << (3 * A.L)) - 8) / 7;
+    uint32_t* g_ni = reinterpret_cast<uint32_t*>(scr + ((max_ops * 4 + 255) & ~255ull));
+    const uint32_t g_nodes = A.L > kSmemLevels + 1 ? (1u << (3 * (A.L - 2))) : 0;  // the one level > 4096 nodes
+    uint32_t* g_av = g_ni + g_nodes;
+
+    for (;;) {
+        if (tid == 0) {
+            S.work = atomicAdd(A.queue, 1u);
+            S.status = 0;
+            if (S.work < A.n) {
+                S.req = A.reqs[S.work];
+                if (S.req.brick < A.nb) S.br = A.bricks[S.req.brick];
+            }
+        }
+        __syncthreads();
+        const uint32_t w = S.work;
+        if (w >= A.n) break;
+        const csv_request req = S.req;
+        const uint32_t t = req.lod;
+        if (req.brick >= A.nb || t >= A.L) {
+            if (tid == 0) A.status[w] = CSV_BRICK_BADREQ;
+            __syncthreads();
+            continue;
+        }
+        const BrickDesc br = S.br;
+        uint64_t* out = A.out + req.dst;
+        const uint64_t* gpal = A.pal + br.pal_off;
+        const uint64_t* pal = gpal;
+        if (br.P <= kPalCache) {
+            for (uint32_t i = tid; i < br.P; i += blockDim.x) S.pal[i] = gpal[i];
+            pal = S.pal;
+        }
+        uint32_t st = (br.flags & BF_TRUNCATED) ? CSV_BRICK_TRUNCATED : 0;
+        __syncthreads();
+
+        if (t == 0 || (br.flags & BF_UNIFORM)) {
+            fill_labels(out, 1ull << (3 * t), pal[0]);
+        } else {
+            // ---- 1. rANS segments -> op records
+            const uint32_t n_need = min(min(br.level_start[t], br.n_ops), br.ck_cap * A.S);
+            const uint32_t nseg = (n_need + A.S - 1) / A.S;
+            const uint8_t* enc = A.enc + br.enc_off;
+            for (uint32_t k = tid; k < nseg; k += blockDim.x) {
+                Checkpoint c = A.ck[br.ck_off + k];
+                uint32_t x = c.state, pos = c.pos, sym = c.sym, ip = c.ip;
+                uint32_t j = k * A.S;
+                const uint32_t jend = min(j + A.S, n_need);
+                while (j < jend) {
+                    if (sym >= br.nsym) { st |= CSV_BRICK_TRUNCATED; break; }
+                    uint32_t v = rans_step(x, pos, enc, S.lut);
+                    ++sym;
+                    uint32_t code = v >> 1, pidx = 0;
+                    if (code == OP_PD) {
+                        uint32_t d = 0;
+                        if (sym >= br.nsym) st |= CSV_BRICK_TRUNCATED;
+                        else { d = rans_step(x, pos, enc, S.lut); ++sym; }
+                        pidx = ip - d - 1;
+                        if (pidx >= br.P) { pidx = br.P - 1; st |= CSV_BRICK_PALETTE; }
+                    } else if (code == OP_PA) {
+                        ++ip;
+                        pidx = ip;
+                        if (pidx >= br.P) { pidx = br.P - 1; st |= CSV_BRICK_PALETTE; }
+                    } else if (code == OP_P0) {
+                        pidx = ip;
+                        if (pidx >= br.P) { pidx = br.P - 1; st |= CSV_BRICK_PALETTE; }
+                    } else if (code == 7) {
+                        pidx = PIDX_LABEL0;
+                        st |= CSV_BRICK_BADOP;
+                    }
+                    recs[j] = code | ((v & 1u) << 3) | (pidx << REC_PIDX_SHIFT);
+                    ++j;
+                }
+            }
+            if (tid == 0) { S.ni[0] = NI_ACT | 0u; S.av[0] = 0; }
+            __syncthreads();
+
+            // ---- 2./3. levels coarse to fine
+            uint32_t n_act = 1;
+            for (uint32_t l = 0; l < t; ++l) {
+                const uint32_t lc = l + 1;
+                LevelView V;
+                V.ni = (l < kSmemLevels) ? S.ni + lvl_off(l) : g_ni;
+                V.av = (l < kSmemLevels) ? S.av + lvl_off(l) : g_av;
+                V.rec = recs;
+                V.o = br.level_start[l];
+                V.n_rec = n_need;
+                const uint32_t n_par = 1u << (3 * l);
+                if (lc < t) {
+                    uint32_t* ni_c = (lc < kSmemLevels) ? S.ni + lvl_off(lc) : g_ni;
+                    uint32_t* av_c = (lc < kSmemLevels) ? S.av + lvl_off(lc) : g_av;
+                    // children with stop 0 per active parent, then their ranks
+                    for (uint32_t r = tid; r < n_act; r += blockDim.x) {
+                        uint32_t cnt = 0;
+#pragma unroll
+                        for (uint32_t c = 0; c < 8; ++c) cnt += (get_rec(V, V.o + 8 * r + c) & 8u) ? 0u : 1u;
+                        S.base[r] = cnt;
+                    }
+                    __syncthreads();
+                    const uint32_t n_act_c = block_exclusive_scan(S.base, n_act, S.warp_sums);
+                    for (uint32_t p = tid; p < n_par; p += blockDim.x) {
+                        const uint32_t info = V.ni[p];
+                        if (!(info & NI_ACT)) {
+#pragma unroll
+                            for (uint32_t c = 0; c < 8; ++c) ni_c[8 * p + c] = info;
+                            continue;
+                        }
+                        const uint32_t r = info & ~NI_ACT;
+                        uint32_t rk = S.base[r];
+#pragma unroll
+                        for (uint32_t c = 0; c < 8; ++c) {
+                            uint32_t rec = get_rec(V, V.o + 8 * r + c);
+                            uint32_t val = resolve(V, rec, 8 * p + c, lc, st);
+                            if (rec & 8u) {
+                                ni_c[8 * p + c] = val;
+                            } else {
+                                ni_c[8 * p + c] = NI_ACT | rk;
+                                av_c[rk] = val;
+                                ++rk;
+                            }
+                        }
+                    }
+                    n_act = n_act_c;
+                    __syncthreads();
+                } else {
+                    // last level: labels to HBM, 64 bytes per parent
+                    const bool vec = (((uintptr_t)out) & 15) == 0;
+                    for (uint32_t p = tid; p < n_par; p += blockDim.x) {
+                        const uint32_t info = V.ni[p];
+                        uint64_t lab[8];
+                        if (!(info & NI_ACT)) {
+                            uint64_t x = label_of(pal, info);
+#pragma unroll
+                            for (int c = 0; c < 8; ++c) lab[c] = x;
+                        } else {
+                            const uint32_t r = info & ~NI_ACT;
+#pragma unroll
+                            for (uint32_t c = 0; c < 8; ++c) {
+                                uint32_t rec = get_rec(V, V.o + 8 * r + c);
+                                lab[c] = label_of(pal, resolve(V, rec, 8 * p + c, lc, st));
+                            }
+                        }
+                        uint64_t* o8 = out + 8ull * p;
+                        if (vec) {
+#pragma unroll
+                            for (int c = 0; c < 8; c += 2) st_cs_v2(o8 + c, lab[c], lab[c + 1]);
+                        } else {
+#pragma unroll
+                            for (int c = 0; c < 8; ++c) o8[c] = lab[c];
+                        }
+                    }
+                }
+            }
+        }
+        if (st) atomicOr(&S.status, st);
+        __syncthreads();
+        if (tid == 0) A.status[w] = S.status;
+        __syncthreads();
+    }
+}
+
+size_t decode_scratch_per_cta(uint32_t b) {
+    uint32_t L = levels_of(b);
+    uint64_t rec_bytes = (max_ops_of(b) * 4 + 255) & ~255ull;
+    uint64_t g_nodes = L > kSmemLevels + 1 ? (1ull << (3 * (L - 2))) : 0;
+    return (size_t)((rec_bytes + 2 * g_nodes * 4 + 255) & ~255ull);
+}
+
+static int g_dec_occ[64] = {0};
+
+uint32_t decode_grid(int device, uint32_t n) {
+    int& occ = g_dec_occ[device & 63];
+    if (occ == 0) {
+        cudaFuncSetAttribute(decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DecShared));
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, decode_kernel, kDecThreads, sizeof(DecShared));
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        occ = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+    }
+    return n < (uint32_t)occ ? n : (uint32_t)occ;
+}
+
+cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, uint32_t n, uint64_t* d_out,
+                          uint32_t* d_status, const DecodeScratch& scr, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    uint32_t grid = decode_grid(ds.device, n);
+    if (grid > scr.ctas) grid = scr.ctas;
+    cudaError_t e = cudaMemsetAsync(scr.d_queue, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    DecodeArgs A;
+    A.bricks = ds.d_bricks;
+    A.pal = ds.d_pal;
+    A.enc = ds.d_enc;
+    A.ck = ds.d_ck;
+    A.lut = ds.d_lut;
+    A.reqs = d_reqs;
+    A.out = d_out;
+    A.status = d_status;
+    A.scratch = scr.base;
+    A.scratch_per_cta = scr.per_cta;
+    A.queue = scr.d_queue;
+    A.nb = ds.nb;
+    A.L = ds.L;
+    A.S = ds.S;
+    A.n = n;
+    decode_kernel<<<grid, kDecThreads, sizeof(DecShared), st>>>(A);
+    return cudaGetLastError();
+}
+
+}  // namespace csv

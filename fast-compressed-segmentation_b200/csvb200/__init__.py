@@ -1,0 +1,263 @@
+"""Python host binding of the B200 compressed-segmentation-volume codec.
+
+A ctypes layer over the C ABI in include/csv.h (libcsvb200.so, built for
+sm_100a).  It mirrors the reference's entry points for this path:
+
+  reference (paths relative to the reference root)      here
+  ---------------------------------------------------   ------------------------------
+  splitGridIntoBricks + compressDataset +                Codec.encode / encode_device
+    saveDatasetToFile (brick.hpp:134,
+    brickEncoding.hpp:467, fileIO.cpp:15)
+  loadDatasetFromFile (fileIO.cpp:101),                  Codec.open
+    loadDatasetFromArrayBuffer (datasetLoader.js:39)
+  decodeRansStream + decodeBrick<b>                      Codec.decode_batch / decode_image
+    (brickDecoding.cpp:153, brickDecoding.hpp:175),
+    decode.wgsl:decodeBrick (:344)
+
+Errors raise ``CsvError`` where the reference throws std::runtime_error.
+Device buffers are torch tensors (torch is used only for device memory and
+streams).  There is no CPU fallback: a missing library or GPU raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcsvb200.so")
+
+CSV_BRICK_TRUNCATED = 0x1
+CSV_BRICK_PALETTE = 0x2
+CSV_BRICK_BADOP = 0x4
+CSV_BRICK_BADREQ = 0x8
+CSV_BRICK_TIMEOUT = 0x10
+
+ERRORS = {-1: "EINVAL", -2: "EFORMAT", -3: "ECUDA", -4: "ENOMEM", -5: "ERANGE", -6: "EBRICK"}
+
+# csv_request: {uint32 brick, uint32 lod, uint64 dst}
+REQUEST_DTYPE = np.dtype([("brick", "<u4"), ("lod", "<u4"), ("dst", "<u8")])
+
+
+class CsvError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class _Info(C.Structure):
+    _fields_ = [("num_bricks", C.c_uint32), ("brick_size", C.c_uint32), ("levels", C.c_uint32),
+                ("ops_per_checkpoint", C.c_uint32), ("stream_bytes", C.c_uint64),
+                ("palette_entries", C.c_uint64), ("freq", C.c_uint32 * 16), ("cum", C.c_uint32 * 16)]
+
+
+_lib = None
+
+
+def library_path() -> str:
+    return LIB_PATH
+
+
+def load_library() -> C.CDLL:
+    """Load libcsvb200.so; raises if it was not built (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} missing: build it with `make -C fast-compressed-segmentation_b200`")
+    L = C.CDLL(LIB_PATH)
+    vp, u8p, u32p, u64p = C.c_void_p, C.POINTER(C.c_uint8), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)
+    L.csv_abi_version.restype = C.c_int
+    L.csv_create.argtypes = [C.c_int, C.POINTER(vp)]
+    L.csv_destroy.argtypes = [vp]
+    L.csv_last_error.restype = C.c_char_p
+    L.csv_last_error.argtypes = [vp]
+    L.csv_free.argtypes = [vp]
+    L.csv_encode.argtypes = [vp, u64p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(u8p),
+                             C.POINTER(C.c_size_t)]
+    L.csv_encode_device.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, vp,
+                                    C.POINTER(C.c_size_t)]
+    L.csv_encoded_image.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_size_t)]
+    L.csv_open.argtypes = [vp, u8p, C.c_size_t, C.POINTER(vp)]
+    L.csv_open_encoded.argtypes = [vp, C.POINTER(vp)]
+    L.csv_dataset_info_get.argtypes = [vp, C.POINTER(_Info)]
+    L.csv_dataset_ids.argtypes = [vp, u32p, C.c_uint32]
+    L.csv_close.argtypes = [vp]
+    L.csv_decode_batch.argtypes = [vp, vp, vp, C.c_uint32, vp, vp, vp]
+    L.csv_decode_image.argtypes = [vp, u8p, C.c_size_t, C.c_uint32, u64p, u32p]
+    L.csv_synth_volume.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_uint32, C.c_uint32,
+                                   C.c_float, C.c_float, C.c_float, C.c_uint64, vp]
+    _lib = L
+    return L
+
+
+def _stream_handle(stream) -> int | None:
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+@dataclass
+class DatasetInfo:
+    num_bricks: int
+    brick_size: int
+    levels: int
+    ops_per_checkpoint: int
+    stream_bytes: int
+    palette_entries: int
+    freq: tuple
+    cum: tuple
+
+
+class Dataset:
+    """A .csbd image staged in HBM with its seek index (csv_open)."""
+
+    def __init__(self, codec: "Codec", handle: int):
+        self.codec = codec
+        self.handle = C.c_void_p(handle)
+        info = _Info()
+        codec.lib.csv_dataset_info_get(self.handle, C.byref(info))
+        self.info = DatasetInfo(info.num_bricks, info.brick_size, info.levels, info.ops_per_checkpoint,
+                                info.stream_bytes, info.palette_entries, tuple(info.freq), tuple(info.cum))
+
+    @property
+    def num_bricks(self) -> int:
+        return self.info.num_bricks
+
+    @property
+    def brick_size(self) -> int:
+        return self.info.brick_size
+
+    def ids(self) -> np.ndarray:
+        out = np.zeros(max(1, self.num_bricks), np.uint32)
+        self.codec._check(self.codec.lib.csv_dataset_ids(self.handle, out.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                                          len(out)))
+        return out[: self.num_bricks]
+
+    def close(self):
+        if self.handle:
+            self.codec.lib.csv_close(self.handle)
+            self.handle = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Codec:
+    """One context on one CUDA device (csv_create)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = C.c_void_p()
+        rc = self.lib.csv_create(device, C.byref(h))
+        if rc:
+            raise CsvError(rc, f"csv_create(device={device}) failed (no usable CUDA device?)")
+        self.handle = h
+        self.device = device
+
+    def _check(self, rc: int):
+        if rc:
+            raise CsvError(rc, self.lib.csv_last_error(self.handle).decode())
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.csv_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- encoder -------------------------------------------------------
+    def encode(self, volume: np.ndarray, brick_size: int = 64) -> bytes:
+        """Host volume (D, H, W) uint64, x fastest -> .csbd v1 bytes."""
+        v = np.ascontiguousarray(volume, dtype=np.uint64)
+        D, H, W = v.shape
+        out = C.POINTER(C.c_uint8)()
+        n = C.c_size_t()
+        self._check(self.lib.csv_encode(self.handle, v.ctypes.data_as(C.POINTER(C.c_uint64)), W, H, D, brick_size,
+                                        C.byref(out), C.byref(n)))
+        data = C.string_at(out, n.value)
+        self.lib.csv_free(out)
+        return data
+
+    def encode_device(self, d_volume, brick_size: int = 64, stream=None) -> int:
+        """Device volume (torch uint64/int64 tensor, shape (D, H, W)) -> image length; the image stays on the
+        device (see encoded_image)."""
+        D, H, W = d_volume.shape
+        n = C.c_size_t()
+        self._check(self.lib.csv_encode_device(self.handle, C.c_void_p(d_volume.data_ptr()), W, H, D, brick_size,
+                                               C.c_void_p(_stream_handle(stream)), C.byref(n)))
+        return n.value
+
+    def encoded_image(self):
+        ptr = C.c_void_p()
+        n = C.c_size_t()
+        self._check(self.lib.csv_encoded_image(self.handle, C.byref(ptr), C.byref(n)))
+        return ptr.value, n.value
+
+    # ---- datasets ------------------------------------------------------
+    def open(self, image: bytes) -> Dataset:
+        a = np.frombuffer(image, np.uint8)
+        h = C.c_void_p()
+        self._check(self.lib.csv_open(self.handle, a.ctypes.data_as(C.POINTER(C.c_uint8)), len(image), C.byref(h)))
+        return Dataset(self, h.value)
+
+    def open_encoded(self) -> Dataset:
+        h = C.c_void_p()
+        self._check(self.lib.csv_open_encoded(self.handle, C.byref(h)))
+        return Dataset(self, h.value)
+
+    # ---- decoder -------------------------------------------------------
+    def decode_batch(self, ds: Dataset, d_reqs, d_out, d_status, stream=None, n: int | None = None):
+        """d_reqs: device tensor holding csv_request records (16 bytes each, e.g. a uint8 tensor from
+        ``requests_tensor``); d_out: uint64/int64 device tensor; d_status: int32 device tensor."""
+        if n is None:
+            n = d_reqs.numel() * d_reqs.element_size() // 16
+        self._check(self.lib.csv_decode_batch(self.handle, ds.handle, C.c_void_p(d_reqs.data_ptr()), n,
+                                              C.c_void_p(d_out.data_ptr()), C.c_void_p(d_status.data_ptr()),
+                                              C.c_void_p(_stream_handle(stream))))
+
+    def decode_image(self, image: bytes, lod: int, check: bool = True):
+        """Host .csbd bytes -> (labels (numBricks, 8^lod) uint64, status (numBricks,) uint32)."""
+        a = np.frombuffer(image, np.uint8)
+        nb = int(np.frombuffer(image[8:12], np.uint32)[0])
+        out = np.zeros((max(1, nb), 1 << (3 * lod)), np.uint64)
+        st = np.zeros(max(1, nb), np.uint32)
+        rc = self.lib.csv_decode_image(self.handle, a.ctypes.data_as(C.POINTER(C.c_uint8)), len(image), lod,
+                                       out.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                       st.ctypes.data_as(C.POINTER(C.c_uint32)))
+        if rc and (check or rc != -6):
+            self._check(rc)
+        return out[:nb], st[:nb]
+
+    # ---- workload generator ---------------------------------------------
+    def synth_volume(self, d_volume, kind: int, n_cells: int, n_tubes: int = 0, r_min: float = 0.0,
+                     r_max: float = 0.0, zero_frac: float = 0.0, seed: int = 0, stream=None):
+        D, H, W = d_volume.shape
+        self._check(self.lib.csv_synth_volume(self.handle, C.c_void_p(d_volume.data_ptr()), W, H, D, kind, n_cells,
+                                              n_tubes, r_min, r_max, zero_frac, seed,
+                                              C.c_void_p(_stream_handle(stream))))
+
+
+def requests(bricks, lods, dsts) -> np.ndarray:
+    r = np.zeros(len(bricks), REQUEST_DTYPE)
+    r["brick"] = bricks
+    r["lod"] = lods
+    r["dst"] = dsts
+    return r
+
+
+def requests_tensor(reqs: np.ndarray, device="cuda"):
+    import torch
+    return torch.from_numpy(reqs.view(np.uint8).copy()).to(device)

@@ -1,0 +1,148 @@
+/* csv.h -- C ABI of the B200 compressed-segmentation-volume (CSV) brick codec.
+ *
+ * One thin C boundary (C linkage, plain pointers and sizes, no C++ or torch
+ * types) over the sm_100a CUDA kernels.  It replaces, for this path, the
+ * reference's in-process C++ encoder/decoder calls and its WebGPU decode
+ * dispatch; each entry point names the reference interface it stands in for
+ * (paths relative to the reference project root).
+ *
+ * Conventions
+ *  - Every call returns CSV_OK (0) or a negative CSV_E* code; the message of
+ *    the last failure on a context is csv_last_error(ctx).  The reference
+ *    throws std::runtime_error in the same places (fileIO.cpp:20,105,119;
+ *    brickDecoding.cpp:23; brick.hpp:137).
+ *  - A context owns its device buffers and is used by one host thread at a
+ *    time.  Pointers named d_* are device pointers on the context's device;
+ *    all others are host pointers.  `stream` is a cudaStream_t (0 = legacy
+ *    default stream).
+ *  - Volumes are uint64 labels, x fastest: vol[x + W*(y + H*z)]
+ *    (brick.hpp:183).  Decoded bricks are 8^lod labels in Morton order
+ *    (brickDecoding.hpp:174-242, decode.wgsl:239-245).
+ *  - lod is the reference's targetLOD: the output has 2^lod voxels per axis,
+ *    log2(brick size) is full resolution and 0 is one voxel
+ *    (decode.wgsl:22-27, camera.js:118).
+ */
+#ifndef CSV_B200_H
+#define CSV_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CSV_ABI_VERSION 1
+
+enum {
+    CSV_OK = 0,
+    CSV_EINVAL = -1,   /* bad argument */
+    CSV_EFORMAT = -2,  /* malformed .csbd image (fileIO.cpp:118-119) */
+    CSV_ECUDA = -3,    /* a CUDA call failed */
+    CSV_ENOMEM = -4,   /* device or host allocation failed */
+    CSV_ERANGE = -5,   /* size beyond a documented limit */
+    CSV_EBRICK = -6    /* at least one brick reported a nonzero status */
+};
+
+/* Per-brick status bits written by the batched decoder (d_status).  The
+ * reference clamps or skips silently in these places; here they are reported. */
+#define CSV_BRICK_TRUNCATED 0x1u /* stream ended inside the level structure (decode.wgsl:449) */
+#define CSV_BRICK_PALETTE 0x2u   /* palette index past the palette, clamped (decode.wgsl:472-485) */
+#define CSV_BRICK_BADOP 0x4u     /* op code 7, label 0 written (decode.wgsl:487-489) */
+#define CSV_BRICK_BADREQ 0x8u    /* brick index or lod out of range (decode.wgsl:365-373) */
+#define CSV_BRICK_TIMEOUT 0x10u  /* a bounded wait gave up */
+
+typedef struct csv_ctx csv_ctx;
+typedef struct csv_dataset csv_dataset;
+
+/* One decode request: brick index in file order (the order of the .csbd and of
+ * splitGridIntoBricks, brick.hpp:152-154), target lod, and the element offset
+ * of its 8^lod output labels in d_out.  Mirrors DynamicBrickInfo
+ * (decode.wgsl:22-27) plus the work-queue entry (decode.wgsl:358). */
+typedef struct csv_request {
+    uint32_t brick;
+    uint32_t lod;
+    uint64_t dst;
+} csv_request;
+
+typedef struct csv_dataset_info {
+    uint32_t num_bricks;
+    uint32_t brick_size;
+    uint32_t levels;             /* log2(brick_size) + 1 (brick.hpp:50) */
+    uint32_t ops_per_checkpoint; /* seek-index spacing */
+    uint64_t stream_bytes;       /* sum of rANS stream lengths */
+    uint64_t palette_entries;    /* sum of palette sizes */
+    uint32_t freq[16];           /* the shared rANS model (fileIO.cpp:38-49) */
+    uint32_t cum[16];
+} csv_dataset_info;
+
+/* ---- context -------------------------------------------------------- */
+int csv_create(int device, csv_ctx** out);
+void csv_destroy(csv_ctx* ctx);
+const char* csv_last_error(const csv_ctx* ctx);
+int csv_abi_version(void);
+void csv_free(void* p); /* frees buffers this library returned (csv_encode) */
+
+/* ---- encoder ----------------------------------------------------------
+ * splitGridIntoBricks<b> (brick.hpp:134) + Encoding::compressDataset<b>
+ * (brickEncoding.hpp:467) + saveDatasetToFile (fileIO.cpp:15), as main.cpp:76-84
+ * runs them: the whole volume becomes one .csbd v1 image, byte-identical to
+ * the reference encoder's file (with brick_size stored in the header; the
+ * reference always writes 64 there, fileIO.cpp:28).  brick_size is a power of
+ * two in [8, 64]. */
+int csv_encode(csv_ctx* ctx, const uint64_t* volume, uint32_t W, uint32_t H, uint32_t D,
+               uint32_t brick_size, uint8_t** out, size_t* out_len);
+/* Same, volume already in device memory; the image stays in a context-owned
+ * device buffer (valid until the next encode on ctx) and its length is
+ * returned; csv_encoded_image() gives the device pointer.  The per-brick
+ * seek index the encoder produced as a by-product is kept with it. */
+int csv_encode_device(csv_ctx* ctx, const uint64_t* d_volume, uint32_t W, uint32_t H, uint32_t D,
+                      uint32_t brick_size, void* stream, size_t* image_len);
+int csv_encoded_image(csv_ctx* ctx, const uint8_t** d_image, size_t* len);
+
+/* ---- dataset -----------------------------------------------------------
+ * loadDatasetFromFile (fileIO.cpp:101-182) / loadDatasetFromArrayBuffer
+ * (web/scripts/datasetLoader.js:39-146): parse a .csbd v1 image, stage
+ * palettes and rANS streams in HBM, and build the seek index on the GPU (one
+ * serial rANS pass per brick; the "cold" step).  Bricks keep file order. */
+int csv_open(csv_ctx* ctx, const uint8_t* image, size_t len, csv_dataset** out);
+/* Open the image the last csv_encode_device produced on ctx, taking its seek
+ * index from the encoder instead of rebuilding it. */
+int csv_open_encoded(csv_ctx* ctx, csv_dataset** out);
+int csv_dataset_info_get(const csv_dataset* ds, csv_dataset_info* info);
+/* Morton brick IDs (datasetLoader.js:113-123) in file order, host array. */
+int csv_dataset_ids(const csv_dataset* ds, uint32_t* ids, uint32_t n);
+void csv_close(csv_dataset* ds);
+
+/* ---- decoder -----------------------------------------------------------
+ * decodeRansStream (brickDecoding.cpp:153-188) + decodeBrick<b>
+ * (brickDecoding.hpp:174-242) at full resolution, and decode.wgsl:decodeBrick
+ * (decode.wgsl:344-509) at any lod, in label space, for a batch of requests
+ * in one launch.  d_reqs: n requests in device memory.  d_out: labels;
+ * request k writes 8^lod labels at d_out + d_reqs[k].dst.  d_status: n
+ * per-request CSV_BRICK_* words (0 = clean).  A brick whose root stop bit is
+ * set (the whole brick is one label) decodes to palette[0] everywhere.
+ * Asynchronous on `stream`. */
+int csv_decode_batch(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_reqs, uint32_t n,
+                     uint64_t* d_out, uint32_t* d_status, void* stream);
+
+/* Host convenience over the above, as main.cpp:86-118 uses the reference
+ * decoder: parse `image`, decode every brick at `lod` and copy the labels to
+ * the host (brick i at out + i*8^lod).  status: numBricks words or NULL. */
+int csv_decode_image(csv_ctx* ctx, const uint8_t* image, size_t len, uint32_t lod, uint64_t* out,
+                     uint32_t* status);
+
+/* ---- workload generator (no reference counterpart) --------------------
+ * Seeded synthetic label volume on the device, x fastest: kind 0 = Voronoi
+ * (n_cells cells, then a random half-space slab of label 0 covering about
+ * zero_frac of the volume); kind 1 = n_tubes cubic tubes with radius in
+ * [r_min, r_max] over a Voronoi background with about zero_frac of its cells
+ * set to 0.  IDs are uniform in [1, 2^64-2]. */
+int csv_synth_volume(csv_ctx* ctx, uint64_t* d_volume, uint32_t W, uint32_t H, uint32_t D, int kind,
+                     uint32_t n_cells, uint32_t n_tubes, float r_min, float r_max, float zero_frac,
+                     uint64_t seed, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CSV_B200_H */

@@ -1,0 +1,183 @@
+"""CPU: the oracle (oracle/csv_oracle.c) against the compiled reference and the golden fixtures."""
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import read_golden
+from csvb200 import synth
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def test_morton_identities(oracle):
+    # utils.cpp:45-68: the children of parent m are 8m + c with c = dx + 2dy + 4dz
+    for m in [0, 1, 7, 100, 4095, 32767]:
+        x, y, z = [], [], []
+        import ctypes as C
+        xx, yy, zz = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        oracle.lib.or_demorton3.argtypes = [C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                            C.POINTER(C.c_uint32)]
+        oracle.lib.or_demorton3(m, C.byref(xx), C.byref(yy), C.byref(zz))
+        for c in range(8):
+            dx, dy, dz = c & 1, (c >> 1) & 1, (c >> 2) & 1
+            assert oracle.morton3(2 * xx.value + dx, 2 * yy.value + dy, 2 * zz.value + dz) == 8 * m + c
+
+
+def test_majority_tie_rule_vs_reference(oracle, reference):
+    rng = np.random.default_rng(0)
+    for hi in (3, 9, 14, 27, 40, 1 << 62):
+        vals = rng.integers(0, hi, size=(20000, 8), dtype=np.uint64)
+        for v in vals:
+            assert oracle.majority8(v) == reference.majority8(v), v
+
+
+def test_build_model_vs_reference(oracle, reference):
+    rng = np.random.default_rng(1)
+    for k in range(3000):
+        kind = k % 4
+        if kind == 0:
+            raw = rng.integers(0, 10, 16)
+        elif kind == 1:
+            raw = rng.integers(0, 100000, 16)
+        elif kind == 2:
+            raw = np.zeros(16, np.int64)
+            raw[rng.integers(0, 16)] = rng.integers(1, 10 ** 6)
+        else:
+            raw = (rng.pareto(0.7, 16) * 50).astype(np.int64)
+        f1, c1 = oracle.build_model(raw)
+        f2, c2 = reference.build_model(raw)
+        assert np.array_equal(f1, f2) and np.array_equal(c1, c2), raw
+        assert c1[16] == 4096
+
+
+@pytest.mark.parametrize("b", [64, 32, 16, 8])
+def test_encode_bytes_vs_reference(oracle, reference, b):
+    vol = synth.tubes_over_voronoi((40, 72, 88), 70, 10, 1.5, 7, seed=100 + b)
+    assert oracle.encode(vol, b) == reference.encode(vol, b)
+
+
+def test_encode_voronoi_slab_vs_reference(oracle, reference):
+    vol = synth.voronoi((64, 128, 96), 200, seed=5)
+    assert oracle.encode(vol, 64) == reference.encode(vol, 64)
+
+
+def test_full_decode_vs_reference_and_source(oracle, reference):
+    vol = synth.tubes_over_voronoi((64, 64, 128), 80, 16, 2, 9, seed=9)
+    img = oracle.encode(vol, 64)
+    dec, st = oracle.decode_image(img, 6)
+    ref, rst, _ = reference.decode_all_full(img, 64)
+    assert st.max() == 0 and rst.max() == 0
+    assert np.array_equal(dec, ref)
+    for i in range(dec.shape[0]):
+        pyr = oracle.pyramid(vol, 64, i)
+        assert np.array_equal(dec[i], pyr[6][0])
+
+
+def test_coarse_lods_equal_pyramid(oracle, reference):
+    vol = synth.tubes_over_voronoi((64, 64, 64), 50, 10, 1, 6, seed=21)
+    img = oracle.encode(vol, 64)
+    ref_pyr = reference.pyramid64(vol, 0)
+    or_pyr = oracle.pyramid(vol, 64, 0)
+    for t in range(7):
+        assert np.array_equal(ref_pyr[t][0], or_pyr[t][0])
+        assert np.array_equal(ref_pyr[t][1], or_pyr[t][1])
+        d, st = oracle.decode_image(img, t)
+        assert st.max() == 0
+        assert np.array_equal(d[0], or_pyr[t][0]), t
+
+
+def test_golden_shipped_subset(oracle, reference, golden):
+    img = read_golden("shipped_subset")
+    g = golden["shipped_subset"]
+    full, st, _ = reference.decode_all_full(img, 64)
+    assert st.max() == 0
+    assert [sha(full[k]) for k in range(full.shape[0])] == g["lod"]["6"]
+    for t in range(7):
+        d, s = oracle.decode_image(img, t)
+        assert s.max() == 0
+        assert [sha(d[k]) for k in range(d.shape[0])] == g["lod"][str(t)], t
+
+
+def crop_volume(dec, shape_dhw, b, ids):
+    """Reassemble bricks (Morton order inside, file order = split order) into a (D, H, W) volume."""
+    D, H, W = shape_dhw
+    nbx, nby, nbz = -(-W // b), -(-H // b), -(-D // b)
+    full = np.zeros((nbz * b, nby * b, nbx * b), np.uint64)
+    from oracle import Oracle
+    O = Oracle()
+    mort = np.array([O.morton3(x, y, z) for z in range(b) for y in range(b) for x in range(b)]).reshape(b, b, b)
+    i = 0
+    for bx in range(nbx):
+        for by in range(nby):
+            for bz in range(nbz):
+                full[bz * b:(bz + 1) * b, by * b:(by + 1) * b, bx * b:(bx + 1) * b] = dec[i][mort]
+                i += 1
+    return full[:D, :H, :W]
+
+
+@pytest.mark.parametrize("name", ["voronoi_96x80x72_b64", "tubes_64_b32", "tubes_64_b16", "uniform_64_b64",
+                                  "mixed_uniform_128x64x64_b64"])
+def test_golden_encode_roundtrip(oracle, golden, name):
+    g = golden[name]
+    img = read_golden(name)
+    assert hashlib.sha256(img).hexdigest() == g["bytes_sha256"]
+    b = g["brick_size"]
+    full, st = oracle.decode_image(img, b.bit_length() - 1)
+    assert st.max() == 0
+    vol = crop_volume(full, g["shape_dhw"], b, None)
+    assert sha(vol) == g["volume_sha256"]
+    assert oracle.encode(vol, b) == img
+    for t in range(b.bit_length()):
+        d, s = oracle.decode_image(img, t)
+        assert [sha(d[k]) for k in range(d.shape[0])] == g["lod"][str(t)]
+
+
+def test_seek_index_checkpoints_resume_decode(oracle):
+    """Each checkpoint (state, byte position, nibble index, palette index) lets the rANS decoder resume."""
+    import struct
+    img = read_golden("shipped_subset")
+    freq = np.frombuffer(img[24:88], np.uint32)
+    cum = np.frombuffer(img[88:152], np.uint32)
+    o = 152
+    for _ in range(3):
+        ID, P = struct.unpack_from("<2I", img, o)
+        o += 8 + 8 * P
+        E = struct.unpack_from("<I", img, o)[0]
+        enc = img[o + 4:o + 4 + E]
+        o += 4 + E
+        ns = struct.unpack_from("<I", img, o)[0]
+        o += 4
+        nib = oracle.rans_decode(freq, cum, enc, ns)
+        nibs = [(nib[i // 2] >> (4 * (1 - i % 2))) & 15 for i in range(ns)]
+        n_ops, ls, ck, st = oracle.seek_index(freq, cum, enc, ns, P, 64, 256)
+        assert st == 0 and ls[6] == n_ops and ck.shape[0] == -(-n_ops // 256)
+        # parse ops serially and check every checkpoint's nibble index and palette index
+        sym, ip, op = 1, 0, 0
+        starts = {}
+        while op < n_ops:
+            if op % 256 == 0:
+                starts[op] = (sym, ip)
+            code = nibs[sym] >> 1
+            sym += 2 if code == 6 else 1
+            ip += code == 4
+            op += 1
+        lut = []
+        for x in range(4096):
+            s = 0
+            while s + 1 < 16 and x >= cum[s + 1]:
+                s += 1
+            lut.append(s)
+        for k, (state, pos, csym, cip) in enumerate(ck):
+            assert (int(csym), int(cip)) == starts[k * 256]
+            x, p = int(state), int(pos)
+            for j in range(int(csym), min(ns, int(csym) + 40)):
+                v = x & 4095
+                s = lut[v]
+                x = int(freq[s]) * (x >> 12) + v - int(cum[s])
+                while x < (1 << 23) and p > 0:
+                    p -= 1
+                    x = ((x << 8) | enc[p]) & 0xFFFFFFFF
+                assert s == nibs[j]
