@@ -351,6 +351,79 @@ int csv_decode_image(csv_ctx* ctx, const uint8_t* image, size_t len, uint32_t lo
     return rc;
 }
 
+int csv_encode_device(csv_ctx* ctx, const uint64_t* d_volume, uint32_t W, uint32_t H, uint32_t D, uint32_t brick_size,
+                      void* stream, size_t* image_len) {
+    if (!ctx || !image_len) return CSV_EINVAL;
+    if (brick_size < 2 || brick_size > 64 || (brick_size & (brick_size - 1)))
+        return fail(ctx, CSV_EINVAL, "brick size must be a power of two in [2, 64]");
+    if ((uint64_t)W * H * D > 0 && !d_volume) return fail(ctx, CSV_EINVAL, "null volume");
+    DeviceGuard g(ctx->device);
+    if (!ctx->enc) ctx->enc = encoder_state_new();
+    std::string err;
+    int rc = encode_device(ctx->enc, ctx->device, d_volume, W, H, D, brick_size, (cudaStream_t)stream, err);
+    if (rc) return fail(ctx, rc, err);
+    const uint8_t* img = encoder_image(ctx->enc, image_len);
+    return img ? CSV_OK : fail(ctx, CSV_EINVAL, "encode produced no image");
+}
+
+int csv_encoded_image(csv_ctx* ctx, const uint8_t** d_image, size_t* len) {
+    if (!ctx || !d_image || !len) return CSV_EINVAL;
+    const uint8_t* p = encoder_image(ctx->enc, len);
+    if (!p) return fail(ctx, CSV_EINVAL, "no encoded image on this context");
+    *d_image = p;
+    return CSV_OK;
+}
+
+int csv_encode(csv_ctx* ctx, const uint64_t* volume, uint32_t W, uint32_t H, uint32_t D, uint32_t brick_size,
+               uint8_t** out, size_t* out_len) {
+    if (!ctx || !out || !out_len) return CSV_EINVAL;
+    *out = nullptr;
+    *out_len = 0;
+    uint64_t n = (uint64_t)W * H * D;
+    if (n && !volume) return fail(ctx, CSV_EINVAL, "null volume");
+    DeviceGuard g(ctx->device);
+    uint64_t* d_vol = nullptr;
+    cudaStream_t st = 0;
+    cudaError_t e = cudaMalloc(&d_vol, 8 * std::max<uint64_t>(n, 1));
+    if (e != cudaSuccess) return fail(ctx, CSV_ENOMEM, std::string("volume: ") + cudaGetErrorString(e));
+    if (n && (e = cudaMemcpyAsync(d_vol, volume, 8 * n, cudaMemcpyHostToDevice, st)) != cudaSuccess) {
+        cudaFree(d_vol);
+        return cuda_fail(ctx, e, "volume copy");
+    }
+    size_t len = 0;
+    int rc = csv_encode_device(ctx, d_vol, W, H, D, brick_size, st, &len);
+    cudaFree(d_vol);
+    if (rc) return rc;
+    const uint8_t* d_img = encoder_image(ctx->enc, &len);
+    uint8_t* h = (uint8_t*)malloc(std::max<size_t>(len, 1));
+    if (!h) return fail(ctx, CSV_ENOMEM, "host allocation");
+    if ((e = cudaMemcpy(h, d_img, len, cudaMemcpyDeviceToHost)) != cudaSuccess) {
+        free(h);
+        return cuda_fail(ctx, e, "image copy");
+    }
+    *out = h;
+    *out_len = len;
+    return CSV_OK;
+}
+
+int csv_open_encoded(csv_ctx* ctx, csv_dataset** out) {
+    if (!ctx || !out) return CSV_EINVAL;
+    *out = nullptr;
+    DeviceGuard g(ctx->device);
+    csv_dataset* ds = new (std::nothrow) csv_dataset();
+    if (!ds) return fail(ctx, CSV_ENOMEM, "host allocation");
+    ds->ctx = ctx;
+    std::string err;
+    int rc = encoder_to_dataset(ctx->enc, ds->d, err);
+    if (rc) {
+        free_dataset(ds->d);
+        delete ds;
+        return fail(ctx, rc, err);
+    }
+    *out = ds;
+    return CSV_OK;
+}
+
 int csv_synth_volume(csv_ctx* ctx, uint64_t* d_volume, uint32_t W, uint32_t H, uint32_t D, int kind, uint32_t n_cells,
                      uint32_t n_tubes, float r_min, float r_max, float zero_frac, uint64_t seed, void* stream) {
     if (!ctx || !d_volume || kind < 0 || kind > 2) return CSV_EINVAL;

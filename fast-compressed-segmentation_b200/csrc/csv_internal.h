@@ -92,7 +92,12 @@ cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, ui
 
 // Encoder state owned by a context (encode.cu).
 struct EncoderState;
+EncoderState* encoder_state_new();
 void encoder_state_free(EncoderState* s);
+int encode_device(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W, uint64_t H, uint64_t D, uint32_t b,
+                  cudaStream_t st, std::string& err);
+int encoder_to_dataset(EncoderState* s, DeviceDataset& d, std::string& err);
+const uint8_t* encoder_image(EncoderState* s, size_t* len);
 
 cudaError_t synth_volume(uint64_t* d_vol, uint32_t W, uint32_t H, uint32_t D, int kind, uint32_t n_cells,
                          uint32_t n_tubes, float r_min, float r_max, float zero_frac, uint64_t seed,

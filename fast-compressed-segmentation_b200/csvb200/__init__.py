@@ -206,6 +206,17 @@ class Codec:
         self._check(self.lib.csv_encoded_image(self.handle, C.byref(ptr), C.byref(n)))
         return ptr.value, n.value
 
+    def encoded_image_tensor(self):
+        """Zero-copy torch view (uint8, on the device) of the image the last encode_device produced; valid
+        until the next encode on this context."""
+        import torch
+        ptr, n = self.encoded_image()
+
+        class _View:
+            __cuda_array_interface__ = {"shape": (n,), "typestr": "|u1", "data": (ptr, False), "version": 2}
+
+        return torch.as_tensor(_View(), device=f"cuda:{self.device}")
+
     # ---- datasets ------------------------------------------------------
     def open(self, image: bytes) -> Dataset:
         a = np.frombuffer(image, np.uint8)

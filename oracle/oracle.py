@@ -166,6 +166,10 @@ class Reference:
         L.ref_majority8.restype = C.c_uint64
         L.ref_majority8.argtypes = [_u64p]
         L.ref_build_model.argtypes = [_u64p, _u32p, _u32p]
+        L.ref_load.restype = C.c_void_p
+        L.ref_load.argtypes = [_u8p, C.c_size_t]
+        L.ref_unload.argtypes = [C.c_void_p]
+        L.ref_decode_range.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, _u64p]
         L.ref_build_pyramid64.argtypes = [_u64p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_uint32, _u64p, _u8p]
         self.lib = L
 
@@ -209,6 +213,29 @@ class Reference:
         if n < 0:
             raise RuntimeError(self.error())
         return (out.reshape(nb, -1) if keep else None), st, {"rans_ms": tr.value, "replay_ms": tp.value}
+
+    def decode_parallel(self, img: bytes, threads: int, out: np.ndarray | None = None) -> int:
+        """Full-resolution decode of every brick, bricks split over `threads` host threads (ctypes releases
+        the GIL).  Returns the number of bricks where the reference threw."""
+        from concurrent.futures import ThreadPoolExecutor
+        a = np.frombuffer(img, np.uint8)
+        h = self.lib.ref_load(_ptr(a, _u8p), len(img))
+        if not h:
+            raise RuntimeError(self.error())
+        nb = int(np.frombuffer(img[8:12], np.uint32)[0])
+        b = int(np.frombuffer(img[12:16], np.uint32)[0])
+        chunk = -(-nb // max(1, threads))
+
+        def run(k):
+            s = k * chunk
+            c = max(0, min(chunk, nb - s))
+            p = None if out is None else out.reshape(-1)[s * b ** 3:].ctypes.data_as(_u64p)
+            return self.lib.ref_decode_range(h, s, c, p) if c else 0
+
+        with ThreadPoolExecutor(max_workers=threads) as ex:
+            bad = sum(ex.map(run, range(threads)))
+        self.lib.ref_unload(h)
+        return bad
 
     def rans_decode(self, img: bytes, index: int, nsym: int) -> bytes:
         a = np.frombuffer(img, np.uint8)

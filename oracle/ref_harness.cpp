@@ -206,6 +206,48 @@ int ref_decode_all_full(const uint8_t* csbd, size_t len, uint64_t* out, uint32_t
     return (int)n;
 }
 
+// A loaded image for repeated, range-wise decoding (the reference arm decodes
+// disjoint brick ranges from several host threads).
+struct RefImage {
+    Encoding::CompressedDataset ds;
+    uint32_t b;
+};
+
+void* ref_load(const uint8_t* csbd, size_t len) {
+    auto* h = new RefImage();
+    if (!load_image(csbd, len, h->ds)) { delete h; return nullptr; }
+    std::memcpy(&h->b, csbd + 12, 4);
+    return h;
+}
+
+void ref_unload(void* h) { delete static_cast<RefImage*>(h); }
+
+// decodeRansStream + decodeBrick<b>(., full) for bricks [start, start+count);
+// out (may be null) receives count * b^3 labels.  Returns bricks that threw.
+int ref_decode_range(void* hv, uint32_t start, uint32_t count, uint64_t* out) {
+    auto* h = static_cast<RefImage*>(hv);
+    int bad = 0;
+    size_t vox = (size_t)h->b * h->b * h->b;
+    for (uint32_t k = 0; k < count && start + k < h->ds.bricks.size(); ++k) {
+        try {
+            Encoding::CompressedBrick cb = h->ds.bricks[start + k];
+            cb.encodedData = decodeRansStream(cb, h->ds.model);
+            std::vector<LabelType> labels;
+            switch (h->b) {
+            case 8: labels = decodeBrick<8>(cb, Brick<8>::Levels - 1); break;
+            case 16: labels = decodeBrick<16>(cb, Brick<16>::Levels - 1); break;
+            case 32: labels = decodeBrick<32>(cb, Brick<32>::Levels - 1); break;
+            case 64: labels = decodeBrick<64>(cb, Brick<64>::Levels - 1); break;
+            default: return -1;
+            }
+            if (out) std::memcpy(out + k * vox, labels.data(), vox * sizeof(uint64_t));
+        } catch (const std::exception&) {
+            ++bad;
+        }
+    }
+    return bad;
+}
+
 // The reference's rANS stage alone (brickDecoding.cpp:153): the repacked nibble
 // bytes of brick `index`.  out must hold ceil(nSymbols/2) bytes.
 int ref_rans_decode(const uint8_t* csbd, size_t len, uint32_t index, uint8_t* out, size_t* out_len) {

@@ -148,14 +148,14 @@ def _patch_brick(img: bytes, index: int, P=None, nsym=None) -> bytes:
 
 def test_forged_palette_overrun_is_clamped_like_wgsl(codec, oracle):
     from csvb200 import CSV_BRICK_PALETTE
-    img = _patch_brick(read_golden("shipped_subset"), 2, P=3)
+    img = _patch_brick(read_golden("shipped_subset"), 3, P=9)  # brick 3 has a 67-entry palette
     for t in (3, 5, 6):
         out, st = codec.decode_image(img, t, check=False)
         ref, rst = oracle.decode_image(img, t)
         # the flag appears once the decoded levels reach a palette index past the cut
-        assert bool(st[2] & CSV_BRICK_PALETTE) == bool(rst[2] & 2), t
+        assert bool(st[3] & CSV_BRICK_PALETTE) == bool(rst[3] & 2), t
         assert np.array_equal(out, ref), t
-    assert st[2] & CSV_BRICK_PALETTE
+    assert st[3] & CSV_BRICK_PALETTE
 
 
 def test_truncated_stream_reports_truncation(codec):
