@@ -117,7 +117,6 @@ void free_dataset(DeviceDataset& d) {
     d = DeviceDataset();
 }
 
-constexpr uint32_t kOpsPerCheckpoint = 512;
 
 int stage_dataset(csv_ctx* ctx, const uint8_t* img, const ImageView& v, DeviceDataset& d, cudaStream_t st) {
     d.device = ctx->device;
@@ -421,6 +420,25 @@ int csv_open_encoded(csv_ctx* ctx, csv_dataset** out) {
         return fail(ctx, rc, err);
     }
     *out = ds;
+    return CSV_OK;
+}
+
+int csv_render(csv_ctx* ctx, const csv_camera* camera, uint32_t width, uint32_t height, float grid_size,
+               uint32_t brick_size, uint32_t bricks_per_axis, const csv_brick_slot* d_slots, uint64_t n_slots,
+               const uint64_t* d_labels, const uint64_t* d_hidden, uint32_t n_hidden, uint64_t* d_label_out,
+               float* d_depth_out, uint32_t* d_requests, void* stream) {
+    if (!ctx || !camera) return CSV_EINVAL;
+    if (width == 0 || height == 0) return CSV_OK;
+    if (!d_label_out || !d_depth_out || (n_slots && (!d_slots || !d_labels)))
+        return fail(ctx, CSV_EINVAL, "null render buffer");
+    if (brick_size < 1 || brick_size > 1024 || (brick_size & (brick_size - 1)))
+        return fail(ctx, CSV_EINVAL, "brick size must be a power of two");
+    if (bricks_per_axis > 1024) return fail(ctx, CSV_ERANGE, "more than 1024 bricks per axis");
+    DeviceGuard g(ctx->device);
+    cudaError_t e = launch_render(*camera, width, height, grid_size, brick_size, bricks_per_axis, d_slots, n_slots,
+                                  d_labels, d_hidden, n_hidden, d_label_out, d_depth_out, d_requests,
+                                  (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "render launch");
     return CSV_OK;
 }
 

@@ -16,6 +16,10 @@ constexpr uint32_t kTotBits = 12;         // LOG_TOTAL_FREQ
 constexpr uint32_t kTot = 1u << kTotBits; // RANS_TOTAL
 constexpr uint32_t kMagic = 0x43534244u;  // fileIO.cpp:25
 constexpr uint32_t kHeaderBytes = 152;    // 16 B header + 136 B model (fileIO.cpp:25-49)
+// Seek-index spacing: one decoder checkpoint (16 bytes) every this many ops.
+// Each checkpoint starts one independent rANS segment in the decoder, so the
+// spacing trades the serial segment length (latency) against index size.
+constexpr uint32_t kOpsPerCheckpoint = 256;
 
 // Op codes (types.hpp:162-171) and nibble layout (op << 1 | stop, brickEncoding.cpp:66-67).
 enum : uint32_t { OP_RP = 0, OP_RX = 1, OP_RY = 2, OP_RZ = 3, OP_PA = 4, OP_P0 = 5, OP_PD = 6 };
@@ -98,6 +102,11 @@ int encode_device(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W
                   cudaStream_t st, std::string& err);
 int encoder_to_dataset(EncoderState* s, DeviceDataset& d, std::string& err);
 const uint8_t* encoder_image(EncoderState* s, size_t* len);
+
+cudaError_t launch_render(const csv_camera& cam, uint32_t W, uint32_t H, float grid, uint32_t bs, uint32_t bpa,
+                          const csv_brick_slot* slots, uint64_t n_slots, const uint64_t* labels, const uint64_t* hidden,
+                          uint32_t n_hidden, uint64_t* out_label, float* out_depth, uint32_t* requests,
+                          cudaStream_t st);
 
 cudaError_t synth_volume(uint64_t* d_vol, uint32_t W, uint32_t H, uint32_t D, int kind, uint32_t n_cells,
                          uint32_t n_tubes, float r_min, float r_max, float zero_frac, uint64_t seed,

@@ -10,44 +10,51 @@
 // thread per workgroup in decode.wgsl).  Here a brick is decoded by a whole
 // CTA:
 //   1. rANS: the brick's op stream is cut at seek checkpoints (decoder state
-//      every S ops, built once per dataset); each thread decodes one segment
-//      and writes one 4-byte record per op (code, stop, resolved palette index).
-//   2. levels, coarse to fine: node values are palette indices.  A node of
-//      level l+1 whose parent is inactive (stop-filled) takes the parent's
-//      value; otherwise its op gives it: Rp -> parent, Pa/P0/Pd -> palette
-//      index, Rx/Ry/Rz -> the neighbour outside the sibling block.  A neighbour
-//      on the +1 side is later in Morton order, so the reference reads its
-//      parent (known, previous level).  A neighbour on the -1 side is earlier,
-//      on the same level; its local index has one more 1-bit than the node's,
-//      so such chains are at most three hops long and are resolved on the fly
-//      without any ordering between threads.
+//      every S ops, built once per dataset or emitted by the encoder); each
+//      thread decodes one segment and writes one 4-byte record per op (code,
+//      stop, resolved palette index).
+//   2. levels, coarse to fine: node values are palette indices.  A node whose
+//      parent is stop-filled ("inactive") takes the parent's value; the 8
+//      children of an active parent take their ops: Rp -> parent, Pa/P0/Pd ->
+//      palette index, Rx/Ry/Rz -> the neighbour outside the sibling block.  A
+//      neighbour on the +1 side is later in Morton order, so the reference
+//      reads its parent (known, previous level).  A neighbour on the -1 side is
+//      earlier, on the same level; its local index has one more 1-bit than the
+//      node's, so such chains are at most three hops long and are resolved on
+//      the fly without any ordering between threads.
+//      Inactive parents (most of them) are filled in one uniform pass; active
+//      parents are walked through a compacted list, so warps never diverge
+//      between the two.
 //   3. the last level is written straight to HBM, 8 children (64 bytes) per
 //      parent, with streaming 16-byte stores.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "block_scan.cuh"
 #include "csv_internal.h"
 
 namespace csv {
 
-constexpr int kDecThreads = 256;
+constexpr int kDecThreads = 512;
+constexpr int kDecMinBlocks = 3;       // CTAs per SM the shared-memory budget allows
 constexpr uint32_t kSmemLevels = 5;    // levels 0..4 (<= 4096 nodes) keep node info in shared memory
-constexpr uint32_t kSmemNodes = 4681;  // sum_{l<5} 8^l
+constexpr uint32_t kSmemNodes = 4684;  // levels 0..4 at 16-byte aligned offsets (soff)
 constexpr uint32_t kPalCache = 1024;   // palettes up to this size are copied to shared memory
 constexpr uint32_t REC_MISSING = OP_RP | 8u;
 
 __host__ __device__ constexpr uint32_t lvl_off(uint32_t l) { return ((1u << (3 * l)) - 1) / 7; }
+// shared-memory level offsets 0, 4, 12, 76, 588: lvl_off rounded up to a multiple of 4 words
+__host__ __device__ constexpr uint32_t soff(uint32_t l) { return l ? lvl_off(l) + 3 : 0; }
 
 struct DecShared {
     uint32_t lut[kTot];
     uint32_t ni[kSmemNodes];
     uint32_t av[kSmemNodes];
-    uint32_t base[4096];
     uint64_t pal[kPalCache];
-    uint32_t warp_sums[kDecThreads / 32];
+    uint32_t warp_sums[kDecThreads / 32 + 1];
     BrickDesc br;
     csv_request req;
-    uint32_t work, status, nact_next, pad;
+    uint32_t work, status;
 };
 
 // ------------------------------------------------------------------ LUT
@@ -79,10 +86,10 @@ __device__ __forceinline__ uint32_t rans_step(uint32_t& x, uint32_t& pos, const 
 // before every S-th op and the first op of every level.  Level l+1 has 8 ops
 // per op of level l with stop bit 0; level 1 has 8 unless the root's stop bit
 // is set (then the brick is one label).
-__global__ void __launch_bounds__(128) build_index_kernel(BrickDesc* __restrict__ bricks, uint32_t nb,
-                                                          const uint8_t* __restrict__ enc_pool,
-                                                          const uint32_t* __restrict__ g_lut,
-                                                          Checkpoint* __restrict__ ck, uint32_t L, uint32_t S) {
+__global__ void __launch_bounds__(32) build_index_kernel(BrickDesc* __restrict__ bricks, uint32_t nb,
+                                                         const uint8_t* __restrict__ enc_pool,
+                                                         const uint32_t* __restrict__ g_lut,
+                                                         Checkpoint* __restrict__ ck, uint32_t L, uint32_t S) {
     __shared__ uint32_t lut[kTot];
     for (uint32_t i = threadIdx.x; i < kTot; i += blockDim.x) lut[i] = g_lut[i];
     __syncthreads();
@@ -105,24 +112,35 @@ __global__ void __launch_bounds__(128) build_index_kernel(BrickDesc* __restrict_
         if (root & 1u) {
             flags = BF_UNIFORM;
         } else {
-            uint32_t ip = 0, need = 8, lvl = 0, act = 0, done = 0;
+            // One symbol per iteration (a Pd op spans two), so the lanes of a warp
+            // never differ in the number of rANS steps an iteration takes.
+            uint32_t ip = 0, need = 8, lvl = 0, act = 0, done = 0, until_ck = 0;
+            bool in_pd = false;
             while (lvl + 1 < L && need > 0) {
-                if (ops % S == 0) {
+                if (!in_pd && until_ck == 0) {  // checkpoint before every S-th op
                     if (n_ck < br.ck_cap) ck[br.ck_off + n_ck] = Checkpoint{x, pos, sym, ip};
                     ++n_ck;
+                    until_ck = S;
                 }
-                if (sym >= br.nsym) { flags |= BF_TRUNCATED; break; }
-                uint32_t v = rans_step(x, pos, enc, lut);
+                if (sym >= br.nsym) {
+                    flags |= BF_TRUNCATED;
+                    if (in_pd) ++ops;
+                    break;
+                }
+                const uint32_t v = rans_step(x, pos, enc, lut);
                 ++sym;
-                uint32_t code = v >> 1;
-                if (code == OP_PD) {
-                    if (sym >= br.nsym) { flags |= BF_TRUNCATED; ++ops; break; }
-                    rans_step(x, pos, enc, lut);
-                    ++sym;
+                if (!in_pd) {
+                    if ((v >> 1) == OP_PD) {
+                        in_pd = true;
+                        if (!(v & 1u)) ++act;
+                        continue;
+                    }
+                    if ((v >> 1) == OP_PA) ++ip;
+                    if (!(v & 1u)) ++act;
                 }
-                if (code == OP_PA) ++ip;
-                if (!(v & 1u)) ++act;
+                in_pd = false;
                 ++ops;
+                --until_ck;
                 if (++done == need) {
                     ++lvl;
                     ls[lvl] = ops;
@@ -144,8 +162,9 @@ __global__ void __launch_bounds__(128) build_index_kernel(BrickDesc* __restrict_
 
 cudaError_t launch_build_index(DeviceDataset& ds, cudaStream_t st) {
     if (ds.nb == 0) return cudaSuccess;
-    uint32_t blocks = (ds.nb + 127) / 128;
-    build_index_kernel<<<blocks, 128, 0, st>>>(ds.d_bricks, ds.nb, ds.d_enc, ds.d_lut, ds.d_ck, ds.L, ds.S);
+    // one warp per block spreads the serial chains over as many SMs as possible
+    uint32_t blocks = (ds.nb + 31) / 32;
+    build_index_kernel<<<blocks, 32, 0, st>>>(ds.d_bricks, ds.nb, ds.d_enc, ds.d_lut, ds.d_ck, ds.L, ds.S);
     return cudaGetLastError();
 }
 
@@ -181,6 +200,17 @@ __device__ void fill_labels(uint64_t* out, uint64_t cnt, uint64_t v) {
     if (((cnt - start) & 1) && threadIdx.x == 0) out[cnt - 1] = v;
 }
 
+// Eight labels of one parent (64 bytes) at o8.
+__device__ __forceinline__ void store8(uint64_t* o8, const uint64_t* lab, bool vec) {
+    if (vec) {
+#pragma unroll
+        for (int c = 0; c < 8; c += 2) st_cs_v2(o8 + c, lab[c], lab[c + 1]);
+    } else {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) o8[c] = lab[c];
+    }
+}
+
 struct LevelView {
     const uint32_t* ni;  // node info of the parent level
     const uint32_t* av;  // active values of the parent level
@@ -191,6 +221,21 @@ struct LevelView {
 
 __device__ __forceinline__ uint32_t get_rec(const LevelView& v, uint32_t idx) {
     return idx < v.n_rec ? v.rec[idx] : REC_MISSING;
+}
+// The 8 records of the r-th active parent.  In a complete brick o is a sum of
+// multiples of 8, so the group is 32-byte aligned and read as two vectors; a
+// truncated brick (o arbitrary, records missing) takes the guarded scalar path.
+__device__ __forceinline__ void get_rec8(const LevelView& v, uint32_t r, uint32_t rec[8]) {
+    const uint32_t i0 = v.o + 8 * r;
+    if ((i0 & 7u) == 0 && i0 + 8 <= v.n_rec) {
+        const uint4* p = reinterpret_cast<const uint4*>(v.rec + i0);
+        const uint4 a = p[0], b = p[1];
+        rec[0] = a.x; rec[1] = a.y; rec[2] = a.z; rec[3] = a.w;
+        rec[4] = b.x; rec[5] = b.y; rec[6] = b.z; rec[7] = b.w;
+    } else {
+#pragma unroll
+        for (uint32_t c = 0; c < 8; ++c) rec[c] = get_rec(v, i0 + c);
+    }
 }
 __device__ __forceinline__ uint32_t node_value(const LevelView& v, uint32_t p) {
     uint32_t i = v.ni[p];
@@ -205,41 +250,33 @@ __device__ __forceinline__ uint32_t node_value(const LevelView& v, uint32_t p) {
 // which for child c > 0 already holds child 0's value (slot aliasing of
 // coarseNodeToOutputIndex); malformed streams only.  Morton indices strictly
 // decrease along a chain, so it terminates; the iteration cap only guards
-// against a corrupt seek index.
-__device__ uint32_t resolve(const LevelView& v, uint32_t rec, uint32_t n, uint32_t lc, uint32_t& st) {
-    const uint32_t lvlmask = (lc >= 10) ? 0x3FFFFFFFu : ((1u << (3 * lc)) - 1u);
+// against a corrupt seek index.  Sets *bad on a capped chain.
+__device__ __forceinline__ uint32_t resolve(const LevelView& v, uint32_t rec, uint32_t n, uint32_t lc, bool* bad) {
+    const uint32_t lvlmask = (1u << (3 * lc)) - 1u;
 #pragma unroll 1
     for (int hop = 0; hop < 4096; ++hop) {
-        uint32_t code = rec & 7u;
+        const uint32_t code = rec & 7u;
         if (code >= OP_PA) return rec >> REC_PIDX_SHIFT;
         if (code == OP_RP) return node_value(v, n >> 3);
-        uint32_t a = code - 1;
-        uint32_t m = (0x09249249u << a) & lvlmask;
-        uint32_t bit = 1u << a;
-        bool oob;
-        uint32_t N;
+        const uint32_t a = code - 1;
+        const uint32_t m = (0x09249249u << a) & lvlmask;
+        const uint32_t bit = 1u << a;
         if (n & bit) {
-            oob = (n & m) == m;
-            N = (((n | ~m) + bit) & m) | (n & ~m);
-            if (!oob) return node_value(v, N >> 3);
-        } else {
-            oob = (n & m) == 0;
-            N = (((n & m) - bit) & m) | (n & ~m);
-            if (!oob) {
-                uint32_t q = v.ni[N >> 3];
-                if (!(q & NI_ACT)) return q;
-                rec = get_rec(v, v.o + 8 * (q & ~NI_ACT) + (N & 7u));
-                n = N;
-                continue;
-            }
+            if ((n & m) != m) return node_value(v, ((((n | ~m) + bit) & m) | (n & ~m)) >> 3);
+        } else if ((n & m) != 0) {
+            const uint32_t N = (((n & m) - bit) & m) | (n & ~m);
+            const uint32_t q = v.ni[N >> 3];
+            if (!(q & NI_ACT)) return q;
+            rec = get_rec(v, v.o + 8 * (q & ~NI_ACT) + (N & 7u));
+            n = N;
+            continue;
         }
         // outside the brick: the parent slot
         if ((n & 7u) == 0) return node_value(v, n >> 3);
-        uint32_t q = v.ni[n >> 3];
-        rec = get_rec(v, v.o + 8 * (q & ~NI_ACT));
+        rec = get_rec(v, v.o + 8 * (v.ni[n >> 3] & ~NI_ACT));
         n &= ~7u;
     }
-    st |= CSV_BRICK_BADOP;
+    *bad = true;
     return 0;
 }
 
@@ -247,57 +284,24 @@ __device__ __forceinline__ uint64_t label_of(const uint64_t* pal, uint32_t pidx)
     return pidx == PIDX_LABEL0 ? 0ull : pal[pidx];
 }
 
-// Block-wide exclusive scan of a[0..n) in place (n <= blockDim * 16); returns the total.
-__device__ uint32_t block_exclusive_scan(uint32_t* a, uint32_t n, uint32_t* warp_sums) {
-    const uint32_t T = blockDim.x, tid = threadIdx.x;
-    const uint32_t per = (n + T - 1) / T;
-    const uint32_t b0 = min(n, tid * per), b1 = min(n, b0 + per);
-    uint32_t s = 0;
-    for (uint32_t i = b0; i < b1; ++i) s += a[i];
-    uint32_t lane = tid & 31, w = tid >> 5;
-    uint32_t inc = s;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        uint32_t y = __shfl_up_sync(0xffffffffu, inc, d);
-        if (lane >= (uint32_t)d) inc += y;
-    }
-    if (lane == 31) warp_sums[w] = inc;
-    __syncthreads();
-    if (w == 0) {
-        uint32_t nw = T / 32;
-        uint32_t ws = lane < nw ? warp_sums[lane] : 0;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, ws, d);
-            if (lane >= (uint32_t)d) ws += y;
-        }
-        if (lane < nw) warp_sums[lane] = ws;
-    }
-    __syncthreads();
-    uint32_t run = inc - s + (w ? warp_sums[w - 1] : 0);
-    for (uint32_t i = b0; i < b1; ++i) {
-        uint32_t t = a[i];
-        a[i] = run;
-        run += t;
-    }
-    uint32_t total = warp_sums[T / 32 - 1];
-    __syncthreads();
-    return total;
-}
-
-__global__ void __launch_bounds__(kDecThreads) decode_kernel(DecodeArgs A) {
+__global__ void __launch_bounds__(kDecThreads, kDecMinBlocks) decode_kernel(DecodeArgs A) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     DecShared& S = *reinterpret_cast<DecShared*>(smem_raw);
-    const uint32_t tid = threadIdx.x;
+    const uint32_t tid = threadIdx.x, T = blockDim.x;
 
-    for (uint32_t i = tid; i < kTot; i += blockDim.x) S.lut[i] = A.lut[i];
+    for (uint32_t i = tid; i < kTot; i += T) S.lut[i] = A.lut[i];
 
+    // per-CTA scratch: op records | node info + active values of the one level
+    // above 4096 nodes | active-node lists of every parent level
     uint8_t* scr = A.scratch + (uint64_t)blockIdx.x * A.scratch_per_cta;
     uint32_t* recs = reinterpret_cast<uint32_t*>(scr);
     const uint64_t max_ops = ((1ull << (3 * A.L)) - 8) / 7;
-    uint32_t* g_ni = reinterpret_cast<uint32_t*>(scr + ((max_ops * 4 + 255) & ~255ull));
-    const uint32_t g_nodes = A.L > kSmemLevels + 1 ? (1u << (3 * (A.L - 2))) : 0;  // the one level > 4096 nodes
+    uint64_t so = (max_ops * 4 + 255) & ~255ull;
+    const uint32_t g_nodes = A.L > kSmemLevels + 1 ? (1u << (3 * (A.L - 2))) : 0;
+    uint32_t* g_ni = reinterpret_cast<uint32_t*>(scr + so);
     uint32_t* g_av = g_ni + g_nodes;
+    so += (8ull * g_nodes + 255) & ~255ull;
+    uint32_t* act = reinterpret_cast<uint32_t*>(scr + so);
 
     for (;;) {
         if (tid == 0) {
@@ -323,10 +327,11 @@ __global__ void __launch_bounds__(kDecThreads) decode_kernel(DecodeArgs A) {
         const uint64_t* gpal = A.pal + br.pal_off;
         const uint64_t* pal = gpal;
         if (br.P <= kPalCache) {
-            for (uint32_t i = tid; i < br.P; i += blockDim.x) S.pal[i] = gpal[i];
+            for (uint32_t i = tid; i < br.P; i += T) S.pal[i] = gpal[i];
             pal = S.pal;
         }
         uint32_t st = (br.flags & BF_TRUNCATED) ? CSV_BRICK_TRUNCATED : 0;
+        bool bad = false;
         __syncthreads();
 
         if (t == 0 || (br.flags & BF_UNIFORM)) {
@@ -336,81 +341,112 @@ __global__ void __launch_bounds__(kDecThreads) decode_kernel(DecodeArgs A) {
             const uint32_t n_need = min(min(br.level_start[t], br.n_ops), br.ck_cap * A.S);
             const uint32_t nseg = (n_need + A.S - 1) / A.S;
             const uint8_t* enc = A.enc + br.enc_off;
-            for (uint32_t k = tid; k < nseg; k += blockDim.x) {
-                Checkpoint c = A.ck[br.ck_off + k];
+            for (uint32_t k = tid; k < nseg; k += T) {
+                const Checkpoint c = A.ck[br.ck_off + k];
                 uint32_t x = c.state, pos = c.pos, sym = c.sym, ip = c.ip;
                 uint32_t j = k * A.S;
                 const uint32_t jend = min(j + A.S, n_need);
+                // one rANS step per iteration; a Pd op's delta nibble is its own
+                // iteration, so lanes never differ in steps per iteration
+                uint32_t pd_stop = 0xFFFFFFFFu;  // != ~0: the primary nibble of a Pd op was read
                 while (j < jend) {
-                    if (sym >= br.nsym) { st |= CSV_BRICK_TRUNCATED; break; }
-                    uint32_t v = rans_step(x, pos, enc, S.lut);
-                    ++sym;
-                    uint32_t code = v >> 1, pidx = 0;
-                    if (code == OP_PD) {
-                        uint32_t d = 0;
-                        if (sym >= br.nsym) st |= CSV_BRICK_TRUNCATED;
-                        else { d = rans_step(x, pos, enc, S.lut); ++sym; }
-                        pidx = ip - d - 1;
-                        if (pidx >= br.P) { pidx = br.P - 1; st |= CSV_BRICK_PALETTE; }
-                    } else if (code == OP_PA) {
-                        ++ip;
-                        pidx = ip;
-                        if (pidx >= br.P) { pidx = br.P - 1; st |= CSV_BRICK_PALETTE; }
-                    } else if (code == OP_P0) {
-                        pidx = ip;
-                        if (pidx >= br.P) { pidx = br.P - 1; st |= CSV_BRICK_PALETTE; }
-                    } else if (code == 7) {
-                        pidx = PIDX_LABEL0;
-                        st |= CSV_BRICK_BADOP;
+                    if (sym >= br.nsym) {
+                        st |= CSV_BRICK_TRUNCATED;
+                        if (pd_stop != 0xFFFFFFFFu) {  // Pd without its delta: delta 0
+                            uint32_t pidx = ip - 1;
+                            if (pidx >= br.P) { pidx = br.P - 1; st |= CSV_BRICK_PALETTE; }
+                            recs[j] = OP_PD | pd_stop | (pidx << REC_PIDX_SHIFT);
+                        }
+                        break;
                     }
-                    recs[j] = code | ((v & 1u) << 3) | (pidx << REC_PIDX_SHIFT);
+                    const uint32_t v = rans_step(x, pos, enc, S.lut);
+                    ++sym;
+                    uint32_t rec;
+                    if (pd_stop != 0xFFFFFFFFu) {
+                        uint32_t pidx = ip - v - 1;
+                        if (pidx >= br.P) { pidx = br.P - 1; st |= CSV_BRICK_PALETTE; }
+                        rec = OP_PD | pd_stop | (pidx << REC_PIDX_SHIFT);
+                        pd_stop = 0xFFFFFFFFu;
+                    } else {
+                        const uint32_t code = v >> 1;
+                        if (code == OP_PD) {
+                            pd_stop = (v & 1u) << 3;
+                            continue;
+                        }
+                        uint32_t pidx = 0;
+                        if (code == OP_PA || code == OP_P0) {
+                            ip += (code == OP_PA);
+                            pidx = ip;
+                            if (pidx >= br.P) { pidx = br.P - 1; st |= CSV_BRICK_PALETTE; }
+                        } else if (code == 7) {
+                            pidx = PIDX_LABEL0;
+                            st |= CSV_BRICK_BADOP;
+                        }
+                        rec = code | ((v & 1u) << 3) | (pidx << REC_PIDX_SHIFT);
+                    }
+                    recs[j] = rec;
                     ++j;
                 }
             }
-            if (tid == 0) { S.ni[0] = NI_ACT | 0u; S.av[0] = 0; }
+            if (tid == 0) {
+                S.ni[0] = NI_ACT | 0u;
+                S.av[0] = 0;
+                act[0] = 0;
+            }
             __syncthreads();
 
             // ---- 2./3. levels coarse to fine
+            const bool vec = (((uintptr_t)out) & 15) == 0;
             uint32_t n_act = 1;
             for (uint32_t l = 0; l < t; ++l) {
                 const uint32_t lc = l + 1;
                 LevelView V;
-                V.ni = (l < kSmemLevels) ? S.ni + lvl_off(l) : g_ni;
-                V.av = (l < kSmemLevels) ? S.av + lvl_off(l) : g_av;
+                V.ni = (l < kSmemLevels) ? S.ni + soff(l) : g_ni;
+                V.av = (l < kSmemLevels) ? S.av + soff(l) : g_av;
                 V.rec = recs;
                 V.o = br.level_start[l];
                 V.n_rec = n_need;
+                const uint32_t* act_l = act + lvl_off(l);
                 const uint32_t n_par = 1u << (3 * l);
                 if (lc < t) {
-                    uint32_t* ni_c = (lc < kSmemLevels) ? S.ni + lvl_off(lc) : g_ni;
-                    uint32_t* av_c = (lc < kSmemLevels) ? S.av + lvl_off(lc) : g_av;
-                    // children with stop 0 per active parent, then their ranks
-                    for (uint32_t r = tid; r < n_act; r += blockDim.x) {
-                        uint32_t cnt = 0;
+                    uint32_t* ni_c = (lc < kSmemLevels) ? S.ni + soff(lc) : g_ni;
+                    uint32_t* av_c = (lc < kSmemLevels) ? S.av + soff(lc) : g_av;
+                    uint32_t* act_c = act + lvl_off(lc);
+                    // active parents in contiguous chunks, so ranks come from one block scan
+                    const uint32_t per = (n_act + T - 1) / T;
+                    const uint32_t r0 = min(n_act, tid * per), r1 = min(n_act, r0 + per);
+                    uint32_t cnt = 0;
+                    for (uint32_t r = r0; r < r1; ++r) {
+                        uint32_t rec[8];
+                        get_rec8(V, r, rec);
 #pragma unroll
-                        for (uint32_t c = 0; c < 8; ++c) cnt += (get_rec(V, V.o + 8 * r + c) & 8u) ? 0u : 1u;
-                        S.base[r] = cnt;
+                        for (int c = 0; c < 8; ++c) cnt += (rec[c] & 8u) ? 0u : 1u;
                     }
-                    __syncthreads();
-                    const uint32_t n_act_c = block_exclusive_scan(S.base, n_act, S.warp_sums);
-                    for (uint32_t p = tid; p < n_par; p += blockDim.x) {
+                    uint32_t n_act_c;
+                    uint32_t rk = block_exclusive<uint32_t>(cnt, S.warp_sums, &n_act_c);
+                    // stop-filled parents: children inherit (one uniform pass)
+                    for (uint32_t p = tid; p < n_par; p += T) {
                         const uint32_t info = V.ni[p];
                         if (!(info & NI_ACT)) {
-#pragma unroll
-                            for (uint32_t c = 0; c < 8; ++c) ni_c[8 * p + c] = info;
-                            continue;
+                            uint4 q = make_uint4(info, info, info, info);
+                            reinterpret_cast<uint4*>(ni_c + 8 * p)[0] = q;
+                            reinterpret_cast<uint4*>(ni_c + 8 * p)[1] = q;
                         }
-                        const uint32_t r = info & ~NI_ACT;
-                        uint32_t rk = S.base[r];
+                    }
+                    for (uint32_t r = r0; r < r1; ++r) {
+                        const uint32_t p = act_l[r];
+                        uint32_t rec[8];
+                        get_rec8(V, r, rec);
 #pragma unroll
                         for (uint32_t c = 0; c < 8; ++c) {
-                            uint32_t rec = get_rec(V, V.o + 8 * r + c);
-                            uint32_t val = resolve(V, rec, 8 * p + c, lc, st);
-                            if (rec & 8u) {
-                                ni_c[8 * p + c] = val;
+                            const uint32_t n = 8 * p + c;
+                            const uint32_t val = resolve(V, rec[c], n, lc, &bad);
+                            if (rec[c] & 8u) {
+                                ni_c[n] = val;
                             } else {
-                                ni_c[8 * p + c] = NI_ACT | rk;
+                                ni_c[n] = NI_ACT | rk;
                                 av_c[rk] = val;
+                                act_c[rk] = n;
                                 ++rk;
                             }
                         }
@@ -419,34 +455,29 @@ __global__ void __launch_bounds__(kDecThreads) decode_kernel(DecodeArgs A) {
                     __syncthreads();
                 } else {
                     // last level: labels to HBM, 64 bytes per parent
-                    const bool vec = (((uintptr_t)out) & 15) == 0;
-                    for (uint32_t p = tid; p < n_par; p += blockDim.x) {
+                    for (uint32_t p = tid; p < n_par; p += T) {
                         const uint32_t info = V.ni[p];
-                        uint64_t lab[8];
                         if (!(info & NI_ACT)) {
-                            uint64_t x = label_of(pal, info);
+                            const uint64_t x = label_of(pal, info);
+                            uint64_t lab[8];
 #pragma unroll
                             for (int c = 0; c < 8; ++c) lab[c] = x;
-                        } else {
-                            const uint32_t r = info & ~NI_ACT;
-#pragma unroll
-                            for (uint32_t c = 0; c < 8; ++c) {
-                                uint32_t rec = get_rec(V, V.o + 8 * r + c);
-                                lab[c] = label_of(pal, resolve(V, rec, 8 * p + c, lc, st));
-                            }
+                            store8(out + 8ull * p, lab, vec);
                         }
-                        uint64_t* o8 = out + 8ull * p;
-                        if (vec) {
+                    }
+                    for (uint32_t r = tid; r < n_act; r += T) {
+                        const uint32_t p = act_l[r];
+                        uint32_t rec[8];
+                        get_rec8(V, r, rec);
+                        uint64_t lab[8];
 #pragma unroll
-                            for (int c = 0; c < 8; c += 2) st_cs_v2(o8 + c, lab[c], lab[c + 1]);
-                        } else {
-#pragma unroll
-                            for (int c = 0; c < 8; ++c) o8[c] = lab[c];
-                        }
+                        for (uint32_t c = 0; c < 8; ++c) lab[c] = label_of(pal, resolve(V, rec[c], 8 * p + c, lc, &bad));
+                        store8(out + 8ull * p, lab, vec);
                     }
                 }
             }
         }
+        if (bad) st |= CSV_BRICK_BADOP;
         if (st) atomicOr(&S.status, st);
         __syncthreads();
         if (tid == 0) A.status[w] = S.status;
@@ -458,7 +489,9 @@ size_t decode_scratch_per_cta(uint32_t b) {
     uint32_t L = levels_of(b);
     uint64_t rec_bytes = (max_ops_of(b) * 4 + 255) & ~255ull;
     uint64_t g_nodes = L > kSmemLevels + 1 ? (1ull << (3 * (L - 2))) : 0;
-    return (size_t)((rec_bytes + 2 * g_nodes * 4 + 255) & ~255ull);
+    uint64_t ni_bytes = (8 * g_nodes + 255) & ~255ull;
+    uint64_t act_bytes = 4ull * lvl_off(L - 1);  // active lists of levels 0 .. L-2
+    return (size_t)((rec_bytes + ni_bytes + act_bytes + 255) & ~255ull);
 }
 
 static int g_dec_occ[64] = {0};

@@ -52,7 +52,7 @@ struct EncMeta {
 
 struct EncoderState {
     int device = 0;
-    uint32_t b = 0, L = 0, nb = 0, S = 512, ck_cap = 0;
+    uint32_t b = 0, L = 0, nb = 0, S = kOpsPerCheckpoint, ck_cap = 0;
     uint64_t W = 0, H = 0, D = 0;
     // buffers (grow-only)
     EncMeta* d_meta = nullptr;
@@ -416,7 +416,8 @@ __global__ void __launch_bounds__(kEncThreads) enc_bricks_kernel(EncArgs A) {
             }
             __syncthreads();
             const uint64_t nib_off = S.nib_off, pal_off = S.pal_off;
-            const bool ok = nib_off + nbytes <= A.nib_cap && pal_off + P <= A.pal_cap;
+            // the rANS kernel reads whole 16-byte chunks of the reservation
+            const bool ok = nib_off + ((nbytes + 15) & ~15u) <= A.nib_cap && pal_off + P <= A.pal_cap;
             const bool sample = (i % 512) == 0;  // brickEncoding.hpp:482
             for (uint32_t q = tid; q < nbytes; q += T) {
                 const uint32_t hi = nib[2 * q], lo = (2 * q + 1 < nsym) ? nib[2 * q + 1] : 0u;
@@ -496,49 +497,76 @@ __global__ void model_kernel(const unsigned long long* hist, uint32_t* model) {
 }
 
 // ------------------------------------------------------------ K3 rANS
-__global__ void __launch_bounds__(64) enc_rans_kernel(EncMeta* __restrict__ meta, uint32_t nb,
+// One encode step (ransEncodeSymbol, brickEncoding.cpp:202-219).  tab: f |
+// start << 13 | shift << 25 | M << 32.  The state is below 2^31 before the step
+// (brickEncoding: 2^19 f after renormalisation, times 4096 / f), so at most two
+// bytes leave per symbol and the reciprocal division is exact.
+__device__ __forceinline__ void rans_enc_step(uint32_t& x, uint32_t& emitted, uint8_t* __restrict__ out,
+                                              uint64_t e) {
+    const uint32_t f = (uint32_t)e & 0x1FFFu;
+    const uint32_t bound = ((kRansL >> kTotBits) << 8) * f;
+    if (x >= bound) {
+        out[emitted++] = (uint8_t)(x & 0xFF);
+        x >>= 8;
+        if (x >= bound) {
+            out[emitted++] = (uint8_t)(x & 0xFF);
+            x >>= 8;
+        }
+    }
+    const uint32_t qd = (uint32_t)(((uint64_t)x * (uint32_t)(e >> 32)) >> ((uint32_t)(e >> 25) & 63u));
+    x = (qd << kTotBits) + (x - qd * f) + (((uint32_t)e >> 13) & 0xFFFu);
+}
+
+__global__ void __launch_bounds__(32) enc_rans_kernel(EncMeta* __restrict__ meta, uint32_t nb,
                                                       const uint8_t* __restrict__ nib_pool,
                                                       const uint64_t* __restrict__ enc_off,
                                                       uint8_t* __restrict__ enc_pool, const uint32_t* __restrict__ model,
                                                       Checkpoint* __restrict__ ck_all, uint32_t ck_cap) {
-    __shared__ uint32_t f_s[16], st_s[16], m_s[16], sh_s[16];
+    __shared__ uint64_t tab[16];
     if (threadIdx.x < 16) {
-        f_s[threadIdx.x] = model[threadIdx.x];
-        st_s[threadIdx.x] = model[16 + threadIdx.x];
-        m_s[threadIdx.x] = model[33 + threadIdx.x];
-        sh_s[threadIdx.x] = model[49 + threadIdx.x];
+        const uint32_t s = threadIdx.x;
+        tab[s] = (uint64_t)model[s] | ((uint64_t)model[16 + s] << 13) | ((uint64_t)model[49 + s] << 25) |
+                 ((uint64_t)model[33 + s] << 32);
     }
     __syncthreads();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nb) return;
-    EncMeta m = meta[i];
+    const EncMeta m = meta[i];
     if (m.flags & EF_OVERFLOW) return;
-    const uint8_t* src = nib_pool + m.nib_off;
+    // the packed nibbles of a brick start 16-byte aligned and are padded to 16
+    const uint4* src4 = reinterpret_cast<const uint4*>(nib_pool + m.nib_off);
     uint8_t* out = enc_pool + enc_off[i];
     Checkpoint* ck = ck_all + (uint64_t)i * ck_cap;
     int k = (int)min(m.n_ck, ck_cap) - 1;
     uint32_t next = k >= 0 ? ck[k].sym : 0xFFFFFFFFu;
     uint32_t x = kRansL, emitted = 0;
-    for (int q = (int)m.nbytes - 1; q >= 0; --q) {
-        const uint32_t byte = src[q];
+    const int nchunk = (int)((m.nbytes + 15) / 16);
+    uint4 cur = nchunk > 0 ? src4[nchunk - 1] : make_uint4(0, 0, 0, 0);
+    for (int c16 = nchunk - 1; c16 >= 0; --c16) {
+        const uint4 nxt = c16 > 0 ? src4[c16 - 1] : make_uint4(0, 0, 0, 0);  // prefetch
+        const uint32_t words[4] = {cur.x, cur.y, cur.z, cur.w};
 #pragma unroll
-        for (int h = 1; h >= 0; --h) {  // low nibble (symbol 2q+1) first: reverse order
-            const uint32_t s = h ? (byte & 15u) : (byte >> 4);
-            const uint32_t f = f_s[s];
-            const uint32_t bound = ((kRansL >> kTotBits) << 8) * f;
-            while (x >= bound) {
-                out[emitted++] = (uint8_t)(x & 0xFF);
-                x >>= 8;
+        for (int b = 15; b >= 0; --b) {
+            const uint32_t q = 16u * (uint32_t)c16 + (uint32_t)b;
+            if (q >= m.nbytes) continue;
+            const uint32_t byte = (words[b >> 2] >> (8 * (b & 3))) & 0xFFu;
+            // low nibble (symbol 2q+1) first: the symbols go in reverse order
+            rans_enc_step(x, emitted, out, tab[byte & 15u]);
+            if (2 * q + 1 == next) {
+                ck[k].state = x;
+                ck[k].pos = emitted;
+                --k;
+                next = k >= 0 ? ck[k].sym : 0xFFFFFFFFu;
             }
-            const uint32_t qd = (uint32_t)(((uint64_t)x * m_s[s]) >> sh_s[s]);
-            x = (qd << kTotBits) + (x - qd * f) + st_s[s];
-            if ((uint32_t)(2 * q + h) == next) {
+            rans_enc_step(x, emitted, out, tab[byte >> 4]);
+            if (2 * q == next) {
                 ck[k].state = x;
                 ck[k].pos = emitted;
                 --k;
                 next = k >= 0 ? ck[k].sym : 0xFFFFFFFFu;
             }
         }
+        cur = nxt;
     }
     for (int b = 0; b < 4; ++b) {  // ransFlush, little-endian
         out[emitted++] = (uint8_t)(x & 0xFF);
@@ -700,7 +728,7 @@ int encode_device(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W
     CK(grow(&s->d_rec_off, &s->rec_cap, std::max<uint32_t>(nb, 1)));
     CK(cudaMemcpyAsync(s->d_enc_off, enc_off.data(), 8ull * nb, cudaMemcpyHostToDevice, st));
     if (nb) {
-        enc_rans_kernel<<<(nb + 63) / 64, 64, 0, st>>>(s->d_meta, nb, s->d_nib, s->d_enc_off, s->d_enc, s->d_model,
+        enc_rans_kernel<<<(nb + 31) / 32, 32, 0, st>>>(s->d_meta, nb, s->d_nib, s->d_enc_off, s->d_enc, s->d_model,
                                                        s->d_ck, s->ck_cap);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(s->h_meta.data(), s->d_meta, sizeof(EncMeta) * nb, cudaMemcpyDeviceToHost, st));

@@ -87,6 +87,8 @@ def load_library() -> C.CDLL:
     L.csv_close.argtypes = [vp]
     L.csv_decode_batch.argtypes = [vp, vp, vp, C.c_uint32, vp, vp, vp]
     L.csv_decode_image.argtypes = [vp, u8p, C.c_size_t, C.c_uint32, u64p, u32p]
+    L.csv_render.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_float, C.c_uint32, C.c_uint32, vp, C.c_uint64, vp,
+                             vp, C.c_uint32, vp, vp, vp, vp]
     L.csv_synth_volume.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_uint32, C.c_uint32,
                                    C.c_float, C.c_float, C.c_float, C.c_uint64, vp]
     _lib = L
@@ -251,6 +253,23 @@ class Codec:
         if rc and (check or rc != -6):
             self._check(rc)
         return out[:nb], st[:nb]
+
+    # ---- ray marcher ----------------------------------------------------
+    def render(self, cam16, width: int, height: int, grid_size: float, brick_size: int, bricks_per_axis: int,
+               d_slots, d_labels, d_label_out, d_depth_out, d_requests=None, d_hidden=None, stream=None):
+        """Label/depth image (csv_render).  cam16: float32[16] from csvb200.camera.camera_uniform; d_slots: device
+        tensor of csv_brick_slot records (16 bytes each)."""
+        from .camera import camera_struct
+        cam = camera_struct(cam16)
+        n_slots = d_slots.numel() * d_slots.element_size() // 16
+        self._check(self.lib.csv_render(
+            self.handle, C.byref(cam), width, height, grid_size, brick_size, bricks_per_axis,
+            C.c_void_p(d_slots.data_ptr()), n_slots, C.c_void_p(d_labels.data_ptr()),
+            C.c_void_p(d_hidden.data_ptr() if d_hidden is not None else None),
+            0 if d_hidden is None else d_hidden.numel(), C.c_void_p(d_label_out.data_ptr()),
+            C.c_void_p(d_depth_out.data_ptr()),
+            C.c_void_p(d_requests.data_ptr() if d_requests is not None else None),
+            C.c_void_p(_stream_handle(stream))))
 
     # ---- workload generator ---------------------------------------------
     def synth_volume(self, d_volume, kind: int, n_cells: int, n_tubes: int = 0, r_min: float = 0.0,

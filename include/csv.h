@@ -132,6 +132,45 @@ int csv_decode_batch(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_r
 int csv_decode_image(csv_ctx* ctx, const uint8_t* image, size_t len, uint32_t lod, uint64_t* out,
                      uint32_t* status);
 
+/* ---- ray marcher ---------------------------------------------------------
+ * rayTrace.wgsl:rayTrace (rayTrace.wgsl:565-906) in label/depth space: per
+ * pixel of a width x height image, the first visible voxel along the camera
+ * ray through the decoded brick cache.  A voxel is visible when its label is
+ * not 0 and not in `d_hidden` (sorted ascending, n_hidden entries; labels the
+ * transfer function hides).  d_label_out receives the label (0 = no hit),
+ * d_depth_out the ray parameter t at which the hit cell was entered (+inf =
+ * no hit).  The camera is camera.js:getUniformData (camera.js:61-77); the
+ * volume is the cube [0, grid_size)^3 of bricks_per_axis^3 bricks
+ * (SceneInfo, rayTrace.wgsl:87-96).  Slots are indexed by brick Morton code
+ * (rayTrace.wgsl:654-657).  d_requests (optional, n_slots words) gets 1 for
+ * every missing slot a ray crossed (brickRequests, rayTrace.wgsl:686).
+ * Bit-identical to the scalar restatement on the CPU (same float operations,
+ * no fused multiply-add). */
+typedef struct csv_camera {
+    float position[3];
+    float tan_half_fov;
+    float forward[3];
+    float pad0;
+    float right[3];
+    float pad1;
+    float up[3];
+    float pad2;
+} csv_camera;
+
+#define CSV_SLOT_EMPTY 0x1u   /* every palette entry is 0 (webgpuSetup.js:315-322) */
+#define CSV_SLOT_MISSING 0x2u /* not resident in the decoded cache */
+
+typedef struct csv_brick_slot {
+    uint64_t offset; /* first of the brick's 8^lod labels in d_labels */
+    uint32_t lod;    /* targetLOD of the resident copy */
+    uint32_t flags;  /* CSV_SLOT_* */
+} csv_brick_slot;
+
+int csv_render(csv_ctx* ctx, const csv_camera* camera, uint32_t width, uint32_t height, float grid_size,
+               uint32_t brick_size, uint32_t bricks_per_axis, const csv_brick_slot* d_slots, uint64_t n_slots,
+               const uint64_t* d_labels, const uint64_t* d_hidden, uint32_t n_hidden, uint64_t* d_label_out,
+               float* d_depth_out, uint32_t* d_requests, void* stream);
+
 /* ---- workload generator (no reference counterpart) --------------------
  * Seeded synthetic label volume on the device, x fastest: kind 0 = Voronoi
  * (n_cells cells, then a random half-space slab of label 0 covering about

@@ -13,6 +13,7 @@
 #include "csv_oracle.h"
 
 #include <stdlib.h>
+#include <math.h>
 #include <string.h>
 
 #define EMPTY_LABEL UINT64_MAX /* types.hpp:19 */
@@ -596,4 +597,206 @@ int or_seek_index(const uint32_t* freq, const uint32_t* cum, const uint8_t* enc,
     for (uint32_t k = lvl + 1; k < 8; ++k) level_start[k] = ops;
     *n_ops = ops;
     return status;
+}
+
+/* ------------------------------------------------------------ LOD rule */
+/* calculateBrickLOD (camera.js:103-137), double precision as in JS.  The
+ * focal length (screenWidth / 2) / tan(fov / 2) is computed once by the caller
+ * (the reference passes min(canvas.width, canvas.height), renderLoop.js:374). */
+uint32_t or_brick_lod(const double* c, double brick_size, const double* cam, double focal, uint32_t max_lod) {
+    double dx = c[0] - cam[0], dy = c[1] - cam[1], dz = c[2] - cam[2];
+    double dist = sqrt(dx * dx + dy * dy + dz * dz);
+    double d = dist > 0.1 ? dist : 0.1;
+    uint32_t best = 0;
+    for (uint32_t lod = 0; lod <= max_lod; ++lod) {
+        double voxel = brick_size / (double)(1u << lod);
+        double px = (focal * voxel) / d;
+        if (px >= 1.0) best = lod;
+        else break;
+    }
+    return best;
+}
+
+/* ------------------------------------------------------------ scalar DDA */
+/* rayTrace.wgsl:565-906 in label/depth space, every float operation in the
+ * shader's order, one rounding per operation (built with -ffp-contract=off).
+ * Shading, shadows, gradients and compositing do not change which voxel is hit
+ * first and are left out.  A voxel is visible when its label is not 0 and not
+ * hidden: every other label maps to alpha >= 0.25 > 0.05 (decode.wgsl:171,
+ * rayTrace.wgsl:794), label 0 and hidden labels to alpha 0. */
+static float fsgn(float x) { return x > 0.f ? 1.f : (x < 0.f ? -1.f : 0.f); }
+static int isgn(float x) { return (x > 0.f ? 1 : 0) + (x < 0.f ? -1 : 0); }
+static int hidden_has(const uint64_t* h, uint32_t n, uint64_t v) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) / 2;
+        if (h[mid] < v) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo < n && h[lo] == v;
+}
+static int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+void or_render(const float* cam, uint32_t W, uint32_t H, float grid, uint32_t bsz, uint32_t bpa,
+               const or_slot* slots, uint64_t n_slots, const uint64_t* labels, const uint64_t* hidden,
+               uint32_t n_hidden, uint64_t* out_label, float* out_depth, uint32_t* miss) {
+    const float o[3] = {cam[0], cam[1], cam[2]};
+    const float thf = cam[3];
+    const float fw = (float)W, fh = (float)H, aspect = fw / fh;
+    const int bs = (int)bsz;
+    int lb = 0;
+    while ((1 << lb) < bs) ++lb;
+    const int numBricks = (int)bpa > 1 ? (int)bpa : 1;
+    for (uint32_t py = 0; py < H; ++py)
+        for (uint32_t px = 0; px < W; ++px) {
+            const size_t pix = (size_t)py * W + px;
+            out_label[pix] = 0;
+            out_depth[pix] = INFINITY;
+            if (miss) miss[pix] = 0;
+            float ndc_x = (((float)px + 0.5f) / fw) * 2.0f - 1.0f;
+            float ndc_y = 1.0f - (((float)py + 0.5f) / fh) * 2.0f;
+            float d[3], inv[3];
+            for (int a = 0; a < 3; ++a) {
+                float r = ((cam[8 + a] * ndc_x) * aspect) * thf;
+                float u = (cam[12 + a] * ndc_y) * thf;
+                d[a] = (cam[4 + a] + r) + u;
+            }
+            float len = sqrtf((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]);
+            for (int a = 0; a < 3; ++a) d[a] = d[a] / len;
+            for (int a = 0; a < 3; ++a) inv[a] = fsgn(d[a]) / fmaxf(fabsf(d[a]), 1e-6f);
+            /* intersectVolume (:457-471) */
+            float t0[3], t1[3];
+            for (int a = 0; a < 3; ++a) {
+                t0[a] = (0.0f - o[a]) * inv[a];
+                t1[a] = (grid - o[a]) * inv[a];
+            }
+            float tmin = fmaxf(fmaxf(fminf(t0[0], t1[0]), fminf(t0[1], t1[1])), fminf(t0[2], t1[2]));
+            float tmax = fminf(fminf(fmaxf(t0[0], t1[0]), fmaxf(t0[1], t1[1])), fmaxf(t0[2], t1[2]));
+            if (tmax < 0.0f || tmin > tmax) continue;
+            const float tEnter = fmaxf(tmin, 0.0f), tExit = tmax;
+            /* initBrickDDA (:519-545) */
+            int brick[3], step[3];
+            float btMax[3], btDelta[3];
+            {
+                float eps = fmaxf(tEnter * 1e-6f, 1e-5f), ts = tEnter + eps;
+                for (int a = 0; a < 3; ++a) {
+                    float pos = o[a] + d[a] * ts;
+                    brick[a] = (int)floorf(pos) / bs;
+                    step[a] = isgn(d[a]);
+                    float bf = (float)brick[a] * (float)bs;
+                    float nb = d[a] > 0.0f ? bf + (float)bs : bf;
+                    btMax[a] = (nb - o[a]) * inv[a];
+                    btDelta[a] = fabsf((float)bs * inv[a]);
+                }
+            }
+            int be[3], bx[3];
+            for (int a = 0; a < 3; ++a) {
+                be[a] = (int)(o[a] + d[a] * tEnter) / bs;
+                bx[a] = (int)(o[a] + d[a] * tExit) / bs;
+            }
+            uint32_t maxCross = (uint32_t)(abs(bx[0] - be[0]) + abs(bx[1] - be[1]) + abs(bx[2] - be[2])) + 6u;
+            float brickEntryT = tEnter;
+            int done = 0;
+            for (uint32_t it = 0; it < maxCross && !done; ++it) {
+                if (brick[0] < 0 || brick[1] < 0 || brick[2] < 0 || brick[0] >= numBricks || brick[1] >= numBricks ||
+                    brick[2] >= numBricks)
+                    break;
+                uint32_t m = or_morton3((uint32_t)brick[0], (uint32_t)brick[1], (uint32_t)brick[2]);
+                int skip = m >= n_slots;
+                or_slot sl = {0, 0, 0};
+                if (!skip) {
+                    sl = slots[m];
+                    if (sl.flags & 1u) skip = 1;
+                    else if (sl.flags & 2u) {
+                        skip = 1;
+                        if (miss) miss[pix]++;
+                    }
+                }
+                if (!skip) {
+                    int bmin[3];
+                    for (int a = 0; a < 3; ++a) bmin[a] = brick[a] * bs;
+                    float tEnterBrick = fmaxf(brickEntryT, tEnter);
+                    float tExitBrick = fminf(fminf(btMax[0], btMax[1]), btMax[2]);
+                    float exitBias = fmaxf(tExitBrick * 1e-6f, 1e-5f);
+                    tExitBrick = fmaxf(tEnterBrick, tExitBrick - exitBias);
+                    /* initDDA (:473-499) */
+                    int vox[3];
+                    float vtMax[3], vtDelta[3];
+                    float eps = fmaxf(tEnterBrick * 1e-6f, 1e-5f), ts = tEnterBrick + eps;
+                    for (int a = 0; a < 3; ++a) {
+                        float pos = o[a] + d[a] * ts;
+                        vox[a] = (int)floorf(pos);
+                        float nb = d[a] > 0.0f ? (float)(vox[a] + 1) : (float)vox[a];
+                        vtMax[a] = (nb - o[a]) * inv[a];
+                        vtDelta[a] = fabsf(inv[a]);
+                    }
+                    const int lodSize = 1 << sl.lod;
+                    const int stride = bs / lodSize;
+                    for (int a = 0; a < 3; ++a) vox[a] -= bmin[a];
+                    if (stride > 1) { /* :706-731 */
+                        for (int a = 0; a < 3; ++a) {
+                            int lv = (vox[a] / stride) * stride;
+                            vox[a] = clampi(lv, 0, bs - 1);
+                            vtDelta[a] = fabsf(inv[a]) * (float)stride;
+                            float lw = (float)bmin[a] + (float)vox[a];
+                            float nb = d[a] > 0.0f ? lw + (float)stride : lw;
+                            vtMax[a] = (nb - o[a]) * inv[a];
+                        }
+                    } else {
+                        for (int a = 0; a < 3; ++a) vox[a] = clampi(vox[a], 0, bs - 1);
+                    }
+                    int le[3], lx[3];
+                    for (int a = 0; a < 3; ++a) {
+                        float ve = o[a] + d[a] * tEnterBrick, vx = o[a] + d[a] * tExitBrick;
+                        float lef = (ve - (float)bmin[a]) / (float)stride;
+                        float lxf = (vx - (float)bmin[a]) / (float)stride;
+                        le[a] = (int)floorf(lef);
+                        lx[a] = (int)ceilf(lxf);
+                    }
+                    uint32_t maxSteps = (uint32_t)(abs(lx[0] - le[0]) + abs(lx[1] - le[1]) + abs(lx[2] - le[2])) + 128u;
+                    float tcell = tEnterBrick;
+                    for (uint32_t vi = 0; vi < maxSteps; ++vi) {
+                        int inb = vox[0] >= 0 && vox[1] >= 0 && vox[2] >= 0 && vox[0] < bs && vox[1] < bs && vox[2] < bs;
+                        if (inb) {
+                            uint64_t lab;
+                            if (sl.lod == 0) lab = labels[sl.offset];
+                            else {
+                                int sh = lb - (int)sl.lod;
+                                lab = labels[sl.offset + or_morton3((uint32_t)vox[0] >> sh, (uint32_t)vox[1] >> sh,
+                                                                    (uint32_t)vox[2] >> sh)];
+                            }
+                            if (lab != 0 && !(n_hidden && hidden_has(hidden, n_hidden, lab))) {
+                                out_label[pix] = lab;
+                                out_depth[pix] = tcell;
+                                done = 1;
+                                break;
+                            }
+                        }
+                        /* advanceDDA (:501-517) */
+                        float t;
+                        if (vtMax[0] < vtMax[1] && vtMax[0] < vtMax[2]) {
+                            t = vtMax[0]; vtMax[0] += vtDelta[0]; vox[0] += step[0];
+                        } else if (vtMax[1] < vtMax[2]) {
+                            t = vtMax[1]; vtMax[1] += vtDelta[1]; vox[1] += step[1];
+                        } else {
+                            t = vtMax[2]; vtMax[2] += vtDelta[2]; vox[2] += step[2];
+                        }
+                        tcell = t;
+                        if (t > tExitBrick) break;
+                    }
+                    if (done) break;
+                }
+                /* advanceBrickDDA (:547-563) */
+                float t;
+                if (btMax[0] < btMax[1] && btMax[0] < btMax[2]) {
+                    t = btMax[0]; btMax[0] += btDelta[0]; brick[0] += step[0];
+                } else if (btMax[1] < btMax[2]) {
+                    t = btMax[1]; btMax[1] += btDelta[1]; brick[1] += step[1];
+                } else {
+                    t = btMax[2]; btMax[2] += btDelta[2]; brick[2] += step[2];
+                }
+                brickEntryT = t + fmaxf(t * 1e-6f, 1e-5f);
+                if (t > tExit) break;
+            }
+        }
 }

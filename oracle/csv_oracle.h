@@ -45,6 +45,27 @@ int or_seek_index(const uint32_t* freq16, const uint32_t* cum16, const uint8_t* 
                   uint32_t* n_ops, uint32_t* level_start /* [8] */, uint32_t* ckpt /* 4 per */,
                   uint32_t max_ckpt, uint32_t* n_ckpt);
 
+/* Per-brick LOD (camera.js:103-137) in double precision, as JS computes it;
+ * focal = (screen_px / 2) / tan(fov / 2) computed once by the caller. */
+uint32_t or_brick_lod(const double* center3, double brick_size, const double* cam3, double focal, uint32_t max_lod);
+
+/* Brick slot of the decoded cache, indexed by the brick's Morton code. */
+typedef struct {
+    uint64_t offset;  /* first label of the brick's 8^lod decoded labels */
+    uint32_t lod;     /* targetLOD */
+    uint32_t flags;   /* bit 0: empty (all palette entries 0), bit 1: not resident */
+} or_slot;
+
+/* Scalar DDA (rayTrace.wgsl:565-906) in label/depth space.  cam: position[3],
+ * tanHalfFov, forward[3], pad, right[3], pad, up[3], pad (camera.js:61-77).
+ * First visible voxel (label != 0 and not in the sorted `hidden` list) gives
+ * the pixel's label and the ray parameter t at which its cell was entered;
+ * no hit gives label 0 and depth +inf.  miss[i] counts non-resident bricks
+ * ray i crossed before its hit. */
+void or_render(const float* cam, uint32_t W, uint32_t H, float grid_size, uint32_t brick_size,
+               uint32_t bricks_per_axis, const or_slot* slots, uint64_t n_slots, const uint64_t* labels,
+               const uint64_t* hidden, uint32_t n_hidden, uint64_t* out_label, float* out_depth, uint32_t* miss);
+
 void or_free(void* p);
 
 #ifdef __cplusplus

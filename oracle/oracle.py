@@ -59,7 +59,32 @@ class Oracle:
         L.or_seek_index.argtypes = [_u32p, _u32p, _u8p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                     C.c_uint32, _u32p, _u32p, _u32p, C.c_uint32, _u32p]
         L.or_free.argtypes = [C.c_void_p]
+        L.or_brick_lod.restype = C.c_uint32
+        L.or_brick_lod.argtypes = [C.POINTER(C.c_double), C.c_double, C.POINTER(C.c_double), C.c_double, C.c_uint32]
+        L.or_render.argtypes = [C.POINTER(C.c_float), C.c_uint32, C.c_uint32, C.c_float, C.c_uint32, C.c_uint32,
+                                C.c_void_p, C.c_uint64, _u64p, _u64p, C.c_uint32, _u64p, C.POINTER(C.c_float), _u32p]
         self.lib = L
+
+    def brick_lod(self, center, brick_size, cam, focal, max_lod) -> int:
+        c = (C.c_double * 3)(*center)
+        p = (C.c_double * 3)(*cam)
+        return int(self.lib.or_brick_lod(c, brick_size, p, focal, max_lod))
+
+    def render(self, cam16: np.ndarray, W: int, H: int, grid: float, brick: int, bpa: int, slots: np.ndarray,
+               labels: np.ndarray, hidden: np.ndarray | None = None):
+        """cam16: float32[16] (camera.js getUniformData layout); slots: structured (offset u8, lod u4, flags u4)."""
+        cam = np.ascontiguousarray(cam16, np.float32)
+        lab = np.ascontiguousarray(labels, np.uint64)
+        hid = np.ascontiguousarray(hidden if hidden is not None else np.zeros(1, np.uint64), np.uint64)
+        nh = 0 if hidden is None else len(hidden)
+        out = np.zeros(W * H, np.uint64)
+        dep = np.zeros(W * H, np.float32)
+        miss = np.zeros(W * H, np.uint32)
+        sl = np.ascontiguousarray(slots)
+        self.lib.or_render(cam.ctypes.data_as(C.POINTER(C.c_float)), W, H, grid, brick, bpa, sl.ctypes.data,
+                           len(sl), _ptr(lab, _u64p), _ptr(hid, _u64p), nh, _ptr(out, _u64p),
+                           dep.ctypes.data_as(C.POINTER(C.c_float)), _ptr(miss, _u32p))
+        return out.reshape(H, W), dep.reshape(H, W), miss.reshape(H, W)
 
     def morton3(self, x, y, z) -> int:
         return self.lib.or_morton3(x, y, z)

@@ -181,3 +181,42 @@ def test_seek_index_checkpoints_resume_decode(oracle):
                     p -= 1
                     x = ((x << 8) | enc[p]) & 0xFFFFFFFF
                 assert s == nibs[j]
+
+
+def test_brick_lod_rule(oracle):
+    """camera.js:103-137 restated: finest LOD whose voxels still cover >= 1 pixel."""
+    import math
+    from csvb200.camera import focal_length
+    f = focal_length(1080, math.pi / 3)
+    for d in [0.05, 10.0, 100.0, 1000.0, 5000.0, 1e5]:
+        lod = oracle.brick_lod((d, 0.0, 0.0), 64.0, (0.0, 0.0, 0.0), f, 6)
+        expect = 0
+        for k in range(7):
+            if f * (64.0 / 2 ** k) / max(d, 0.1) >= 1.0:
+                expect = k
+            else:
+                break
+        assert lod == expect
+
+
+def test_scalar_dda_sees_the_volume(oracle):
+    """Scalar DDA smoke on the CPU: a full-resolution cache of a two-label volume, camera outside."""
+    import math
+    from csvb200.camera import SLOT_DTYPE, camera_uniform, orbit
+    vol = np.zeros((32, 32, 32), np.uint64)
+    vol[8:24, 8:24, 8:24] = 7
+    img = oracle.encode(vol, 16)
+    dec, st = oracle.decode_image(img, 4)
+    slots = np.zeros(8, SLOT_DTYPE)
+    for i in range(8):
+        slots[i] = (i * 4096, 4, 0)
+    # split order is bx, by, bz (bz fastest); slots are indexed by Morton ID
+    ids = [oracle.morton3(bx, by, bz) for bx in range(2) for by in range(2) for bz in range(2)]
+    lab = np.zeros(8 * 4096, np.uint64)
+    for i, m in enumerate(ids):
+        lab[m * 4096:(m + 1) * 4096] = dec[i]
+        slots[m] = (m * 4096, 4, 0)
+    pos, d = orbit((16.0, 16.0, 16.0), 80.0, 0.3, 0.2)
+    l, dep, miss = oracle.render(camera_uniform(pos, d, math.pi / 3), 32, 32, 32.0, 16, 2, slots, lab)
+    assert (l == 7).sum() > 20 and set(np.unique(l)) <= {0, 7}
+    assert np.isfinite(dep[l == 7]).all() and np.isinf(dep[l == 0]).all()

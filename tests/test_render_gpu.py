@@ -1,0 +1,125 @@
+"""GPU: the label/depth ray marcher (csv_render) is bit-identical to the scalar DDA restatement.
+
+Both read the same decoded brick cache (bricks decoded on the GPU at a per-brick
+LOD); labels must be equal and depths equal bit for bit (float32 compared as
+integers).
+"""
+import math
+import struct
+
+import numpy as np
+import pytest
+
+from csvb200.camera import SLOT_DTYPE, SLOT_EMPTY, SLOT_MISSING, camera_uniform, orbit
+
+pytestmark = pytest.mark.gpu
+
+
+def palettes_all_zero(img: bytes):
+    nb = struct.unpack_from("<I", img, 8)[0]
+    o = 152
+    out = []
+    for _ in range(nb):
+        ID, P = struct.unpack_from("<2I", img, o)
+        pal = np.frombuffer(img, np.uint64, P, o + 8)
+        out.append(bool(np.all(pal == 0)))
+        o += 8 + 8 * P
+        E = struct.unpack_from("<I", img, o)[0]
+        o += 4 + E + 4
+    return out
+
+
+def build_cache(codec, img, lods):
+    """Decode every brick at lods[i] into one label buffer; slots indexed by brick Morton ID."""
+    import torch
+    from csvb200 import requests, requests_tensor
+    ds = codec.open(img)
+    nb = ds.num_bricks
+    ids = ds.ids()
+    sizes = 8 ** lods.astype(np.uint64)
+    offs = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.uint64)
+    labels = torch.zeros(int(sizes.sum()), dtype=torch.int64, device="cuda")
+    st = torch.zeros(nb, dtype=torch.int32, device="cuda")
+    codec.decode_batch(ds, requests_tensor(requests(np.arange(nb), lods, offs)), labels, st)
+    torch.cuda.synchronize()
+    assert int(st.abs().max()) == 0
+    empty = palettes_all_zero(img)
+    slots = np.zeros(int(ids.max()) + 1, SLOT_DTYPE)
+    slots["flags"] = SLOT_EMPTY  # IDs absent from the dataset
+    for i in range(nb):
+        slots[ids[i]] = (offs[i], lods[i], SLOT_EMPTY if empty[i] else 0)
+    ds.close()
+    return slots, labels
+
+
+def render_both(codec, oracle, cam, W, H, grid, b, bpa, slots, labels, hidden=None):
+    import torch
+    d_slots = torch.from_numpy(slots.view(np.uint8).copy()).cuda()
+    out = torch.empty(W * H, dtype=torch.int64, device="cuda")
+    dep = torch.empty(W * H, dtype=torch.float32, device="cuda")
+    req = torch.zeros(len(slots), dtype=torch.int32, device="cuda")
+    d_hidden = None if hidden is None else torch.from_numpy(np.sort(hidden).astype(np.int64)).cuda()
+    codec.render(cam, W, H, grid, b, bpa, d_slots, labels, out, dep, d_requests=req, d_hidden=d_hidden)
+    torch.cuda.synchronize()
+    ref_l, ref_d, miss = oracle.render(cam, W, H, grid, b, bpa, slots, labels.cpu().numpy().view(np.uint64),
+                                       None if hidden is None else np.sort(hidden).astype(np.uint64))
+    got_l = out.cpu().numpy().view(np.uint64).reshape(H, W)
+    got_d = dep.cpu().numpy().reshape(H, W)
+    return got_l, got_d, ref_l, ref_d, req.cpu().numpy(), miss
+
+
+@pytest.fixture(scope="module")
+def scene(codec):
+    import torch
+    vol = torch.empty((128, 128, 128), dtype=torch.int64, device="cuda")
+    codec.synth_volume(vol, 1, 300, 60, 1.5, 7.0, 0.3, 17)
+    torch.cuda.synchronize()
+    codec.encode_device(vol, 16)
+    img = bytes(codec.encoded_image_tensor().cpu().numpy())
+    rng = np.random.default_rng(5)
+    lods = rng.integers(0, 5, 512).astype(np.uint32)
+    slots, labels = build_cache(codec, img, lods)
+    return img, slots, labels
+
+
+POSES = [  # (radius, yaw, pitch, fov)
+    (300.0, 0.7, 0.3, math.pi / 3),
+    (200.0, -2.1, -0.5, math.pi / 4),
+    (90.0, 3.0, 1.2, math.pi / 2),
+    (40.0, 0.2, 0.1, math.pi / 3),     # inside the volume
+    (250.0, 0.0, 0.0, math.pi / 3),    # axis-aligned view: dir.x == 0 exactly on the centre column
+    (500.0, 1.0, 1.55, math.pi / 6),   # near the pole (world-up switch)
+]
+
+
+@pytest.mark.parametrize("pose", range(len(POSES)))
+def test_render_bit_exact_vs_scalar_dda(codec, oracle, scene, pose):
+    img, slots, labels = scene
+    r, yaw, pitch, fov = POSES[pose]
+    pos, d = orbit((64.0, 64.0, 64.0), r, yaw, pitch)
+    cam = camera_uniform(pos, d, fov)
+    gl, gd, rl, rd, req, miss = render_both(codec, oracle, cam, 96, 72, 128.0, 16, 8, slots, labels)
+    assert np.array_equal(gl, rl)
+    assert np.array_equal(gd.view(np.uint32), rd.view(np.uint32))
+    assert (gl != 0).any() or pose == 2
+
+
+def test_render_hidden_labels_and_missing_bricks(codec, oracle, scene):
+    img, slots, labels = scene
+    lab = labels.cpu().numpy().view(np.uint64)
+    vals, counts = np.unique(lab[lab != 0], return_counts=True)
+    hidden = vals[np.argsort(-counts)[:5]]
+    sl = slots.copy()
+    rng = np.random.default_rng(9)
+    miss_ids = rng.choice(len(sl), 60, replace=False)
+    sl["flags"][miss_ids] |= SLOT_MISSING
+    pos, d = orbit((64.0, 64.0, 64.0), 260.0, 0.4, 0.35, )
+    cam = camera_uniform(pos, d, math.pi / 3)
+    gl, gd, rl, rd, req, miss = render_both(codec, oracle, cam, 96, 72, 128.0, 16, 8, sl, labels, hidden=hidden)
+    assert np.array_equal(gl, rl)
+    assert np.array_equal(gd.view(np.uint32), rd.view(np.uint32))
+    assert not np.isin(gl, hidden).any()
+    flagged = set(np.nonzero(req)[0].tolist())
+    missing = set(np.nonzero((sl["flags"] & SLOT_MISSING) & ~(sl["flags"] & SLOT_EMPTY))[0].tolist())
+    assert flagged <= missing
+    assert (len(flagged) > 0) == bool(miss.sum() > 0)
