@@ -148,6 +148,7 @@ int stage_dataset(csv_ctx* ctx, const uint8_t* img, const ImageView& v, DeviceDa
         enc_n += (r.E + 15) & ~15ull;
         ck_n += b.ck_cap;
         d.max_nsym = std::max(d.max_nsym, r.nsym);
+        d.max_P = std::max(d.max_P, r.P);
     }
     if (ck_n > 0xFFFFFFFFull) return fail(ctx, CSV_ERANGE, "dataset too large for the seek index");
     d.stream_bytes = 0;

@@ -70,7 +70,7 @@ struct DeviceDataset {
     uint32_t nb = 0, b = 0, L = 0, S = 0;
     uint32_t freq[16] = {}, cum[16] = {}, total = 0;
     uint64_t stream_bytes = 0, palette_entries = 0, ck_entries = 0;
-    uint32_t max_nsym = 0;
+    uint32_t max_nsym = 0, max_P = 0;
     BrickDesc* d_bricks = nullptr;
     uint64_t* d_pal = nullptr;
     uint8_t* d_enc = nullptr;

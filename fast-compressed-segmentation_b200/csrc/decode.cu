@@ -13,22 +13,26 @@
 //      every S ops, built once per dataset or emitted by the encoder); each
 //      thread decodes one segment and writes one 4-byte record per op (code,
 //      stop, resolved palette index).
-//   2. levels, coarse to fine: node values are palette indices.  A node whose
-//      parent is stop-filled ("inactive") takes the parent's value; the 8
-//      children of an active parent take their ops: Rp -> parent, Pa/P0/Pd ->
-//      palette index, Rx/Ry/Rz -> the neighbour outside the sibling block.  A
-//      neighbour on the +1 side is later in Morton order, so the reference
-//      reads its parent (known, previous level).  A neighbour on the -1 side is
-//      earlier, on the same level; its local index has one more 1-bit than the
-//      node's, so such chains are at most three hops long and are resolved on
-//      the fly without any ordering between threads.
-//      Inactive parents (most of them) are filled in one uniform pass; active
-//      parents are walked through a compacted list, so warps never diverge
-//      between the two.
+//   2. levels, coarse to fine, held in shared memory: the value of every node
+//      as a palette index (16-bit when the palette allows), a bitmask of the
+//      nodes with stop bit 0 ("active": their children have ops), and per
+//      32-node word the count of active nodes before it, so the rank of an
+//      active node -- which locates its children's ops -- is one popcount.
+//      Children of inactive parents inherit the parent's value in one uniform
+//      pass; the 8 children of each active parent (walked through a compacted
+//      list) take their ops: Rp -> parent, Pa/P0/Pd -> palette index,
+//      Rx/Ry/Rz -> the neighbour outside the sibling block.  A neighbour on the
+//      +1 side is later in Morton order, so the reference reads its parent
+//      (known, previous level).  A neighbour on the -1 side is earlier, on the
+//      same level; its local index has one more 1-bit than the node's, so such
+//      chains are at most three hops long and are resolved on the fly without
+//      any ordering between threads.
 //   3. the last level is written straight to HBM, 8 children (64 bytes) per
 //      parent, with streaming 16-byte stores.
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <algorithm>
 
 #include "block_scan.cuh"
 #include "csv_internal.h"
@@ -36,20 +40,25 @@
 namespace csv {
 
 constexpr int kDecThreads = 512;
-constexpr int kDecMinBlocks = 3;       // CTAs per SM the shared-memory budget allows
-constexpr uint32_t kSmemLevels = 5;    // levels 0..4 (<= 4096 nodes) keep node info in shared memory
-constexpr uint32_t kSmemNodes = 4684;  // levels 0..4 at 16-byte aligned offsets (soff)
-constexpr uint32_t kPalCache = 1024;   // palettes up to this size are copied to shared memory
+constexpr uint32_t kDecLevels = 6;       // parent levels 0..5 (a 64^3 brick has 7 levels)
+constexpr uint32_t kPalCache = 1024;     // palettes up to this size are copied to shared memory
 constexpr uint32_t REC_MISSING = OP_RP | 8u;
 
+// Node values of level l at val + voff(l): lvl_off rounded up to 8 entries (16 bytes for u16).
 __host__ __device__ constexpr uint32_t lvl_off(uint32_t l) { return ((1u << (3 * l)) - 1) / 7; }
-// shared-memory level offsets 0, 4, 12, 76, 588: lvl_off rounded up to a multiple of 4 words
-__host__ __device__ constexpr uint32_t soff(uint32_t l) { return l ? lvl_off(l) + 3 : 0; }
+__host__ __device__ constexpr uint32_t voff(uint32_t l) { return (lvl_off(l) + 7) & ~7u; }
+// Activity bitmask words of level l at mask + moff(l).
+__host__ __device__ constexpr uint32_t mwords(uint32_t l) { return l < 2 ? 1u : (1u << (3 * l)) / 32; }
+__host__ __device__ constexpr uint32_t moff(uint32_t l) { return l == 0 ? 0u : moff(l - 1) + mwords(l - 1); }
+constexpr uint32_t kValEntries = voff(kDecLevels);   // 37456
+constexpr uint32_t kMaskWords = moff(kDecLevels);    // 1172
 
+template <class V>
 struct DecShared {
     uint32_t lut[kTot];
-    uint32_t ni[kSmemNodes];
-    uint32_t av[kSmemNodes];
+    V val[kValEntries];
+    uint32_t mask[kMaskWords];
+    uint16_t pre[kMaskWords];
     uint64_t pal[kPalCache];
     uint32_t warp_sums[kDecThreads / 32 + 1];
     BrickDesc br;
@@ -211,21 +220,26 @@ __device__ __forceinline__ void store8(uint64_t* o8, const uint64_t* lab, bool v
     }
 }
 
+// The parent level as the resolver sees it.
+template <class V>
 struct LevelView {
-    const uint32_t* ni;  // node info of the parent level
-    const uint32_t* av;  // active values of the parent level
-    const uint32_t* rec; // op records of the brick
-    uint32_t o;          // first op of the child level
-    uint32_t n_rec;      // records available
+    const V* val;           // node values of the parent level
+    const uint32_t* mask;   // activity bits of the parent level
+    const uint16_t* pre;    // active nodes before each mask word
+    const uint32_t* rec;    // op records of the brick
+    uint32_t o;             // first op of the child level
+    uint32_t n_rec;         // records available
 };
 
-__device__ __forceinline__ uint32_t get_rec(const LevelView& v, uint32_t idx) {
+template <class V>
+__device__ __forceinline__ uint32_t get_rec(const LevelView<V>& v, uint32_t idx) {
     return idx < v.n_rec ? v.rec[idx] : REC_MISSING;
 }
 // The 8 records of the r-th active parent.  In a complete brick o is a sum of
 // multiples of 8, so the group is 32-byte aligned and read as two vectors; a
 // truncated brick (o arbitrary, records missing) takes the guarded scalar path.
-__device__ __forceinline__ void get_rec8(const LevelView& v, uint32_t r, uint32_t rec[8]) {
+template <class V>
+__device__ __forceinline__ void get_rec8(const LevelView<V>& v, uint32_t r, uint32_t rec[8]) {
     const uint32_t i0 = v.o + 8 * r;
     if ((i0 & 7u) == 0 && i0 + 8 <= v.n_rec) {
         const uint4* p = reinterpret_cast<const uint4*>(v.rec + i0);
@@ -237,9 +251,14 @@ __device__ __forceinline__ void get_rec8(const LevelView& v, uint32_t r, uint32_
         for (uint32_t c = 0; c < 8; ++c) rec[c] = get_rec(v, i0 + c);
     }
 }
-__device__ __forceinline__ uint32_t node_value(const LevelView& v, uint32_t p) {
-    uint32_t i = v.ni[p];
-    return (i & NI_ACT) ? v.av[i & ~NI_ACT] : i;
+// rank of an active parent-level node q (its children's ops start at o + 8 * rank)
+template <class V>
+__device__ __forceinline__ uint32_t rank_of(const LevelView<V>& v, uint32_t q) {
+    return v.pre[q >> 5] + __popc(v.mask[q >> 5] & ((1u << (q & 31)) - 1u));
+}
+template <class V>
+__device__ __forceinline__ bool is_active(const LevelView<V>& v, uint32_t q) {
+    return (v.mask[q >> 5] >> (q & 31)) & 1u;
 }
 
 // Value (palette index) of node n on level lc whose op record is `rec`; the
@@ -251,57 +270,56 @@ __device__ __forceinline__ uint32_t node_value(const LevelView& v, uint32_t p) {
 // coarseNodeToOutputIndex); malformed streams only.  Morton indices strictly
 // decrease along a chain, so it terminates; the iteration cap only guards
 // against a corrupt seek index.  Sets *bad on a capped chain.
-__device__ __forceinline__ uint32_t resolve(const LevelView& v, uint32_t rec, uint32_t n, uint32_t lc, bool* bad) {
+template <class V>
+__device__ __forceinline__ uint32_t resolve(const LevelView<V>& v, uint32_t rec, uint32_t n, uint32_t lc, bool* bad) {
     const uint32_t lvlmask = (1u << (3 * lc)) - 1u;
 #pragma unroll 1
     for (int hop = 0; hop < 4096; ++hop) {
         const uint32_t code = rec & 7u;
         if (code >= OP_PA) return rec >> REC_PIDX_SHIFT;
-        if (code == OP_RP) return node_value(v, n >> 3);
+        if (code == OP_RP) return v.val[n >> 3];
         const uint32_t a = code - 1;
         const uint32_t m = (0x09249249u << a) & lvlmask;
         const uint32_t bit = 1u << a;
         if (n & bit) {
-            if ((n & m) != m) return node_value(v, ((((n | ~m) + bit) & m) | (n & ~m)) >> 3);
+            if ((n & m) != m) return v.val[((((n | ~m) + bit) & m) | (n & ~m)) >> 3];
         } else if ((n & m) != 0) {
             const uint32_t N = (((n & m) - bit) & m) | (n & ~m);
-            const uint32_t q = v.ni[N >> 3];
-            if (!(q & NI_ACT)) return q;
-            rec = get_rec(v, v.o + 8 * (q & ~NI_ACT) + (N & 7u));
+            const uint32_t q = N >> 3;
+            if (!is_active(v, q)) return v.val[q];
+            rec = get_rec(v, v.o + 8 * rank_of(v, q) + (N & 7u));
             n = N;
             continue;
         }
         // outside the brick: the parent slot
-        if ((n & 7u) == 0) return node_value(v, n >> 3);
-        rec = get_rec(v, v.o + 8 * (v.ni[n >> 3] & ~NI_ACT));
+        if ((n & 7u) == 0) return v.val[n >> 3];
+        rec = get_rec(v, v.o + 8 * rank_of(v, n >> 3));
         n &= ~7u;
     }
     *bad = true;
     return 0;
 }
 
-__device__ __forceinline__ uint64_t label_of(const uint64_t* pal, uint32_t pidx) {
-    return pidx == PIDX_LABEL0 ? 0ull : pal[pidx];
+__device__ __forceinline__ uint64_t label_of(const uint64_t* pal, uint32_t pidx, uint32_t label0) {
+    return pidx == label0 ? 0ull : pal[pidx];
 }
 
-__global__ void __launch_bounds__(kDecThreads, kDecMinBlocks) decode_kernel(DecodeArgs A) {
+// V = uint16_t when every palette of the dataset has fewer than 65535 entries
+// (value 0xFFFF stands for "label 0"), else uint32_t (one CTA per SM).
+template <class V>
+__global__ void __launch_bounds__(kDecThreads) decode_kernel(DecodeArgs A) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
-    DecShared& S = *reinterpret_cast<DecShared*>(smem_raw);
+    DecShared<V>& S = *reinterpret_cast<DecShared<V>*>(smem_raw);
     const uint32_t tid = threadIdx.x, T = blockDim.x;
+    constexpr uint32_t LABEL0 = sizeof(V) == 2 ? 0xFFFFu : PIDX_LABEL0;
 
     for (uint32_t i = tid; i < kTot; i += T) S.lut[i] = A.lut[i];
 
-    // per-CTA scratch: op records | node info + active values of the one level
-    // above 4096 nodes | active-node lists of every parent level
+    // per-CTA scratch: op records | active-node lists of every parent level
     uint8_t* scr = A.scratch + (uint64_t)blockIdx.x * A.scratch_per_cta;
     uint32_t* recs = reinterpret_cast<uint32_t*>(scr);
     const uint64_t max_ops = ((1ull << (3 * A.L)) - 8) / 7;
-    uint64_t so = (max_ops * 4 + 255) & ~255ull;
-    const uint32_t g_nodes = A.L > kSmemLevels + 1 ? (1u << (3 * (A.L - 2))) : 0;
-    uint32_t* g_ni = reinterpret_cast<uint32_t*>(scr + so);
-    uint32_t* g_av = g_ni + g_nodes;
-    so += (8ull * g_nodes + 255) & ~255ull;
-    uint32_t* act = reinterpret_cast<uint32_t*>(scr + so);
+    uint32_t* act = reinterpret_cast<uint32_t*>(scr + ((max_ops * 4 + 255) & ~255ull));
 
     for (;;) {
         if (tid == 0) {
@@ -338,7 +356,9 @@ __global__ void __launch_bounds__(kDecThreads, kDecMinBlocks) decode_kernel(Deco
             fill_labels(out, 1ull << (3 * t), pal[0]);
         } else {
             // ---- 1. rANS segments -> op records
-            const uint32_t n_need = min(min(br.level_start[t], br.n_ops), br.ck_cap * A.S);
+            // (level_start is read from shared memory: a runtime index into a
+            // register copy of the descriptor would put it on the stack)
+            const uint32_t n_need = min(min(S.br.level_start[t], br.n_ops), br.ck_cap * A.S);
             const uint32_t nseg = (n_need + A.S - 1) / A.S;
             const uint8_t* enc = A.enc + br.enc_off;
             for (uint32_t k = tid; k < nseg; k += T) {
@@ -379,7 +399,7 @@ __global__ void __launch_bounds__(kDecThreads, kDecMinBlocks) decode_kernel(Deco
                             pidx = ip;
                             if (pidx >= br.P) { pidx = br.P - 1; st |= CSV_BRICK_PALETTE; }
                         } else if (code == 7) {
-                            pidx = PIDX_LABEL0;
+                            pidx = LABEL0;
                             st |= CSV_BRICK_BADOP;
                         }
                         rec = code | ((v & 1u) << 3) | (pidx << REC_PIDX_SHIFT);
@@ -388,9 +408,11 @@ __global__ void __launch_bounds__(kDecThreads, kDecMinBlocks) decode_kernel(Deco
                     ++j;
                 }
             }
+            // level 0: the root, value palette[0], active; clear the other masks
+            for (uint32_t i = tid; i < moff(t); i += T) S.mask[i] = i == 0 ? 1u : 0u;
             if (tid == 0) {
-                S.ni[0] = NI_ACT | 0u;
-                S.av[0] = 0;
+                S.val[0] = 0;
+                S.pre[0] = 0;
                 act[0] = 0;
             }
             __syncthreads();
@@ -400,55 +422,60 @@ __global__ void __launch_bounds__(kDecThreads, kDecMinBlocks) decode_kernel(Deco
             uint32_t n_act = 1;
             for (uint32_t l = 0; l < t; ++l) {
                 const uint32_t lc = l + 1;
-                LevelView V;
-                V.ni = (l < kSmemLevels) ? S.ni + soff(l) : g_ni;
-                V.av = (l < kSmemLevels) ? S.av + soff(l) : g_av;
-                V.rec = recs;
-                V.o = br.level_start[l];
-                V.n_rec = n_need;
+                LevelView<V> Vw;
+                Vw.val = S.val + voff(l);
+                Vw.mask = S.mask + moff(l);
+                Vw.pre = S.pre + moff(l);
+                Vw.rec = recs;
+                Vw.o = S.br.level_start[l];
+                Vw.n_rec = n_need;
                 const uint32_t* act_l = act + lvl_off(l);
                 const uint32_t n_par = 1u << (3 * l);
                 if (lc < t) {
-                    uint32_t* ni_c = (lc < kSmemLevels) ? S.ni + soff(lc) : g_ni;
-                    uint32_t* av_c = (lc < kSmemLevels) ? S.av + soff(lc) : g_av;
-                    uint32_t* act_c = act + lvl_off(lc);
-                    // active parents in contiguous chunks, so ranks come from one block scan
-                    const uint32_t per = (n_act + T - 1) / T;
-                    const uint32_t r0 = min(n_act, tid * per), r1 = min(n_act, r0 + per);
-                    uint32_t cnt = 0;
-                    for (uint32_t r = r0; r < r1; ++r) {
-                        uint32_t rec[8];
-                        get_rec8(V, r, rec);
-#pragma unroll
-                        for (int c = 0; c < 8; ++c) cnt += (rec[c] & 8u) ? 0u : 1u;
-                    }
-                    uint32_t n_act_c;
-                    uint32_t rk = block_exclusive<uint32_t>(cnt, S.warp_sums, &n_act_c);
-                    // stop-filled parents: children inherit (one uniform pass)
+                    V* val_c = S.val + voff(lc);
+                    uint32_t* mask_c = S.mask + moff(lc);
+                    // children of stop-filled parents inherit (16 bytes of u16 or 2 x 16 of u32)
                     for (uint32_t p = tid; p < n_par; p += T) {
-                        const uint32_t info = V.ni[p];
-                        if (!(info & NI_ACT)) {
-                            uint4 q = make_uint4(info, info, info, info);
-                            reinterpret_cast<uint4*>(ni_c + 8 * p)[0] = q;
-                            reinterpret_cast<uint4*>(ni_c + 8 * p)[1] = q;
+                        if (!is_active(Vw, p)) {
+                            const uint32_t v = Vw.val[p];
+                            if (sizeof(V) == 2) {
+                                const uint32_t vv = v | (v << 16);
+                                reinterpret_cast<uint4*>(val_c + 8 * p)[0] = make_uint4(vv, vv, vv, vv);
+                            } else {
+                                reinterpret_cast<uint4*>(val_c + 8 * p)[0] = make_uint4(v, v, v, v);
+                                reinterpret_cast<uint4*>(val_c + 8 * p)[1] = make_uint4(v, v, v, v);
+                            }
                         }
                     }
-                    for (uint32_t r = r0; r < r1; ++r) {
+                    // children of active parents take their ops
+                    for (uint32_t r = tid; r < n_act; r += T) {
                         const uint32_t p = act_l[r];
                         uint32_t rec[8];
-                        get_rec8(V, r, rec);
+                        get_rec8(Vw, r, rec);
+                        uint32_t bits = 0;
 #pragma unroll
                         for (uint32_t c = 0; c < 8; ++c) {
-                            const uint32_t n = 8 * p + c;
-                            const uint32_t val = resolve(V, rec[c], n, lc, &bad);
-                            if (rec[c] & 8u) {
-                                ni_c[n] = val;
-                            } else {
-                                ni_c[n] = NI_ACT | rk;
-                                av_c[rk] = val;
-                                act_c[rk] = n;
-                                ++rk;
-                            }
+                            val_c[8 * p + c] = (V)resolve(Vw, rec[c], 8 * p + c, lc, &bad);
+                            bits |= ((rec[c] & 8u) ? 0u : 1u) << c;
+                        }
+                        if (bits) atomicOr(mask_c + ((8 * p) >> 5), bits << ((8 * p) & 31));
+                    }
+                    __syncthreads();
+                    // ranks: active nodes before each mask word, then the compacted list
+                    const uint32_t nw = mwords(lc);
+                    const uint32_t per = (nw + T - 1) / T;
+                    const uint32_t w0 = min(nw, tid * per), w1 = min(nw, w0 + per);
+                    uint32_t cnt = 0;
+                    for (uint32_t i = w0; i < w1; ++i) cnt += __popc(mask_c[i]);
+                    uint32_t n_act_c;
+                    uint32_t run = block_exclusive<uint32_t>(cnt, S.warp_sums, &n_act_c);
+                    uint32_t* act_c = act + lvl_off(lc);
+                    for (uint32_t i = w0; i < w1; ++i) {
+                        S.pre[moff(lc) + i] = (uint16_t)run;
+                        uint32_t m = mask_c[i];
+                        while (m) {
+                            act_c[run++] = 32 * i + (__ffs(m) - 1);
+                            m &= m - 1;
                         }
                     }
                     n_act = n_act_c;
@@ -456,23 +483,34 @@ __global__ void __launch_bounds__(kDecThreads, kDecMinBlocks) decode_kernel(Deco
                 } else {
                     // last level: labels to HBM, 64 bytes per parent
                     for (uint32_t p = tid; p < n_par; p += T) {
-                        const uint32_t info = V.ni[p];
-                        if (!(info & NI_ACT)) {
-                            const uint64_t x = label_of(pal, info);
-                            uint64_t lab[8];
+                        if (!is_active(Vw, p)) {
+                            const uint64_t x = label_of(pal, Vw.val[p], LABEL0);
+                            uint64_t* o8 = out + 8ull * p;
+                            if (vec) {
 #pragma unroll
-                            for (int c = 0; c < 8; ++c) lab[c] = x;
-                            store8(out + 8ull * p, lab, vec);
+                                for (int c = 0; c < 8; c += 2) st_cs_v2(o8 + c, x, x);
+                            } else {
+#pragma unroll
+                                for (int c = 0; c < 8; ++c) o8[c] = x;
+                            }
                         }
                     }
                     for (uint32_t r = tid; r < n_act; r += T) {
                         const uint32_t p = act_l[r];
                         uint32_t rec[8];
-                        get_rec8(V, r, rec);
-                        uint64_t lab[8];
+                        get_rec8(Vw, r, rec);
+                        uint64_t* o8 = out + 8ull * p;
 #pragma unroll
-                        for (uint32_t c = 0; c < 8; ++c) lab[c] = label_of(pal, resolve(V, rec[c], 8 * p + c, lc, &bad));
-                        store8(out + 8ull * p, lab, vec);
+                        for (uint32_t c = 0; c < 8; c += 2) {
+                            const uint64_t a = label_of(pal, resolve(Vw, rec[c], 8 * p + c, lc, &bad), LABEL0);
+                            const uint64_t b = label_of(pal, resolve(Vw, rec[c + 1], 8 * p + c + 1, lc, &bad), LABEL0);
+                            if (vec) {
+                                st_cs_v2(o8 + c, a, b);
+                            } else {
+                                o8[c] = a;
+                                o8[c + 1] = b;
+                            }
+                        }
                     }
                 }
             }
@@ -488,31 +526,39 @@ __global__ void __launch_bounds__(kDecThreads, kDecMinBlocks) decode_kernel(Deco
 size_t decode_scratch_per_cta(uint32_t b) {
     uint32_t L = levels_of(b);
     uint64_t rec_bytes = (max_ops_of(b) * 4 + 255) & ~255ull;
-    uint64_t g_nodes = L > kSmemLevels + 1 ? (1ull << (3 * (L - 2))) : 0;
-    uint64_t ni_bytes = (8 * g_nodes + 255) & ~255ull;
     uint64_t act_bytes = 4ull * lvl_off(L - 1);  // active lists of levels 0 .. L-2
-    return (size_t)((rec_bytes + ni_bytes + act_bytes + 255) & ~255ull);
+    return (size_t)((rec_bytes + act_bytes + 255) & ~255ull);
 }
 
-static int g_dec_occ[64] = {0};
+static int g_dec_occ[2][64] = {{0}};
 
-uint32_t decode_grid(int device, uint32_t n) {
-    int& occ = g_dec_occ[device & 63];
+template <class V>
+static int occupancy(int device) {
+    int& occ = g_dec_occ[sizeof(V) == 2 ? 0 : 1][device & 63];
     if (occ == 0) {
-        cudaFuncSetAttribute(decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DecShared));
+        cudaFuncSetAttribute(decode_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(DecShared<V>));
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, decode_kernel, kDecThreads, sizeof(DecShared));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, decode_kernel<V>, kDecThreads, sizeof(DecShared<V>));
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         occ = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
     }
-    return n < (uint32_t)occ ? n : (uint32_t)occ;
+    return occ;
+}
+
+uint32_t decode_grid(int device, uint32_t n) {
+    uint32_t occ = (uint32_t)std::max(occupancy<uint16_t>(device), occupancy<uint32_t>(device));
+    return n < occ ? n : occ;
 }
 
 cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, uint32_t n, uint64_t* d_out,
                           uint32_t* d_status, const DecodeScratch& scr, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
-    uint32_t grid = decode_grid(ds.device, n);
+    if (ds.L > kDecLevels + 1) return cudaErrorInvalidValue;  // bricks up to 64^3
+    const bool narrow = ds.max_P < 0xFFFFu;
+    uint32_t grid = (uint32_t)(narrow ? occupancy<uint16_t>(ds.device) : occupancy<uint32_t>(ds.device));
+    if (grid > n) grid = n;
     if (grid > scr.ctas) grid = scr.ctas;
     cudaError_t e = cudaMemsetAsync(scr.d_queue, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
@@ -532,7 +578,8 @@ cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, ui
     A.L = ds.L;
     A.S = ds.S;
     A.n = n;
-    decode_kernel<<<grid, kDecThreads, sizeof(DecShared), st>>>(A);
+    if (narrow) decode_kernel<uint16_t><<<grid, kDecThreads, sizeof(DecShared<uint16_t>), st>>>(A);
+    else decode_kernel<uint32_t><<<grid, kDecThreads, sizeof(DecShared<uint32_t>), st>>>(A);
     return cudaGetLastError();
 }
 

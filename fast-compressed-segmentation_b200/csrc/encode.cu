@@ -807,6 +807,7 @@ int encoder_to_dataset(EncoderState* s, DeviceDataset& d, std::string& err) {
         d.stream_bytes += m.E;
         d.palette_entries += m.P;
         d.max_nsym = std::max(d.max_nsym, m.nsym);
+        d.max_P = std::max(d.max_P, m.P);
     }
     d.ck_entries = (uint64_t)nb * s->ck_cap;
     uint32_t lut[kTot];
