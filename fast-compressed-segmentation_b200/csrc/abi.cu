@@ -302,6 +302,17 @@ int csv_decode_batch(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_r
     return CSV_OK;
 }
 
+int csv_decode_batch_static(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_reqs, uint32_t n,
+                            uint64_t* d_out, uint32_t* d_status, void* stream) {
+    if (!ctx || !ds) return CSV_EINVAL;
+    if (n == 0) return CSV_OK;
+    if (!d_reqs || !d_out || !d_status) return fail(ctx, CSV_EINVAL, "null request, output or status pointer");
+    DeviceGuard g(ctx->device);
+    std::string err;
+    int rc = decode_batch_static(ctx->device, ds->d, d_reqs, n, d_out, d_status, (cudaStream_t)stream, err);
+    return rc ? fail(ctx, rc, err) : CSV_OK;
+}
+
 int csv_decode_image(csv_ctx* ctx, const uint8_t* image, size_t len, uint32_t lod, uint64_t* out, uint32_t* status) {
     if (!ctx || !out) return CSV_EINVAL;
     DeviceGuard g(ctx->device);

@@ -103,6 +103,9 @@ int encode_device(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W
 int encoder_to_dataset(EncoderState* s, DeviceDataset& d, std::string& err);
 const uint8_t* encoder_image(EncoderState* s, size_t* len);
 
+int decode_batch_static(int device, const DeviceDataset& ds, const csv_request* d_reqs, uint32_t n, uint64_t* d_out,
+                        uint32_t* d_status, cudaStream_t st, std::string& err);
+
 cudaError_t launch_render(const csv_camera& cam, uint32_t W, uint32_t H, float grid, uint32_t bs, uint32_t bpa,
                           const csv_brick_slot* slots, uint64_t n_slots, const uint64_t* labels, const uint64_t* hidden,
                           uint32_t n_hidden, uint64_t* out_label, float* out_depth, uint32_t* requests,

@@ -87,6 +87,7 @@ def load_library() -> C.CDLL:
     L.csv_close.argtypes = [vp]
     L.csv_decode_batch.argtypes = [vp, vp, vp, C.c_uint32, vp, vp, vp]
     L.csv_decode_image.argtypes = [vp, u8p, C.c_size_t, C.c_uint32, u64p, u32p]
+    L.csv_decode_batch_static.argtypes = [vp, vp, vp, C.c_uint32, vp, vp, vp]
     L.csv_render.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_float, C.c_uint32, C.c_uint32, vp, C.c_uint64, vp,
                              vp, C.c_uint32, vp, vp, vp, vp]
     L.csv_synth_volume.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_uint32, C.c_uint32,
@@ -240,6 +241,15 @@ class Codec:
         self._check(self.lib.csv_decode_batch(self.handle, ds.handle, C.c_void_p(d_reqs.data_ptr()), n,
                                               C.c_void_p(d_out.data_ptr()), C.c_void_p(d_status.data_ptr()),
                                               C.c_void_p(_stream_handle(stream))))
+
+    def decode_batch_static(self, ds: Dataset, d_reqs, d_out, d_status, stream=None, n: int | None = None):
+        """csv_decode_batch_static: the same decode with no allocation; its scratch is the library's fixed
+        device array (see include/csv.h), so calls that overlap on the GPU race."""
+        if n is None:
+            n = d_reqs.numel() * d_reqs.element_size() // 16
+        self._check(self.lib.csv_decode_batch_static(self.handle, ds.handle, C.c_void_p(d_reqs.data_ptr()), n,
+                                                     C.c_void_p(d_out.data_ptr()), C.c_void_p(d_status.data_ptr()),
+                                                     C.c_void_p(_stream_handle(stream))))
 
     def decode_image(self, image: bytes, lod: int, check: bool = True):
         """Host .csbd bytes -> (labels (numBricks, 8^lod) uint64, status (numBricks,) uint32)."""

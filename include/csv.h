@@ -126,6 +126,25 @@ void csv_close(csv_dataset* ds);
 int csv_decode_batch(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_reqs, uint32_t n,
                      uint64_t* d_out, uint32_t* d_status, void* stream);
 
+/* No counterpart in the reference.  csv_decode_batch without any allocation,
+ * for callers that cannot call cudaMalloc when they decode: render or serving
+ * loops that must not stall the device (cudaMalloc can synchronize it), and
+ * hosts that route all device memory through their own arena.  The decode
+ * scratch (op records, active-node lists, the work-queue counter) lives in one
+ * file-scope device array of CSV_STATIC_SCRATCH_BYTES that every GPU loading
+ * this library reserves until the process exits; the caller still passes the
+ * dataset, requests, outputs and status words.  The array holds as many
+ * concurrent bricks as fit (47 for 64^3 bricks), so large batches run slower
+ * than with csv_decode_batch; a brick size whose per-CTA scratch exceeds the
+ * array is rejected with CSV_ERANGE.  The first call on a device looks up the
+ * array's device address with that device current (make that first call
+ * before any stream capture).  Every call shares the one array and leaves its
+ * contents behind: calls that overlap on the GPU (other streams, other host
+ * threads) race and must be serialized by the caller. */
+#define CSV_STATIC_SCRATCH_BYTES (64u << 20)
+int csv_decode_batch_static(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_reqs, uint32_t n,
+                            uint64_t* d_out, uint32_t* d_status, void* stream);
+
 /* Host convenience over the above, as main.cpp:86-118 uses the reference
  * decoder: parse `image`, decode every brick at `lod` and copy the labels to
  * the host (brick i at out + i*8^lod).  status: numBricks words or NULL. */
