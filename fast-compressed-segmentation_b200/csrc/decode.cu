@@ -56,7 +56,10 @@ constexpr uint32_t kMaskWords = moff(kDecLevels);    // 1172
 template <class V>
 struct DecShared {
     uint32_t lut[kTot];
-    V val[kValEntries];
+    // During the rANS phase the level arrays (val, mask, pre: contiguous) are
+    // idle: the brick's compressed stream is staged over them by one bulk
+    // (TMA) copy when it fits (stage_cap bytes).
+    alignas(16) V val[kValEntries];
     uint32_t mask[kMaskWords];
     uint16_t pre[kMaskWords];
     uint64_t pal[kPalCache];
@@ -64,7 +67,46 @@ struct DecShared {
     BrickDesc br;
     csv_request req;
     uint32_t work, status;
+    alignas(8) uint64_t bar;  // mbarrier of the stream copy
 };
+template <class V>
+__host__ __device__ constexpr uint32_t stage_cap() {
+    return (uint32_t)(sizeof(V) * kValEntries + 6 * kMaskWords) & ~15u;
+}
+static_assert((sizeof(uint16_t) * kValEntries) % 16 == 0, "mask follows val without padding");
+
+// ---- bulk copy global -> shared with an mbarrier (cp.async.bulk, sm_90+)
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// Issue one bulk copy of `bytes` (multiple of 16, 16-byte aligned ends) into shared memory.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+// Wait for the barrier phase `parity` to complete; gives up after a bounded number of polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t a = smem_addr(bar);
+#pragma unroll 1
+    for (uint32_t it = 0; it < (1u << 22); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
 
 // ------------------------------------------------------------------ LUT
 // findSymbol (brickDecoding.cpp:126-135) over the loaded 16-entry cumulative
@@ -79,14 +121,16 @@ cudaError_t build_lut(const uint32_t* freq, const uint32_t* cum, uint32_t* h_lut
 }
 
 // One rANS decode step (ransDecodeSymbol, brickDecoding.cpp:137-151), totalFreq
-// 4096 so % and / are a mask and a shift.
+// 4096 so % and / are a mask and a shift.  GLOBAL: enc is global memory (read
+// through the non-coherent path); otherwise a generic pointer (shared staging).
+template <bool GLOBAL = true>
 __device__ __forceinline__ uint32_t rans_step(uint32_t& x, uint32_t& pos, const uint8_t* __restrict__ enc,
                                               const uint32_t* __restrict__ lut) {
     uint32_t v = x & (kTot - 1);
     uint32_t e = lut[v];
     uint32_t f = (e >> 4) & 0x1FFFu, st = e >> 17;
     x = f * (x >> kTotBits) + v - st;
-    while (x < kRansL && pos > 0) x = (x << 8) | __ldg(enc + (--pos));
+    while (x < kRansL && pos > 0) x = (x << 8) | (GLOBAL ? __ldg(enc + (--pos)) : enc[--pos]);
     return e & 15u;
 }
 
@@ -304,6 +348,71 @@ __device__ __forceinline__ uint64_t label_of(const uint64_t* pal, uint32_t pidx,
     return pidx == label0 ? 0ull : pal[pidx];
 }
 
+// Step 1: every thread decodes seek segments of the brick (S ops each) into op
+// records.  One rANS step per iteration; a Pd op's delta nibble is its own
+// iteration, so the lanes of a warp never differ in steps per iteration.
+template <bool GLOBAL>
+__device__ __forceinline__ void decode_segments(const DecodeArgs& A, const BrickDesc& br, const uint8_t* enc,
+                                                const uint32_t* lut, uint32_t n_need, uint32_t nseg,
+                                                uint32_t* __restrict__ recs, uint32_t& st, uint32_t LABEL0) {
+    for (uint32_t k = threadIdx.x; k < nseg; k += blockDim.x) {
+        const Checkpoint c = A.ck[br.ck_off + k];
+        uint32_t x = c.state, pos = c.pos, sym = c.sym, ip = c.ip;
+        uint32_t j = k * A.S;  // a multiple of 4 (S is)
+        const uint32_t jend = min(j + A.S, n_need);
+        uint32_t pd_stop = 0xFFFFFFFFu;  // != ~0: the primary nibble of a Pd op was read
+        // records leave in 16-byte groups: lanes write different segments, so a
+        // 4-byte store per op would cost one memory transaction per lane per op
+        uint32_t q0 = 0, q1 = 0, q2 = 0, q3 = 0;
+        while (j < jend) {
+            if (sym >= br.nsym) {
+                st |= CSV_BRICK_TRUNCATED;
+                if (pd_stop != 0xFFFFFFFFu) {  // Pd without its delta: delta 0
+                    uint32_t pidx = ip - 1;
+                    if (pidx >= br.P) { pidx = br.P - 1; st |= CSV_BRICK_PALETTE; }
+                    q0 = q1; q1 = q2; q2 = q3;
+                    q3 = OP_PD | pd_stop | (pidx << REC_PIDX_SHIFT);
+                    ++j;
+                }
+                break;
+            }
+            const uint32_t v = rans_step<GLOBAL>(x, pos, enc, lut);
+            ++sym;
+            uint32_t rec;
+            if (pd_stop != 0xFFFFFFFFu) {
+                uint32_t pidx = ip - v - 1;
+                if (pidx >= br.P) { pidx = br.P - 1; st |= CSV_BRICK_PALETTE; }
+                rec = OP_PD | pd_stop | (pidx << REC_PIDX_SHIFT);
+                pd_stop = 0xFFFFFFFFu;
+            } else {
+                const uint32_t code = v >> 1;
+                if (code == OP_PD) {
+                    pd_stop = (v & 1u) << 3;
+                    continue;
+                }
+                uint32_t pidx = 0;
+                if (code == OP_PA || code == OP_P0) {
+                    ip += (code == OP_PA);
+                    pidx = ip;
+                    if (pidx >= br.P) { pidx = br.P - 1; st |= CSV_BRICK_PALETTE; }
+                } else if (code == 7) {
+                    pidx = LABEL0;
+                    st |= CSV_BRICK_BADOP;
+                }
+                rec = code | ((v & 1u) << 3) | (pidx << REC_PIDX_SHIFT);
+            }
+            q0 = q1; q1 = q2; q2 = q3; q3 = rec;
+            ++j;
+            if ((j & 3u) == 0) reinterpret_cast<uint4*>(recs + j - 4)[0] = make_uint4(q0, q1, q2, q3);
+        }
+        // the last partial group (segment end or truncation): q3 is record j-1, q2 is j-2, ...
+        const uint32_t rem = j & 3u;
+        if (rem >= 1) recs[j - 1] = q3;
+        if (rem >= 2) recs[j - 2] = q2;
+        if (rem >= 3) recs[j - 3] = q1;
+    }
+}
+
 // V = uint16_t when every palette of the dataset has fewer than 65535 entries
 // (value 0xFFFF stands for "label 0"), else uint32_t (one CTA per SM).
 template <class V>
@@ -314,6 +423,9 @@ __global__ void __launch_bounds__(kDecThreads) decode_kernel(DecodeArgs A) {
     constexpr uint32_t LABEL0 = sizeof(V) == 2 ? 0xFFFFu : PIDX_LABEL0;
 
     for (uint32_t i = tid; i < kTot; i += T) S.lut[i] = A.lut[i];
+    if (tid == 0) mbar_init(&S.bar);
+    uint32_t phase = 0;     // parity of the stream-copy barrier
+    bool stage_ok = true;   // cleared if a copy ever fails to land
 
     // per-CTA scratch: op records | active-node lists of every parent level
     uint8_t* scr = A.scratch + (uint64_t)blockIdx.x * A.scratch_per_cta;
@@ -341,6 +453,10 @@ __global__ void __launch_bounds__(kDecThreads) decode_kernel(DecodeArgs A) {
             continue;
         }
         const BrickDesc br = S.br;
+        // stage the compressed stream in shared memory (one bulk copy) while the palette loads
+        const uint32_t E16 = (br.E + 15u) & ~15u;
+        const bool stage = stage_ok && t > 0 && !(br.flags & BF_UNIFORM) && E16 >= 16 && E16 <= stage_cap<V>();
+        if (stage && tid == 0) bulk_copy_g2s(S.val, A.enc + br.enc_off, E16, &S.bar);
         uint64_t* out = A.out + req.dst;
         const uint64_t* gpal = A.pal + br.pal_off;
         const uint64_t* pal = gpal;
@@ -360,54 +476,21 @@ __global__ void __launch_bounds__(kDecThreads) decode_kernel(DecodeArgs A) {
             // register copy of the descriptor would put it on the stack)
             const uint32_t n_need = min(min(S.br.level_start[t], br.n_ops), br.ck_cap * A.S);
             const uint32_t nseg = (n_need + A.S - 1) / A.S;
-            const uint8_t* enc = A.enc + br.enc_off;
-            for (uint32_t k = tid; k < nseg; k += T) {
-                const Checkpoint c = A.ck[br.ck_off + k];
-                uint32_t x = c.state, pos = c.pos, sym = c.sym, ip = c.ip;
-                uint32_t j = k * A.S;
-                const uint32_t jend = min(j + A.S, n_need);
-                // one rANS step per iteration; a Pd op's delta nibble is its own
-                // iteration, so lanes never differ in steps per iteration
-                uint32_t pd_stop = 0xFFFFFFFFu;  // != ~0: the primary nibble of a Pd op was read
-                while (j < jend) {
-                    if (sym >= br.nsym) {
-                        st |= CSV_BRICK_TRUNCATED;
-                        if (pd_stop != 0xFFFFFFFFu) {  // Pd without its delta: delta 0
-                            uint32_t pidx = ip - 1;
-                            if (pidx >= br.P) { pidx = br.P - 1; st |= CSV_BRICK_PALETTE; }
-                            recs[j] = OP_PD | pd_stop | (pidx << REC_PIDX_SHIFT);
-                        }
-                        break;
-                    }
-                    const uint32_t v = rans_step(x, pos, enc, S.lut);
-                    ++sym;
-                    uint32_t rec;
-                    if (pd_stop != 0xFFFFFFFFu) {
-                        uint32_t pidx = ip - v - 1;
-                        if (pidx >= br.P) { pidx = br.P - 1; st |= CSV_BRICK_PALETTE; }
-                        rec = OP_PD | pd_stop | (pidx << REC_PIDX_SHIFT);
-                        pd_stop = 0xFFFFFFFFu;
-                    } else {
-                        const uint32_t code = v >> 1;
-                        if (code == OP_PD) {
-                            pd_stop = (v & 1u) << 3;
-                            continue;
-                        }
-                        uint32_t pidx = 0;
-                        if (code == OP_PA || code == OP_P0) {
-                            ip += (code == OP_PA);
-                            pidx = ip;
-                            if (pidx >= br.P) { pidx = br.P - 1; st |= CSV_BRICK_PALETTE; }
-                        } else if (code == 7) {
-                            pidx = LABEL0;
-                            st |= CSV_BRICK_BADOP;
-                        }
-                        rec = code | ((v & 1u) << 3) | (pidx << REC_PIDX_SHIFT);
-                    }
-                    recs[j] = rec;
-                    ++j;
+            bool staged = false;
+            if (stage) {
+                staged = mbar_wait(&S.bar, phase);
+                phase ^= 1u;
+                if (!staged) {  // the copy did not land in time: read this brick from global memory
+                    st |= CSV_BRICK_TIMEOUT;
+                    stage_ok = false;
                 }
             }
+            if (staged)
+                decode_segments<false>(A, br, reinterpret_cast<const uint8_t*>(S.val), S.lut, n_need, nseg, recs,
+                                       st, LABEL0);
+            else
+                decode_segments<true>(A, br, A.enc + br.enc_off, S.lut, n_need, nseg, recs, st, LABEL0);
+            __syncthreads();  // the staged stream is dead: its space becomes the level arrays
             // level 0: the root, value palette[0], active; clear the other masks
             for (uint32_t i = tid; i < moff(t); i += T) S.mask[i] = i == 0 ? 1u : 0u;
             if (tid == 0) {
@@ -481,35 +564,47 @@ __global__ void __launch_bounds__(kDecThreads) decode_kernel(DecodeArgs A) {
                     n_act = n_act_c;
                     __syncthreads();
                 } else {
-                    // last level: labels to HBM, 64 bytes per parent
-                    for (uint32_t p = tid; p < n_par; p += T) {
+                    // last level: labels to HBM.  Each thread writes 16 bytes (two
+                    // children) per step so that a warp's store covers 512
+                    // contiguous bytes.  Stop-filled parents: chunk q is children
+                    // 2q, 2q+1 of parent q / 4.
+                    const uint32_t n_chunk = 4 * n_par;
+                    for (uint32_t q = tid; q < n_chunk; q += T) {
+                        const uint32_t p = q >> 2;
                         if (!is_active(Vw, p)) {
                             const uint64_t x = label_of(pal, Vw.val[p], LABEL0);
-                            uint64_t* o8 = out + 8ull * p;
+                            uint64_t* o2 = out + 2ull * q;
                             if (vec) {
-#pragma unroll
-                                for (int c = 0; c < 8; c += 2) st_cs_v2(o8 + c, x, x);
+                                st_cs_v2(o2, x, x);
                             } else {
-#pragma unroll
-                                for (int c = 0; c < 8; ++c) o8[c] = x;
+                                o2[0] = x;
+                                o2[1] = x;
                             }
                         }
                     }
-                    for (uint32_t r = tid; r < n_act; r += T) {
-                        const uint32_t p = act_l[r];
-                        uint32_t rec[8];
-                        get_rec8(Vw, r, rec);
-                        uint64_t* o8 = out + 8ull * p;
-#pragma unroll
-                        for (uint32_t c = 0; c < 8; c += 2) {
-                            const uint64_t a = label_of(pal, resolve(Vw, rec[c], 8 * p + c, lc, &bad), LABEL0);
-                            const uint64_t b = label_of(pal, resolve(Vw, rec[c + 1], 8 * p + c + 1, lc, &bad), LABEL0);
-                            if (vec) {
-                                st_cs_v2(o8 + c, a, b);
-                            } else {
-                                o8[c] = a;
-                                o8[c + 1] = b;
-                            }
+                    // active parents: four lanes per parent, two children each
+                    const uint32_t sub = tid & 3u;
+                    for (uint32_t g = tid >> 2; g < n_act; g += T >> 2) {
+                        const uint32_t p = act_l[g];
+                        const uint32_t i0 = Vw.o + 8 * g + 2 * sub;
+                        uint32_t r0, r1;
+                        if ((i0 & 1u) == 0 && i0 + 2 <= Vw.n_rec) {
+                            const uint2 rr = *reinterpret_cast<const uint2*>(Vw.rec + i0);
+                            r0 = rr.x;
+                            r1 = rr.y;
+                        } else {
+                            r0 = get_rec(Vw, i0);
+                            r1 = get_rec(Vw, i0 + 1);
+                        }
+                        const uint32_t n0 = 8 * p + 2 * sub;
+                        const uint64_t a = label_of(pal, resolve(Vw, r0, n0, lc, &bad), LABEL0);
+                        const uint64_t b = label_of(pal, resolve(Vw, r1, n0 + 1, lc, &bad), LABEL0);
+                        uint64_t* o2 = out + n0;
+                        if (vec) {
+                            st_cs_v2(o2, a, b);
+                        } else {
+                            o2[0] = a;
+                            o2[1] = b;
                         }
                     }
                 }
