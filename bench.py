@@ -1,13 +1,18 @@
 """Benchmark of the B200 compressed-segmentation-volume codec.
 
-Headline (value): bit-exact batched brick decode throughput in Gvox/s, with
-its %HBM roofline, on the neurite-like workload: a 512^3 uint64 volume of 400
-cubic-spline tubes (radius 2-12 voxels) over a 3000-cell Voronoi background
-with ~15% label 0, 64^3 bricks (512 bricks), every brick decoded at full
-resolution.  One step = one csv_decode_batch launch over all 512 bricks from
-the HBM-resident compressed dataset.  The same line carries the GPU encode
-throughput (Mvox/s) next to the reference CPU encoder, and the end-to-end
-number through the C ABI with host buffers.
+Headline (value): bit-exact batched brick decode throughput in Gvox/s and its
+%HBM roofline on the uneven-batch workload `mixed1024`: a 1024^3 uint64
+volume whose x < 512 half is smooth Voronoi (2000 cells) stored in 32^3 bricks
+and whose x >= 512 half is dense tubes (5000 splines, radius 1-4) over it,
+stored in 64^3 bricks -- two .csbd images (one brick size per file), 16384 +
+2048 bricks, decoded at full resolution in ONE launch (csv_dataset_concat),
+captured in a CUDA graph with the configuration the autotuner picks.  One step
+= one graph replay (8 GiB of labels written).
+
+The same JSON line carries, on the neurite-like workload `neurite512` (512^3,
+400 tubes of radius 2-12 over 3000 Voronoi cells, 64^3 bricks): GPU encode
+Mvox/s against the reference encoder compiled from its sources and run on the
+host (bytes compared), and that workload's decode throughput.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -30,8 +35,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "fast-compressed-segmentation_b200"))
 
 METRIC = "bit-exact decode Gvox/s & %HBM peak; encode Mvox/s vs CPU; p99 frame ms"
-WORKLOAD = dict(name="neurite512_b64", shape=(512, 512, 512), brick=64, kind=1, n_cells=3000, n_tubes=400,
-                r_min=2.0, r_max=12.0, zero_frac=0.15, seed=2)
+MIXED = dict(name="mixed1024", shape=(1024, 1024, 1024), kind=2, n_cells=2000, n_tubes=5000, r_min=1.0, r_max=4.0,
+             zero_frac=0.0, seed=3, split_x=512, brick_left=32, brick_right=64)
+NEURITE = dict(name="neurite512", shape=(512, 512, 512), brick=64, kind=1, n_cells=3000, n_tubes=400, r_min=2.0,
+               r_max=12.0, zero_frac=0.15, seed=2)
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -84,11 +91,7 @@ class Clocks:
                 "samples": len(self.samples)}
 
 
-def flush_l2(buf):
-    buf.add_(1)  # 256 MiB read+write, larger than the 126 MB L2
-
-
-def dist_setup(args):
+def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -116,94 +119,132 @@ def barrier(pg):
         pg.barrier()
 
 
-def cpu_reference(vol_np: np.ndarray, brick: int, gpu_image: bytes):
-    """The reference encoder and decoder on the host cores (1 thread: the reference is single-threaded)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    from oracle import REF_SO, Oracle, Reference
-    nvox = int(np.prod(vol_np.shape))
-    if os.path.exists(REF_SO):
-        R = Reference()
-        t0 = time.perf_counter()
-        img, tm = R.encode(vol_np, brick, timings=True)
-        enc_s = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        _, st, dtm = R.decode_all_full(img, brick, keep=False)
-        dec_s = time.perf_counter() - t0
-        kind = "reference"
-    else:
-        O = Oracle()
-        t0 = time.perf_counter()
-        img = O.encode(vol_np, brick)
-        enc_s = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        O.decode_image(img, brick.bit_length() - 1)
-        dec_s = time.perf_counter() - t0
-        kind = "port"
-    return {"kind": kind, "encode_s": enc_s, "decode_s": dec_s, "encode_mvox_s": nvox / enc_s / 1e6,
-            "decode_gvox_s": nvox / dec_s / 1e9, "bytes_identical": img == gpu_image}
+def morton_table(b, device):
+    import torch
+    idx = torch.arange(b, device=device)
+    m = torch.zeros((b, b, b), dtype=torch.int64, device=device)
+    for bit in range(10):
+        m |= ((idx[None, None, :] >> bit) & 1) << (3 * bit)
+        m |= ((idx[None, :, None] >> bit) & 1) << (3 * bit + 1)
+        m |= ((idx[:, None, None] >> bit) & 1) << (3 * bit + 2)
+    return m
+
+
+def check_against_volume(out, off, vol, b):
+    """Full-resolution bricks at out[off...] (split order, Morton inside) equal the source volume."""
+    D, H, W = vol.shape
+    nbx, nby, nbz = -(-W // b), -(-H // b), -(-D // b)
+    m = morton_table(b, vol.device)
+    i = 0
+    for bx in range(nbx):
+        for by in range(nby):
+            for bz in range(nbz):
+                brick = out[off + i * b ** 3: off + (i + 1) * b ** 3]
+                src = vol[bz * b:(bz + 1) * b, by * b:(by + 1) * b, bx * b:(bx + 1) * b]
+                if not bool((brick[m] == src).all()):
+                    return False
+                i += 1
+    return True
+
+
+def image_bricks(img: bytes):
+    """(nSymbols, E) per brick of a .csbd image."""
+    import struct
+    nb = struct.unpack_from("<I", img, 8)[0]
+    o, ns = 152, []
+    for _ in range(nb):
+        P = struct.unpack_from("<I", img, o + 4)[0]
+        o += 8 + 8 * P
+        E = struct.unpack_from("<I", img, o)[0]
+        o += 4 + E
+        ns.append(struct.unpack_from("<I", img, o)[0])
+        o += 4
+    return nb, ns
+
+
+def encode_to_host(codec, vol, b):
+    import torch
+    codec.encode_device(vol, b)
+    torch.cuda.synchronize()
+    return bytes(codec.encoded_image_tensor().cpu().numpy())
+
+
+def time_encode(codec, vol, b, reps=3):
+    import torch
+    s = torch.cuda.current_stream()
+    codec.encode_device(vol, b)
+    ts = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        codec.encode_device(vol, b)
+        e1.record(s)
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return min(ts)
 
 
 def run_b200(args):
+    import ctypes as C
+
     import torch
     from csvb200 import Codec, requests, requests_tensor
 
-    world, rank, local, pg = dist_setup(args)
+    world, rank, local, pg = dist_setup()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     codec = Codec(local)
-    W = WORKLOAD
+    W = MIXED
     D, H, Wd = W["shape"]
-    b = W["brick"]
     nvox = D * H * Wd
-    vol = torch.empty(W["shape"], dtype=torch.int64, device=dev)
-    codec.synth_volume(vol, W["kind"], W["n_cells"], W["n_tubes"], W["r_min"], W["r_max"], W["zero_frac"],
-                       W["seed"])
-    torch.cuda.synchronize()
+    sx = W["split_x"]
+    bl, br = W["brick_left"], W["brick_right"]
 
-    # ---- GPU encode (csv_encode_device), timed on its own
-    stream = torch.cuda.current_stream()
-    for _ in range(max(1, min(2, args.warmup))):
-        img_len = codec.encode_device(vol, b)
-    enc_ms = []
-    for _ in range(3):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        img_len = codec.encode_device(vol, b)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        enc_ms.append(e0.elapsed_time(e1))
-    enc_ms_best = min(enc_ms)
-    img_dev = codec.encoded_image_tensor()
-    n = img_dev.numel()
-    image = bytes(img_dev.cpu().numpy())
-    ds = codec.open_encoded()
-    nb = ds.num_bricks
-    lod = b.bit_length() - 1
-    per = 1 << (3 * lod)
-    reqs = requests_tensor(requests(np.arange(nb), np.full(nb, lod), np.arange(nb, dtype=np.uint64) * per), dev)
-    out = torch.empty(nb * per, dtype=torch.int64, device=dev)
-    status = torch.zeros(nb, dtype=torch.int32, device=dev)
+    # ---- workload: generate, encode both halves on the GPU, open, concatenate
+    vol = torch.empty(W["shape"], dtype=torch.int64, device=dev)
+    codec.synth_volume(vol, W["kind"], W["n_cells"], W["n_tubes"], W["r_min"], W["r_max"], W["zero_frac"], W["seed"])
+    left = vol[:, :, :sx].contiguous()
+    right = vol[:, :, sx:].contiguous()
+    enc_ms_left = time_encode(codec, left, bl)
+    img_left = encode_to_host(codec, left, bl)
+    ds_left = codec.open_encoded()
+    enc_ms_right = time_encode(codec, right, br)
+    img_right = encode_to_host(codec, right, br)
+    ds_right = codec.open_encoded()
+    cat = codec.concat([ds_left, ds_right])
+    nl, nr = ds_left.num_bricks, ds_right.num_bricks
+    n = nl + nr
+    lods = np.array([bl.bit_length() - 1] * nl + [br.bit_length() - 1] * nr)
+    sizes = 8 ** lods.astype(np.uint64)
+    dst = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.uint64)
+    d_reqs = requests_tensor(requests(np.arange(n), lods, dst), dev)
+    out = torch.empty(int(sizes.sum()), dtype=torch.int64, device=dev)
+    status = torch.zeros(n, dtype=torch.int32, device=dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
 
-    # ---- correctness gate on the bench workload: full-resolution decode == source volume
-    codec.decode_batch(ds, reqs, out, status)
+    # ---- autotune (grid, staging, order), capture the winner, check it
+    best, tune_ms = codec.autotune(cat, d_reqs, out, status, reps=3)
+    graph = codec.decode_graph(cat, d_reqs, out, status, best)
+    graph.launch()
     torch.cuda.synchronize()
     assert int(status.abs().max()) == 0, "decode status"
-    check = check_against_volume(out, vol, nb, b, W["shape"])
+    check = (check_against_volume(out, 0, left, bl) and check_against_volume(out, nl * bl ** 3, right, br))
+    del left, right
 
+    stream = torch.cuda.current_stream()
     for _ in range(args.warmup):
-        flush_l2(flush)
-        codec.decode_batch(ds, reqs, out, status)
+        flush.add_(1)
+        graph.launch()
     torch.cuda.synchronize()
     clk = Clocks(local)
     barrier(pg)
     torch.cuda.synchronize()
     times = []
     for _ in range(args.steps):
-        flush_l2(flush)
+        flush.add_(1)  # 256 MiB: the L2 holds nothing of the previous step
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        codec.decode_batch(ds, reqs, out, status)
+        graph.launch(stream)
         e1.record(stream)
         e1.synchronize()
         times.append(e0.elapsed_time(e1))
@@ -213,98 +254,166 @@ def run_b200(args):
     ms = statistics.mean(times)
     ms_max = max_over_ranks(ms, pg, dev)
     value = world * nvox / (ms_max * 1e-3) / 1e9
-
-    info = ds.info
-    alg_bytes = info.stream_bytes + 8 * info.palette_entries + 16 * nb + 8 * nb * per
+    info = cat.info
+    alg_bytes = info.stream_bytes + 8 * info.palette_entries + 16 * n + 8 * int(sizes.sum())
     hbm, hbm_kind = peaks()
     achieved = alg_bytes / (ms * 1e-3) / 1e9
-    traffic = load_traffic("decode_kernel", W["name"])
 
-    # ---- end to end through the C ABI with host buffers (csv_decode_image: open + seek index + decode + D2H)
-    host_img = np.frombuffer(image, np.uint8)
+    # ---- end to end through the C ABI with host buffers: both images, open + seek index + decode + D2H
+    per_img = [(img_left, bl, nl), (img_right, br, nr)]
+    h_outs = [torch.empty((nb_, b_ ** 3), dtype=torch.int64, pin_memory=True) for _, b_, nb_ in per_img]
+    h_st = [np.zeros(nb_, np.uint32) for _, _, nb_ in per_img]
+    host_imgs = [np.frombuffer(im, np.uint8) for im, _, _ in per_img]
     e2e_ms = []
-    h_out = torch.empty((nb, per), dtype=torch.int64, pin_memory=True)
-    h_st = np.zeros(nb, np.uint32)
-    lib = codec.lib
-    import ctypes as C
-    for k in range(max(2, min(args.steps, 5)) + 1):
+    for k in range(4):
         barrier(pg)
         t0 = time.perf_counter()
-        rc = lib.csv_decode_image(codec.handle, host_img.ctypes.data_as(C.POINTER(C.c_uint8)), len(image), lod,
-                                  C.cast(h_out.data_ptr(), C.POINTER(C.c_uint64)),
-                                  h_st.ctypes.data_as(C.POINTER(C.c_uint32)))
+        for j, (im, b_, nb_) in enumerate(per_img):
+            rc = codec.lib.csv_decode_image(codec.handle, host_imgs[j].ctypes.data_as(C.POINTER(C.c_uint8)), len(im),
+                                            b_.bit_length() - 1, C.cast(h_outs[j].data_ptr(), C.POINTER(C.c_uint64)),
+                                            h_st[j].ctypes.data_as(C.POINTER(C.c_uint32)))
+            assert rc == 0, codec.lib.csv_last_error(codec.handle)
         t1 = time.perf_counter()
-        assert rc == 0, codec.lib.csv_last_error(codec.handle)
         if k > 0:
             e2e_ms.append((t1 - t0) * 1e3)
-    e2e_best = max_over_ranks(statistics.mean(e2e_ms), pg, dev)
-    e2e = {"value": world * nvox / (e2e_best * 1e-3) / 1e9, "unit": "Gvox/s", "h2d_bytes_per_step": len(image),
-           "d2h_bytes_per_step": 8 * nb * per + 4 * nb, "ms_per_step": e2e_best,
-           "path": "csv_decode_image: host .csbd -> open (H2D, seek index) -> decode -> D2H labels"}
-    e2e_ok = bool(np.array_equal(h_out.numpy().view(np.uint64).reshape(-1),
-                                 out.cpu().numpy().view(np.uint64)))
+    e2e_t = max_over_ranks(statistics.mean(e2e_ms), pg, dev)
+    e2e_ok = bool(torch.equal(h_outs[0].view(-1).to(dev), out[: nl * bl ** 3]) and
+                  torch.equal(h_outs[1].view(-1).to(dev), out[nl * bl ** 3:]))
+    e2e = {"value": round(world * nvox / (e2e_t * 1e-3) / 1e9, 3), "unit": "Gvox/s",
+           "h2d_bytes_per_step": len(img_left) + len(img_right), "d2h_bytes_per_step": 8 * nvox + 4 * n,
+           "ms_per_step": round(e2e_t, 2),
+           "path": "csv_decode_image per image: host .csbd -> open (H2D, seek index) -> decode -> D2H labels"}
+    del h_outs
+
+    # ---- neurite512: encode vs the reference encoder on this host, and its decode
+    neur = neurite512(codec, dev, args, rank == 0 and world == 1 and not args.no_cpu)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        vol_np = vol.cpu().numpy().view(np.uint64)
-        ref = cpu_reference(vol_np, b, image)
-        cpu = {"value": ref["decode_gvox_s"], "unit": "Gvox/s", "cores": 1, "kind": ref["kind"],
-               "sample": f"whole workload ({nb} bricks, {nvox} voxels): splitGridIntoBricks+compressDataset+"
-                         f"saveDatasetToFile then decodeRansStream+decodeBrick<64> for every brick, 1 thread",
-               "encode_mvox_s": ref["encode_mvox_s"], "encode_s": ref["encode_s"], "decode_s": ref["decode_s"],
-               "encode_bytes_identical": ref["bytes_identical"]}
+        cpu = cpu_decode_sample(img_left, img_right, bl, br)
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "Gvox/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": W["name"], "volume": list(W["shape"][::-1]), "brick": b, "bricks": nb,
-                       "lod": lod, "tubes": W["n_tubes"], "radius": [W["r_min"], W["r_max"]],
-                       "voronoi_cells": W["n_cells"], "zero_frac": W["zero_frac"], "seed": W["seed"],
+            "config": {"workload": W["name"], "volume": [Wd, H, D],
+                       "bricks": {"32^3": nl, "64^3": nr, "split_x": sx},
+                       "left": f"Voronoi {W['n_cells']} cells, 32^3 bricks",
+                       "right": f"{W['n_tubes']} tubes r {W['r_min']}-{W['r_max']} over it, 64^3 bricks",
+                       "lod": "full resolution", "seed": W["seed"], "launch": "one CUDA graph (csv_decode_graph)",
+                       "autotuned": best.as_dict(), "autotune_ms": round(tune_ms, 4),
+                       "stream_bytes": info.stream_bytes, "image_bytes": [len(img_left), len(img_right)],
                        "l2": "flushed between timed steps (256 MiB buffer)",
                        "parallelism": f"weak x{world}, bricks independent, no collective"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-                         "frac": round(achieved / hbm, 4), "traffic": traffic,
+                         "frac": round(achieved / hbm, 4), "traffic": load_traffic("decode_kernel", W["name"]),
                          "algorithmic_bytes": alg_bytes, "peak_kind": hbm_kind},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": args.steps,
             "clocks": clocks,
-            "encode": {"value": round(nvox / (enc_ms_best * 1e-3) / 1e6, 1), "unit": "Mvox/s",
-                       "ms": round(enc_ms_best, 3), "image_bytes": n,
-                       "speedup_vs_cpu": (round(nvox / (enc_ms_best * 1e-3) / 1e6 / cpu["encode_mvox_s"], 1)
-                                          if cpu else None),
-                       "bytes_identical_to_reference": cpu["encode_bytes_identical"] if cpu else None},
+            "encode": {"value": round(nvox / ((enc_ms_left + enc_ms_right) * 1e-3) / 1e6, 1), "unit": "Mvox/s",
+                       "ms": round(enc_ms_left + enc_ms_right, 3), "workload": W["name"]},
+            "neurite512": neur,
             "checks": {"decode_equals_source": check, "e2e_equals_device": e2e_ok},
         }
         print(json.dumps(line))
-    ds.close()
+    graph.close()
+    cat.close()
+    ds_left.close()
+    ds_right.close()
     if pg is not None:
         pg.destroy_process_group()
 
 
-def check_against_volume(out, vol, nb, b, shape):
-    """Full-resolution decode equals the source volume (bricks in split order, Morton order inside)."""
+def neurite512(codec, dev, args, with_cpu):
+    """GPU encode (timed), bytes vs the reference encoder, full-resolution decode throughput."""
     import torch
-    D, H, W = shape
-    nbx, nby, nbz = -(-W // b), -(-H // b), -(-D // b)
-    idx = torch.arange(b, device=out.device)
-    m = torch.zeros((b, b, b), dtype=torch.int64, device=out.device)
-    for bit in range(10):
-        m |= ((idx[None, None, :] >> bit) & 1) << (3 * bit)
-        m |= ((idx[None, :, None] >> bit) & 1) << (3 * bit + 1)
-        m |= ((idx[:, None, None] >> bit) & 1) << (3 * bit + 2)
-    bricks = out.view(nb, b ** 3)
-    i = 0
-    for bx in range(nbx):
-        for by in range(nby):
-            for bz in range(nbz):
-                src = vol[bz * b:(bz + 1) * b, by * b:(by + 1) * b, bx * b:(bx + 1) * b]
-                if not torch.equal(bricks[i][m], src):
-                    return False
-                i += 1
-    return True
+    from csvb200 import requests, requests_tensor
+    W = NEURITE
+    b = W["brick"]
+    vol = torch.empty(W["shape"], dtype=torch.int64, device=dev)
+    codec.synth_volume(vol, W["kind"], W["n_cells"], W["n_tubes"], W["r_min"], W["r_max"], W["zero_frac"], W["seed"])
+    nvox = vol.numel()
+    enc_ms = time_encode(codec, vol, b)
+    image = encode_to_host(codec, vol, b)
+    ds = codec.open_encoded()
+    nb = ds.num_bricks
+    per = b ** 3
+    d_reqs = requests_tensor(requests(np.arange(nb), np.full(nb, 6), np.arange(nb, dtype=np.uint64) * per), dev)
+    out = torch.empty(nb * per, dtype=torch.int64, device=dev)
+    st = torch.zeros(nb, dtype=torch.int32, device=dev)
+    graph = codec.decode_graph(ds, d_reqs, out, st)
+    graph.launch()
+    torch.cuda.synchronize()
+    ok = check_against_volume(out, 0, vol, b)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    ts = []
+    s = torch.cuda.current_stream()
+    for k in range(args.warmup + 20):
+        flush.add_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        graph.launch(s)
+        e1.record(s)
+        e1.synchronize()
+        if k >= args.warmup:
+            ts.append(e0.elapsed_time(e1))
+    dec_ms = statistics.mean(ts)
+    res = {"volume": list(W["shape"][::-1]), "bricks": nb, "brick": b, "tubes": W["n_tubes"],
+           "radius": [W["r_min"], W["r_max"]], "voronoi_cells": W["n_cells"], "zero_frac": W["zero_frac"],
+           "decode_gvox_s": round(nvox / (dec_ms * 1e-3) / 1e9, 2), "decode_ms": round(dec_ms, 4),
+           "decode_equals_source": ok, "encode_mvox_s": round(nvox / (enc_ms * 1e-3) / 1e6, 1),
+           "encode_ms": round(enc_ms, 3), "image_bytes": len(image)}
+    graph.close()
+    ds.close()
+    if with_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        from oracle import REF_SO, Oracle, Reference
+        vol_np = vol.cpu().numpy().view(np.uint64)
+        del vol
+        if os.path.exists(REF_SO):
+            t0 = time.perf_counter()
+            ref_img = Reference().encode(vol_np, b)
+            kind = "reference"
+        else:
+            t0 = time.perf_counter()
+            ref_img = Oracle().encode(vol_np, b)
+            kind = "port"
+        cpu_s = time.perf_counter() - t0
+        res["cpu_encode"] = {"kind": kind, "cores": 1, "seconds": round(cpu_s, 3),
+                             "mvox_s": round(nvox / cpu_s / 1e6, 2),
+                             "sample": "whole neurite512 volume: splitGridIntoBricks + compressDataset + "
+                                       "saveDatasetToFile, 1 thread"}
+        res["encode_speedup_vs_cpu"] = round(res["encode_mvox_s"] / res["cpu_encode"]["mvox_s"], 1)
+        res["bytes_identical_to_reference"] = ref_img == image
+    return res
+
+
+def cpu_decode_sample(img_left, img_right, bl, br, n_left=2048, n_right=256):
+    """The reference decoder (decodeRansStream + decodeBrick<b>, 1 thread) on the first bricks of each image."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import REF_SO, Oracle, Reference
+    if os.path.exists(REF_SO):
+        R = Reference()
+        t0 = time.perf_counter()
+        _, st1, _ = R.decode_all_full(img_left, bl, max_bricks=n_left, keep=False)
+        _, st2, _ = R.decode_all_full(img_right, br, max_bricks=n_right, keep=False)
+        s = time.perf_counter() - t0
+        kind = "reference"
+    else:
+        O = Oracle()
+        t0 = time.perf_counter()
+        O.decode_image(img_left, bl.bit_length() - 1)
+        O.decode_image(img_right, br.bit_length() - 1)
+        s = time.perf_counter() - t0
+        kind, n_left, n_right = "port", image_bricks(img_left)[0], image_bricks(img_right)[0]
+    vox = n_left * bl ** 3 + n_right * br ** 3
+    return {"value": round(vox / s / 1e9, 5), "unit": "Gvox/s", "cores": 1, "kind": kind,
+            "sample": f"{n_left} 32^3 bricks + {n_right} 64^3 bricks of the mixed1024 images at full resolution "
+                      f"({vox} voxels), decodeRansStream + decodeBrick<b>, 1 thread",
+            "seconds": round(s, 3)}
 
 
 def load_traffic(kernel: str, workload: str):
@@ -316,59 +425,61 @@ def load_traffic(kernel: str, workload: str):
 
 
 def run_reference(args):
-    """The reference's own CPU decoder (oracle/_ref: decodeRansStream + decodeBrick<64>), all host threads."""
+    """The reference's own CPU decoder (oracle/_ref: decodeRansStream + decodeBrick<b>) on every host thread."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     import torch
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    from oracle import REF_SO, Oracle, Reference
-    W = WORKLOAD
-    D, H, Wd = W["shape"]
-    b = W["brick"]
-    nvox = D * H * Wd
     from csvb200 import Codec
+    from oracle import REF_SO, Oracle, Reference
+    W = MIXED
+    D, H, Wd = W["shape"]
+    sx = W["split_x"]
+    bl, br = W["brick_left"], W["brick_right"]
     codec = Codec(0)
     vol = torch.empty(W["shape"], dtype=torch.int64, device="cuda")
-    codec.synth_volume(vol, W["kind"], W["n_cells"], W["n_tubes"], W["r_min"], W["r_max"], W["zero_frac"],
-                       W["seed"])
-    vol_np = vol.cpu().numpy().view(np.uint64)
+    codec.synth_volume(vol, W["kind"], W["n_cells"], W["n_tubes"], W["r_min"], W["r_max"], W["zero_frac"], W["seed"])
+    # the input images: the reference encoder's bytes equal the GPU encoder's (tests/test_encode_gpu.py)
+    img_left = encode_to_host(codec, vol[:, :, :sx].contiguous(), bl)
+    img_right = encode_to_host(codec, vol[:, :, sx:].contiguous(), br)
     del vol
+    nl, nr = image_bricks(img_left)[0], image_bricks(img_right)[0]
     threads = os.cpu_count() or 1
     if os.path.exists(REF_SO):
         R = Reference()
-        image = R.encode(vol_np, b)
         kind = "reference"
 
         def step():
-            bad = R.decode_parallel(image, threads)
-            assert bad == 0
+            assert R.decode_parallel(img_left, threads) == 0
+            assert R.decode_parallel(img_right, threads) == 0
     else:
         O = Oracle()
-        image = O.encode(vol_np, b)
-        kind = "port"
-        threads = 1
+        kind, threads = "port", 1
 
         def step():
-            O.decode_image(image, b.bit_length() - 1)
-    for _ in range(args.warmup):
+            O.decode_image(img_left, bl.bit_length() - 1)
+            O.decode_image(img_right, br.bit_length() - 1)
+    for _ in range(min(args.warmup, 1)):
         step()
     times = []
-    for _ in range(args.steps):
+    for _ in range(min(args.steps, 3)):
         t0 = time.perf_counter()
         step()
         times.append(time.perf_counter() - t0)
     s = statistics.mean(times)
+    nvox = D * H * Wd
     v = nvox / s / 1e9
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": "Gvox/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(s * 1e3, 2), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": {"workload": W["name"], "volume": list(W["shape"][::-1]), "brick": b, "lod": b.bit_length() - 1},
+        "steps": len(times), "warmup": min(args.warmup, 1), "ms_per_step": round(s * 1e3, 2),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": W["name"], "volume": [Wd, H, D], "bricks": {"32^3": nl, "64^3": nr},
+                   "lod": "full resolution"},
         "cpu_baseline": {"value": round(v, 4), "unit": "Gvox/s", "cores": threads, "kind": kind,
-                         "sample": f"every step decodes all {nvox // b ** 3} bricks at full resolution "
-                                   f"(decodeRansStream + decodeBrick<64>), bricks split over {threads} host threads"},
+                         "sample": f"every step decodes all {nl + nr} bricks of both images at full resolution "
+                                   f"(decodeRansStream + decodeBrick<b>), bricks split over {threads} host threads"},
         "e2e": {"value": round(v, 4), "unit": "Gvox/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
@@ -379,7 +490,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline legs")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

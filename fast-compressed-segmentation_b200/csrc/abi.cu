@@ -114,6 +114,7 @@ void free_dataset(DeviceDataset& d) {
     cudaFree(d.d_ck);
     cudaFree(d.d_lut);
     free(d.h_ids);
+    free(d.h_cost);
     d = DeviceDataset();
 }
 
@@ -130,6 +131,7 @@ int stage_dataset(csv_ctx* ctx, const uint8_t* img, const ImageView& v, DeviceDa
     std::vector<BrickDesc> desc(v.nb);
     uint64_t pal_n = 0, enc_n = 0, ck_n = 0;
     d.h_ids = (uint32_t*)malloc(sizeof(uint32_t) * std::max<uint32_t>(1, v.nb));
+    d.h_cost = (uint32_t*)malloc(sizeof(uint32_t) * std::max<uint32_t>(1, v.nb));
     for (uint32_t i = 0; i < v.nb; ++i) {
         const auto& r = v.recs[i];
         BrickDesc& b = desc[i];
@@ -142,8 +144,9 @@ int stage_dataset(csv_ctx* ctx, const uint8_t* img, const ImageView& v, DeviceDa
         b.id = r.id;
         b.ck_off = (uint32_t)ck_n;
         b.ck_cap = (r.nsym + d.S - 1) / d.S + 1;
-        b.flags = BF_NOINDEX;
+        b.flags = BF_NOINDEX | (d.L << BF_LEVELS_SHIFT);
         d.h_ids[i] = r.id;
+        d.h_cost[i] = r.nsym;
         pal_n += r.P;
         enc_n += (r.E + 15) & ~15ull;
         ck_n += b.ck_cap;
@@ -155,6 +158,8 @@ int stage_dataset(csv_ctx* ctx, const uint8_t* img, const ImageView& v, DeviceDa
     for (auto& r : v.recs) d.stream_bytes += r.E;
     d.palette_entries = pal_n;
     d.ck_entries = ck_n;
+    d.enc_pool_bytes = std::max<uint64_t>(16, enc_n);
+    d.pal_pool_entries = std::max<uint64_t>(1, pal_n);
     std::vector<uint64_t> pal(std::max<uint64_t>(1, pal_n));
     std::vector<uint8_t> enc(std::max<uint64_t>(16, enc_n), 0);
     for (uint32_t i = 0; i < v.nb; ++i) {
@@ -432,6 +437,258 @@ int csv_open_encoded(csv_ctx* ctx, csv_dataset** out) {
         return fail(ctx, rc, err);
     }
     *out = ds;
+    return CSV_OK;
+}
+
+int csv_dataset_concat(csv_ctx* ctx, const csv_dataset* const* parts, uint32_t n, csv_dataset** out) {
+    if (!ctx || !parts || !out || n == 0) return CSV_EINVAL;
+    *out = nullptr;
+    DeviceGuard g(ctx->device);
+    uint64_t nb = 0, pal_n = 0, enc_n = 0, ck_n = 0;
+    uint32_t n_models = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        if (!parts[k]) return fail(ctx, CSV_EINVAL, "null part");
+        const DeviceDataset& p = parts[k]->d;
+        if (p.S != kOpsPerCheckpoint) return fail(ctx, CSV_EINVAL, "parts with different seek-index spacing");
+        nb += p.nb;
+        pal_n += p.pal_pool_entries;
+        enc_n += (p.enc_pool_bytes + 15) & ~15ull;
+        ck_n += p.ck_entries;
+        n_models += p.n_models;
+    }
+    if (nb > 0xFFFFFFFFull || ck_n > 0xFFFFFFFFull || n_models > 255)
+        return fail(ctx, CSV_ERANGE, "concatenation too large");
+    csv_dataset* ds = new (std::nothrow) csv_dataset();
+    if (!ds) return fail(ctx, CSV_ENOMEM, "host allocation");
+    ds->ctx = ctx;
+    DeviceDataset& d = ds->d;
+    d.device = ctx->device;
+    d.nb = (uint32_t)nb;
+    d.S = kOpsPerCheckpoint;
+    d.total = kTot;
+    d.n_models = n_models;
+    d.h_ids = (uint32_t*)malloc(sizeof(uint32_t) * std::max<uint64_t>(1, nb));
+    d.h_cost = (uint32_t*)malloc(sizeof(uint32_t) * std::max<uint64_t>(1, nb));
+    d.enc_pool_bytes = std::max<uint64_t>(16, enc_n);
+    d.pal_pool_entries = std::max<uint64_t>(1, pal_n);
+    d.ck_entries = ck_n;
+    std::vector<BrickDesc> all;
+    all.reserve(nb);
+    cudaError_t e;
+    int rc = CSV_OK;
+    if ((e = cudaMalloc(&d.d_bricks, sizeof(BrickDesc) * std::max<uint64_t>(1, nb))) != cudaSuccess ||
+        (e = cudaMalloc(&d.d_pal, 8 * d.pal_pool_entries)) != cudaSuccess ||
+        (e = cudaMalloc(&d.d_enc, d.enc_pool_bytes)) != cudaSuccess ||
+        (e = cudaMalloc(&d.d_ck, sizeof(Checkpoint) * std::max<uint64_t>(1, ck_n))) != cudaSuccess ||
+        (e = cudaMalloc(&d.d_lut, sizeof(uint32_t) * kTot * n_models)) != cudaSuccess) {
+        rc = fail(ctx, CSV_ENOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
+    }
+    uint64_t pal_base = 0, enc_base = 0, ck_base = 0;
+    uint32_t model_base = 0, id_base = 0;
+    for (uint32_t k = 0; k < n && rc == CSV_OK; ++k) {
+        const DeviceDataset& p = parts[k]->d;
+        std::vector<BrickDesc> pb(p.nb);
+        if ((p.nb && (e = cudaMemcpy(pb.data(), p.d_bricks, sizeof(BrickDesc) * p.nb, cudaMemcpyDeviceToHost)) !=
+                         cudaSuccess) ||
+            (e = cudaMemcpy(d.d_pal + pal_base, p.d_pal, 8 * p.pal_pool_entries, cudaMemcpyDeviceToDevice)) !=
+                cudaSuccess ||
+            (e = cudaMemcpy(d.d_enc + enc_base, p.d_enc, p.enc_pool_bytes, cudaMemcpyDeviceToDevice)) != cudaSuccess ||
+            (p.ck_entries && (e = cudaMemcpy(d.d_ck + ck_base, p.d_ck, sizeof(Checkpoint) * p.ck_entries,
+                                             cudaMemcpyDeviceToDevice)) != cudaSuccess) ||
+            (e = cudaMemcpy(d.d_lut + (size_t)kTot * model_base, p.d_lut, sizeof(uint32_t) * kTot * p.n_models,
+                            cudaMemcpyDeviceToDevice)) != cudaSuccess) {
+            rc = cuda_fail(ctx, e, "concat copy");
+            break;
+        }
+        for (BrickDesc& b : pb) {
+            const uint32_t model = ((b.flags >> BF_MODEL_SHIFT) & 255u) + model_base;
+            b.pal_off += pal_base;
+            b.enc_off += enc_base;
+            b.ck_off += (uint32_t)ck_base;
+            b.flags = (b.flags & ~(255u << BF_MODEL_SHIFT)) | (model << BF_MODEL_SHIFT);
+            all.push_back(b);
+        }
+        memcpy(d.h_ids + id_base, p.h_ids, sizeof(uint32_t) * p.nb);
+        memcpy(d.h_cost + id_base, p.h_cost, sizeof(uint32_t) * p.nb);
+        d.b = std::max(d.b, p.b);
+        d.L = std::max(d.L, p.L);
+        d.max_P = std::max(d.max_P, p.max_P);
+        d.max_nsym = std::max(d.max_nsym, p.max_nsym);
+        d.stream_bytes += p.stream_bytes;
+        d.palette_entries += p.palette_entries;
+        if (k == 0) {
+            memcpy(d.freq, p.freq, sizeof d.freq);
+            memcpy(d.cum, p.cum, sizeof d.cum);
+        }
+        pal_base += p.pal_pool_entries;
+        enc_base += (p.enc_pool_bytes + 15) & ~15ull;
+        ck_base += p.ck_entries;
+        model_base += p.n_models;
+        id_base += p.nb;
+    }
+    if (rc == CSV_OK && nb &&
+        (e = cudaMemcpy(d.d_bricks, all.data(), sizeof(BrickDesc) * nb, cudaMemcpyHostToDevice)) != cudaSuccess)
+        rc = cuda_fail(ctx, e, "concat copy");
+    if (rc) {
+        free_dataset(d);
+        delete ds;
+        return rc;
+    }
+    *out = ds;
+    return CSV_OK;
+}
+
+}  // extern "C"
+
+struct csv_graph {
+    csv_ctx* ctx = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint32_t* d_order = nullptr;
+};
+
+namespace {
+
+// Largest-first order of the requests: estimated work = nSymbols of the brick
+// (rANS + replay) + a quarter of the labels written.
+int lpt_order(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_reqs, uint32_t n, uint32_t** d_order) {
+    std::vector<csv_request> h(n);
+    cudaError_t e = cudaMemcpy(h.data(), d_reqs, sizeof(csv_request) * n, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "request copy");
+    std::vector<uint64_t> cost(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        uint64_t c = 0;
+        if (h[i].brick < ds->d.nb && h[i].lod < 8) c = ds->d.h_cost[h[i].brick] + ((1ull << (3 * h[i].lod)) >> 2);
+        cost[i] = c;
+    }
+    std::vector<uint32_t> ord(n);
+    for (uint32_t i = 0; i < n; ++i) ord[i] = i;
+    std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
+    if ((e = cudaMalloc(d_order, sizeof(uint32_t) * std::max<uint32_t>(1, n))) != cudaSuccess)
+        return fail(ctx, CSV_ENOMEM, "order allocation");
+    if ((e = cudaMemcpy(*d_order, ord.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return cuda_fail(ctx, e, "order copy");
+    return CSV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int csv_decode_graph_create(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_reqs, uint32_t n,
+                            uint64_t* d_out, uint32_t* d_status, const csv_decode_config* cfg, csv_graph** out) {
+    if (!ctx || !ds || !out) return CSV_EINVAL;
+    *out = nullptr;
+    if (n && (!d_reqs || !d_out || !d_status)) return fail(ctx, CSV_EINVAL, "null request, output or status pointer");
+    DeviceGuard g(ctx->device);
+    int rc = ensure_scratch(ctx, ds->d.b);
+    if (rc) return rc;
+    decode_grid(ctx->device, 1);  // occupancy queries happen outside the capture
+    csv_graph* gr = new (std::nothrow) csv_graph();
+    if (!gr) return fail(ctx, CSV_ENOMEM, "host allocation");
+    gr->ctx = ctx;
+    DecodeConfig dc;
+    if (cfg) {
+        dc.ctas_per_sm = cfg->ctas_per_sm;
+        dc.stage = cfg->stage;
+    }
+    if (cfg && cfg->lpt && n) {
+        rc = lpt_order(ctx, ds, d_reqs, n, &gr->d_order);
+        if (rc) {
+            csv_graph_destroy(gr);
+            return rc;
+        }
+        dc.order = gr->d_order;
+    }
+    cudaStream_t s;
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        csv_graph_destroy(gr);
+        return cuda_fail(ctx, e, "capture stream");
+    }
+    e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        cudaError_t le = launch_decode(ds->d, d_reqs, n, d_out, d_status, ctx->scr, s, &dc);
+        e = cudaStreamEndCapture(s, &gr->graph);
+        if (le != cudaSuccess) e = le;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&gr->exec, gr->graph, 0);
+    cudaStreamDestroy(s);
+    if (e != cudaSuccess) {
+        csv_graph_destroy(gr);
+        return cuda_fail(ctx, e, "graph capture");
+    }
+    *out = gr;
+    return CSV_OK;
+}
+
+int csv_graph_launch(csv_graph* gr, void* stream) {
+    if (!gr || !gr->exec) return CSV_EINVAL;
+    DeviceGuard g(gr->ctx->device);
+    cudaError_t e = cudaGraphLaunch(gr->exec, (cudaStream_t)stream);
+    return e == cudaSuccess ? CSV_OK : cuda_fail(gr->ctx, e, "graph launch");
+}
+
+void csv_graph_destroy(csv_graph* gr) {
+    if (!gr) return;
+    DeviceGuard g(gr->ctx->device);
+    if (gr->exec) cudaGraphExecDestroy(gr->exec);
+    if (gr->graph) cudaGraphDestroy(gr->graph);
+    cudaFree(gr->d_order);
+    delete gr;
+}
+
+int csv_decode_autotune(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_reqs, uint32_t n, uint64_t* d_out,
+                        uint32_t* d_status, uint32_t reps, csv_decode_config* best, float* best_ms) {
+    if (!ctx || !ds || !best) return CSV_EINVAL;
+    DeviceGuard g(ctx->device);
+    if (reps == 0) reps = 5;
+    cudaStream_t s;
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "tune stream");
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best_t = 1e30f;
+    csv_decode_config bestc{0, 1, 0, 0};
+    int rc = CSV_OK;
+    const uint32_t per_sm_options[] = {2, 1};
+    for (uint32_t ps : per_sm_options) {
+        for (uint32_t stage = 0; stage <= 1 && rc == CSV_OK; ++stage) {
+            for (uint32_t lpt = 0; lpt <= 1 && rc == CSV_OK; ++lpt) {
+                csv_decode_config c{ps, stage, lpt, 0};
+                csv_graph* gr = nullptr;
+                rc = csv_decode_graph_create(ctx, ds, d_reqs, n, d_out, d_status, &c, &gr);
+                if (rc) break;
+                std::vector<float> ts;
+                csv_graph_launch(gr, s);  // warm-up
+                for (uint32_t r = 0; r < reps; ++r) {
+                    cudaEventRecord(e0, s);
+                    csv_graph_launch(gr, s);
+                    cudaEventRecord(e1, s);
+                    cudaEventSynchronize(e1);
+                    float ms = 0;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    ts.push_back(ms);
+                }
+                csv_graph_destroy(gr);
+                std::sort(ts.begin(), ts.end());
+                const float med = ts[ts.size() / 2];
+                if (med < best_t) {
+                    best_t = med;
+                    bestc = c;
+                }
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    e = cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "tune");
+    *best = bestc;
+    if (best_ms) *best_ms = best_t;
     return CSV_OK;
 }
 

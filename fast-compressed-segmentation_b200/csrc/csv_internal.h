@@ -19,7 +19,7 @@ constexpr uint32_t kHeaderBytes = 152;    // 16 B header + 136 B model (fileIO.c
 // Seek-index spacing: one decoder checkpoint (16 bytes) every this many ops.
 // Each checkpoint starts one independent rANS segment in the decoder, so the
 // spacing trades the serial segment length (latency) against index size.
-constexpr uint32_t kOpsPerCheckpoint = 256;
+constexpr uint32_t kOpsPerCheckpoint = 128;
 
 // Op codes (types.hpp:162-171) and nibble layout (op << 1 | stop, brickEncoding.cpp:66-67).
 enum : uint32_t { OP_RP = 0, OP_RX = 1, OP_RY = 2, OP_RZ = 3, OP_PA = 4, OP_P0 = 5, OP_PD = 6 };
@@ -28,6 +28,9 @@ enum : uint32_t { OP_RP = 0, OP_RX = 1, OP_RY = 2, OP_RZ = 3, OP_PA = 4, OP_P0 =
 constexpr uint32_t BF_UNIFORM = 1u;   // root stop bit set: the whole brick is palette[0]
 constexpr uint32_t BF_TRUNCATED = 2u; // the stream ends inside the level structure
 constexpr uint32_t BF_NOINDEX = 4u;   // no seek index (not built)
+constexpr uint32_t BF_STATUS_MASK = 0xFFu;
+constexpr uint32_t BF_LEVELS_SHIFT = 8;   // bits 8..11: levels of this brick, log2(b) + 1
+constexpr uint32_t BF_MODEL_SHIFT = 16;   // bits 16..23: rANS model (LUT) of this brick
 
 // Per-brick device descriptor, file order.
 struct BrickDesc {
@@ -71,6 +74,9 @@ struct DeviceDataset {
     uint32_t freq[16] = {}, cum[16] = {}, total = 0;
     uint64_t stream_bytes = 0, palette_entries = 0, ck_entries = 0;
     uint32_t max_nsym = 0, max_P = 0;
+    uint32_t n_models = 1;  // LUTs at d_lut (a concatenation of datasets keeps each part's model)
+    uint64_t enc_pool_bytes = 0, pal_pool_entries = 0;  // sizes of d_enc and d_pal
+    uint32_t* h_cost = nullptr;  // per brick: decode work estimate (nSymbols), for scheduling
     BrickDesc* d_bricks = nullptr;
     uint64_t* d_pal = nullptr;
     uint8_t* d_enc = nullptr;
@@ -91,8 +97,16 @@ struct DecodeScratch {
 };
 size_t decode_scratch_per_cta(uint32_t b);
 uint32_t decode_grid(int device, uint32_t n);
+// Launch knobs the autotuner chooses (defaults: occupancy-limited grid, staging on, request order).
+struct DecodeConfig {
+    uint32_t ctas_per_sm = 0;         // 0: as many as fit
+    uint32_t stage = 1;               // stage brick streams in shared memory
+    const uint32_t* order = nullptr;  // device permutation of the requests, or null
+    const uint32_t* n_dev = nullptr;  // device-resident request count (<= n), or null
+};
 cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, uint32_t n, uint64_t* d_out,
-                          uint32_t* d_status, const DecodeScratch& scr, cudaStream_t st);
+                          uint32_t* d_status, const DecodeScratch& scr, cudaStream_t st,
+                          const DecodeConfig* cfg = nullptr);
 
 // Encoder state owned by a context (encode.cu).
 struct EncoderState;

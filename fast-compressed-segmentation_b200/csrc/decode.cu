@@ -130,7 +130,16 @@ __device__ __forceinline__ uint32_t rans_step(uint32_t& x, uint32_t& pos, const 
     uint32_t e = lut[v];
     uint32_t f = (e >> 4) & 0x1FFFu, st = e >> 17;
     x = f * (x >> kTotBits) + v - st;
-    while (x < kRansL && pos > 0) x = (x << 8) | (GLOBAL ? __ldg(enc + (--pos)) : enc[--pos]);
+    // renormalisation (the reference's while loop): in a well-formed stream it
+    // reads at most two bytes, since after a step x >= f * 2^11 >= 2^11 and two
+    // bytes lift that past 2^23; the loop only continues on malformed data
+    if (x < kRansL && pos > 0) {
+        x = (x << 8) | (GLOBAL ? __ldg(enc + (--pos)) : enc[--pos]);
+        if (x < kRansL && pos > 0) {
+            x = (x << 8) | (GLOBAL ? __ldg(enc + (--pos)) : enc[--pos]);
+            while (x < kRansL && pos > 0) x = (x << 8) | (GLOBAL ? __ldg(enc + (--pos)) : enc[--pos]);
+        }
+    }
     return e & 15u;
 }
 
@@ -208,7 +217,7 @@ __global__ void __launch_bounds__(32) build_index_kernel(BrickDesc* __restrict__
     }
     BrickDesc& o = bricks[bi];
     o.n_ops = ops;
-    o.flags = flags;
+    o.flags = (br.flags & ~BF_STATUS_MASK) | flags;
 #pragma unroll
     for (int k = 0; k < 8; ++k) o.level_start[k] = ls[k];
 }
@@ -235,6 +244,10 @@ struct DecodeArgs {
     uint64_t scratch_per_cta;
     uint32_t* queue;
     uint32_t nb, L, S, n;
+    const uint32_t* order;  // optional processing order of the requests
+    const uint32_t* n_dev;  // optional device-resident request count (at most n)
+    uint32_t stage_cap;     // largest stream staged in shared memory (0: never)
+    uint32_t n_models;      // LUTs at lut, kTot entries each
 };
 
 __device__ __forceinline__ void st_cs_v2(uint64_t* p, uint64_t a, uint64_t b) {
@@ -433,29 +446,42 @@ __global__ void __launch_bounds__(kDecThreads) decode_kernel(DecodeArgs A) {
     const uint64_t max_ops = ((1ull << (3 * A.L)) - 8) / 7;
     uint32_t* act = reinterpret_cast<uint32_t*>(scr + ((max_ops * 4 + 255) & ~255ull));
 
+    // the request count: fixed at launch, or produced on the device by an
+    // earlier kernel in the same stream (the serving loop's admission)
+    const uint32_t n_req = A.n_dev ? min(*A.n_dev, A.n) : A.n;
+    uint32_t cur_model = 0;  // the LUT in shared memory is model 0's
     for (;;) {
         if (tid == 0) {
-            S.work = atomicAdd(A.queue, 1u);
+            const uint32_t k = atomicAdd(A.queue, 1u);
+            // an optional schedule (e.g. longest brick first) maps queue slots to requests
+            S.work = (k < n_req && A.order) ? A.order[k] : k;
             S.status = 0;
-            if (S.work < A.n) {
+            if (k >= n_req) S.work = 0xFFFFFFFFu;
+            if (S.work < n_req) {
                 S.req = A.reqs[S.work];
                 if (S.req.brick < A.nb) S.br = A.bricks[S.req.brick];
             }
         }
         __syncthreads();
         const uint32_t w = S.work;
-        if (w >= A.n) break;
+        if (w >= n_req) break;
         const csv_request req = S.req;
         const uint32_t t = req.lod;
-        if (req.brick >= A.nb || t >= A.L) {
+        // bricks of a concatenated dataset carry their own level count and model
+        const uint32_t Lb = (S.br.flags >> BF_LEVELS_SHIFT) & 15u, model = (S.br.flags >> BF_MODEL_SHIFT) & 255u;
+        if (req.brick >= A.nb || t >= Lb || Lb > A.L || model >= A.n_models) {
             if (tid == 0) A.status[w] = CSV_BRICK_BADREQ;
             __syncthreads();
             continue;
         }
+        if (model != cur_model) {  // made visible by the barrier after the palette copy
+            for (uint32_t i = tid; i < kTot; i += T) S.lut[i] = A.lut[(size_t)model * kTot + i];
+            cur_model = model;
+        }
         const BrickDesc br = S.br;
         // stage the compressed stream in shared memory (one bulk copy) while the palette loads
         const uint32_t E16 = (br.E + 15u) & ~15u;
-        const bool stage = stage_ok && t > 0 && !(br.flags & BF_UNIFORM) && E16 >= 16 && E16 <= stage_cap<V>();
+        const bool stage = stage_ok && t > 0 && !(br.flags & BF_UNIFORM) && E16 >= 16 && E16 <= A.stage_cap;
         if (stage && tid == 0) bulk_copy_g2s(S.val, A.enc + br.enc_off, E16, &S.bar);
         uint64_t* out = A.out + req.dst;
         const uint64_t* gpal = A.pal + br.pal_off;
@@ -648,11 +674,16 @@ uint32_t decode_grid(int device, uint32_t n) {
 }
 
 cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, uint32_t n, uint64_t* d_out,
-                          uint32_t* d_status, const DecodeScratch& scr, cudaStream_t st) {
+                          uint32_t* d_status, const DecodeScratch& scr, cudaStream_t st, const DecodeConfig* cfg) {
     if (n == 0) return cudaSuccess;
     if (ds.L > kDecLevels + 1) return cudaErrorInvalidValue;  // bricks up to 64^3
     const bool narrow = ds.max_P < 0xFFFFu;
     uint32_t grid = (uint32_t)(narrow ? occupancy<uint16_t>(ds.device) : occupancy<uint32_t>(ds.device));
+    if (cfg && cfg->ctas_per_sm) {
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ds.device);
+        grid = std::min<uint32_t>(grid, cfg->ctas_per_sm * (uint32_t)std::max(sms, 1));
+    }
     if (grid > n) grid = n;
     if (grid > scr.ctas) grid = scr.ctas;
     cudaError_t e = cudaMemsetAsync(scr.d_queue, 0, sizeof(uint32_t), st);
@@ -673,6 +704,10 @@ cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, ui
     A.L = ds.L;
     A.S = ds.S;
     A.n = n;
+    A.order = cfg ? cfg->order : nullptr;
+    A.n_dev = cfg ? cfg->n_dev : nullptr;
+    A.stage_cap = (cfg && !cfg->stage) ? 0u : (narrow ? stage_cap<uint16_t>() : stage_cap<uint32_t>());
+    A.n_models = ds.n_models ? ds.n_models : 1u;
     if (narrow) decode_kernel<uint16_t><<<grid, kDecThreads, sizeof(DecShared<uint16_t>), st>>>(A);
     else decode_kernel<uint32_t><<<grid, kDecThreads, sizeof(DecShared<uint32_t>), st>>>(A);
     return cudaGetLastError();

@@ -786,6 +786,7 @@ int encoder_to_dataset(EncoderState* s, DeviceDataset& d, std::string& err) {
     std::vector<BrickDesc> desc(std::max<uint32_t>(nb, 1));
     uint64_t pal_n = 0, enc_n = 0;
     d.h_ids = (uint32_t*)malloc(sizeof(uint32_t) * std::max<uint32_t>(1, nb));
+    d.h_cost = (uint32_t*)malloc(sizeof(uint32_t) * std::max<uint32_t>(1, nb));
     for (uint32_t i = 0; i < nb; ++i) {
         const EncMeta& m = s->h_meta[i];
         BrickDesc& bd = desc[i];
@@ -799,9 +800,10 @@ int encoder_to_dataset(EncoderState* s, DeviceDataset& d, std::string& err) {
         bd.ck_off = (uint32_t)((uint64_t)i * s->ck_cap);
         bd.ck_cap = s->ck_cap;
         bd.n_ops = m.n_ops;
-        bd.flags = (m.flags & EF_UNIFORM) ? BF_UNIFORM : 0u;
+        bd.flags = ((m.flags & EF_UNIFORM) ? BF_UNIFORM : 0u) | (s->L << BF_LEVELS_SHIFT);
         for (int k = 0; k < 8; ++k) bd.level_start[k] = m.level_start[k];
         d.h_ids[i] = m.id;
+        d.h_cost[i] = m.nsym;
         pal_n = std::max<uint64_t>(pal_n, m.pal_off + m.P);
         enc_n = std::max<uint64_t>(enc_n, m.enc_off + ((m.E + 15) & ~15u));
         d.stream_bytes += m.E;
@@ -810,6 +812,8 @@ int encoder_to_dataset(EncoderState* s, DeviceDataset& d, std::string& err) {
         d.max_P = std::max(d.max_P, m.P);
     }
     d.ck_entries = (uint64_t)nb * s->ck_cap;
+    d.enc_pool_bytes = std::max<uint64_t>(16, enc_n);
+    d.pal_pool_entries = std::max<uint64_t>(1, pal_n);
     uint32_t lut[kTot];
     build_lut(s->freq, s->cum, lut);
     cudaError_t e;

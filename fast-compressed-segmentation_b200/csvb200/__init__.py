@@ -53,6 +53,14 @@ class _Info(C.Structure):
                 ("palette_entries", C.c_uint64), ("freq", C.c_uint32 * 16), ("cum", C.c_uint32 * 16)]
 
 
+class DecodeConfig(C.Structure):
+    """csv_decode_config: grid CTAs per SM (0 = all that fit), stream staging, largest-first order."""
+    _fields_ = [("ctas_per_sm", C.c_uint32), ("stage", C.c_uint32), ("lpt", C.c_uint32), ("reserved", C.c_uint32)]
+
+    def as_dict(self):
+        return {"ctas_per_sm": self.ctas_per_sm, "stage": self.stage, "lpt": self.lpt}
+
+
 _lib = None
 
 
@@ -88,6 +96,12 @@ def load_library() -> C.CDLL:
     L.csv_decode_batch.argtypes = [vp, vp, vp, C.c_uint32, vp, vp, vp]
     L.csv_decode_image.argtypes = [vp, u8p, C.c_size_t, C.c_uint32, u64p, u32p]
     L.csv_decode_batch_static.argtypes = [vp, vp, vp, C.c_uint32, vp, vp, vp]
+    L.csv_dataset_concat.argtypes = [vp, C.POINTER(vp), C.c_uint32, C.POINTER(vp)]
+    L.csv_decode_graph_create.argtypes = [vp, vp, vp, C.c_uint32, vp, vp, C.POINTER(DecodeConfig), C.POINTER(vp)]
+    L.csv_graph_launch.argtypes = [vp, vp]
+    L.csv_graph_destroy.argtypes = [vp]
+    L.csv_decode_autotune.argtypes = [vp, vp, vp, C.c_uint32, vp, vp, C.c_uint32, C.POINTER(DecodeConfig),
+                                      C.POINTER(C.c_float)]
     L.csv_render.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_float, C.c_uint32, C.c_uint32, vp, C.c_uint64, vp,
                              vp, C.c_uint32, vp, vp, vp, vp]
     L.csv_synth_volume.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_uint32, C.c_uint32,
@@ -145,6 +159,27 @@ class Dataset:
     def close(self):
         if self.handle:
             self.codec.lib.csv_close(self.handle)
+            self.handle = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DecodeGraph:
+    """A captured decode (csv_decode_graph_create); keeps its buffers alive."""
+
+    def __init__(self, codec: "Codec", handle: int, keep):
+        self.codec, self.handle, self._keep = codec, C.c_void_p(handle), keep
+
+    def launch(self, stream=None):
+        self.codec._check(self.codec.lib.csv_graph_launch(self.handle, C.c_void_p(_stream_handle(stream))))
+
+    def close(self):
+        if self.handle:
+            self.codec.lib.csv_graph_destroy(self.handle)
             self.handle = C.c_void_p(None)
 
     def __del__(self):
@@ -226,6 +261,34 @@ class Codec:
         h = C.c_void_p()
         self._check(self.lib.csv_open(self.handle, a.ctypes.data_as(C.POINTER(C.c_uint8)), len(image), C.byref(h)))
         return Dataset(self, h.value)
+
+    def concat(self, parts) -> Dataset:
+        """csv_dataset_concat: one dataset with the bricks of every part (each keeps its brick size and model)."""
+        arr = (C.c_void_p * len(parts))(*[p.handle.value for p in parts])
+        h = C.c_void_p()
+        self._check(self.lib.csv_dataset_concat(self.handle, arr, len(parts), C.byref(h)))
+        return Dataset(self, h.value)
+
+    def decode_graph(self, ds: Dataset, d_reqs, d_out, d_status, cfg: DecodeConfig | None = None,
+                     n: int | None = None) -> "DecodeGraph":
+        if n is None:
+            n = d_reqs.numel() * d_reqs.element_size() // 16
+        g = C.c_void_p()
+        self._check(self.lib.csv_decode_graph_create(self.handle, ds.handle, C.c_void_p(d_reqs.data_ptr()), n,
+                                                      C.c_void_p(d_out.data_ptr()), C.c_void_p(d_status.data_ptr()),
+                                                      C.byref(cfg) if cfg is not None else None, C.byref(g)))
+        return DecodeGraph(self, g.value, (ds, d_reqs, d_out, d_status))
+
+    def autotune(self, ds: Dataset, d_reqs, d_out, d_status, reps: int = 5, n: int | None = None):
+        """csv_decode_autotune -> (DecodeConfig, median ms)."""
+        if n is None:
+            n = d_reqs.numel() * d_reqs.element_size() // 16
+        best = DecodeConfig()
+        ms = C.c_float()
+        self._check(self.lib.csv_decode_autotune(self.handle, ds.handle, C.c_void_p(d_reqs.data_ptr()), n,
+                                                  C.c_void_p(d_out.data_ptr()), C.c_void_p(d_status.data_ptr()), reps,
+                                                  C.byref(best), C.byref(ms)))
+        return best, ms.value
 
     def open_encoded(self) -> Dataset:
         h = C.c_void_p()

@@ -145,6 +145,41 @@ int csv_decode_batch(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_r
 int csv_decode_batch_static(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_reqs, uint32_t n,
                             uint64_t* d_out, uint32_t* d_status, void* stream);
 
+/* ---- mixed brick sizes ---------------------------------------------------
+ * One dataset made of several: the bricks of parts[0], then of parts[1], ...
+ * (file order inside each part), every brick keeping its own brick size and
+ * rANS model, so that one decode launch can mix, e.g., 32^3 and 64^3 bricks.
+ * (A .csbd file holds one brick size, fileIO.cpp:28.)  Brick indices of
+ * requests are global: brick i of part k is sum_{j<k} num_bricks(parts[j]) + i.
+ * The parts stay valid and independent of the result. */
+int csv_dataset_concat(csv_ctx* ctx, const csv_dataset* const* parts, uint32_t n, csv_dataset** out);
+
+/* ---- captured decode and its autotuner (no reference counterpart) ---------
+ * The decode of a fixed request array into a fixed output, captured once into
+ * a CUDA graph (work-queue reset + the persistent decode kernel) and replayed
+ * by csv_graph_launch.  Knobs: ctas_per_sm (0 = as many as fit), stage (1 =
+ * stage each brick's compressed stream in shared memory by a bulk copy), lpt
+ * (1 = hand out the largest bricks first: a request permutation computed at
+ * creation). */
+typedef struct csv_decode_config {
+    uint32_t ctas_per_sm;
+    uint32_t stage;
+    uint32_t lpt;
+    uint32_t reserved;
+} csv_decode_config;
+
+typedef struct csv_graph csv_graph;
+
+int csv_decode_graph_create(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_reqs, uint32_t n,
+                            uint64_t* d_out, uint32_t* d_status, const csv_decode_config* cfg, csv_graph** out);
+int csv_graph_launch(csv_graph* g, void* stream);
+void csv_graph_destroy(csv_graph* g);
+/* Times every candidate configuration on this batch (a captured graph each,
+ * `reps` timed replays after one warm-up, median) and returns the fastest and
+ * its time in milliseconds.  Writes d_out / d_status like a decode. */
+int csv_decode_autotune(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_reqs, uint32_t n, uint64_t* d_out,
+                        uint32_t* d_status, uint32_t reps, csv_decode_config* best, float* best_ms);
+
 /* Host convenience over the above, as main.cpp:86-118 uses the reference
  * decoder: parse `image`, decode every brick at `lod` and copy the labels to
  * the host (brick i at out + i*8^lod).  status: numBricks words or NULL. */

@@ -1,0 +1,133 @@
+"""GPU: mixed brick sizes in one launch (csv_dataset_concat), the captured decode (CUDA graph) and the autotuner.
+
+Every output is compared label for label with the oracle's decode of each part's
+own .csbd image.
+"""
+import numpy as np
+import pytest
+
+from conftest import read_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _parts(codec, oracle):
+    """A 32^3-brick dataset and a 64^3-brick dataset with different rANS models."""
+    import torch
+    imgs = []
+    for shape, kind, b, seed in [((64, 96, 128), 0, 32, 31), ((64, 128, 128), 1, 64, 32)]:
+        vol = torch.empty(shape, dtype=torch.int64, device="cuda")
+        codec.synth_volume(vol, kind, 120 if kind == 0 else 300, 0 if kind == 0 else 30, 1.0, 4.0, 0.1, seed)
+        codec.encode_device(vol, b)
+        imgs.append(bytes(codec.encoded_image_tensor().cpu().numpy()))
+    imgs.append(read_golden("shipped_subset"))  # a third model: the reference's own file
+    return imgs
+
+
+def _mixed_requests(sizes_b, rng, n_extra=40):
+    """All bricks at full resolution, plus random (brick, lod) repeats; returns requests and expected keys."""
+    from csvb200 import requests
+    total = sum(n for n, b in sizes_b)
+    bricks, lods = [], []
+    base = 0
+    for n, b in sizes_b:
+        full = b.bit_length() - 1
+        bricks += list(range(base, base + n))
+        lods += [full] * n
+        base += n
+    brick_b = np.concatenate([[b] * n for n, b in sizes_b])
+    for _ in range(n_extra):
+        k = int(rng.integers(0, total))
+        bricks.append(k)
+        lods.append(int(rng.integers(0, int(brick_b[k]).bit_length())))
+    bricks, lods = np.array(bricks), np.array(lods)
+    sizes = 8 ** lods.astype(np.uint64)
+    dst = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.uint64)
+    return requests(bricks, lods, dst), bricks, lods, dst, int(sizes.sum())
+
+
+def _check(out, bricks, lods, dst, parts_ref, offsets):
+    for k in range(len(bricks)):
+        g = int(bricks[k])
+        part = max(i for i, o in enumerate(offsets) if o <= g)
+        ref = parts_ref[(part, int(lods[k]))][g - offsets[part]]
+        got = out[int(dst[k]):int(dst[k]) + len(ref)]
+        assert np.array_equal(got, ref), (k, g, int(lods[k]))
+
+
+@pytest.fixture(scope="module")
+def mixed(codec, oracle):
+    imgs = _parts(codec, oracle)
+    dss = [codec.open(im) for im in imgs]
+    cat = codec.concat(dss)
+    sizes_b = [(d.num_bricks, d.brick_size) for d in dss]
+    offsets = list(np.cumsum([0] + [n for n, _ in sizes_b])[:-1])
+    parts_ref = {}
+    for i, im in enumerate(imgs):
+        for t in range(sizes_b[i][1].bit_length()):
+            parts_ref[(i, t)] = oracle.decode_image(im, t)[0]
+    yield cat, dss, sizes_b, offsets, parts_ref
+    cat.close()
+    for d in dss:
+        d.close()
+
+
+def test_concat_mixed_brick_sizes_one_launch(codec, mixed):
+    import torch
+    from csvb200 import requests_tensor
+    cat, dss, sizes_b, offsets, parts_ref = mixed
+    assert cat.num_bricks == sum(n for n, _ in sizes_b)
+    reqs, bricks, lods, dst, total = _mixed_requests(sizes_b, np.random.default_rng(4))
+    out = torch.full((total,), -3, dtype=torch.int64, device="cuda")
+    st = torch.full((len(reqs),), -1, dtype=torch.int32, device="cuda")
+    codec.decode_batch(cat, requests_tensor(reqs), out, st)
+    torch.cuda.synchronize()
+    assert int(st.abs().max()) == 0
+    _check(out.cpu().numpy().view(np.uint64), bricks, lods, dst, parts_ref, offsets)
+
+
+def test_concat_rejects_lod_beyond_its_brick(codec, mixed):
+    import torch
+    from csvb200 import CSV_BRICK_BADREQ, requests, requests_tensor
+    cat, dss, sizes_b, offsets, parts_ref = mixed
+    reqs = requests([0, offsets[1]], [6, 6], [0, 0])  # brick 0 is 32^3 (levels 0..5): lod 6 is invalid
+    out = torch.zeros(64 ** 3, dtype=torch.int64, device="cuda")
+    st = torch.zeros(2, dtype=torch.int32, device="cuda")
+    codec.decode_batch(cat, requests_tensor(reqs), out, st)
+    assert st.cpu().numpy().tolist() == [CSV_BRICK_BADREQ, 0]
+
+
+@pytest.mark.parametrize("cfg", [(0, 1, 1), (1, 0, 0), (2, 1, 0), (1, 1, 1)])
+def test_graph_replay_matches(codec, mixed, cfg):
+    import torch
+    from csvb200 import DecodeConfig, requests_tensor
+    cat, dss, sizes_b, offsets, parts_ref = mixed
+    reqs, bricks, lods, dst, total = _mixed_requests(sizes_b, np.random.default_rng(5))
+    out = torch.zeros(total, dtype=torch.int64, device="cuda")
+    st = torch.full((len(reqs),), -1, dtype=torch.int32, device="cuda")
+    g = codec.decode_graph(cat, requests_tensor(reqs), out, st, DecodeConfig(*cfg, 0))
+    for _ in range(3):
+        out.zero_()
+        g.launch()
+        torch.cuda.synchronize()
+        assert int(st.abs().max()) == 0
+        _check(out.cpu().numpy().view(np.uint64), bricks, lods, dst, parts_ref, offsets)
+    g.close()
+
+
+def test_autotune_returns_a_working_config(codec, mixed):
+    import torch
+    from csvb200 import requests_tensor
+    cat, dss, sizes_b, offsets, parts_ref = mixed
+    reqs, bricks, lods, dst, total = _mixed_requests(sizes_b, np.random.default_rng(6))
+    d_reqs = requests_tensor(reqs)
+    out = torch.zeros(total, dtype=torch.int64, device="cuda")
+    st = torch.zeros(len(reqs), dtype=torch.int32, device="cuda")
+    best, ms = codec.autotune(cat, d_reqs, out, st, reps=3)
+    assert ms > 0 and best.ctas_per_sm in (1, 2) and best.stage in (0, 1) and best.lpt in (0, 1)
+    out.zero_()
+    g = codec.decode_graph(cat, d_reqs, out, st, best)
+    g.launch()
+    torch.cuda.synchronize()
+    _check(out.cpu().numpy().view(np.uint64), bricks, lods, dst, parts_ref, offsets)
+    g.close()
