@@ -37,6 +37,9 @@ sys.path.insert(0, os.path.join(ROOT, "fast-compressed-segmentation_b200"))
 METRIC = "bit-exact decode Gvox/s & %HBM peak; encode Mvox/s vs CPU; p99 frame ms"
 MIXED = dict(name="mixed1024", shape=(1024, 1024, 1024), kind=2, n_cells=2000, n_tubes=5000, r_min=1.0, r_max=4.0,
              zero_frac=0.0, seed=3, split_x=512, brick_left=32, brick_right=64)
+# The same generator at 1/8 of the volume (cells and tubes scaled with it): the small case for profiler captures.
+MIXED512 = dict(MIXED, name="mixed512", shape=(512, 512, 512), n_cells=250, n_tubes=625, split_x=256)
+WORKLOADS = {w["name"]: w for w in (MIXED, MIXED512)}
 NEURITE = dict(name="neurite512", shape=(512, 512, 512), brick=64, kind=1, n_cells=3000, n_tubes=400, r_min=2.0,
                r_max=12.0, zero_frac=0.15, seed=2)
 FALLBACK_HBM_GBS = 6650.0
@@ -132,18 +135,17 @@ def morton_table(b, device):
 
 def check_against_volume(out, off, vol, b):
     """Full-resolution bricks at out[off...] (split order, Morton inside) equal the source volume."""
+    import torch
     D, H, W = vol.shape
     nbx, nby, nbz = -(-W // b), -(-H // b), -(-D // b)
     m = morton_table(b, vol.device)
-    i = 0
+    col =nby * nbz * b ** 3  # one column of bricks at fixed bx (by outer, bz inner)
     for bx in range(nbx):
-        for by in range(nby):
-            for bz in range(nbz):
-                brick = out[off + i * b ** 3: off + (i + 1) * b ** 3]
-                src = vol[bz * b:(bz + 1) * b, by * b:(by + 1) * b, bx * b:(bx + 1) * b]
-                if not bool((brick[m] == src).all()):
-                    return False
-                i += 1
+        bricks = out[off + bx * col: off + (bx + 1) * col].view(nby, nbz, b ** 3)[:, :, m]  # (by, bz, z, y, x)
+        grid = bricks.permute(1, 2, 0, 3, 4).reshape(nbz * b, nby * b, b)
+        src = vol[:, :, bx * b:(bx + 1) * b]
+        if not torch.equal(grid[:D, :H, :src.shape[2]], src):
+            return False
     return True
 
 
@@ -194,7 +196,7 @@ def run_b200(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     codec = Codec(local)
-    W = MIXED
+    W = WORKLOADS[args.workload]
     D, H, Wd = W["shape"]
     nvox = D * H * Wd
     sx = W["split_x"]
@@ -434,7 +436,7 @@ def run_reference(args):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from csvb200 import Codec
     from oracle import REF_SO, Oracle, Reference
-    W = MIXED
+    W = WORKLOADS[args.workload]
     D, H, Wd = W["shape"]
     sx = W["split_x"]
     bl, br = W["brick_left"], W["brick_right"]
@@ -491,6 +493,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline legs")
+    ap.add_argument("--workload", default="mixed1024", choices=sorted(WORKLOADS),
+                    help="mixed1024: the headline; mixed512: the same generator at 1/8 size (profiler captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
