@@ -14,44 +14,46 @@
 #include <string>
 #include <vector>
 
+#include "abi_internal.h"
 #include "csv_internal.h"
 
 using namespace csv;
 
-struct csv_ctx {
-    int device = 0;
-    std::string err;
-    DecodeScratch scr;
-    uint32_t scr_b = 0;
-    EncoderState* enc = nullptr;
-};
+namespace csv {
 
-struct csv_dataset {
-    csv_ctx* ctx = nullptr;
-    DeviceDataset d;
-};
-
-namespace {
-
-int fail(csv_ctx* ctx, int code, const std::string& msg) {
+int abi_fail(csv_ctx* ctx, int code, const std::string& msg) {
     if (ctx) ctx->err = msg;
     return code;
 }
-int cuda_fail(csv_ctx* ctx, cudaError_t e, const char* where) {
-    return fail(ctx, CSV_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
+int abi_cuda_fail(csv_ctx* ctx, cudaError_t e, const char* where) {
+    return abi_fail(ctx, CSV_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
 
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-        if (prev != dev) cudaSetDevice(dev);
+int abi_ensure_scratch(csv_ctx* ctx, uint32_t b) {
+    if (ctx->scr.base && ctx->scr_b >= b) return CSV_OK;
+    size_t per = decode_scratch_per_cta(b);
+    uint32_t ctas = decode_grid(ctx->device, 0xFFFFFFFFu);
+    cudaFree(ctx->scr.base);
+    ctx->scr.base = nullptr;
+    cudaError_t e = cudaMalloc(&ctx->scr.base, per * ctas);
+    if (e != cudaSuccess) return abi_fail(ctx, CSV_ENOMEM, std::string("decode scratch: ") + cudaGetErrorString(e));
+    if (!ctx->scr.d_queue) {
+        e = cudaMalloc(&ctx->scr.d_queue, 64);
+        if (e != cudaSuccess) return abi_fail(ctx, CSV_ENOMEM, "decode queue");
     }
-    ~DeviceGuard() {
-        int cur = -1;
-        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
-    }
-};
+    ctx->scr.per_cta = per;
+    ctx->scr.ctas = ctas;
+    ctx->scr_b = b;
+    return CSV_OK;
+}
+
+}  // namespace csv
+
+namespace {
+
+int fail(csv_ctx* ctx, int code, const std::string& msg) { return abi_fail(ctx, code, msg); }
+int cuda_fail(csv_ctx* ctx, cudaError_t e, const char* where) { return abi_cuda_fail(ctx, e, where); }
+int ensure_scratch(csv_ctx* ctx, uint32_t b) { return abi_ensure_scratch(ctx, b); }
 
 uint32_t rd32(const uint8_t* p) {
     uint32_t v;
@@ -184,24 +186,6 @@ int stage_dataset(csv_ctx* ctx, const uint8_t* img, const ImageView& v, DeviceDa
         return cuda_fail(ctx, e, "staging copy");
     // the host vectors go out of scope: finish the copies first
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "staging copy");
-    return CSV_OK;
-}
-
-int ensure_scratch(csv_ctx* ctx, uint32_t b) {
-    if (ctx->scr.base && ctx->scr_b >= b) return CSV_OK;
-    size_t per = decode_scratch_per_cta(b);
-    uint32_t ctas = decode_grid(ctx->device, 0xFFFFFFFFu);
-    cudaFree(ctx->scr.base);
-    ctx->scr.base = nullptr;
-    cudaError_t e = cudaMalloc(&ctx->scr.base, per * ctas);
-    if (e != cudaSuccess) return fail(ctx, CSV_ENOMEM, std::string("decode scratch: ") + cudaGetErrorString(e));
-    if (!ctx->scr.d_queue) {
-        e = cudaMalloc(&ctx->scr.d_queue, 64);
-        if (e != cudaSuccess) return fail(ctx, CSV_ENOMEM, "decode queue");
-    }
-    ctx->scr.per_cta = per;
-    ctx->scr.ctas = ctas;
-    ctx->scr_b = b;
     return CSV_OK;
 }
 

@@ -1,0 +1,45 @@
+// abi_internal.h -- the opaque handles of include/csv.h and the host helpers the
+// C-ABI translation units (abi.cu, serve.cu) share.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "csv_internal.h"
+
+struct csv_ctx {
+    int device = 0;
+    std::string err;
+    csv::DecodeScratch scr;
+    uint32_t scr_b = 0;
+    csv::EncoderState* enc = nullptr;
+};
+
+struct csv_dataset {
+    csv_ctx* ctx = nullptr;
+    csv::DeviceDataset d;
+};
+
+namespace csv {
+
+// Record `msg` as the context's last error and return `code`.
+int abi_fail(csv_ctx* ctx, int code, const std::string& msg);
+int abi_cuda_fail(csv_ctx* ctx, cudaError_t e, const char* where);
+// Size the context's decode scratch for bricks of edge b (grows, never shrinks).
+int abi_ensure_scratch(csv_ctx* ctx, uint32_t b);
+
+// Makes `dev` current for the scope and restores the caller's device after.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace csv

@@ -13,9 +13,10 @@
 //
 // Brick slots are indexed by the brick's Morton code (rayTrace.wgsl:654-657,
 // bricks sorted by ID in datasetLoader.js:143).  A slot flagged empty is
-// skipped (rayTrace.wgsl:673-682); a slot flagged missing (not resident in the
-// decoded cache) is skipped too and its request word is set, the analogue of
-// brickRequests (rayTrace.wgsl:686).
+// skipped (rayTrace.wgsl:673-682).  Every other brick a ray enters gets its
+// request word set, as brickRequests (rayTrace.wgsl:684-686): 1 when the brick
+// is resident, 3 when its slot is flagged missing (not in the decoded cache),
+// in which case the ray skips it.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -134,9 +135,12 @@ __global__ void __launch_bounds__(128) render_kernel(RayArgs A) {
                 sl = A.slots[m];
                 if (sl.flags & CSV_SLOT_EMPTY) {
                     skip = true;
-                } else if (sl.flags & CSV_SLOT_MISSING) {
-                    skip = true;
-                    if (A.requests) A.requests[m] = 1u;
+                } else {
+                    // a non-empty brick entered by the ray (rayTrace.wgsl:684-686); the value is a
+                    // property of the slot, so concurrent writers store the same word
+                    const uint32_t rq = (sl.flags & CSV_SLOT_MISSING) ? 3u : 1u;
+                    if (A.requests && A.requests[m] != rq) A.requests[m] = rq;
+                    skip = (sl.flags & CSV_SLOT_MISSING) != 0;
                 }
             }
             if (!skip) {

@@ -1,0 +1,886 @@
+// serve.cu -- the viewer's frame loop on the device: plan, cache, decode, render.
+//
+// The reference runs this loop in JavaScript on the host (renderLoop.js:208-340,
+// cacheProcessing.js:99-232, cacheManager.js:10-246, camera.js:103-137,
+// culling.js:22-171) and hands the GPU one work queue per frame.  Here every
+// per-brick decision runs on the device, in one stream, with no host round
+// trip between the steps of a frame:
+//
+//   plan_kernel    per brick: the LOD each view asks for (camera.js:103-137) and
+//                  the cone test (culling.js:87-153); keep / free / admit; the
+//                  brick's rank among the CTA's bricks of the same kind and LOD
+//   scan_kernel    one CTA: per-CTA bases of those ranks, then the cache policy
+//                  (free stacks per LOD, bump pointer, rebuild) for the frame
+//   push_kernel    per brick: freed blocks onto their LOD's stack
+//   pop_kernel     per brick: admitted bricks pop a block or take fresh space;
+//                  their decode requests; the brick slot table the rays read
+//   decode_kernel  (decode.cu) the admitted requests, count read on the device
+//   render_kernel  (ray.cu) one launch per view
+//   census_kernel  per brick: bricks the rays entered, and how many were missing
+//
+// Orders the reference leaves open are fixed so that the result is
+// deterministic and equal to the CPU restatement (oracle/csv_oracle_serve.c):
+// frees are pushed in brick order; admissions are served LOD by LOD (coarse
+// first), in brick order within a LOD, popping the LOD's stack from the top and
+// then taking fresh space; a frame whose fresh space does not fit rebuilds the
+// cache (every needed brick placed again, coarse LODs first, until the space
+// runs out).  LOD-0 bricks and uniform bricks take no block: their slot reads
+// palette[0] from a table at the start of the cache.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <deque>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "abi_internal.h"
+#include "csv_internal.h"
+
+using namespace csv;
+
+namespace csv {
+namespace {
+
+constexpr uint32_t kMaxViews = 8;
+constexpr uint32_t kBlk = 256;  // bricks per CTA in the per-brick kernels
+constexpr uint32_t kWarps = kBlk / 32;
+constexpr uint32_t kLods = 8;   // LOD slots; bricks up to 64^3 use 0..6
+constexpr uint8_t kNone = 0xFF;
+constexpr uint32_t kRing = 64;  // steps in flight before the host harvests one
+enum : uint32_t { CNT_FREE = 0, CNT_ALLOC = kLods, CNT_WANT = 2 * kLods, kCnt = 3 * kLods };
+enum : uint8_t { BK_HAS = 1, BK_UNIFORM = 2 };
+
+struct ViewD {
+    double p[3], d[3];
+};
+
+// Device-resident cache state and the plan of the current step.
+struct ServeState {
+    uint32_t top[kLods];       // free-stack sizes
+    uint32_t T[kLods];         // stack sizes after this step's pushes
+    uint32_t top_old[kLods];   // stack sizes before them
+    uint32_t fit[kLods];       // rebuild: bricks placed per LOD
+    uint32_t req_base[kLods];  // first request index of each LOD
+    uint64_t base[kLods];      // first fresh offset per LOD (overflow / rebuild placement)
+    uint64_t bump, cap;
+    uint32_t mode;             // 0: keep the cache, 1: rebuild
+    uint32_t n_req;            // admitted requests (read by the decode kernel)
+    uint32_t resident;
+    uint32_t pad;
+};
+
+// One step's counters (the same words as the CPU restatement's OR_ST_*).
+struct StepStats {
+    uint32_t planned, visible, decoded, freed, resident, rebuilt, entered, missing, vox_lo, vox_hi;
+};
+
+struct PlanArgs {
+    ViewD v[kMaxViews];
+    uint32_t n_views, b, max_lod, nb;
+    double focal, cos_half, radius, half;
+    const uint32_t* ids;
+    const uint8_t* bflag;
+    const uint8_t* res_lod;
+    uint8_t* want;
+    uint32_t* rank;  // free | alloc << 8 | want << 16: ranks among the CTA's bricks of the same kind and LOD
+    uint32_t* cnt;   // [kCnt][n_cta]
+    uint32_t n_cta;
+    StepStats* stats;
+};
+
+__device__ __forceinline__ uint32_t compact3(uint32_t v) {
+    v &= 0x09249249u;
+    v = (v | (v >> 2)) & 0x030c30c3u;
+    v = (v | (v >> 4)) & 0x0300f00fu;
+    v = (v | (v >> 8)) & 0x030000ffu;
+    v = (v | (v >> 16)) & 0x000003ffu;
+    return v;
+}
+
+// culling.js:87-153 (margin sin(atan2(r, d)) as r / sqrt(r^2 + d^2)); bricks
+// closer than twice their radius are always in.
+__device__ __forceinline__ bool in_cone(const PlanArgs& A, const double* c, const ViewD& v) {
+    const double tx = c[0] - v.p[0], ty = c[1] - v.p[1], tz = c[2] - v.p[2];
+    const double dist = sqrt(tx * tx + ty * ty + tz * tz);
+    if (dist < 2.0 * A.radius) return true;
+    const double dot = (tx / dist) * v.d[0] + (ty / dist) * v.d[1] + (tz / dist) * v.d[2];
+    const double margin = A.radius / sqrt(A.radius * A.radius + dist * dist);
+    return !(dot < A.cos_half - margin);
+}
+
+// camera.js:103-137: the finest LOD whose voxels still cover a pixel.
+__device__ __forceinline__ uint32_t brick_lod(const PlanArgs& A, const double* c, const ViewD& v) {
+    const double dx = c[0] - v.p[0], dy = c[1] - v.p[1], dz = c[2] - v.p[2];
+    const double dist = sqrt(dx * dx + dy * dy + dz * dz);
+    const double d = dist > 0.1 ? dist : 0.1;
+    uint32_t best = 0;
+    for (uint32_t lod = 0; lod <= A.max_lod; ++lod) {
+        const double voxel = (double)A.b / (double)(1u << lod);
+        if ((A.focal * voxel) / d >= 1.0) best = lod;
+        else break;
+    }
+    return best;
+}
+
+// Rank of this thread among the CTA's threads with the same key (kNone: none),
+// in thread order; per-warp counts go to s_wc[warp][key].
+__device__ __forceinline__ uint32_t warp_rank(uint32_t key, uint32_t (*s_wc)[kLods]) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t peers = __match_any_sync(0xffffffffu, key);
+    if (key != kNone && lane == (uint32_t)(__ffs(peers) - 1)) s_wc[warp][key] = __popc(peers);
+    return __popc(peers & ((1u << lane) - 1u));
+}
+
+__global__ void __launch_bounds__(kBlk) plan_kernel(PlanArgs A) {
+    __shared__ uint32_t s_wc[3][kWarps][kLods];
+    __shared__ uint32_t s_wb[3][kWarps][kLods];
+    __shared__ uint32_t s_vis;
+    const uint32_t tid = threadIdx.x, i = blockIdx.x * kBlk + tid;
+    for (uint32_t k = tid; k < 3 * kWarps * kLods; k += kBlk) (&s_wc[0][0][0])[k] = 0;
+    if (tid == 0) s_vis = 0;
+    __syncthreads();
+    uint32_t w = kNone, r = kNone;
+    bool uni = false;
+    if (i < A.nb) {
+        const uint8_t bf = A.bflag[i];
+        uni = (bf & BK_UNIFORM) != 0;
+        r = A.res_lod[i];
+        if (bf & BK_HAS) {
+            const uint32_t id = A.ids[i];
+            const double c[3] = {(double)compact3(id) * (double)A.b + A.half,
+                                 (double)compact3(id >> 1) * (double)A.b + A.half,
+                                 (double)compact3(id >> 2) * (double)A.b + A.half};
+            for (uint32_t s = 0; s < A.n_views; ++s) {
+                if (!in_cone(A, c, A.v[s])) continue;
+                const uint32_t l = brick_lod(A, c, A.v[s]);
+                if (w == kNone || l > w) w = l;
+            }
+        }
+        A.want[i] = (uint8_t)w;
+    }
+    const bool cached = w != kNone && w > 0 && !uni;
+    const bool keep = cached && r == w;
+    const uint32_t kfree = (r != kNone && !keep) ? r : kNone;
+    const uint32_t kalloc = (cached && !keep) ? w : kNone;
+    const uint32_t kwant = cached ? w : kNone;
+    const uint32_t rf = warp_rank(kfree, s_wc[0]);
+    const uint32_t ra = warp_rank(kalloc, s_wc[1]);
+    const uint32_t rw = warp_rank(kwant, s_wc[2]);
+    const uint32_t vis = __popc(__ballot_sync(0xffffffffu, w != kNone));
+    if ((tid & 31u) == 0 && vis) atomicAdd(&s_vis, vis);
+    __syncthreads();
+    if (tid < 3 * kLods) {  // exclusive scan over the warps, per (kind, LOD)
+        const uint32_t kind = tid / kLods, l = tid % kLods;
+        uint32_t acc = 0;
+        for (uint32_t wp = 0; wp < kWarps; ++wp) {
+            s_wb[kind][wp][l] = acc;
+            acc += s_wc[kind][wp][l];
+        }
+        A.cnt[(kind * kLods + l) * A.n_cta + blockIdx.x] = acc;
+    }
+    __syncthreads();
+    if (i < A.nb) {
+        const uint32_t wp = tid >> 5;
+        uint32_t pk = 0;
+        if (kfree != kNone) pk |= (s_wb[0][wp][kfree] + rf);
+        if (kalloc != kNone) pk |= (s_wb[1][wp][kalloc] + ra) << 8;
+        if (kwant != kNone) pk |= (s_wb[2][wp][kwant] + rw) << 16;
+        A.rank[i] = pk;
+    }
+    if (tid == 0 && s_vis) atomicAdd(&A.stats->visible, s_vis);
+}
+
+// One CTA: exclusive scans of the per-CTA counts (one warp per counter), then
+// the frame's cache policy by thread 0.
+__global__ void __launch_bounds__(1024) scan_kernel(const uint32_t* __restrict__ cnt, uint32_t* __restrict__ base,
+                                                    uint32_t n_cta, uint32_t max_lod, uint32_t nb,
+                                                    ServeState* __restrict__ S, StepStats* __restrict__ st) {
+    __shared__ uint32_t tot[kCnt];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    if (warp < kCnt) {
+        uint32_t carry = 0;
+        for (uint32_t c0 = 0; c0 < n_cta; c0 += 32) {
+            const uint32_t j = c0 + lane;
+            const uint32_t v = j < n_cta ? cnt[warp * n_cta + j] : 0u;
+            uint32_t x = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+                if ((int)lane >= o) x += y;
+            }
+            if (j < n_cta) base[warp * n_cta + j] = carry + x - v;
+            carry += __shfl_sync(0xffffffffu, x, 31);
+        }
+        if (lane == 0) tot[warp] = carry;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    uint64_t need = 0;
+    uint32_t over[kLods] = {}, nfree = 0, nalloc = 0;
+    bool rebuild = false;
+    for (uint32_t l = 1; l <= max_lod; ++l) {
+        const uint32_t F = tot[CNT_FREE + l], A = tot[CNT_ALLOC + l];
+        S->top_old[l] = S->top[l];
+        S->T[l] = S->top[l] + F;
+        if (S->T[l] > nb) rebuild = true;  // cannot happen: a LOD never holds more blocks than bricks
+        over[l] = A > S->T[l] ? A - S->T[l] : 0u;
+        need += (uint64_t)over[l] << (3 * l);
+        nfree += F;
+        nalloc += A;
+    }
+    if (S->bump + need > S->cap) rebuild = true;
+    uint64_t vox = 0;
+    if (!rebuild) {
+        uint64_t b = S->bump;
+        for (uint32_t l = 1; l <= max_lod; ++l) {
+            S->base[l] = b;
+            b += (uint64_t)over[l] << (3 * l);
+            const uint32_t A = tot[CNT_ALLOC + l];
+            S->top[l] = S->T[l] - (A < S->T[l] ? A : S->T[l]);
+            vox += (uint64_t)A << (3 * l);
+        }
+        S->bump = b;
+        uint32_t acc = 0;
+        for (uint32_t l = max_lod; l >= 1; --l) {  // finest LOD first: the longest decodes start first
+            S->req_base[l] = acc;
+            acc += tot[CNT_ALLOC + l];
+        }
+        S->n_req = acc;
+        S->mode = 0;
+        S->resident = S->resident - nfree + nalloc;
+    } else {
+        uint64_t b = 0;
+        for (uint32_t l = 1; l <= max_lod; ++l) {
+            const uint32_t W = tot[CNT_WANT + l];
+            const uint64_t room = S->cap > b ? (S->cap - b) >> (3 * l) : 0ull;
+            S->fit[l] = (uint32_t)(room < W ? room : W);
+            S->base[l] = b;
+            b += (uint64_t)S->fit[l] << (3 * l);
+            S->top[l] = 0;
+            S->top_old[l] = 0;
+            S->T[l] = 0;
+            vox += (uint64_t)S->fit[l] << (3 * l);
+        }
+        S->bump = b;
+        uint32_t acc = 0;
+        for (uint32_t l = max_lod; l >= 1; --l) {
+            S->req_base[l] = acc;
+            acc += S->fit[l];
+        }
+        S->n_req = acc;
+        S->mode = 1;
+        S->resident = acc;
+    }
+    st->planned = 1;
+    st->decoded = S->n_req;
+    st->freed = nfree;
+    st->rebuilt = rebuild ? 1u : 0u;
+    st->vox_lo = (uint32_t)vox;
+    st->vox_hi = (uint32_t)(vox >> 32);
+}
+
+struct CacheArgs {
+    uint32_t nb, n_cta;
+    const uint8_t* bflag;
+    const uint8_t* want;
+    const uint32_t* rank;
+    const uint32_t* base;  // [kCnt][n_cta]
+    const uint32_t* ids;
+    uint8_t* res_lod;
+    uint64_t* res_off;
+    uint64_t* stack;       // [kLods][nb]
+    const ServeState* S;
+    csv_request* reqs;
+    csv_brick_slot* slots;
+    uint64_t pal_region;
+};
+
+__global__ void __launch_bounds__(kBlk) push_kernel(CacheArgs A) {
+    const uint32_t i = blockIdx.x * kBlk + threadIdx.x;
+    if (i >= A.nb) return;
+    const uint32_t r = A.res_lod[i];
+    if (r == kNone) return;
+    const uint32_t w = A.want[i];
+    const bool cached = w != kNone && w > 0 && !(A.bflag[i] & BK_UNIFORM);
+    if (A.S->mode == 1) {
+        A.res_lod[i] = kNone;
+        return;
+    }
+    if (cached && r == w) return;  // kept
+    const uint32_t pos = A.S->top_old[r] + A.base[(CNT_FREE + r) * A.n_cta + blockIdx.x] + (A.rank[i] & 255u);
+    A.stack[(size_t)r * A.nb + pos] = A.res_off[i];
+    A.res_lod[i] = kNone;
+}
+
+__global__ void __launch_bounds__(kBlk) pop_kernel(CacheArgs A) {
+    const uint32_t i = blockIdx.x * kBlk + threadIdx.x;
+    if (i >= A.nb) return;
+    const uint8_t bf = A.bflag[i];
+    const uint32_t w = A.want[i];
+    const bool uni = (bf & BK_UNIFORM) != 0;
+    const bool cached = w != kNone && w > 0 && !uni;
+    uint32_t r = A.res_lod[i];
+    if (cached && r != w) {
+        uint32_t k;
+        uint64_t off = 0;
+        bool placed = true;
+        if (A.S->mode == 0) {
+            k = A.base[(CNT_ALLOC + w) * A.n_cta + blockIdx.x] + ((A.rank[i] >> 8) & 255u);
+            const uint32_t T = A.S->T[w];
+            off = k < T ? A.stack[(size_t)w * A.nb + (T - 1 - k)] : A.S->base[w] + ((uint64_t)(k - T) << (3 * w));
+        } else {
+            k = A.base[(CNT_WANT + w) * A.n_cta + blockIdx.x] + ((A.rank[i] >> 16) & 255u);
+            placed = k < A.S->fit[w];
+            if (placed) off = A.S->base[w] + ((uint64_t)k << (3 * w));
+        }
+        if (placed) {
+            A.res_lod[i] = (uint8_t)w;
+            A.res_off[i] = off;
+            r = w;
+            csv_request q;
+            q.brick = i;
+            q.lod = w;
+            q.dst = A.pal_region + off;
+            A.reqs[A.S->req_base[w] + k] = q;
+        }
+    }
+    csv_brick_slot sl;
+    sl.offset = 0;
+    sl.lod = 0;
+    sl.flags = 0;
+    if (!(bf & BK_HAS)) sl.flags = CSV_SLOT_EMPTY;
+    else if (r != kNone) {
+        sl.offset = A.pal_region + A.res_off[i];
+        sl.lod = r;
+    } else if (uni || w == 0) sl.offset = i;
+    else sl.flags = CSV_SLOT_MISSING;
+    A.slots[A.ids[i]] = sl;
+}
+
+__global__ void __launch_bounds__(kBlk) census_kernel(uint32_t nb, const uint32_t* __restrict__ ids,
+                                                      uint32_t* __restrict__ req_words, const ServeState* S,
+                                                      StepStats* st) {
+    __shared__ uint32_t s_e, s_m;
+    const uint32_t i = blockIdx.x * kBlk + threadIdx.x;
+    if (threadIdx.x == 0) s_e = s_m = 0;
+    __syncthreads();
+    uint32_t v = 0;
+    if (i < nb) {
+        const uint32_t m = ids[i];
+        v = req_words[m];
+        if (v) req_words[m] = 0;
+    }
+    const uint32_t e = __popc(__ballot_sync(0xffffffffu, v != 0)), ms = __popc(__ballot_sync(0xffffffffu, v == 3));
+    if ((threadIdx.x & 31u) == 0) {
+        if (e) atomicAdd(&s_e, e);
+        if (ms) atomicAdd(&s_m, ms);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (s_e) atomicAdd(&st->entered, s_e);
+        if (s_m) atomicAdd(&st->missing, s_m);
+        if (blockIdx.x == 0) st->resident = S->resident;
+    }
+}
+
+// Per brick: the palette-0 table, the transfer-function flag (culling.js:162-171)
+// and the uniform flag; every slot starts empty.
+__global__ void __launch_bounds__(kBlk) setup_kernel(const BrickDesc* __restrict__ bricks, const uint64_t* __restrict__ pal,
+                                                     uint32_t nb, const uint64_t* __restrict__ hidden, uint32_t n_hidden,
+                                                     uint64_t* __restrict__ cache, uint8_t* __restrict__ bflag,
+                                                     uint32_t* __restrict__ ids) {
+    const uint32_t i = blockIdx.x * kBlk + threadIdx.x;
+    if (i >= nb) return;
+    const BrickDesc br = bricks[i];
+    const uint64_t* p = pal + br.pal_off;
+    uint8_t f = (br.flags & BF_UNIFORM) ? BK_UNIFORM : 0;
+    for (uint32_t k = 0; k < br.P; ++k) {
+        const uint64_t v = p[k];
+        if (v == 0) continue;
+        uint32_t lo = 0, hi = n_hidden;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (hidden[mid] < v) lo = mid + 1;
+            else hi = mid;
+        }
+        if (!(lo < n_hidden && hidden[lo] == v)) {
+            f |= BK_HAS;
+            break;
+        }
+    }
+    bflag[i] = f;
+    cache[i] = br.P ? p[0] : 0ull;
+    ids[i] = br.id;
+}
+
+__global__ void slots_clear_kernel(csv_brick_slot* slots, uint64_t n) {
+    for (uint64_t m = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; m < n; m += (uint64_t)gridDim.x * blockDim.x) {
+        csv_brick_slot s;
+        s.offset = 0;
+        s.lod = 0;
+        s.flags = CSV_SLOT_EMPTY;
+        slots[m] = s;
+    }
+}
+
+}  // namespace
+}  // namespace csv
+
+struct csv_server {
+    csv_ctx* ctx = nullptr;
+    const csv_dataset* ds = nullptr;
+    uint32_t W = 0, H = 0, cone = 0, b = 0, max_lod = 0, nb = 0, bpa = 0, n_cta = 0, max_sessions = 1;
+    double fov = 0, focal = 0, cos_half = 0, radius = 0;
+    uint64_t total = 0, pal_region = 0, n_slots = 0;
+    uint64_t* d_cache = nullptr;
+    csv_brick_slot* d_slots = nullptr;
+    uint32_t* d_req_words = nullptr;
+    uint32_t* d_ids = nullptr;
+    uint8_t* d_bflag = nullptr;
+    uint8_t* d_res_lod = nullptr;
+    uint64_t* d_res_off = nullptr;
+    uint8_t* d_want = nullptr;
+    uint32_t* d_rank = nullptr;
+    uint64_t* d_stack = nullptr;
+    uint32_t* d_cnt = nullptr;
+    uint32_t* d_base = nullptr;
+    ServeState* d_state = nullptr;
+    csv_request* d_reqs = nullptr;
+    uint32_t* d_status = nullptr;
+    uint64_t* d_hidden = nullptr;
+    uint32_t n_hidden = 0;
+    StepStats* d_stats = nullptr;  // kRing slots
+    StepStats* h_stats = nullptr;  // pinned mirror
+    struct Pending {
+        bool set = false;
+        double v[6];
+        uint64_t* lab = nullptr;
+        float* dep = nullptr;
+    };
+    std::vector<Pending> pend;
+    bool planned_once = false;
+    std::vector<uint32_t> last_sess;
+    std::vector<double> last_view;
+    struct StepRec {
+        uint64_t seq = 0;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        std::vector<uint32_t> sess;
+        bool busy = false;
+    };
+    StepRec ring[kRing];
+    uint64_t next_seq = 0, harvest_seq = 0;
+    std::deque<csv_frame_stats> done;
+};
+
+namespace {
+
+int fail(csv_ctx* ctx, int code, const std::string& m) { return abi_fail(ctx, code, m); }
+int cfail(csv_ctx* ctx, cudaError_t e, const char* w) { return abi_cuda_fail(ctx, e, w); }
+
+void server_free(csv_server* s) {
+    cudaFree(s->d_cache);
+    cudaFree(s->d_slots);
+    cudaFree(s->d_req_words);
+    cudaFree(s->d_ids);
+    cudaFree(s->d_bflag);
+    cudaFree(s->d_res_lod);
+    cudaFree(s->d_res_off);
+    cudaFree(s->d_want);
+    cudaFree(s->d_rank);
+    cudaFree(s->d_stack);
+    cudaFree(s->d_cnt);
+    cudaFree(s->d_base);
+    cudaFree(s->d_state);
+    cudaFree(s->d_reqs);
+    cudaFree(s->d_status);
+    cudaFree(s->d_hidden);
+    cudaFree(s->d_stats);
+    if (s->h_stats) cudaFreeHost(s->h_stats);
+    for (auto& r : s->ring) {
+        if (r.e0) cudaEventDestroy(r.e0);
+        if (r.e1) cudaEventDestroy(r.e1);
+    }
+    delete s;
+}
+
+// culling.js:22-56 over the sessions of a step: re-plan when the set of
+// sessions changed or a camera moved more than 0.5 units / turned more than 0.05 rad.
+bool views_moved(const csv_server* s, const std::vector<uint32_t>& sess, const std::vector<double>& v) {
+    if (!s->planned_once || sess != s->last_sess) return true;
+    const double cos_rot = cos(0.05);
+    for (size_t k = 0; k < sess.size(); ++k) {
+        const double* a = &v[6 * k];
+        const double* p = &s->last_view[6 * k];
+        const double dx = a[0] - p[0], dy = a[1] - p[1], dz = a[2] - p[2];
+        const double moved = dx * dx + dy * dy + dz * dz;
+        const double dot = a[3] * p[3] + a[4] * p[4] + a[5] * p[5];
+        if (moved > 0.5 * 0.5 || dot < cos_rot) return true;
+    }
+    return false;
+}
+
+// camera.js:61-77 (getUniformData) in double, then float.
+void camera_of(const double* v, double fov, csv_camera* c) {
+    double f[3], r[3], u[3], wu[3];
+    double n = sqrt(v[3] * v[3] + v[4] * v[4] + v[5] * v[5]);
+    if (n == 0.0) n = 1.0;
+    for (int a = 0; a < 3; ++a) f[a] = v[3 + a] / n;
+    if (fabs(f[1]) > 0.999) {
+        wu[0] = 1.0;
+        wu[1] = 0.0;
+        wu[2] = 0.0;
+    } else {
+        wu[0] = 0.0;
+        wu[1] = 1.0;
+        wu[2] = 0.0;
+    }
+    r[0] = f[1] * wu[2] - f[2] * wu[1];
+    r[1] = f[2] * wu[0] - f[0] * wu[2];
+    r[2] = f[0] * wu[1] - f[1] * wu[0];
+    n = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    if (n == 0.0) n = 1.0;
+    for (int a = 0; a < 3; ++a) r[a] /= n;
+    u[0] = r[1] * f[2] - r[2] * f[1];
+    u[1] = r[2] * f[0] - r[0] * f[2];
+    u[2] = r[0] * f[1] - r[1] * f[0];
+    n = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    if (n == 0.0) n = 1.0;
+    for (int a = 0; a < 3; ++a) u[a] /= n;
+    for (int a = 0; a < 3; ++a) {
+        c->position[a] = (float)v[a];
+        c->forward[a] = (float)f[a];
+        c->right[a] = (float)r[a];
+        c->up[a] = (float)u[a];
+    }
+    c->tan_half_fov = (float)tan(fov * 0.5);
+    c->pad0 = c->pad1 = c->pad2 = 0.f;
+}
+
+// Move finished steps from the ring to the host queue (wait: block on the oldest).
+int harvest(csv_server* s, bool wait_all, bool wait_one) {
+    while (s->harvest_seq < s->next_seq) {
+        auto& r = s->ring[s->harvest_seq % kRing];
+        cudaError_t e = (wait_all || wait_one) ? cudaEventSynchronize(r.e1) : cudaEventQuery(r.e1);
+        if (e == cudaErrorNotReady) return CSV_OK;
+        if (e != cudaSuccess) return cfail(s->ctx, e, "serve step");
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, r.e0, r.e1);
+        const StepStats& t = s->h_stats[s->harvest_seq % kRing];
+        for (uint32_t ses : r.sess) {
+            csv_frame_stats f;
+            memset(&f, 0, sizeof f);
+            f.step = r.seq;
+            f.session = ses;
+            f.planned = t.planned;
+            f.visible = t.visible;
+            f.decoded = t.decoded;
+            f.freed = t.freed;
+            f.resident = t.resident;
+            f.rebuilt = t.rebuilt;
+            f.entered = t.entered;
+            f.missing = t.missing;
+            f.decoded_voxels = (uint64_t)t.vox_lo | ((uint64_t)t.vox_hi << 32);
+            f.ms = ms;
+            s->done.push_back(f);
+        }
+        r.busy = false;
+        ++s->harvest_seq;
+        wait_one = false;
+    }
+    return CSV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int csv_serve_create(csv_ctx* ctx, const csv_dataset* ds, const csv_serve_config* cfg, const uint64_t* hidden,
+                     uint32_t n_hidden, csv_server** out) {
+    if (!ctx || !ds || !cfg || !out) return CSV_EINVAL;
+    *out = nullptr;
+    if (cfg->width == 0 || cfg->height == 0 || !(cfg->fov > 0.0 && cfg->fov < 3.14159))
+        return fail(ctx, CSV_EINVAL, "serve: viewport and field of view must be positive");
+    const uint32_t ms = cfg->max_sessions ? cfg->max_sessions : 1u;
+    if (ms > kMaxViews) return fail(ctx, CSV_ERANGE, "serve: at most 8 sessions per server");
+    if (ds->d.n_models > 1) return fail(ctx, CSV_EINVAL, "serve: one brick size per server (not a concatenation)");
+    if (n_hidden && !hidden) return fail(ctx, CSV_EINVAL, "serve: hidden labels pointer is null");
+    DeviceGuard g(ctx->device);
+    const DeviceDataset& d = ds->d;
+    csv_server* s = new (std::nothrow) csv_server();
+    if (!s) return fail(ctx, CSV_ENOMEM, "serve: host allocation");
+    s->ctx = ctx;
+    s->ds = ds;
+    s->W = cfg->width;
+    s->H = cfg->height;
+    s->cone = cfg->cone;
+    s->fov = cfg->fov;
+    s->b = d.b;
+    s->nb = d.nb;
+    s->max_sessions = ms;
+    s->max_lod = 0;
+    while ((1u << s->max_lod) < s->b) ++s->max_lod;
+    const double screen = (double)std::min(s->W, s->H);
+    s->focal = (screen / 2.0) / tan(s->fov / 2.0);
+    if (s->cone == 0) {
+        s->cos_half = cos(s->fov / 2.0);
+    } else {
+        const double a = (double)s->W / (double)s->H;
+        s->cos_half = cos(atan(tan(s->fov / 2.0) * sqrt(a * a + 1.0)));
+    }
+    s->radius = sqrt(3.0) * ((double)s->b / 2.0);
+    uint32_t maxc = 0;
+    for (uint32_t i = 0; i < s->nb; ++i) {
+        uint32_t id = d.h_ids[i], c[3] = {0, 0, 0};
+        for (int bit = 0; bit < 10; ++bit)
+            for (int a = 0; a < 3; ++a) c[a] |= ((id >> (3 * bit + a)) & 1u) << bit;
+        maxc = std::max({maxc, c[0], c[1], c[2]});
+    }
+    s->bpa = maxc + 1;
+    uint64_t p2 = 1;
+    while (p2 < s->bpa) p2 <<= 1;
+    s->n_slots = p2 * p2 * p2;
+    s->n_cta = (s->nb + kBlk - 1) / kBlk;
+    s->total = (cfg->cache_bytes ? cfg->cache_bytes : (24ull << 30)) / 8;
+    s->pal_region = ((uint64_t)s->nb + 31) & ~31ull;
+    if (s->total <= s->pal_region) {
+        server_free(s);
+        return fail(ctx, CSV_ERANGE, "serve: cache smaller than its palette table");
+    }
+    const size_t nbx = std::max<uint32_t>(s->nb, 1);
+    cudaError_t e = cudaSuccess;
+    auto alloc = [&](void** p, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc(p, std::max<size_t>(bytes, 16));
+    };
+    alloc((void**)&s->d_cache, s->total * 8);
+    alloc((void**)&s->d_slots, s->n_slots * sizeof(csv_brick_slot));
+    alloc((void**)&s->d_req_words, s->n_slots * 4);
+    alloc((void**)&s->d_ids, nbx * 4);
+    alloc((void**)&s->d_bflag, nbx);
+    alloc((void**)&s->d_res_lod, nbx);
+    alloc((void**)&s->d_res_off, nbx * 8);
+    alloc((void**)&s->d_want, nbx);
+    alloc((void**)&s->d_rank, nbx * 4);
+    alloc((void**)&s->d_stack, (size_t)kLods * nbx * 8);
+    alloc((void**)&s->d_cnt, (size_t)kCnt * std::max<uint32_t>(s->n_cta, 1) * 4);
+    alloc((void**)&s->d_base, (size_t)kCnt * std::max<uint32_t>(s->n_cta, 1) * 4);
+    alloc((void**)&s->d_state, sizeof(ServeState));
+    alloc((void**)&s->d_reqs, nbx * sizeof(csv_request));
+    alloc((void**)&s->d_status, nbx * 4);
+    alloc((void**)&s->d_hidden, std::max<uint32_t>(n_hidden, 1) * 8);
+    alloc((void**)&s->d_stats, kRing * sizeof(StepStats));
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&s->h_stats, kRing * sizeof(StepStats));
+    if (e != cudaSuccess) {
+        server_free(s);
+        return fail(ctx, CSV_ENOMEM, std::string("serve: device allocation: ") + cudaGetErrorString(e));
+    }
+    for (auto& r : s->ring) {
+        if (e == cudaSuccess) e = cudaEventCreate(&r.e0);
+        if (e == cudaSuccess) e = cudaEventCreate(&r.e1);
+    }
+    if (e == cudaSuccess && n_hidden) {
+        std::vector<uint64_t> h(hidden, hidden + n_hidden);
+        std::sort(h.begin(), h.end());
+        e = cudaMemcpy(s->d_hidden, h.data(), 8ull * n_hidden, cudaMemcpyHostToDevice);
+    }
+    s->n_hidden = n_hidden;
+    ServeState st0;
+    memset(&st0, 0, sizeof st0);
+    st0.cap = s->total - s->pal_region;
+    if (e == cudaSuccess) e = cudaMemcpy(s->d_state, &st0, sizeof st0, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(s->d_res_lod, kNone, nbx);
+    if (e == cudaSuccess) e = cudaMemset(s->d_req_words, 0, s->n_slots * 4);
+    if (e == cudaSuccess && s->nb) {
+        setup_kernel<<<s->n_cta, kBlk>>>(d.d_bricks, d.d_pal, s->nb, s->d_hidden, s->n_hidden, s->d_cache, s->d_bflag,
+                                         s->d_ids);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        slots_clear_kernel<<<1024, 256>>>(s->d_slots, s->n_slots);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        server_free(s);
+        return cfail(ctx, e, "serve: setup");
+    }
+    int rc = abi_ensure_scratch(ctx, s->b);
+    if (rc) {
+        server_free(s);
+        return rc;
+    }
+    s->pend.resize(ms);
+    *out = s;
+    return CSV_OK;
+}
+
+int csv_serve_submit(csv_server* s, uint32_t session, const csv_view* view, uint64_t* d_label, float* d_depth) {
+    if (!s || !view || !d_label || !d_depth) return CSV_EINVAL;
+    if (session >= s->max_sessions) return fail(s->ctx, CSV_ERANGE, "serve: session id beyond max_sessions");
+    auto& p = s->pend[session];
+    p.set = true;  // a newer frame of the same session replaces one not yet stepped
+    for (int a = 0; a < 3; ++a) {
+        p.v[a] = view->position[a];
+        p.v[3 + a] = view->direction[a];
+    }
+    p.lab = d_label;
+    p.dep = d_depth;
+    return CSV_OK;
+}
+
+int csv_serve_step(csv_server* s, void* stream, uint64_t* step_id) {
+    if (!s) return CSV_EINVAL;
+    cudaStream_t st = (cudaStream_t)stream;
+    std::vector<uint32_t> sess;
+    std::vector<double> views;  // position, unit direction (camera.js:63)
+    for (uint32_t k = 0; k < s->max_sessions; ++k) {
+        if (!s->pend[k].set) continue;
+        sess.push_back(k);
+        const double* v = s->pend[k].v;
+        double n = sqrt(v[3] * v[3] + v[4] * v[4] + v[5] * v[5]);
+        if (n == 0.0) n = 1.0;
+        views.insert(views.end(), {v[0], v[1], v[2], v[3] / n, v[4] / n, v[5] / n});
+    }
+    if (sess.empty()) return fail(s->ctx, CSV_EINVAL, "serve: no frame submitted since the last step");
+    DeviceGuard g(s->ctx->device);
+    // a full ring: wait for the oldest step and keep its counters for csv_serve_poll
+    if (s->next_seq - s->harvest_seq >= kRing) {
+        int rc = harvest(s, false, true);
+        if (rc) return rc;
+    }
+    const uint32_t slot = (uint32_t)(s->next_seq % kRing);
+    auto& rec = s->ring[slot];
+    StepStats* stats = s->d_stats + slot;
+    cudaError_t e = cudaEventRecord(rec.e0, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(stats, 0, sizeof(StepStats), st);
+    const bool plan = views_moved(s, sess, views);
+    if (e == cudaSuccess && plan && s->nb) {
+        PlanArgs P;
+        memset(&P, 0, sizeof P);
+        for (size_t k = 0; k < sess.size(); ++k)
+            for (int a = 0; a < 3; ++a) {
+                P.v[k].p[a] = views[6 * k + a];
+                P.v[k].d[a] = views[6 * k + 3 + a];
+            }
+        P.n_views = (uint32_t)sess.size();
+        P.b = s->b;
+        P.max_lod = s->max_lod;
+        P.nb = s->nb;
+        P.focal = s->focal;
+        P.cos_half = s->cos_half;
+        P.radius = s->radius;
+        P.half = (double)s->b / 2.0;
+        P.ids = s->d_ids;
+        P.bflag = s->d_bflag;
+        P.res_lod = s->d_res_lod;
+        P.want = s->d_want;
+        P.rank = s->d_rank;
+        P.cnt = s->d_cnt;
+        P.n_cta = s->n_cta;
+        P.stats = stats;
+        plan_kernel<<<s->n_cta, kBlk, 0, st>>>(P);
+        scan_kernel<<<1, 1024, 0, st>>>(s->d_cnt, s->d_base, s->n_cta, s->max_lod, s->nb, s->d_state, stats);
+        CacheArgs C;
+        C.nb = s->nb;
+        C.n_cta = s->n_cta;
+        C.bflag = s->d_bflag;
+        C.want = s->d_want;
+        C.rank = s->d_rank;
+        C.base = s->d_base;
+        C.ids = s->d_ids;
+        C.res_lod = s->d_res_lod;
+        C.res_off = s->d_res_off;
+        C.stack = s->d_stack;
+        C.S = s->d_state;
+        C.reqs = s->d_reqs;
+        C.slots = s->d_slots;
+        C.pal_region = s->pal_region;
+        push_kernel<<<s->n_cta, kBlk, 0, st>>>(C);
+        pop_kernel<<<s->n_cta, kBlk, 0, st>>>(C);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) {
+            DecodeConfig dc;
+            dc.n_dev = &s->d_state->n_req;
+            e = launch_decode(s->ds->d, s->d_reqs, s->nb, s->d_cache, s->d_status, s->ctx->scr, st, &dc);
+        }
+        if (e == cudaSuccess) {
+            s->planned_once = true;
+            s->last_sess = sess;
+            s->last_view = views;
+        }
+    }
+    for (size_t k = 0; k < sess.size() && e == cudaSuccess; ++k) {
+        csv_camera cam;
+        camera_of(s->pend[sess[k]].v, s->fov, &cam);
+        e = launch_render(cam, s->W, s->H, (float)(s->bpa * s->b), s->b, s->bpa, s->d_slots, s->n_slots, s->d_cache,
+                          s->n_hidden ? s->d_hidden : nullptr, s->n_hidden, s->pend[sess[k]].lab,
+                          s->pend[sess[k]].dep, s->d_req_words, st);
+    }
+    if (e == cudaSuccess && s->nb) {
+        census_kernel<<<s->n_cta, kBlk, 0, st>>>(s->nb, s->d_ids, s->d_req_words, s->d_state, stats);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->h_stats + slot, stats, sizeof(StepStats), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaEventRecord(rec.e1, st);
+    if (e != cudaSuccess) return cfail(s->ctx, e, "serve step");
+    rec.seq = s->next_seq;
+    rec.sess = sess;
+    rec.busy = true;
+    if (step_id) *step_id = s->next_seq;
+    ++s->next_seq;
+    for (uint32_t k : sess) s->pend[k].set = false;
+    return CSV_OK;
+}
+
+int csv_serve_poll(csv_server* s, csv_frame_stats* out, uint32_t max, uint32_t* n_out, int wait) {
+    if (!s || !n_out || (max && !out)) return CSV_EINVAL;
+    *n_out = 0;
+    DeviceGuard g(s->ctx->device);
+    int rc = harvest(s, wait != 0, false);
+    if (rc) return rc;
+    uint32_t n = 0;
+    while (n < max && !s->done.empty()) {
+        out[n++] = s->done.front();
+        s->done.pop_front();
+    }
+    *n_out = n;
+    return CSV_OK;
+}
+
+int csv_serve_camera(const csv_server* s, const csv_view* view, csv_camera* out) {
+    if (!s || !view || !out) return CSV_EINVAL;
+    double v[6] = {view->position[0], view->position[1], view->position[2],
+                   view->direction[0], view->direction[1], view->direction[2]};
+    camera_of(v, s->fov, out);
+    return CSV_OK;
+}
+
+int csv_serve_state(const csv_server* s, csv_serve_info* info) {
+    if (!s || !info) return CSV_EINVAL;
+    info->slots = s->d_slots;
+    info->n_slots = s->n_slots;
+    info->cache = s->d_cache;
+    info->cache_labels = s->total;
+    info->palette_table = s->pal_region;
+    info->bricks_per_axis = s->bpa;
+    info->brick_size = s->b;
+    info->grid_size = (float)(s->bpa * s->b);
+    info->focal = s->focal;
+    info->cos_half = s->cos_half;
+    info->decode_status = s->d_status;
+    return CSV_OK;
+}
+
+int csv_serve_destroy(csv_server* s) {
+    if (!s) return CSV_OK;
+    DeviceGuard g(s->ctx->device);
+    for (uint64_t q = s->harvest_seq; q < s->next_seq; ++q) cudaEventSynchronize(s->ring[q % kRing].e1);
+    server_free(s);
+    return CSV_OK;
+}
+
+}  // extern "C"

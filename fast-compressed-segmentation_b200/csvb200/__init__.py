@@ -61,6 +61,40 @@ class DecodeConfig(C.Structure):
         return {"ctas_per_sm": self.ctas_per_sm, "stage": self.stage, "lpt": self.lpt}
 
 
+CONE_REFERENCE = 0
+CONE_SCREEN = 1
+
+
+class ServeConfig(C.Structure):
+    """csv_serve_config."""
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("max_sessions", C.c_uint32), ("cone", C.c_uint32),
+                ("fov", C.c_double), ("cache_bytes", C.c_uint64)]
+
+
+class View(C.Structure):
+    """csv_view: camera position and view direction (double)."""
+    _fields_ = [("position", C.c_double * 3), ("direction", C.c_double * 3)]
+
+
+class FrameStats(C.Structure):
+    """csv_frame_stats."""
+    _fields_ = [("step", C.c_uint64), ("session", C.c_uint32), ("planned", C.c_uint32), ("visible", C.c_uint32),
+                ("decoded", C.c_uint32), ("freed", C.c_uint32), ("resident", C.c_uint32), ("rebuilt", C.c_uint32),
+                ("entered", C.c_uint32), ("missing", C.c_uint32), ("reserved", C.c_uint32),
+                ("decoded_voxels", C.c_uint64), ("ms", C.c_float), ("reserved2", C.c_uint32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("reserved")}
+
+
+class ServeInfo(C.Structure):
+    """csv_serve_info."""
+    _fields_ = [("slots", C.c_void_p), ("n_slots", C.c_uint64), ("cache", C.c_void_p), ("cache_labels", C.c_uint64),
+                ("palette_table", C.c_uint64), ("bricks_per_axis", C.c_uint32), ("brick_size", C.c_uint32),
+                ("grid_size", C.c_float), ("pad", C.c_uint32), ("focal", C.c_double), ("cos_half", C.c_double),
+                ("decode_status", C.c_void_p)]
+
+
 _lib = None
 
 
@@ -106,6 +140,13 @@ def load_library() -> C.CDLL:
                              vp, C.c_uint32, vp, vp, vp, vp]
     L.csv_synth_volume.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_uint32, C.c_uint32,
                                    C.c_float, C.c_float, C.c_float, C.c_uint64, vp]
+    L.csv_serve_create.argtypes = [vp, vp, C.POINTER(ServeConfig), u64p, C.c_uint32, C.POINTER(vp)]
+    L.csv_serve_submit.argtypes = [vp, C.c_uint32, C.POINTER(View), vp, vp]
+    L.csv_serve_step.argtypes = [vp, vp, C.POINTER(C.c_uint64)]
+    L.csv_serve_poll.argtypes = [vp, C.POINTER(FrameStats), C.c_uint32, C.POINTER(C.c_uint32), C.c_int]
+    L.csv_serve_camera.argtypes = [vp, C.POINTER(View), vp]
+    L.csv_serve_state.argtypes = [vp, C.POINTER(ServeInfo)]
+    L.csv_serve_destroy.argtypes = [vp]
     _lib = L
     return L
 
@@ -351,6 +392,91 @@ class Codec:
         self._check(self.lib.csv_synth_volume(self.handle, C.c_void_p(d_volume.data_ptr()), W, H, D, kind, n_cells,
                                               n_tubes, r_min, r_max, zero_frac, seed,
                                               C.c_void_p(_stream_handle(stream))))
+
+
+class Server:
+    """The viewer's frame loop on the device (csv_serve_*): sessions submit cameras, steps plan, cache, decode and
+    render on one stream; poll returns per-frame counters and step times."""
+
+    def __init__(self, codec: Codec, dataset: Dataset, width: int, height: int, fov: float, cache_bytes: int = 0,
+                 max_sessions: int = 1, cone: int = CONE_SCREEN, hidden=None):
+        self.codec, self.dataset, self.lib = codec, dataset, codec.lib
+        cfg = ServeConfig(width, height, max_sessions, cone, fov, cache_bytes)
+        hid = np.ascontiguousarray(hidden if hidden is not None else np.zeros(1, np.uint64), np.uint64)
+        h = C.c_void_p()
+        codec._check(self.lib.csv_serve_create(codec.handle, dataset.handle, C.byref(cfg),
+                                               hid.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                               0 if hidden is None else len(hidden), C.byref(h)))
+        self.handle = h
+        self.width, self.height, self.fov = width, height, fov
+        self._keep = {}
+
+    @staticmethod
+    def view(position, direction) -> View:
+        v = View()
+        for a in range(3):
+            v.position[a] = float(position[a])
+            v.direction[a] = float(direction[a])
+        return v
+
+    def submit(self, session: int, position, direction, d_label, d_depth):
+        v = self.view(position, direction)
+        self._keep[session] = (d_label, d_depth)
+        self.codec._check(self.lib.csv_serve_submit(self.handle, session, C.byref(v), C.c_void_p(d_label.data_ptr()),
+                                                    C.c_void_p(d_depth.data_ptr())))
+
+    def step(self, stream=None) -> int:
+        sid = C.c_uint64()
+        self.codec._check(self.lib.csv_serve_step(self.handle, C.c_void_p(_stream_handle(stream)), C.byref(sid)))
+        return sid.value
+
+    def poll(self, wait: bool = True, max_frames: int = 4096):
+        out = (FrameStats * max_frames)()
+        n = C.c_uint32()
+        self.codec._check(self.lib.csv_serve_poll(self.handle, out, max_frames, C.byref(n), 1 if wait else 0))
+        return [out[i].as_dict() for i in range(n.value)]
+
+    def camera(self, position, direction) -> np.ndarray:
+        """The float32[16] camera the server renders this view with."""
+        v = self.view(position, direction)
+        cam = (C.c_float * 16)()
+        self.codec._check(self.lib.csv_serve_camera(self.handle, C.byref(v), cam))
+        return np.array(cam[:], np.float32)
+
+    def info(self) -> ServeInfo:
+        i = ServeInfo()
+        self.codec._check(self.lib.csv_serve_state(self.handle, C.byref(i)))
+        return i
+
+    def slots_tensor(self):
+        """Device view (uint8, n_slots * 16 bytes) of the brick slot table."""
+        i = self.info()
+        return _device_view(i.slots, int(i.n_slots) * 16, "|u1", self.codec.device)
+
+    def cache_tensor(self):
+        """Device view (int64) of the label cache: palette-0 table, then blocks."""
+        i = self.info()
+        return _device_view(i.cache, int(i.cache_labels), "<i8", self.codec.device)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.csv_serve_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _device_view(ptr: int, n: int, typestr: str, device: int):
+    import torch
+
+    class _View:
+        __cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False), "version": 2}
+
+    return torch.as_tensor(_View(), device=f"cuda:{device}")
 
 
 def requests(bricks, lods, dsts) -> np.ndarray:

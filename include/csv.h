@@ -196,8 +196,9 @@ int csv_decode_image(csv_ctx* ctx, const uint8_t* image, size_t len, uint32_t lo
  * no hit).  The camera is camera.js:getUniformData (camera.js:61-77); the
  * volume is the cube [0, grid_size)^3 of bricks_per_axis^3 bricks
  * (SceneInfo, rayTrace.wgsl:87-96).  Slots are indexed by brick Morton code
- * (rayTrace.wgsl:654-657).  d_requests (optional, n_slots words) gets 1 for
- * every missing slot a ray crossed (brickRequests, rayTrace.wgsl:686).
+ * (rayTrace.wgsl:654-657).  d_requests (optional, n_slots words, zeroed by
+ * the caller) gets 1 for every non-empty resident brick a ray entered and 3
+ * for every missing one it crossed (brickRequests, rayTrace.wgsl:684-686).
  * Bit-identical to the scalar restatement on the CPU (same float operations,
  * no fused multiply-add). */
 typedef struct csv_camera {
@@ -224,6 +225,90 @@ int csv_render(csv_ctx* ctx, const csv_camera* camera, uint32_t width, uint32_t 
                uint32_t brick_size, uint32_t bricks_per_axis, const csv_brick_slot* d_slots, uint64_t n_slots,
                const uint64_t* d_labels, const uint64_t* d_hidden, uint32_t n_hidden, uint64_t* d_label_out,
                float* d_depth_out, uint32_t* d_requests, void* stream);
+
+/* ---- serving loop --------------------------------------------------------
+ * The viewer's frame loop with its cache on the device.  Replaces the host
+ * side of renderLoop.js:208-340 (frame), cacheProcessing.js:99-232
+ * (processCache), cacheManager.js:10-246 (CacheState), camera.js:103-137
+ * (calculateBrickLOD), culling.js:22-171 (camera-moved, cone and
+ * transfer-function tests), and drives the decoder and ray marcher above.
+ *
+ * A server holds one dataset (one brick size), a label cache in HBM and the
+ * brick slot table.  Up to max_sessions viewers share it: each submits frames
+ * (a camera and two device images); csv_serve_step serves every session with
+ * a pending frame in one step -- one plan over all their views (a brick is
+ * needed at the finest LOD any of them asks for), one decode launch for all
+ * admitted bricks, one render per view -- all enqueued on `stream` with no
+ * host synchronisation.  A session that submits again before the step
+ * replaces its pending frame (the newest camera wins).  The plan runs only
+ * when the set of sessions changed or a camera moved more than 0.5 units or
+ * turned more than 0.05 rad since the last plan (culling.js:6-56); otherwise
+ * the step only renders.  csv_serve_poll returns per-frame counters and the
+ * device time of each finished step.  One host thread per server. */
+typedef struct csv_server csv_server;
+
+#define CSV_CONE_REFERENCE 0u /* cone half-angle fov/2 (culling.js:132) */
+#define CSV_CONE_SCREEN 1u    /* cone half-angle to the screen corner: every brick a ray can reach */
+
+typedef struct csv_serve_config {
+    uint32_t width, height;   /* viewport of every session (pixels) */
+    uint32_t max_sessions;    /* sessions served together, 1..8 (0 = 1) */
+    uint32_t cone;            /* CSV_CONE_* */
+    double fov;               /* vertical field of view, radians (camera.js:19: pi/3) */
+    uint64_t cache_bytes;     /* label cache incl. a palette-0 table of 8 B per brick; 0 = 24 GiB */
+} csv_serve_config;
+
+typedef struct csv_view {
+    double position[3];  /* camera position, voxel units */
+    double direction[3]; /* view direction (normalised by the server) */
+} csv_view;
+
+typedef struct csv_frame_stats {
+    uint64_t step;           /* step sequence number */
+    uint32_t session;
+    uint32_t planned;        /* 1 when the step re-planned */
+    uint32_t visible;        /* bricks some view needs */
+    uint32_t decoded;        /* (brick, LOD) pairs admitted and decoded */
+    uint32_t freed;          /* cache blocks released */
+    uint32_t resident;       /* bricks holding a cache block after the step */
+    uint32_t rebuilt;        /* 1 when the cache was rebuilt (allocation failure) */
+    uint32_t entered;        /* non-empty bricks some ray entered */
+    uint32_t missing;        /* of those, bricks with no data in the cache */
+    uint32_t reserved;
+    uint64_t decoded_voxels;
+    float ms;                /* device time of the whole step (CUDA events) */
+    uint32_t reserved2;
+} csv_frame_stats;
+
+/* Device views of a server's state, for checks and custom passes. */
+typedef struct csv_serve_info {
+    const csv_brick_slot* slots; /* n_slots entries, by brick Morton code */
+    uint64_t n_slots;
+    const uint64_t* cache;       /* cache_labels u64: palette-0 table, then blocks */
+    uint64_t cache_labels;
+    uint64_t palette_table;      /* labels before the first block */
+    uint32_t bricks_per_axis, brick_size;
+    float grid_size;
+    uint32_t pad;
+    double focal;                /* LOD focal length, (min(W, H)/2) / tan(fov/2) */
+    double cos_half;             /* cosine of the cone's half-angle */
+    const uint32_t* decode_status; /* per admitted request of the last planned step */
+} csv_serve_info;
+
+/* `hidden`: labels the transfer function hides (host array, any order); a
+ * brick whose palette has no other non-zero label is empty. */
+int csv_serve_create(csv_ctx* ctx, const csv_dataset* ds, const csv_serve_config* cfg, const uint64_t* hidden,
+                     uint32_t n_hidden, csv_server** out);
+/* d_label (W*H u64) and d_depth (W*H f32) are device images the step writes. */
+int csv_serve_submit(csv_server* srv, uint32_t session, const csv_view* view, uint64_t* d_label, float* d_depth);
+int csv_serve_step(csv_server* srv, void* stream, uint64_t* step_id);
+/* Up to `max` finished frames (one per session of each finished step), oldest
+ * first; wait != 0 blocks until every step enqueued so far has finished. */
+int csv_serve_poll(csv_server* srv, csv_frame_stats* out, uint32_t max, uint32_t* n_out, int wait);
+/* The float camera the server renders a view with (camera.js:61-77). */
+int csv_serve_camera(const csv_server* srv, const csv_view* view, csv_camera* out);
+int csv_serve_state(const csv_server* srv, csv_serve_info* info);
+int csv_serve_destroy(csv_server* srv);
 
 /* ---- workload generator (no reference counterpart) --------------------
  * Seeded synthetic label volume on the device, x fastest: kind 0 = Voronoi

@@ -640,6 +640,14 @@ static int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v
 void or_render(const float* cam, uint32_t W, uint32_t H, float grid, uint32_t bsz, uint32_t bpa,
                const or_slot* slots, uint64_t n_slots, const uint64_t* labels, const uint64_t* hidden,
                uint32_t n_hidden, uint64_t* out_label, float* out_depth, uint32_t* miss) {
+    or_render_rows(cam, W, H, 0, 1, grid, bsz, bpa, slots, n_slots, labels, hidden, n_hidden, out_label, out_depth,
+                   miss, NULL);
+}
+
+void or_render_rows(const float* cam, uint32_t W, uint32_t H, uint32_t y0, uint32_t ystep, float grid, uint32_t bsz,
+                    uint32_t bpa, const or_slot* slots, uint64_t n_slots, const uint64_t* labels,
+                    const uint64_t* hidden, uint32_t n_hidden, uint64_t* out_label, float* out_depth, uint32_t* miss,
+                    uint32_t* requests) {
     const float o[3] = {cam[0], cam[1], cam[2]};
     const float thf = cam[3];
     const float fw = (float)W, fh = (float)H, aspect = fw / fh;
@@ -647,7 +655,8 @@ void or_render(const float* cam, uint32_t W, uint32_t H, float grid, uint32_t bs
     int lb = 0;
     while ((1 << lb) < bs) ++lb;
     const int numBricks = (int)bpa > 1 ? (int)bpa : 1;
-    for (uint32_t py = 0; py < H; ++py)
+    if (ystep == 0) ystep = 1;
+    for (uint32_t py = y0; py < H; py += ystep)
         for (uint32_t px = 0; px < W; ++px) {
             const size_t pix = (size_t)py * W + px;
             out_label[pix] = 0;
@@ -707,9 +716,13 @@ void or_render(const float* cam, uint32_t W, uint32_t H, float grid, uint32_t bs
                 if (!skip) {
                     sl = slots[m];
                     if (sl.flags & 1u) skip = 1;
-                    else if (sl.flags & 2u) {
-                        skip = 1;
-                        if (miss) miss[pix]++;
+                    else {
+                        /* brickRequests (rayTrace.wgsl:684-686): 1 resident, 3 missing */
+                        if (requests) requests[m] = (sl.flags & 2u) ? 3u : 1u;
+                        if (sl.flags & 2u) {
+                            skip = 1;
+                            if (miss) miss[pix]++;
+                        }
                     }
                 }
                 if (!skip) {

@@ -65,6 +65,50 @@ typedef struct {
 void or_render(const float* cam, uint32_t W, uint32_t H, float grid_size, uint32_t brick_size,
                uint32_t bricks_per_axis, const or_slot* slots, uint64_t n_slots, const uint64_t* labels,
                const uint64_t* hidden, uint32_t n_hidden, uint64_t* out_label, float* out_depth, uint32_t* miss);
+/* The same for rows y0, y0 + ystep, ... only (the other rows of the outputs
+ * are left as they are); requests (n_slots words or NULL) receives 1 for every
+ * non-empty resident brick a ray entered and 3 for every missing one. */
+void or_render_rows(const float* cam, uint32_t W, uint32_t H, uint32_t y0, uint32_t ystep, float grid_size,
+                    uint32_t brick_size, uint32_t bricks_per_axis, const or_slot* slots, uint64_t n_slots,
+                    const uint64_t* labels, const uint64_t* hidden, uint32_t n_hidden, uint64_t* out_label,
+                    float* out_depth, uint32_t* miss, uint32_t* requests);
+
+/* camera.js:61-77 (getUniformData): float32[16] from a double position,
+ * direction and vertical field of view. */
+void or_camera_uniform(const double* pos, const double* dir, double fov, float* out16);
+/* Planning constants of a W x H viewer: focal length (camera.js:114 with
+ * min(W, H), renderLoop.js:374), the cosine of the cone's half-angle (cone 0:
+ * fov/2 as culling.js:132; cone 1: the screen's half-diagonal) and the brick's
+ * bounding radius (culling.js:128). */
+void or_serve_constants(uint32_t W, uint32_t H, double fov, uint32_t cone, uint32_t b, double* focal,
+                        double* cos_half, double* radius);
+
+/* The viewer's frame loop (csv_oracle_serve.c): plan, cache, decode, render. */
+typedef struct or_server or_server;
+enum {
+    OR_ST_PLANNED = 0,  /* 1 when the step re-planned (a camera moved) */
+    OR_ST_VISIBLE = 1,  /* bricks some view needs */
+    OR_ST_DECODED = 2,  /* (brick, LOD) pairs admitted and decoded */
+    OR_ST_FREED = 3,    /* blocks returned to the free stacks */
+    OR_ST_RESIDENT = 4, /* bricks holding a block after the step */
+    OR_ST_REBUILT = 5,  /* 1 when the cache was rebuilt */
+    OR_ST_ENTERED = 6,  /* non-empty bricks some ray entered */
+    OR_ST_MISSING = 7,  /* of those, bricks not resident */
+    OR_ST_VOX_LO = 8,   /* decoded labels, low and high words */
+    OR_ST_VOX_HI = 9,
+    OR_SERVE_STATS = 10
+};
+or_server* or_serve_new(const uint8_t* img, size_t len, uint32_t W, uint32_t H, double fov, uint32_t cone,
+                        uint64_t cache_bytes, const uint64_t* hidden, uint32_t n_hidden);
+/* One step for n views (sessions sess[k], view k = position[3], direction[3]);
+ * images k at out_label + k*W*H, out_depth + k*W*H; stats: OR_SERVE_STATS words. */
+int or_serve_step(or_server* s, const uint32_t* sess, const double* views, uint32_t n, uint64_t* out_label,
+                  float* out_depth, uint32_t* stats);
+uint64_t or_serve_n_slots(const or_server* s);
+uint32_t or_serve_bricks_per_axis(const or_server* s);
+const or_slot* or_serve_slots(const or_server* s);
+const uint64_t* or_serve_cache(const or_server* s);
+void or_serve_free(or_server* s);
 
 void or_free(void* p);
 

@@ -63,6 +63,27 @@ class Oracle:
         L.or_brick_lod.argtypes = [C.POINTER(C.c_double), C.c_double, C.POINTER(C.c_double), C.c_double, C.c_uint32]
         L.or_render.argtypes = [C.POINTER(C.c_float), C.c_uint32, C.c_uint32, C.c_float, C.c_uint32, C.c_uint32,
                                 C.c_void_p, C.c_uint64, _u64p, _u64p, C.c_uint32, _u64p, C.POINTER(C.c_float), _u32p]
+        L.or_camera_uniform.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double,
+                                        C.POINTER(C.c_float)]
+        L.or_serve_constants.argtypes = [C.c_uint32, C.c_uint32, C.c_double, C.c_uint32, C.c_uint32,
+                                         C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.or_serve_new.restype = C.c_void_p
+        L.or_serve_new.argtypes = [_u8p, C.c_size_t, C.c_uint32, C.c_uint32, C.c_double, C.c_uint32, C.c_uint64,
+                                   _u64p, C.c_uint32]
+        L.or_serve_step.argtypes = [C.c_void_p, _u32p, C.POINTER(C.c_double), C.c_uint32, _u64p,
+                                    C.POINTER(C.c_float), _u32p]
+        L.or_serve_n_slots.restype = C.c_uint64
+        L.or_serve_n_slots.argtypes = [C.c_void_p]
+        L.or_serve_bricks_per_axis.restype = C.c_uint32
+        L.or_serve_bricks_per_axis.argtypes = [C.c_void_p]
+        L.or_serve_slots.restype = C.c_void_p
+        L.or_serve_slots.argtypes = [C.c_void_p]
+        L.or_serve_cache.restype = C.c_void_p
+        L.or_serve_cache.argtypes = [C.c_void_p]
+        L.or_serve_free.argtypes = [C.c_void_p]
+        L.or_render_rows.argtypes = [C.POINTER(C.c_float), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float,
+                                     C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint64, _u64p, _u64p, C.c_uint32, _u64p,
+                                     C.POINTER(C.c_float), _u32p, _u32p]
         self.lib = L
 
     def brick_lod(self, center, brick_size, cam, focal, max_lod) -> int:
@@ -71,8 +92,10 @@ class Oracle:
         return int(self.lib.or_brick_lod(c, brick_size, p, focal, max_lod))
 
     def render(self, cam16: np.ndarray, W: int, H: int, grid: float, brick: int, bpa: int, slots: np.ndarray,
-               labels: np.ndarray, hidden: np.ndarray | None = None):
-        """cam16: float32[16] (camera.js getUniformData layout); slots: structured (offset u8, lod u4, flags u4)."""
+               labels: np.ndarray, hidden: np.ndarray | None = None, rows=None, with_requests: bool = False):
+        """cam16: float32[16] (camera.js getUniformData layout); slots: structured (offset u8, lod u4, flags u4).
+
+        rows=(y0, ystep) renders only those rows; with_requests adds the per-slot request words."""
         cam = np.ascontiguousarray(cam16, np.float32)
         lab = np.ascontiguousarray(labels, np.uint64)
         hid = np.ascontiguousarray(hidden if hidden is not None else np.zeros(1, np.uint64), np.uint64)
@@ -81,9 +104,13 @@ class Oracle:
         dep = np.zeros(W * H, np.float32)
         miss = np.zeros(W * H, np.uint32)
         sl = np.ascontiguousarray(slots)
-        self.lib.or_render(cam.ctypes.data_as(C.POINTER(C.c_float)), W, H, grid, brick, bpa, sl.ctypes.data,
-                           len(sl), _ptr(lab, _u64p), _ptr(hid, _u64p), nh, _ptr(out, _u64p),
-                           dep.ctypes.data_as(C.POINTER(C.c_float)), _ptr(miss, _u32p))
+        y0, ystep = rows if rows is not None else (0, 1)
+        req = np.zeros(len(sl), np.uint32)
+        self.lib.or_render_rows(cam.ctypes.data_as(C.POINTER(C.c_float)), W, H, y0, ystep, grid, brick, bpa,
+                                sl.ctypes.data, len(sl), _ptr(lab, _u64p), _ptr(hid, _u64p), nh, _ptr(out, _u64p),
+                                dep.ctypes.data_as(C.POINTER(C.c_float)), _ptr(miss, _u32p), _ptr(req, _u32p))
+        if with_requests:
+            return out.reshape(H, W), dep.reshape(H, W), miss.reshape(H, W), req
         return out.reshape(H, W), dep.reshape(H, W), miss.reshape(H, W)
 
     def morton3(self, x, y, z) -> int:
@@ -170,6 +197,69 @@ class Oracle:
         st = self.lib.or_seek_index(_ptr(f, _u32p), _ptr(c, _u32p), _ptr(e, _u8p), len(enc), nsym, P, brick, S,
                                     _ptr(nops, _u32p), _ptr(ls, _u32p), _ptr(ck, _u32p), maxc, _ptr(nck, _u32p))
         return int(nops[0]), ls, ck[:4 * int(nck[0])].reshape(-1, 4), st
+
+
+SERVE_STATS = ["planned", "visible", "decoded", "freed", "resident", "rebuilt", "entered", "missing"]
+SLOT_DTYPE = np.dtype([("offset", "<u8"), ("lod", "<u4"), ("flags", "<u4")])
+
+
+def camera_uniform(oracle: "Oracle", position, direction, fov: float) -> np.ndarray:
+    p = (C.c_double * 3)(*position)
+    d = (C.c_double * 3)(*direction)
+    out = (C.c_float * 16)()
+    oracle.lib.or_camera_uniform(p, d, fov, out)
+    return np.array(out[:], np.float32)
+
+
+class OracleServer:
+    """The viewer's frame loop restated on the CPU (csv_oracle_serve.c)."""
+
+    def __init__(self, oracle: "Oracle", image: bytes, W: int, H: int, fov: float, cone: int, cache_bytes: int,
+                 hidden=None):
+        self.lib, self.W, self.H = oracle.lib, W, H
+        self._img = np.frombuffer(image, np.uint8).copy()
+        hid = np.ascontiguousarray(np.sort(hidden) if hidden is not None else np.zeros(1, np.uint64), np.uint64)
+        self.h = self.lib.or_serve_new(_ptr(self._img, _u8p), len(self._img), W, H, fov, cone, cache_bytes,
+                                       _ptr(hid, _u64p), 0 if hidden is None else len(hidden))
+        if not self.h:
+            raise ValueError("or_serve_new failed")
+        self.n_slots = int(self.lib.or_serve_n_slots(self.h))
+        self.bpa = int(self.lib.or_serve_bricks_per_axis(self.h))
+
+    def step(self, sessions, views):
+        """views: per session (position[3], direction[3]); returns labels (n, H, W), depth (n, H, W), stats dict."""
+        n = len(sessions)
+        ss = np.ascontiguousarray(sessions, np.uint32)
+        vv = np.ascontiguousarray([list(p) + list(d) for p, d in views], np.float64)
+        lab = np.zeros(n * self.W * self.H, np.uint64)
+        dep = np.zeros(n * self.W * self.H, np.float32)
+        st = np.zeros(10, np.uint32)
+        rc = self.lib.or_serve_step(self.h, _ptr(ss, _u32p), vv.ctypes.data_as(C.POINTER(C.c_double)), n,
+                                    _ptr(lab, _u64p), dep.ctypes.data_as(C.POINTER(C.c_float)), _ptr(st, _u32p))
+        if rc:
+            raise ValueError("or_serve_step failed")
+        stats = {k: int(st[i]) for i, k in enumerate(SERVE_STATS)}
+        stats["decoded_voxels"] = int(st[8]) | (int(st[9]) << 32)
+        return lab.reshape(n, self.H, self.W), dep.reshape(n, self.H, self.W), stats
+
+    def slots(self) -> np.ndarray:
+        buf = (C.c_uint8 * (16 * self.n_slots)).from_address(self.lib.or_serve_slots(self.h))
+        return np.frombuffer(bytes(buf), SLOT_DTYPE)
+
+    def cache(self, n: int) -> np.ndarray:
+        buf = (C.c_uint64 * n).from_address(self.lib.or_serve_cache(self.h))
+        return np.frombuffer(bytes(buf), np.uint64)
+
+    def close(self):
+        if self.h:
+            self.lib.or_serve_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Reference:

@@ -61,11 +61,14 @@ def render_both(codec, oracle, cam, W, H, grid, b, bpa, slots, labels, hidden=No
     d_hidden = None if hidden is None else torch.from_numpy(np.sort(hidden).astype(np.int64)).cuda()
     codec.render(cam, W, H, grid, b, bpa, d_slots, labels, out, dep, d_requests=req, d_hidden=d_hidden)
     torch.cuda.synchronize()
-    ref_l, ref_d, miss = oracle.render(cam, W, H, grid, b, bpa, slots, labels.cpu().numpy().view(np.uint64),
-                                       None if hidden is None else np.sort(hidden).astype(np.uint64))
+    ref_l, ref_d, miss, ref_req = oracle.render(cam, W, H, grid, b, bpa, slots, labels.cpu().numpy().view(np.uint64),
+                                                None if hidden is None else np.sort(hidden).astype(np.uint64),
+                                                with_requests=True)
     got_l = out.cpu().numpy().view(np.uint64).reshape(H, W)
     got_d = dep.cpu().numpy().reshape(H, W)
-    return got_l, got_d, ref_l, ref_d, req.cpu().numpy(), miss
+    got_req = req.cpu().numpy().view(np.uint32)
+    assert np.array_equal(got_req, ref_req)  # the same bricks entered, the same resident/missing words
+    return got_l, got_d, ref_l, ref_d, got_req, miss
 
 
 @pytest.fixture(scope="module")
@@ -119,7 +122,9 @@ def test_render_hidden_labels_and_missing_bricks(codec, oracle, scene):
     assert np.array_equal(gl, rl)
     assert np.array_equal(gd.view(np.uint32), rd.view(np.uint32))
     assert not np.isin(gl, hidden).any()
-    flagged = set(np.nonzero(req)[0].tolist())
+    flagged = set(np.nonzero(req == 3)[0].tolist())
     missing = set(np.nonzero((sl["flags"] & SLOT_MISSING) & ~(sl["flags"] & SLOT_EMPTY))[0].tolist())
     assert flagged <= missing
     assert (len(flagged) > 0) == bool(miss.sum() > 0)
+    entered = set(np.nonzero(req == 1)[0].tolist())
+    assert entered and not (entered & missing)

@@ -1,0 +1,180 @@
+"""GPU: the serving loop (csv_serve_*) step by step against the CPU restatement of the viewer's frame loop.
+
+Every step is compared with the oracle server fed the same cameras: the brick
+slot table (which bricks are resident, at which LOD and at which cache
+offset), the per-step counters, and every session's label and depth image,
+bit for bit.  Small caches force evictions, free-stack reuse and rebuilds.
+"""
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+W, H = 96, 64
+FOV = math.pi / 3
+
+
+def _image(codec, shape, b, seed, kind=1):
+    import torch
+    vol = torch.empty(shape, dtype=torch.int64, device="cuda")
+    codec.synth_volume(vol, kind, 200, 40 if kind == 1 else 0, 1.5, 6.0, 0.3, seed)
+    codec.encode_device(vol, b)
+    return bytes(codec.encoded_image_tensor().cpu().numpy())
+
+
+@pytest.fixture(scope="module")
+def cube16(codec):
+    return _image(codec, (128, 128, 128), 16, 41)
+
+
+@pytest.fixture(scope="module")
+def slab32(codec):
+    return _image(codec, (96, 128, 256), 32, 42)  # 8 x 4 x 3 bricks: the slot grid holds absent bricks
+
+
+def _orbit_views(center, n, r0, r1, yaw0=0.2, pitch=0.25):
+    from csvb200.camera import orbit
+    out = []
+    for f in range(n):
+        r = r0 + (r1 - r0) * f / max(1, n - 1)
+        out.append(orbit(center, r, yaw0 + 0.35 * f, pitch - 0.04 * f))
+    return out
+
+
+def _run_pair(codec, oracle, img, steps, cache_bytes, cone, sessions=1, hidden=None):
+    """steps: list of per-step lists of (session, (pos, dir)); compares GPU and oracle after every step."""
+    import torch
+    from csvb200 import Server
+    from oracle import SLOT_DTYPE, OracleServer, camera_uniform
+    ds = codec.open(img)
+    srv = Server(codec, ds, W, H, FOV, cache_bytes=cache_bytes, max_sessions=sessions, cone=cone, hidden=hidden)
+    ref = OracleServer(oracle, img, W, H, FOV, cone, cache_bytes, hidden=hidden)
+    labs = [torch.zeros(W * H, dtype=torch.int64, device="cuda") for _ in range(sessions)]
+    deps = [torch.zeros(W * H, dtype=torch.float32, device="cuda") for _ in range(sessions)]
+    info = srv.info()
+    assert info.n_slots == ref.n_slots and info.bricks_per_axis == ref.bpa
+    seen = {"rebuilt": 0, "freed": 0, "planned0": 0}
+    for k, step in enumerate(steps):
+        for s, (pos, d) in step:
+            srv.submit(s, pos, d, labs[s], deps[s])
+            assert np.array_equal(srv.camera(pos, d), camera_uniform(oracle, pos, d, FOV))
+        sid = srv.step()
+        frames = srv.poll(wait=True)
+        assert [f["step"] for f in frames] == [sid] * len(step)
+        rl, rd, rst = ref.step([s for s, _ in step], [v for _, v in step])
+        got = frames[0]
+        for key in ["planned", "visible", "decoded", "freed", "resident", "rebuilt", "entered", "missing",
+                    "decoded_voxels"]:
+            assert got[key] == rst[key], (k, key, got[key], rst[key])
+        slots = srv.slots_tensor().cpu().numpy().view(SLOT_DTYPE)
+        assert np.array_equal(slots, ref.slots()), k
+        if got["planned"] and got["decoded"]:
+            assert int(_status(srv, got["decoded"]).max()) == 0
+        for j, (s, _) in enumerate(step):
+            gl = labs[s].cpu().numpy().view(np.uint64).reshape(H, W)
+            gd = deps[s].cpu().numpy().reshape(H, W)
+            assert np.array_equal(gl, rl[j]), (k, s, int((gl != rl[j]).sum()))
+            assert np.array_equal(gd.view(np.uint32), rd[j].view(np.uint32)), (k, s)
+        seen["rebuilt"] += got["rebuilt"]
+        seen["freed"] += got["freed"]
+        seen["planned0"] += got["planned"] == 0
+    # the resident labels equal the oracle's cache wherever a slot points
+    cache = srv.cache_tensor().cpu().numpy().view(np.uint64)
+    rc = ref.cache(len(cache))
+    for sl in slots[(slots["flags"] == 0)]:
+        n = 8 ** int(sl["lod"]) if sl["offset"] >= info.palette_table else 1
+        o = int(sl["offset"])
+        assert np.array_equal(cache[o:o + n], rc[o:o + n])
+    srv.close()
+    ref.close()
+    ds.close()
+    return seen
+
+
+def _status(srv, n):
+    from csvb200 import _device_view
+    return _device_view(srv.info().decode_status, n, "<u4", srv.codec.device).cpu().numpy()
+
+
+@pytest.mark.parametrize("cone", [0, 1])
+def test_serve_orbit_large_cache(codec, oracle, cube16, cone):
+    views = _orbit_views((64.0, 64.0, 64.0), 8, 170.0, 90.0)
+    steps = [[(0, v)] for v in views]
+    steps.insert(3, [(0, views[2])])  # camera did not move: render only
+    seen = _run_pair(codec, oracle, cube16, steps, 64 << 20, cone)
+    assert seen["planned0"] == 1 and seen["rebuilt"] == 0 and seen["freed"] > 0
+
+
+def test_serve_small_cache_rebuilds(codec, oracle, cube16):
+    views = _orbit_views((64.0, 64.0, 64.0), 8, 150.0, 60.0)
+    seen = _run_pair(codec, oracle, cube16, [[(0, v)] for v in views], 512 << 10, 1)
+    assert seen["rebuilt"] > 0
+
+
+def test_serve_medium_cache_reuses_free_blocks(codec, oracle, slab32):
+    views = _orbit_views((128.0, 64.0, 48.0), 10, 260.0, 120.0, yaw0=1.0, pitch=0.4)
+    _run_pair(codec, oracle, slab32, [[(0, v)] for v in views], 6 << 20, 1)
+
+
+def test_serve_two_sessions_one_step(codec, oracle, cube16):
+    a = _orbit_views((64.0, 64.0, 64.0), 5, 160.0, 100.0)
+    b = _orbit_views((64.0, 64.0, 64.0), 5, 120.0, 200.0, yaw0=2.5, pitch=-0.3)
+    steps = [[(0, a[k]), (1, b[k])] for k in range(5)]
+    steps.insert(2, [(1, b[1])])  # one session alone: the session set changed, so the step re-plans
+    _run_pair(codec, oracle, cube16, steps, 8 << 20, 1, sessions=2)
+
+
+def test_serve_hidden_labels(codec, oracle, cube16):
+    lab = oracle.decode_image(cube16, 4)[0]
+    vals, counts = np.unique(lab[lab != 0], return_counts=True)
+    hidden = vals[np.argsort(-counts)[:6]].astype(np.uint64)
+    views = _orbit_views((64.0, 64.0, 64.0), 4, 160.0, 110.0)
+    _run_pair(codec, oracle, cube16, [[(0, v)] for v in views], 64 << 20, 1, hidden=hidden)
+
+
+def test_serve_newest_frame_wins_and_errors(codec, cube16):
+    import torch
+    from csvb200 import CsvError, Server
+    ds = codec.open(cube16)
+    srv = Server(codec, ds, W, H, FOV, cache_bytes=16 << 20)
+    l1 = torch.zeros(W * H, dtype=torch.int64, device="cuda")
+    d1 = torch.zeros(W * H, dtype=torch.float32, device="cuda")
+    l2 = torch.zeros_like(l1)
+    d2 = torch.zeros_like(d1)
+    v = _orbit_views((64.0, 64.0, 64.0), 2, 160.0, 150.0)
+    srv.submit(0, *v[0], l1, d1)
+    srv.submit(0, *v[1], l2, d2)  # replaces the first
+    srv.step()
+    frames = srv.poll(wait=True)
+    assert len(frames) == 1
+    torch.cuda.synchronize()
+    assert int((l1 != 0).sum()) == 0 and int((l2 != 0).sum()) > 0
+    with pytest.raises(CsvError) as e:
+        srv.step()  # nothing submitted
+    assert e.value.code == -1
+    with pytest.raises(CsvError) as e:
+        srv.submit(1, *v[0], l1, d1)  # one session only
+    assert e.value.code == -5
+    srv.close()
+    ds.close()
+
+
+def test_serve_many_steps_without_polling(codec, cube16):
+    """More steps in flight than the ring holds: the server harvests the oldest itself; poll returns all."""
+    import torch
+    from csvb200 import Server
+    ds = codec.open(cube16)
+    srv = Server(codec, ds, W, H, FOV, cache_bytes=16 << 20)
+    lab = torch.zeros(W * H, dtype=torch.int64, device="cuda")
+    dep = torch.zeros(W * H, dtype=torch.float32, device="cuda")
+    views = _orbit_views((64.0, 64.0, 64.0), 150, 170.0, 80.0)
+    for v in views:
+        srv.submit(0, *v, lab, dep)
+        srv.step()
+    frames = srv.poll(wait=True, max_frames=1000)
+    assert [f["step"] for f in frames] == list(range(150))
+    assert all(f["ms"] > 0 for f in frames)
+    srv.close()
+    ds.close()
