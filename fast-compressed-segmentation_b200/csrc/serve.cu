@@ -6,25 +6,33 @@
 // per-brick decision runs on the device, in one stream, with no host round
 // trip between the steps of a frame:
 //
-//   plan_kernel    per brick: the LOD each view asks for (camera.js:103-137) and
-//                  the cone test (culling.js:87-153); keep / free / admit; the
-//                  brick's rank among the CTA's bricks of the same kind and LOD
-//   scan_kernel    one CTA: per-CTA bases of those ranks, then the cache policy
-//                  (free stacks per LOD, bump pointer, rebuild) for the frame
+//   plan_kernel    per brick: the LOD each open session asks for
+//                  (camera.js:103-137) and the cone test (culling.js:87-153);
+//                  the (brick, LOD) blocks to keep, free and admit; per-CTA counts
+//   scan_kernel    one CTA: per-CTA bases of those counts, then the cache policy
+//                  (free stacks per LOD, bump pointer, rebuild) for the step
 //   push_kernel    per brick: freed blocks onto their LOD's stack
-//   pop_kernel     per brick: admitted bricks pop a block or take fresh space;
-//                  their decode requests; the brick slot table the rays read
+//   pop_kernel     per brick: admitted blocks pop a stack entry or take fresh
+//                  space; their decode requests; every open session's slot table
 //   decode_kernel  (decode.cu) the admitted requests, count read on the device
-//   render_kernel  (ray.cu) one launch per view
-//   census_kernel  per brick: bricks the rays entered, and how many were missing
+//   render_kernel  (ray.cu) one launch per session with a new frame
+//   census_kernel  per brick: bricks each session's rays entered, and how many
+//                  had no data
+//
+// Sessions share the cache but not their LODs: a block is keyed by (brick,
+// LOD), each session's slot table points at the blocks of its own LODs, and a
+// session's plan uses the camera of its own last re-plan (it re-plans when it
+// moved more than 0.5 units or turned more than 0.05 rad, culling.js:6-56).
+// So a session's image is the same whichever other sessions are open, as long
+// as the cache has room for all of them.
 //
 // Orders the reference leaves open are fixed so that the result is
 // deterministic and equal to the CPU restatement (oracle/csv_oracle_serve.c):
 // frees are pushed in brick order; admissions are served LOD by LOD (coarse
 // first), in brick order within a LOD, popping the LOD's stack from the top and
-// then taking fresh space; a frame whose fresh space does not fit rebuilds the
-// cache (every needed brick placed again, coarse LODs first, until the space
-// runs out).  LOD-0 bricks and uniform bricks take no block: their slot reads
+// then taking fresh space; a step whose fresh space does not fit rebuilds the
+// cache (every needed block placed again, coarse LODs first, while space
+// remains).  LOD-0 bricks and uniform bricks take no block: their slot reads
 // palette[0] from a table at the start of the cache.
 #include <cuda_runtime.h>
 #include <math.h>
@@ -51,7 +59,7 @@ constexpr uint32_t kWarps = kBlk / 32;
 constexpr uint32_t kLods = 8;   // LOD slots; bricks up to 64^3 use 0..6
 constexpr uint8_t kNone = 0xFF;
 constexpr uint32_t kRing = 64;  // steps in flight before the host harvests one
-enum : uint32_t { CNT_FREE = 0, CNT_ALLOC = kLods, CNT_WANT = 2 * kLods, kCnt = 3 * kLods };
+enum : uint32_t { CNT_FREE = 0, CNT_ALLOC = kLods, CNT_NEED = 2 * kLods, kCnt = 3 * kLods };
 enum : uint8_t { BK_HAS = 1, BK_UNIFORM = 2 };
 
 struct ViewD {
@@ -63,32 +71,33 @@ struct ServeState {
     uint32_t top[kLods];       // free-stack sizes
     uint32_t T[kLods];         // stack sizes after this step's pushes
     uint32_t top_old[kLods];   // stack sizes before them
-    uint32_t fit[kLods];       // rebuild: bricks placed per LOD
+    uint32_t fit[kLods];       // rebuild: blocks placed per LOD
     uint32_t req_base[kLods];  // first request index of each LOD
     uint64_t base[kLods];      // first fresh offset per LOD (overflow / rebuild placement)
     uint64_t bump, cap;
     uint32_t mode;             // 0: keep the cache, 1: rebuild
     uint32_t n_req;            // admitted requests (read by the decode kernel)
-    uint32_t resident;
+    uint32_t resident;         // resident blocks
     uint32_t pad;
 };
 
-// One step's counters (the same words as the CPU restatement's OR_ST_*).
+// One step's counters; entered/missing per rendered session.
 struct StepStats {
-    uint32_t planned, visible, decoded, freed, resident, rebuilt, entered, missing, vox_lo, vox_hi;
+    uint32_t planned, visible, decoded, freed, resident, rebuilt, vox_lo, vox_hi;
+    uint32_t entered[kMaxViews], missing[kMaxViews];
 };
 
 struct PlanArgs {
     ViewD v[kMaxViews];
-    uint32_t n_views, b, max_lod, nb;
+    uint32_t sid[kMaxViews];
+    uint32_t n_views, b, max_lod, nb, n_cta;
     double focal, cos_half, radius, half;
     const uint32_t* ids;
     const uint8_t* bflag;
-    const uint8_t* res_lod;
-    uint8_t* want;
-    uint32_t* rank;  // free | alloc << 8 | want << 16: ranks among the CTA's bricks of the same kind and LOD
-    uint32_t* cnt;   // [kCnt][n_cta]
-    uint32_t n_cta;
+    const uint8_t* res;   // bit l: block at LOD l resident
+    uint8_t* want;        // [session][brick]
+    uint8_t* need;        // bit l: some open session needs LOD l of the brick
+    uint32_t* cnt;        // [kCnt][n_cta]
     StepStats* stats;
 };
 
@@ -126,76 +135,77 @@ __device__ __forceinline__ uint32_t brick_lod(const PlanArgs& A, const double* c
     return best;
 }
 
-// Rank of this thread among the CTA's threads with the same key (kNone: none),
-// in thread order; per-warp counts go to s_wc[warp][key].
-__device__ __forceinline__ uint32_t warp_rank(uint32_t key, uint32_t (*s_wc)[kLods]) {
+// Per LOD l: counts of the CTA's threads whose `mask` has bit l (s_tot[l]) and,
+// in rank[l], this thread's rank among them in thread order.  Every thread of
+// the CTA calls it; s_wc is [kWarps][kLods] shared scratch.
+__device__ __forceinline__ void cta_ranks(uint32_t mask, uint32_t (&rank)[kLods], uint32_t (*s_wc)[kLods],
+                                          uint32_t* s_tot) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    const uint32_t peers = __match_any_sync(0xffffffffu, key);
-    if (key != kNone && lane == (uint32_t)(__ffs(peers) - 1)) s_wc[warp][key] = __popc(peers);
-    return __popc(peers & ((1u << lane) - 1u));
+    const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+    for (uint32_t l = 0; l < kLods; ++l) {
+        const uint32_t b = __ballot_sync(0xffffffffu, (mask >> l) & 1u);
+        rank[l] = __popc(b & lt);
+        if (lane == 0) s_wc[warp][l] = __popc(b);
+    }
+    __syncthreads();
+    if (threadIdx.x < kLods) {
+        uint32_t acc = 0;
+        for (uint32_t w = 0; w < kWarps; ++w) {
+            const uint32_t t = s_wc[w][threadIdx.x];
+            s_wc[w][threadIdx.x] = acc;
+            acc += t;
+        }
+        s_tot[threadIdx.x] = acc;
+    }
+    __syncthreads();
+#pragma unroll
+    for (uint32_t l = 0; l < kLods; ++l) rank[l] += s_wc[warp][l];
 }
 
 __global__ void __launch_bounds__(kBlk) plan_kernel(PlanArgs A) {
-    __shared__ uint32_t s_wc[3][kWarps][kLods];
-    __shared__ uint32_t s_wb[3][kWarps][kLods];
+    __shared__ uint32_t s_wc[kWarps][kLods];
+    __shared__ uint32_t s_tot[kLods];
     __shared__ uint32_t s_vis;
     const uint32_t tid = threadIdx.x, i = blockIdx.x * kBlk + tid;
-    for (uint32_t k = tid; k < 3 * kWarps * kLods; k += kBlk) (&s_wc[0][0][0])[k] = 0;
     if (tid == 0) s_vis = 0;
-    __syncthreads();
-    uint32_t w = kNone, r = kNone;
-    bool uni = false;
+    uint32_t need = 0, res = 0;
+    bool vis = false;
     if (i < A.nb) {
         const uint8_t bf = A.bflag[i];
-        uni = (bf & BK_UNIFORM) != 0;
-        r = A.res_lod[i];
-        if (bf & BK_HAS) {
-            const uint32_t id = A.ids[i];
-            const double c[3] = {(double)compact3(id) * (double)A.b + A.half,
-                                 (double)compact3(id >> 1) * (double)A.b + A.half,
-                                 (double)compact3(id >> 2) * (double)A.b + A.half};
-            for (uint32_t s = 0; s < A.n_views; ++s) {
-                if (!in_cone(A, c, A.v[s])) continue;
-                const uint32_t l = brick_lod(A, c, A.v[s]);
-                if (w == kNone || l > w) w = l;
+        const bool uni = (bf & BK_UNIFORM) != 0;
+        res = A.res[i];
+        const uint32_t id = A.ids[i];
+        const double c[3] = {(double)compact3(id) * (double)A.b + A.half,
+                             (double)compact3(id >> 1) * (double)A.b + A.half,
+                             (double)compact3(id >> 2) * (double)A.b + A.half};
+        for (uint32_t s = 0; s < A.n_views; ++s) {
+            uint32_t w = kNone;
+            if ((bf & BK_HAS) && in_cone(A, c, A.v[s])) w = brick_lod(A, c, A.v[s]);
+            A.want[(size_t)A.sid[s] * A.nb + i] = (uint8_t)w;
+            if (w != kNone) {
+                vis = true;
+                if (w > 0 && !uni) need |= 1u << w;
             }
         }
-        A.want[i] = (uint8_t)w;
+        A.need[i] = (uint8_t)need;
     }
-    const bool cached = w != kNone && w > 0 && !uni;
-    const bool keep = cached && r == w;
-    const uint32_t kfree = (r != kNone && !keep) ? r : kNone;
-    const uint32_t kalloc = (cached && !keep) ? w : kNone;
-    const uint32_t kwant = cached ? w : kNone;
-    const uint32_t rf = warp_rank(kfree, s_wc[0]);
-    const uint32_t ra = warp_rank(kalloc, s_wc[1]);
-    const uint32_t rw = warp_rank(kwant, s_wc[2]);
-    const uint32_t vis = __popc(__ballot_sync(0xffffffffu, w != kNone));
-    if ((tid & 31u) == 0 && vis) atomicAdd(&s_vis, vis);
+    const uint32_t nv = __popc(__ballot_sync(0xffffffffu, vis));
     __syncthreads();
-    if (tid < 3 * kLods) {  // exclusive scan over the warps, per (kind, LOD)
-        const uint32_t kind = tid / kLods, l = tid % kLods;
-        uint32_t acc = 0;
-        for (uint32_t wp = 0; wp < kWarps; ++wp) {
-            s_wb[kind][wp][l] = acc;
-            acc += s_wc[kind][wp][l];
-        }
-        A.cnt[(kind * kLods + l) * A.n_cta + blockIdx.x] = acc;
-    }
-    __syncthreads();
-    if (i < A.nb) {
-        const uint32_t wp = tid >> 5;
-        uint32_t pk = 0;
-        if (kfree != kNone) pk |= (s_wb[0][wp][kfree] + rf);
-        if (kalloc != kNone) pk |= (s_wb[1][wp][kalloc] + ra) << 8;
-        if (kwant != kNone) pk |= (s_wb[2][wp][kwant] + rw) << 16;
-        A.rank[i] = pk;
+    if ((tid & 31u) == 0 && nv) atomicAdd(&s_vis, nv);
+    uint32_t rank[kLods];
+    const uint32_t masks[3] = {res & ~need, need & ~res, need};
+#pragma unroll
+    for (uint32_t kind = 0; kind < 3; ++kind) {
+        cta_ranks(masks[kind], rank, s_wc, s_tot);
+        if (tid < kLods) A.cnt[(kind * kLods + tid) * A.n_cta + blockIdx.x] = s_tot[tid];
+        __syncthreads();
     }
     if (tid == 0 && s_vis) atomicAdd(&A.stats->visible, s_vis);
 }
 
 // One CTA: exclusive scans of the per-CTA counts (one warp per counter), then
-// the frame's cache policy by thread 0.
+// the step's cache policy by thread 0.
 __global__ void __launch_bounds__(1024) scan_kernel(const uint32_t* __restrict__ cnt, uint32_t* __restrict__ base,
                                                     uint32_t n_cta, uint32_t max_lod, uint32_t nb,
                                                     ServeState* __restrict__ S, StepStats* __restrict__ st) {
@@ -255,7 +265,7 @@ __global__ void __launch_bounds__(1024) scan_kernel(const uint32_t* __restrict__
     } else {
         uint64_t b = 0;
         for (uint32_t l = 1; l <= max_lod; ++l) {
-            const uint32_t W = tot[CNT_WANT + l];
+            const uint32_t W = tot[CNT_NEED + l];
             const uint64_t room = S->cap > b ? (S->cap - b) >> (3 * l) : 0ull;
             S->fit[l] = (uint32_t)(room < W ? room : W);
             S->base[l] = b;
@@ -284,111 +294,147 @@ __global__ void __launch_bounds__(1024) scan_kernel(const uint32_t* __restrict__
 }
 
 struct CacheArgs {
-    uint32_t nb, n_cta;
+    uint32_t sid[kMaxViews];
+    uint32_t n_views, nb, n_cta, max_lod;
+    uint64_t n_slots;
     const uint8_t* bflag;
-    const uint8_t* want;
-    const uint32_t* rank;
+    const uint8_t* want;   // [session][brick]
+    const uint8_t* need;
     const uint32_t* base;  // [kCnt][n_cta]
     const uint32_t* ids;
-    uint8_t* res_lod;
-    uint64_t* res_off;
+    uint8_t* res;
+    uint64_t* off;         // [brick][kLods]
     uint64_t* stack;       // [kLods][nb]
     const ServeState* S;
     csv_request* reqs;
-    csv_brick_slot* slots;
+    csv_brick_slot* slots; // [session][n_slots]
     uint64_t pal_region;
 };
 
 __global__ void __launch_bounds__(kBlk) push_kernel(CacheArgs A) {
+    __shared__ uint32_t s_wc[kWarps][kLods];
+    __shared__ uint32_t s_tot[kLods];
     const uint32_t i = blockIdx.x * kBlk + threadIdx.x;
-    if (i >= A.nb) return;
-    const uint32_t r = A.res_lod[i];
-    if (r == kNone) return;
-    const uint32_t w = A.want[i];
-    const bool cached = w != kNone && w > 0 && !(A.bflag[i] & BK_UNIFORM);
-    if (A.S->mode == 1) {
-        A.res_lod[i] = kNone;
+    const uint32_t mode = A.S->mode;
+    uint32_t res = 0, need = 0;
+    if (i < A.nb) {
+        res = A.res[i];
+        need = A.need[i];
+    }
+    if (mode == 1) {  // rebuild: every block is dropped
+        if (i < A.nb && res) A.res[i] = 0;
         return;
     }
-    if (cached && r == w) return;  // kept
-    const uint32_t pos = A.S->top_old[r] + A.base[(CNT_FREE + r) * A.n_cta + blockIdx.x] + (A.rank[i] & 255u);
-    A.stack[(size_t)r * A.nb + pos] = A.res_off[i];
-    A.res_lod[i] = kNone;
+    const uint32_t fr = res & ~need;
+    uint32_t rank[kLods];
+    cta_ranks(fr, rank, s_wc, s_tot);
+    if (i >= A.nb || !fr) return;
+#pragma unroll
+    for (uint32_t l = 1; l < kLods; ++l) {
+        if (!((fr >> l) & 1u)) continue;
+        const uint32_t pos = A.S->top_old[l] + A.base[(CNT_FREE + l) * A.n_cta + blockIdx.x] + rank[l];
+        A.stack[(size_t)l * A.nb + pos] = A.off[(size_t)i * kLods + l];
+    }
+    A.res[i] = (uint8_t)(res & need);
 }
 
 __global__ void __launch_bounds__(kBlk) pop_kernel(CacheArgs A) {
+    __shared__ uint32_t s_wc[kWarps][kLods];
+    __shared__ uint32_t s_tot[kLods];
     const uint32_t i = blockIdx.x * kBlk + threadIdx.x;
+    const uint32_t mode = A.S->mode;
+    uint32_t res = 0, need = 0;
+    if (i < A.nb) {
+        res = A.res[i];
+        need = A.need[i];
+    }
+    const uint32_t adm = mode == 0 ? (need & ~res) : need;
+    uint32_t rank[kLods];
+    cta_ranks(adm, rank, s_wc, s_tot);
     if (i >= A.nb) return;
-    const uint8_t bf = A.bflag[i];
-    const uint32_t w = A.want[i];
-    const bool uni = (bf & BK_UNIFORM) != 0;
-    const bool cached = w != kNone && w > 0 && !uni;
-    uint32_t r = A.res_lod[i];
-    if (cached && r != w) {
-        uint32_t k;
-        uint64_t off = 0;
-        bool placed = true;
-        if (A.S->mode == 0) {
-            k = A.base[(CNT_ALLOC + w) * A.n_cta + blockIdx.x] + ((A.rank[i] >> 8) & 255u);
-            const uint32_t T = A.S->T[w];
-            off = k < T ? A.stack[(size_t)w * A.nb + (T - 1 - k)] : A.S->base[w] + ((uint64_t)(k - T) << (3 * w));
-        } else {
-            k = A.base[(CNT_WANT + w) * A.n_cta + blockIdx.x] + ((A.rank[i] >> 16) & 255u);
-            placed = k < A.S->fit[w];
-            if (placed) off = A.S->base[w] + ((uint64_t)k << (3 * w));
-        }
-        if (placed) {
-            A.res_lod[i] = (uint8_t)w;
-            A.res_off[i] = off;
-            r = w;
+    if (adm) {
+#pragma unroll
+        for (uint32_t l = 1; l < kLods; ++l) {
+            if (!((adm >> l) & 1u)) continue;
+            uint32_t k;
+            uint64_t o;
+            if (mode == 0) {
+                k = A.base[(CNT_ALLOC + l) * A.n_cta + blockIdx.x] + rank[l];
+                const uint32_t T = A.S->T[l];
+                o = k < T ? A.stack[(size_t)l * A.nb + (T - 1 - k)] : A.S->base[l] + ((uint64_t)(k - T) << (3 * l));
+            } else {
+                k = A.base[(CNT_NEED + l) * A.n_cta + blockIdx.x] + rank[l];
+                if (k >= A.S->fit[l]) continue;
+                o = A.S->base[l] + ((uint64_t)k << (3 * l));
+            }
+            res |= 1u << l;
+            A.off[(size_t)i * kLods + l] = o;
             csv_request q;
             q.brick = i;
-            q.lod = w;
-            q.dst = A.pal_region + off;
-            A.reqs[A.S->req_base[w] + k] = q;
+            q.lod = l;
+            q.dst = A.pal_region + o;
+            A.reqs[A.S->req_base[l] + k] = q;
         }
+        A.res[i] = (uint8_t)res;
     }
-    csv_brick_slot sl;
-    sl.offset = 0;
-    sl.lod = 0;
-    sl.flags = 0;
-    if (!(bf & BK_HAS)) sl.flags = CSV_SLOT_EMPTY;
-    else if (r != kNone) {
-        sl.offset = A.pal_region + A.res_off[i];
-        sl.lod = r;
-    } else if (uni || w == 0) sl.offset = i;
-    else sl.flags = CSV_SLOT_MISSING;
-    A.slots[A.ids[i]] = sl;
+    const uint8_t bf = A.bflag[i];
+    const uint32_t m = A.ids[i];
+    for (uint32_t s = 0; s < A.n_views; ++s) {
+        const uint32_t w = A.want[(size_t)A.sid[s] * A.nb + i];
+        csv_brick_slot sl;
+        sl.offset = 0;
+        sl.lod = 0;
+        sl.flags = 0;
+        if (!(bf & BK_HAS)) sl.flags = CSV_SLOT_EMPTY;
+        else if ((bf & BK_UNIFORM) || w == 0) sl.offset = i;
+        else if (w != kNone && ((res >> w) & 1u)) {
+            sl.offset = A.pal_region + A.off[(size_t)i * kLods + w];
+            sl.lod = w;
+        } else sl.flags = CSV_SLOT_MISSING;
+        A.slots[(size_t)A.sid[s] * A.n_slots + m] = sl;
+    }
 }
 
-__global__ void __launch_bounds__(kBlk) census_kernel(uint32_t nb, const uint32_t* __restrict__ ids,
-                                                      uint32_t* __restrict__ req_words, const ServeState* S,
-                                                      StepStats* st) {
-    __shared__ uint32_t s_e, s_m;
+struct CensusArgs {
+    uint32_t sid[kMaxViews];
+    uint32_t n_views, nb;
+    uint64_t n_slots;
+    const uint32_t* ids;
+    uint32_t* req_words;  // [session][n_slots]
+    const ServeState* S;
+    StepStats* st;
+};
+
+__global__ void __launch_bounds__(kBlk) census_kernel(CensusArgs A) {
+    __shared__ uint32_t s_e[kMaxViews], s_m[kMaxViews];
     const uint32_t i = blockIdx.x * kBlk + threadIdx.x;
-    if (threadIdx.x == 0) s_e = s_m = 0;
+    if (threadIdx.x < kMaxViews) s_e[threadIdx.x] = s_m[threadIdx.x] = 0;
     __syncthreads();
-    uint32_t v = 0;
-    if (i < nb) {
-        const uint32_t m = ids[i];
-        v = req_words[m];
-        if (v) req_words[m] = 0;
-    }
-    const uint32_t e = __popc(__ballot_sync(0xffffffffu, v != 0)), ms = __popc(__ballot_sync(0xffffffffu, v == 3));
-    if ((threadIdx.x & 31u) == 0) {
-        if (e) atomicAdd(&s_e, e);
-        if (ms) atomicAdd(&s_m, ms);
+    const uint32_t m = i < A.nb ? A.ids[i] : 0u;
+    for (uint32_t s = 0; s < A.n_views; ++s) {
+        uint32_t v = 0;
+        if (i < A.nb) {
+            uint32_t* w = A.req_words + (size_t)A.sid[s] * A.n_slots + m;
+            v = *w;
+            if (v) *w = 0;
+        }
+        const uint32_t e = __popc(__ballot_sync(0xffffffffu, v != 0));
+        const uint32_t ms = __popc(__ballot_sync(0xffffffffu, v == 3));
+        if ((threadIdx.x & 31u) == 0) {
+            if (e) atomicAdd(&s_e[s], e);
+            if (ms) atomicAdd(&s_m[s], ms);
+        }
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        if (s_e) atomicAdd(&st->entered, s_e);
-        if (s_m) atomicAdd(&st->missing, s_m);
-        if (blockIdx.x == 0) st->resident = S->resident;
+    if (threadIdx.x < A.n_views) {
+        if (s_e[threadIdx.x]) atomicAdd(&A.st->entered[threadIdx.x], s_e[threadIdx.x]);
+        if (s_m[threadIdx.x]) atomicAdd(&A.st->missing[threadIdx.x], s_m[threadIdx.x]);
     }
+    if (threadIdx.x == 0 && blockIdx.x == 0) A.st->resident = A.S->resident;
 }
 
 // Per brick: the palette-0 table, the transfer-function flag (culling.js:162-171)
-// and the uniform flag; every slot starts empty.
+// and the uniform flag.
 __global__ void __launch_bounds__(kBlk) setup_kernel(const BrickDesc* __restrict__ bricks, const uint64_t* __restrict__ pal,
                                                      uint32_t nb, const uint64_t* __restrict__ hidden, uint32_t n_hidden,
                                                      uint64_t* __restrict__ cache, uint8_t* __restrict__ bflag,
@@ -437,14 +483,14 @@ struct csv_server {
     double fov = 0, focal = 0, cos_half = 0, radius = 0;
     uint64_t total = 0, pal_region = 0, n_slots = 0;
     uint64_t* d_cache = nullptr;
-    csv_brick_slot* d_slots = nullptr;
-    uint32_t* d_req_words = nullptr;
+    csv_brick_slot* d_slots = nullptr;  // [session][n_slots]
+    uint32_t* d_req_words = nullptr;    // [session][n_slots]
     uint32_t* d_ids = nullptr;
     uint8_t* d_bflag = nullptr;
-    uint8_t* d_res_lod = nullptr;
-    uint64_t* d_res_off = nullptr;
+    uint8_t* d_res = nullptr;
+    uint64_t* d_off = nullptr;
     uint8_t* d_want = nullptr;
-    uint32_t* d_rank = nullptr;
+    uint8_t* d_need = nullptr;
     uint64_t* d_stack = nullptr;
     uint32_t* d_cnt = nullptr;
     uint32_t* d_base = nullptr;
@@ -455,21 +501,19 @@ struct csv_server {
     uint32_t n_hidden = 0;
     StepStats* d_stats = nullptr;  // kRing slots
     StepStats* h_stats = nullptr;  // pinned mirror
-    struct Pending {
-        bool set = false;
-        double v[6];
+    struct Session {
+        bool open = false, pending = false, planned = false;
+        double v[6];      // latest submitted camera (raw direction)
+        double pv[6];     // camera of the session's last re-plan (unit direction)
         uint64_t* lab = nullptr;
         float* dep = nullptr;
     };
-    std::vector<Pending> pend;
-    bool planned_once = false;
-    std::vector<uint32_t> last_sess;
-    std::vector<double> last_view;
+    std::vector<Session> ses;
+    std::vector<uint32_t> last_open;  // open sessions at the last plan
     struct StepRec {
         uint64_t seq = 0;
         cudaEvent_t e0 = nullptr, e1 = nullptr;
-        std::vector<uint32_t> sess;
-        bool busy = false;
+        std::vector<uint32_t> rendered;
     };
     StepRec ring[kRing];
     uint64_t next_seq = 0, harvest_seq = 0;
@@ -487,10 +531,10 @@ void server_free(csv_server* s) {
     cudaFree(s->d_req_words);
     cudaFree(s->d_ids);
     cudaFree(s->d_bflag);
-    cudaFree(s->d_res_lod);
-    cudaFree(s->d_res_off);
+    cudaFree(s->d_res);
+    cudaFree(s->d_off);
     cudaFree(s->d_want);
-    cudaFree(s->d_rank);
+    cudaFree(s->d_need);
     cudaFree(s->d_stack);
     cudaFree(s->d_cnt);
     cudaFree(s->d_base);
@@ -507,20 +551,12 @@ void server_free(csv_server* s) {
     delete s;
 }
 
-// culling.js:22-56 over the sessions of a step: re-plan when the set of
-// sessions changed or a camera moved more than 0.5 units / turned more than 0.05 rad.
-bool views_moved(const csv_server* s, const std::vector<uint32_t>& sess, const std::vector<double>& v) {
-    if (!s->planned_once || sess != s->last_sess) return true;
-    const double cos_rot = cos(0.05);
-    for (size_t k = 0; k < sess.size(); ++k) {
-        const double* a = &v[6 * k];
-        const double* p = &s->last_view[6 * k];
-        const double dx = a[0] - p[0], dy = a[1] - p[1], dz = a[2] - p[2];
-        const double moved = dx * dx + dy * dy + dz * dz;
-        const double dot = a[3] * p[3] + a[4] * p[4] + a[5] * p[5];
-        if (moved > 0.5 * 0.5 || dot < cos_rot) return true;
-    }
-    return false;
+// culling.js:22-56: moved more than 0.5 units or turned more than 0.05 rad.
+bool view_moved(const double* v, const double* p) {
+    const double dx = v[0] - p[0], dy = v[1] - p[1], dz = v[2] - p[2];
+    const double moved = dx * dx + dy * dy + dz * dz;
+    const double dot = v[3] * p[3] + v[4] * p[4] + v[5] * p[5];
+    return moved > 0.5 * 0.5 || dot < cos(0.05);
 }
 
 // camera.js:61-77 (getUniformData) in double, then float.
@@ -560,7 +596,8 @@ void camera_of(const double* v, double fov, csv_camera* c) {
     c->pad0 = c->pad1 = c->pad2 = 0.f;
 }
 
-// Move finished steps from the ring to the host queue (wait: block on the oldest).
+// Move finished steps from the ring to the host queue (wait_all: block until
+// every step finished; wait_one: block on the oldest only).
 int harvest(csv_server* s, bool wait_all, bool wait_one) {
     while (s->harvest_seq < s->next_seq) {
         auto& r = s->ring[s->harvest_seq % kRing];
@@ -570,24 +607,23 @@ int harvest(csv_server* s, bool wait_all, bool wait_one) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, r.e0, r.e1);
         const StepStats& t = s->h_stats[s->harvest_seq % kRing];
-        for (uint32_t ses : r.sess) {
+        for (size_t j = 0; j < r.rendered.size(); ++j) {
             csv_frame_stats f;
             memset(&f, 0, sizeof f);
             f.step = r.seq;
-            f.session = ses;
+            f.session = r.rendered[j];
             f.planned = t.planned;
             f.visible = t.visible;
             f.decoded = t.decoded;
             f.freed = t.freed;
             f.resident = t.resident;
             f.rebuilt = t.rebuilt;
-            f.entered = t.entered;
-            f.missing = t.missing;
+            f.entered = t.entered[j];
+            f.missing = t.missing[j];
             f.decoded_voxels = (uint64_t)t.vox_lo | ((uint64_t)t.vox_hi << 32);
             f.ms = ms;
             s->done.push_back(f);
         }
-        r.busy = false;
         ++s->harvest_seq;
         wait_one = false;
     }
@@ -621,7 +657,6 @@ int csv_serve_create(csv_ctx* ctx, const csv_dataset* ds, const csv_serve_config
     s->b = d.b;
     s->nb = d.nb;
     s->max_sessions = ms;
-    s->max_lod = 0;
     while ((1u << s->max_lod) < s->b) ++s->max_lod;
     const double screen = (double)std::min(s->W, s->H);
     s->focal = (screen / 2.0) / tan(s->fov / 2.0);
@@ -651,25 +686,26 @@ int csv_serve_create(csv_ctx* ctx, const csv_dataset* ds, const csv_serve_config
         return fail(ctx, CSV_ERANGE, "serve: cache smaller than its palette table");
     }
     const size_t nbx = std::max<uint32_t>(s->nb, 1);
+    const size_t ncx = std::max<uint32_t>(s->n_cta, 1);
     cudaError_t e = cudaSuccess;
     auto alloc = [&](void** p, size_t bytes) {
         if (e == cudaSuccess) e = cudaMalloc(p, std::max<size_t>(bytes, 16));
     };
     alloc((void**)&s->d_cache, s->total * 8);
-    alloc((void**)&s->d_slots, s->n_slots * sizeof(csv_brick_slot));
-    alloc((void**)&s->d_req_words, s->n_slots * 4);
+    alloc((void**)&s->d_slots, (size_t)ms * s->n_slots * sizeof(csv_brick_slot));
+    alloc((void**)&s->d_req_words, (size_t)ms * s->n_slots * 4);
     alloc((void**)&s->d_ids, nbx * 4);
     alloc((void**)&s->d_bflag, nbx);
-    alloc((void**)&s->d_res_lod, nbx);
-    alloc((void**)&s->d_res_off, nbx * 8);
-    alloc((void**)&s->d_want, nbx);
-    alloc((void**)&s->d_rank, nbx * 4);
+    alloc((void**)&s->d_res, nbx);
+    alloc((void**)&s->d_off, nbx * kLods * 8);
+    alloc((void**)&s->d_want, (size_t)kMaxViews * nbx);
+    alloc((void**)&s->d_need, nbx);
     alloc((void**)&s->d_stack, (size_t)kLods * nbx * 8);
-    alloc((void**)&s->d_cnt, (size_t)kCnt * std::max<uint32_t>(s->n_cta, 1) * 4);
-    alloc((void**)&s->d_base, (size_t)kCnt * std::max<uint32_t>(s->n_cta, 1) * 4);
+    alloc((void**)&s->d_cnt, (size_t)kCnt * ncx * 4);
+    alloc((void**)&s->d_base, (size_t)kCnt * ncx * 4);
     alloc((void**)&s->d_state, sizeof(ServeState));
-    alloc((void**)&s->d_reqs, nbx * sizeof(csv_request));
-    alloc((void**)&s->d_status, nbx * 4);
+    alloc((void**)&s->d_reqs, nbx * kLods * sizeof(csv_request));
+    alloc((void**)&s->d_status, nbx * kLods * 4);
     alloc((void**)&s->d_hidden, std::max<uint32_t>(n_hidden, 1) * 8);
     alloc((void**)&s->d_stats, kRing * sizeof(StepStats));
     if (e == cudaSuccess) e = cudaMallocHost((void**)&s->h_stats, kRing * sizeof(StepStats));
@@ -691,15 +727,15 @@ int csv_serve_create(csv_ctx* ctx, const csv_dataset* ds, const csv_serve_config
     memset(&st0, 0, sizeof st0);
     st0.cap = s->total - s->pal_region;
     if (e == cudaSuccess) e = cudaMemcpy(s->d_state, &st0, sizeof st0, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemset(s->d_res_lod, kNone, nbx);
-    if (e == cudaSuccess) e = cudaMemset(s->d_req_words, 0, s->n_slots * 4);
+    if (e == cudaSuccess) e = cudaMemset(s->d_res, 0, nbx);
+    if (e == cudaSuccess) e = cudaMemset(s->d_req_words, 0, (size_t)ms * s->n_slots * 4);
     if (e == cudaSuccess && s->nb) {
         setup_kernel<<<s->n_cta, kBlk>>>(d.d_bricks, d.d_pal, s->nb, s->d_hidden, s->n_hidden, s->d_cache, s->d_bflag,
                                          s->d_ids);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) {
-        slots_clear_kernel<<<1024, 256>>>(s->d_slots, s->n_slots);
+        slots_clear_kernel<<<1024, 256>>>(s->d_slots, (uint64_t)ms * s->n_slots);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -712,7 +748,7 @@ int csv_serve_create(csv_ctx* ctx, const csv_dataset* ds, const csv_serve_config
         server_free(s);
         return rc;
     }
-    s->pend.resize(ms);
+    s->ses.resize(ms);
     *out = s;
     return CSV_OK;
 }
@@ -720,8 +756,9 @@ int csv_serve_create(csv_ctx* ctx, const csv_dataset* ds, const csv_serve_config
 int csv_serve_submit(csv_server* s, uint32_t session, const csv_view* view, uint64_t* d_label, float* d_depth) {
     if (!s || !view || !d_label || !d_depth) return CSV_EINVAL;
     if (session >= s->max_sessions) return fail(s->ctx, CSV_ERANGE, "serve: session id beyond max_sessions");
-    auto& p = s->pend[session];
-    p.set = true;  // a newer frame of the same session replaces one not yet stepped
+    auto& p = s->ses[session];
+    p.open = true;     // a submit opens the session
+    p.pending = true;  // a newer frame of the same session replaces one not yet stepped
     for (int a = 0; a < 3; ++a) {
         p.v[a] = view->position[a];
         p.v[3 + a] = view->direction[a];
@@ -731,20 +768,35 @@ int csv_serve_submit(csv_server* s, uint32_t session, const csv_view* view, uint
     return CSV_OK;
 }
 
+int csv_serve_close(csv_server* s, uint32_t session) {
+    if (!s) return CSV_EINVAL;
+    if (session >= s->max_sessions) return fail(s->ctx, CSV_ERANGE, "serve: session id beyond max_sessions");
+    auto& p = s->ses[session];
+    p.open = p.pending = p.planned = false;  // its blocks are released at the next step
+    return CSV_OK;
+}
+
 int csv_serve_step(csv_server* s, void* stream, uint64_t* step_id) {
     if (!s) return CSV_EINVAL;
     cudaStream_t st = (cudaStream_t)stream;
-    std::vector<uint32_t> sess;
-    std::vector<double> views;  // position, unit direction (camera.js:63)
+    std::vector<uint32_t> open, rendered;
+    bool changed = false;
     for (uint32_t k = 0; k < s->max_sessions; ++k) {
-        if (!s->pend[k].set) continue;
-        sess.push_back(k);
-        const double* v = s->pend[k].v;
-        double n = sqrt(v[3] * v[3] + v[4] * v[4] + v[5] * v[5]);
+        auto& p = s->ses[k];
+        if (!p.open) continue;
+        open.push_back(k);
+        if (p.pending) rendered.push_back(k);
+        double n = sqrt(p.v[3] * p.v[3] + p.v[4] * p.v[4] + p.v[5] * p.v[5]);
         if (n == 0.0) n = 1.0;
-        views.insert(views.end(), {v[0], v[1], v[2], v[3] / n, v[4] / n, v[5] / n});
+        const double u[6] = {p.v[0], p.v[1], p.v[2], p.v[3] / n, p.v[4] / n, p.v[5] / n};
+        if (!p.planned || view_moved(u, p.pv)) {
+            memcpy(p.pv, u, sizeof u);
+            p.planned = true;
+            changed = true;
+        }
     }
-    if (sess.empty()) return fail(s->ctx, CSV_EINVAL, "serve: no frame submitted since the last step");
+    if (open != s->last_open) changed = true;
+    if (rendered.empty() && !changed) return fail(s->ctx, CSV_EINVAL, "serve: no frame submitted since the last step");
     DeviceGuard g(s->ctx->device);
     // a full ring: wait for the oldest step and keep its counters for csv_serve_poll
     if (s->next_seq - s->harvest_seq >= kRing) {
@@ -756,43 +808,50 @@ int csv_serve_step(csv_server* s, void* stream, uint64_t* step_id) {
     StepStats* stats = s->d_stats + slot;
     cudaError_t e = cudaEventRecord(rec.e0, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(stats, 0, sizeof(StepStats), st);
-    const bool plan = views_moved(s, sess, views);
-    if (e == cudaSuccess && plan && s->nb) {
+    if (e == cudaSuccess && changed && s->nb) {
         PlanArgs P;
         memset(&P, 0, sizeof P);
-        for (size_t k = 0; k < sess.size(); ++k)
+        for (size_t k = 0; k < open.size(); ++k) {
+            const auto& p = s->ses[open[k]];
             for (int a = 0; a < 3; ++a) {
-                P.v[k].p[a] = views[6 * k + a];
-                P.v[k].d[a] = views[6 * k + 3 + a];
+                P.v[k].p[a] = p.pv[a];
+                P.v[k].d[a] = p.pv[3 + a];
             }
-        P.n_views = (uint32_t)sess.size();
+            P.sid[k] = open[k];
+        }
+        P.n_views = (uint32_t)open.size();
         P.b = s->b;
         P.max_lod = s->max_lod;
         P.nb = s->nb;
+        P.n_cta = s->n_cta;
         P.focal = s->focal;
         P.cos_half = s->cos_half;
         P.radius = s->radius;
         P.half = (double)s->b / 2.0;
         P.ids = s->d_ids;
         P.bflag = s->d_bflag;
-        P.res_lod = s->d_res_lod;
+        P.res = s->d_res;
         P.want = s->d_want;
-        P.rank = s->d_rank;
+        P.need = s->d_need;
         P.cnt = s->d_cnt;
-        P.n_cta = s->n_cta;
         P.stats = stats;
         plan_kernel<<<s->n_cta, kBlk, 0, st>>>(P);
         scan_kernel<<<1, 1024, 0, st>>>(s->d_cnt, s->d_base, s->n_cta, s->max_lod, s->nb, s->d_state, stats);
         CacheArgs C;
+        memset(&C, 0, sizeof C);
+        for (size_t k = 0; k < open.size(); ++k) C.sid[k] = open[k];
+        C.n_views = (uint32_t)open.size();
         C.nb = s->nb;
         C.n_cta = s->n_cta;
+        C.max_lod = s->max_lod;
+        C.n_slots = s->n_slots;
         C.bflag = s->d_bflag;
         C.want = s->d_want;
-        C.rank = s->d_rank;
+        C.need = s->d_need;
         C.base = s->d_base;
         C.ids = s->d_ids;
-        C.res_lod = s->d_res_lod;
-        C.res_off = s->d_res_off;
+        C.res = s->d_res;
+        C.off = s->d_off;
         C.stack = s->d_stack;
         C.S = s->d_state;
         C.reqs = s->d_reqs;
@@ -804,23 +863,31 @@ int csv_serve_step(csv_server* s, void* stream, uint64_t* step_id) {
         if (e == cudaSuccess) {
             DecodeConfig dc;
             dc.n_dev = &s->d_state->n_req;
-            e = launch_decode(s->ds->d, s->d_reqs, s->nb, s->d_cache, s->d_status, s->ctx->scr, st, &dc);
+            e = launch_decode(s->ds->d, s->d_reqs, s->nb * kLods, s->d_cache, s->d_status, s->ctx->scr, st, &dc);
         }
-        if (e == cudaSuccess) {
-            s->planned_once = true;
-            s->last_sess = sess;
-            s->last_view = views;
-        }
+        if (e == cudaSuccess) s->last_open = open;
     }
-    for (size_t k = 0; k < sess.size() && e == cudaSuccess; ++k) {
+    for (size_t k = 0; k < rendered.size() && e == cudaSuccess; ++k) {
+        const auto& p = s->ses[rendered[k]];
         csv_camera cam;
-        camera_of(s->pend[sess[k]].v, s->fov, &cam);
-        e = launch_render(cam, s->W, s->H, (float)(s->bpa * s->b), s->b, s->bpa, s->d_slots, s->n_slots, s->d_cache,
-                          s->n_hidden ? s->d_hidden : nullptr, s->n_hidden, s->pend[sess[k]].lab,
-                          s->pend[sess[k]].dep, s->d_req_words, st);
+        camera_of(p.v, s->fov, &cam);
+        e = launch_render(cam, s->W, s->H, (float)(s->bpa * s->b), s->b, s->bpa,
+                          s->d_slots + (size_t)rendered[k] * s->n_slots, s->n_slots, s->d_cache,
+                          s->n_hidden ? s->d_hidden : nullptr, s->n_hidden, p.lab, p.dep,
+                          s->d_req_words + (size_t)rendered[k] * s->n_slots, st);
     }
-    if (e == cudaSuccess && s->nb) {
-        census_kernel<<<s->n_cta, kBlk, 0, st>>>(s->nb, s->d_ids, s->d_req_words, s->d_state, stats);
+    if (e == cudaSuccess && s->nb && !rendered.empty()) {
+        CensusArgs A;
+        memset(&A, 0, sizeof A);
+        for (size_t k = 0; k < rendered.size(); ++k) A.sid[k] = rendered[k];
+        A.n_views = (uint32_t)rendered.size();
+        A.nb = s->nb;
+        A.n_slots = s->n_slots;
+        A.ids = s->d_ids;
+        A.req_words = s->d_req_words;
+        A.S = s->d_state;
+        A.st = stats;
+        census_kernel<<<s->n_cta, kBlk, 0, st>>>(A);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess)
@@ -828,11 +895,10 @@ int csv_serve_step(csv_server* s, void* stream, uint64_t* step_id) {
     if (e == cudaSuccess) e = cudaEventRecord(rec.e1, st);
     if (e != cudaSuccess) return cfail(s->ctx, e, "serve step");
     rec.seq = s->next_seq;
-    rec.sess = sess;
-    rec.busy = true;
+    rec.rendered = rendered;
     if (step_id) *step_id = s->next_seq;
     ++s->next_seq;
-    for (uint32_t k : sess) s->pend[k].set = false;
+    for (uint32_t k : rendered) s->ses[k].pending = false;
     return CSV_OK;
 }
 
@@ -859,9 +925,10 @@ int csv_serve_camera(const csv_server* s, const csv_view* view, csv_camera* out)
     return CSV_OK;
 }
 
-int csv_serve_state(const csv_server* s, csv_serve_info* info) {
+int csv_serve_state(const csv_server* s, uint32_t session, csv_serve_info* info) {
     if (!s || !info) return CSV_EINVAL;
-    info->slots = s->d_slots;
+    if (session >= s->max_sessions) return fail(s->ctx, CSV_ERANGE, "serve: session id beyond max_sessions");
+    info->slots = s->d_slots + (size_t)session * s->n_slots;
     info->n_slots = s->n_slots;
     info->cache = s->d_cache;
     info->cache_labels = s->total;

@@ -145,7 +145,8 @@ def load_library() -> C.CDLL:
     L.csv_serve_step.argtypes = [vp, vp, C.POINTER(C.c_uint64)]
     L.csv_serve_poll.argtypes = [vp, C.POINTER(FrameStats), C.c_uint32, C.POINTER(C.c_uint32), C.c_int]
     L.csv_serve_camera.argtypes = [vp, C.POINTER(View), vp]
-    L.csv_serve_state.argtypes = [vp, C.POINTER(ServeInfo)]
+    L.csv_serve_state.argtypes = [vp, C.c_uint32, C.POINTER(ServeInfo)]
+    L.csv_serve_close.argtypes = [vp, C.c_uint32]
     L.csv_serve_destroy.argtypes = [vp]
     _lib = L
     return L
@@ -443,14 +444,18 @@ class Server:
         self.codec._check(self.lib.csv_serve_camera(self.handle, C.byref(v), cam))
         return np.array(cam[:], np.float32)
 
-    def info(self) -> ServeInfo:
+    def leave(self, session: int):
+        """The session closes; its cache blocks are released by the next step."""
+        self.codec._check(self.lib.csv_serve_close(self.handle, session))
+
+    def info(self, session: int = 0) -> ServeInfo:
         i = ServeInfo()
-        self.codec._check(self.lib.csv_serve_state(self.handle, C.byref(i)))
+        self.codec._check(self.lib.csv_serve_state(self.handle, session, C.byref(i)))
         return i
 
-    def slots_tensor(self):
-        """Device view (uint8, n_slots * 16 bytes) of the brick slot table."""
-        i = self.info()
+    def slots_tensor(self, session: int = 0):
+        """Device view (uint8, n_slots * 16 bytes) of a session's brick slot table."""
+        i = self.info(session)
         return _device_view(i.slots, int(i.n_slots) * 16, "|u1", self.codec.device)
 
     def cache_tensor(self):

@@ -236,15 +236,20 @@ int csv_render(csv_ctx* ctx, const csv_camera* camera, uint32_t width, uint32_t 
  * A server holds one dataset (one brick size), a label cache in HBM and the
  * brick slot table.  Up to max_sessions viewers share it: each submits frames
  * (a camera and two device images); csv_serve_step serves every session with
- * a pending frame in one step -- one plan over all their views (a brick is
- * needed at the finest LOD any of them asks for), one decode launch for all
- * admitted bricks, one render per view -- all enqueued on `stream` with no
- * host synchronisation.  A session that submits again before the step
- * replaces its pending frame (the newest camera wins).  The plan runs only
- * when the set of sessions changed or a camera moved more than 0.5 units or
- * turned more than 0.05 rad since the last plan (culling.js:6-56); otherwise
- * the step only renders.  csv_serve_poll returns per-frame counters and the
- * device time of each finished step.  One host thread per server. */
+ * a pending frame in one step -- one plan over every open session, one
+ * decode launch for all admitted blocks, one render per new frame -- all
+ * enqueued on `stream` with no host synchronisation.  Sessions join (first
+ * submit) and leave (csv_serve_close) between steps; their decode work shares
+ * the launches of the sessions already open.  Cache blocks are keyed by
+ * (brick, LOD) and every session has its own slot table and LODs, so a
+ * session's image does not depend on which other sessions are open while the
+ * cache has room for all of them.  A session that submits again before the
+ * step replaces its pending frame (the newest camera wins).  A session's LODs
+ * are re-planned when its camera moved more than 0.5 units or turned more
+ * than 0.05 rad since its last re-plan (culling.js:6-56); a step with no such
+ * change and no session joining or leaving only renders.  csv_serve_poll
+ * returns per-frame counters and the device time of each finished step.  One
+ * host thread per server. */
 typedef struct csv_server csv_server;
 
 #define CSV_CONE_REFERENCE 0u /* cone half-angle fov/2 (culling.js:132) */
@@ -267,13 +272,13 @@ typedef struct csv_frame_stats {
     uint64_t step;           /* step sequence number */
     uint32_t session;
     uint32_t planned;        /* 1 when the step re-planned */
-    uint32_t visible;        /* bricks some view needs */
-    uint32_t decoded;        /* (brick, LOD) pairs admitted and decoded */
+    uint32_t visible;        /* bricks some open session needs */
+    uint32_t decoded;        /* (brick, LOD) blocks admitted and decoded */
     uint32_t freed;          /* cache blocks released */
-    uint32_t resident;       /* bricks holding a cache block after the step */
+    uint32_t resident;       /* cache blocks resident after the step */
     uint32_t rebuilt;        /* 1 when the cache was rebuilt (allocation failure) */
-    uint32_t entered;        /* non-empty bricks some ray entered */
-    uint32_t missing;        /* of those, bricks with no data in the cache */
+    uint32_t entered;        /* non-empty bricks this session's rays entered */
+    uint32_t missing;        /* of those, bricks with no data in its slot table */
     uint32_t reserved;
     uint64_t decoded_voxels;
     float ms;                /* device time of the whole step (CUDA events) */
@@ -305,9 +310,12 @@ int csv_serve_step(csv_server* srv, void* stream, uint64_t* step_id);
 /* Up to `max` finished frames (one per session of each finished step), oldest
  * first; wait != 0 blocks until every step enqueued so far has finished. */
 int csv_serve_poll(csv_server* srv, csv_frame_stats* out, uint32_t max, uint32_t* n_out, int wait);
+/* A session leaves: its cache blocks are released by the next step. */
+int csv_serve_close(csv_server* srv, uint32_t session);
 /* The float camera the server renders a view with (camera.js:61-77). */
 int csv_serve_camera(const csv_server* srv, const csv_view* view, csv_camera* out);
-int csv_serve_state(const csv_server* srv, csv_serve_info* info);
+/* Device views of the cache and of `session`'s slot table. */
+int csv_serve_state(const csv_server* srv, uint32_t session, csv_serve_info* info);
 int csv_serve_destroy(csv_server* srv);
 
 /* ---- workload generator (no reference counterpart) --------------------

@@ -86,27 +86,32 @@ void or_serve_constants(uint32_t W, uint32_t H, double fov, uint32_t cone, uint3
 /* The viewer's frame loop (csv_oracle_serve.c): plan, cache, decode, render. */
 typedef struct or_server or_server;
 enum {
-    OR_ST_PLANNED = 0,  /* 1 when the step re-planned (a camera moved) */
-    OR_ST_VISIBLE = 1,  /* bricks some view needs */
-    OR_ST_DECODED = 2,  /* (brick, LOD) pairs admitted and decoded */
+    OR_ST_PLANNED = 0,  /* 1 when the step re-planned */
+    OR_ST_VISIBLE = 1,  /* bricks some open session needs */
+    OR_ST_DECODED = 2,  /* (brick, LOD) blocks admitted and decoded */
     OR_ST_FREED = 3,    /* blocks returned to the free stacks */
-    OR_ST_RESIDENT = 4, /* bricks holding a block after the step */
+    OR_ST_RESIDENT = 4, /* blocks resident after the step */
     OR_ST_REBUILT = 5,  /* 1 when the cache was rebuilt */
-    OR_ST_ENTERED = 6,  /* non-empty bricks some ray entered */
-    OR_ST_MISSING = 7,  /* of those, bricks not resident */
-    OR_ST_VOX_LO = 8,   /* decoded labels, low and high words */
-    OR_ST_VOX_HI = 9,
-    OR_SERVE_STATS = 10
+    OR_ST_VOX_LO = 6,   /* decoded labels, low and high words */
+    OR_ST_VOX_HI = 7,
+    OR_ST_SESSION = 8,  /* then per rendered session k: entered (8 + 2k), missing (9 + 2k) */
+    OR_SERVE_STATS = 8 + 2 * 8
 };
+#define OR_MAX_SESSIONS 8
 or_server* or_serve_new(const uint8_t* img, size_t len, uint32_t W, uint32_t H, double fov, uint32_t cone,
                         uint64_t cache_bytes, const uint64_t* hidden, uint32_t n_hidden);
-/* One step for n views (sessions sess[k], view k = position[3], direction[3]);
- * images k at out_label + k*W*H, out_depth + k*W*H; stats: OR_SERVE_STATS words. */
-int or_serve_step(or_server* s, const uint32_t* sess, const double* views, uint32_t n, uint64_t* out_label,
-                  float* out_depth, uint32_t* stats);
+/* One step.  The n open sessions sess[k] (ascending ids) with their latest
+ * views (position[3], direction[3]); render[k] != 0 for the sessions that
+ * submitted a frame this step, whose images are written in order at
+ * out_label + j*W*H, out_depth + j*W*H (j counts rendered sessions).
+ * A session absent from sess is closed: its blocks are released at the next
+ * plan.  stats: OR_SERVE_STATS words. */
+int or_serve_step(or_server* s, const uint32_t* sess, const double* views, const uint8_t* render, uint32_t n,
+                  uint64_t* out_label, float* out_depth, uint32_t* stats);
 uint64_t or_serve_n_slots(const or_server* s);
 uint32_t or_serve_bricks_per_axis(const or_server* s);
-const or_slot* or_serve_slots(const or_server* s);
+/* The slot table session `session` renders with. */
+const or_slot* or_serve_slots(const or_server* s, uint32_t session);
 const uint64_t* or_serve_cache(const or_server* s);
 void or_serve_free(or_server* s);
 

@@ -4,34 +4,39 @@
  * slot table and pixel for pixel.
  *
  * Follows, per frame (renderLoop.js:208-340 with LOD_UPDATE_INTERVAL 1):
- *   - the camera-moved test (culling.js:22-56): re-plan only when a camera
- *     moved more than 0.5 units or turned more than 0.05 rad since the last plan;
+ *   - the camera-moved test (culling.js:22-56): a view is re-planned only when
+ *     its camera moved more than 0.5 units or turned more than 0.05 rad since
+ *     the view its plan used;
  *   - the LOD of every brick (camera.js:103-137, screen size min(W, H),
  *     renderLoop.js:374) and the cone test (culling.js:87-153), with the
  *     transfer-function test (culling.js:162-171) as a per-brick flag;
  *   - the cache (cacheManager.js:10-246, cacheProcessing.js:99-232): per-LOD
  *     free stacks of blocks of 8^lod labels, a bump pointer, eviction of the
- *     bricks the frame does not need, a rebuild when an allocation fails;
- *   - the decode of the newly admitted (brick, LOD) pairs and the label/depth
- *     render of every view (or_render_rows).
+ *     blocks no view needs, a rebuild when an allocation fails;
+ *   - the decode of the newly admitted (brick, LOD) blocks and the label/depth
+ *     render of every view that submitted a frame (or_render_rows).
+ *
+ * Several sessions (viewers) share one cache.  Each keeps its own LODs and its
+ * own slot table, so a session's image does not depend on which other
+ * sessions are open (given room in the cache): a block is keyed by (brick,
+ * LOD), and a brick two sessions see at different LODs holds two blocks.
+ * With one session this is the reference's loop.
  *
  * Where the reference leaves an order or a corner case open, this file fixes
  * it, and the device server follows the same rules:
- *   - frees are pushed in brick (file) order; allocations are served LOD by
+ *   - frees are pushed in brick (file) order; admissions are served LOD by
  *     LOD (coarse first), in brick order within a LOD, each popping its LOD's
  *     stack (last pushed first) and taking fresh space from the bump pointer
  *     once the stack is empty;
  *   - when the frame's fresh space does not fit, the cache is rebuilt: every
- *     block is dropped and every needed brick is placed again, LOD by LOD
- *     (coarse first) in brick order, until the space runs out (the bricks
- *     that do not fit stay missing for this frame);
+ *     block is dropped and every needed block is placed again, LOD by LOD
+ *     (coarse first) in brick order, while space remains (the blocks that do
+ *     not fit stay missing for this frame);
  *   - LOD-0 bricks and uniform bricks (root stop bit: the whole brick is
  *     palette[0]) take no block: their slot reads palette[0] from a table at
  *     the start of the cache (rayTrace.wgsl:167-178 reads palette[0] for LOD 0;
  *     a uniform brick decodes to palette[0] at every LOD, so the image is the
  *     one a decoded copy would give);
- *   - several views in one step (sessions served together) need a brick when
- *     any of them does, at the finest LOD any of them asks for;
  *   - the cone's margin sin(atan2(r, d)) is evaluated as r / sqrt(r^2 + d^2),
  *     the same number for d > 0 up to rounding; the half-angle is fov/2
  *     (cone 0, the reference) or the half-diagonal of the screen (cone 1), and
@@ -45,7 +50,7 @@
 #include "csv_oracle.h"
 
 #define OR_NONE 0xFFu
-#define OR_MAXV 8
+#define OR_LODS 8
 
 struct or_server {
     uint32_t nb, b, max_lod, bpa, W, H, cone, n_hidden;
@@ -55,27 +60,27 @@ struct or_server {
     uint32_t* id;
     uint8_t* has;      /* a palette entry is neither 0 nor hidden */
     uint8_t* uni;      /* uniform brick */
-    uint64_t* pal0;    /* palette[0] */
     const uint8_t** enc;
     uint32_t* E;
     uint32_t* nsym;
-    const uint64_t** pal;
+    const uint8_t* pal_bytes;
+    size_t* pal_at;
     uint32_t* P;
-    uint8_t* res_lod;
-    uint64_t* res_off;
+    uint8_t* res;      /* bit l: a block at LOD l is resident */
+    uint64_t* off;     /* [brick][OR_LODS] block offsets */
+    uint8_t* want[OR_MAX_SESSIONS]; /* per session and brick: its LOD, OR_NONE when it does not need the brick */
     /* cache */
     uint64_t pal_region, cap, bump;
     uint64_t* cache;
-    uint64_t* stack[OR_MAXV]; /* per LOD, nb entries */
-    uint32_t top[OR_MAXV];
-    or_slot* slots;
+    uint64_t* stack[OR_LODS]; /* per LOD, nb entries */
+    uint32_t top[OR_LODS];
+    or_slot* slots[OR_MAX_SESSIONS];
     uint64_t n_slots;
     uint64_t* hidden;
-    /* last plan */
-    uint32_t n_last;
-    uint32_t last_sess[OR_MAXV];
-    double last_view[OR_MAXV][6];
-    int planned_once;
+    /* plan bookkeeping */
+    uint8_t planned[OR_MAX_SESSIONS];     /* the session has a planned view */
+    double pview[OR_MAX_SESSIONS][6];     /* the view its plan used */
+    uint8_t last_open[OR_MAX_SESSIONS];   /* open at the last plan */
 };
 
 static uint32_t rd32(const uint8_t* p) {
@@ -127,7 +132,7 @@ void or_serve_constants(uint32_t W, uint32_t H, double fov, uint32_t cone, uint3
     *radius = sqrt(3.0) * ((double)b / 2.0);                /* culling.js:128 */
 }
 
-/* LOD (camera.js:103-137) and cone (culling.js:87-153) of one brick for one view. */
+/* culling.js:87-153 for one brick centre and one view (position, unit direction). */
 static int brick_in_cone(const or_server* s, const double* c, const double* v) {
     const double tx = c[0] - v[0], ty = c[1] - v[1], tz = c[2] - v[2];
     const double dist = sqrt(tx * tx + ty * ty + tz * tz);
@@ -147,13 +152,18 @@ static int has_hidden(const uint64_t* h, uint32_t n, uint64_t v) {
     return lo < n && h[lo] == v;
 }
 
+static uint64_t pal_entry(const or_server* s, uint32_t i, uint32_t k) {
+    uint64_t v;
+    memcpy(&v, s->pal_bytes + s->pal_at[i] + 8ull * k, 8);
+    return v;
+}
+
 or_server* or_serve_new(const uint8_t* img, size_t len, uint32_t W, uint32_t H, double fov, uint32_t cone,
                         uint64_t cache_bytes, const uint64_t* hidden, uint32_t n_hidden) {
     if (!img || len < 152 || rd32(img) != 0x43534244u) return NULL;
     or_server* s = (or_server*)calloc(1, sizeof *s);
     s->nb = rd32(img + 8);
     s->b = rd32(img + 12);
-    s->max_lod = 0;
     while ((1u << s->max_lod) < s->b) ++s->max_lod;
     s->W = W;
     s->H = H;
@@ -172,33 +182,32 @@ or_server* or_serve_new(const uint8_t* img, size_t len, uint32_t W, uint32_t H, 
     s->id = (uint32_t*)calloc(nb + 1, 4);
     s->has = (uint8_t*)calloc(nb + 1, 1);
     s->uni = (uint8_t*)calloc(nb + 1, 1);
-    s->pal0 = (uint64_t*)calloc(nb + 1, 8);
     s->enc = (const uint8_t**)calloc(nb + 1, sizeof(void*));
-    s->pal = (const uint64_t**)calloc(nb + 1, sizeof(void*));
+    s->pal_at = (size_t*)calloc(nb + 1, sizeof(size_t));
     s->E = (uint32_t*)calloc(nb + 1, 4);
     s->nsym = (uint32_t*)calloc(nb + 1, 4);
     s->P = (uint32_t*)calloc(nb + 1, 4);
-    s->res_lod = (uint8_t*)malloc(nb + 1);
-    memset(s->res_lod, OR_NONE, nb + 1);
-    s->res_off = (uint64_t*)calloc(nb + 1, 8);
+    s->res = (uint8_t*)calloc(nb + 1, 1);
+    s->off = (uint64_t*)calloc((size_t)(nb + 1) * OR_LODS, 8);
+    for (int k = 0; k < OR_MAX_SESSIONS; ++k) {
+        s->want[k] = (uint8_t*)malloc(nb + 1);
+        memset(s->want[k], OR_NONE, nb + 1);
+    }
+    s->pal_bytes = img;
     size_t o = 152;
     uint32_t maxc = 0;
     for (uint32_t i = 0; i < nb; ++i) {
         s->id[i] = rd32(img + o);
         s->P[i] = rd32(img + o + 4);
-        s->pal[i] = (const uint64_t*)(img + o + 8);
+        s->pal_at[i] = o + 8;
         o += 8 + 8ull * s->P[i];
         s->E[i] = rd32(img + o);
         s->enc[i] = img + o + 4;
         o += 4 + s->E[i];
         s->nsym[i] = rd32(img + o);
         o += 4;
-        uint64_t p0;
-        memcpy(&p0, s->pal[i], 8);
-        s->pal0[i] = p0;
         for (uint32_t k = 0; k < s->P[i]; ++k) {
-            uint64_t v;
-            memcpy(&v, (const uint8_t*)s->pal[i] + 8ull * k, 8);
+            const uint64_t v = pal_entry(s, i, k);
             if (v != 0 && !has_hidden(s->hidden, n_hidden, v)) {
                 s->has[i] = 1;
                 break;
@@ -215,90 +224,80 @@ or_server* or_serve_new(const uint8_t* img, size_t len, uint32_t W, uint32_t H, 
         if (y > maxc) maxc = y;
         if (z > maxc) maxc = z;
     }
-    (void)len;
     s->bpa = maxc + 1;
     uint32_t p2 = 1;
     while (p2 < s->bpa) p2 <<= 1;
     s->n_slots = (uint64_t)p2 * p2 * p2;
-    s->slots = (or_slot*)calloc(s->n_slots, sizeof(or_slot));
-    for (uint64_t m = 0; m < s->n_slots; ++m) s->slots[m].flags = 1u;
+    for (int k = 0; k < OR_MAX_SESSIONS; ++k) {
+        s->slots[k] = (or_slot*)calloc(s->n_slots, sizeof(or_slot));
+        for (uint64_t m = 0; m < s->n_slots; ++m) s->slots[k][m].flags = 1u;
+    }
     const uint64_t total = cache_bytes / 8;
     s->pal_region = ((uint64_t)nb + 31) & ~31ull;
     s->cap = total > s->pal_region ? total - s->pal_region : 0;
     s->cache = (uint64_t*)calloc(total ? total : 1, 8);
-    for (uint32_t i = 0; i < nb; ++i) s->cache[i] = s->pal0[i];
-    for (uint32_t l = 0; l < OR_MAXV; ++l) s->stack[l] = (uint64_t*)calloc(nb + 1, 8);
+    for (uint32_t i = 0; i < nb && i < total; ++i) s->cache[i] = s->P[i] ? pal_entry(s, i, 0) : 0;
+    for (uint32_t l = 0; l < OR_LODS; ++l) s->stack[l] = (uint64_t*)calloc(nb + 1, 8);
     return s;
 }
 
 void or_serve_free(or_server* s) {
     if (!s) return;
-    free(s->id); free(s->has); free(s->uni); free(s->pal0); free(s->enc); free(s->pal); free(s->E);
-    free(s->nsym); free(s->P); free(s->res_lod); free(s->res_off); free(s->cache); free(s->slots); free(s->hidden);
-    for (uint32_t l = 0; l < OR_MAXV; ++l) free(s->stack[l]);
+    free(s->id); free(s->has); free(s->uni); free(s->enc); free(s->pal_at); free(s->E);
+    free(s->nsym); free(s->P); free(s->res); free(s->off); free(s->cache); free(s->hidden);
+    for (int k = 0; k < OR_MAX_SESSIONS; ++k) {
+        free(s->want[k]);
+        free(s->slots[k]);
+    }
+    for (uint32_t l = 0; l < OR_LODS; ++l) free(s->stack[l]);
     free(s);
 }
 
 uint64_t or_serve_n_slots(const or_server* s) { return s->n_slots; }
 uint32_t or_serve_bricks_per_axis(const or_server* s) { return s->bpa; }
-const or_slot* or_serve_slots(const or_server* s) { return s->slots; }
+const or_slot* or_serve_slots(const or_server* s, uint32_t session) {
+    return session < OR_MAX_SESSIONS ? s->slots[session] : NULL;
+}
 const uint64_t* or_serve_cache(const or_server* s) { return s->cache; }
 
-/* culling.js:22-56 over the views of a step. */
-static int views_moved(const or_server* s, const uint32_t* sess, const double* views, uint32_t n) {
-    if (!s->planned_once || n != s->n_last) return 1;
-    const double cos_rot = cos(0.05);
-    for (uint32_t k = 0; k < n; ++k) {
-        if (sess[k] != s->last_sess[k]) return 1;
-        const double* v = views + 6 * k;
-        const double* p = s->last_view[k];
-        const double dx = v[0] - p[0], dy = v[1] - p[1], dz = v[2] - p[2];
-        const double moved = dx * dx + dy * dy + dz * dz;
-        const double dot = v[3] * p[3] + v[4] * p[4] + v[5] * p[5];
-        if (moved > 0.5 * 0.5 || dot < cos_rot) return 1;
-    }
-    return 0;
+/* culling.js:22-56: moved more than 0.5 units or turned more than 0.05 rad. */
+static int view_moved(const double* v, const double* p) {
+    const double dx = v[0] - p[0], dy = v[1] - p[1], dz = v[2] - p[2];
+    const double moved = dx * dx + dy * dy + dz * dz;
+    const double dot = v[3] * p[3] + v[4] * p[4] + v[5] * p[5];
+    return moved > 0.5 * 0.5 || dot < cos(0.05);
 }
 
 static void decode_into(or_server* s, uint32_t i, uint32_t lod, uint64_t* dst) {
     const uint32_t ns = s->nsym[i];
     uint8_t* nib = (uint8_t*)calloc(ns / 2 + 2, 1);
     if (s->E[i] >= 4 && ns >= 1) or_rans_decode(s->freq, s->cum, 4096, s->enc[i], s->E[i], ns, nib);
-    uint64_t* pal = (uint64_t*)malloc(8ull * s->P[i]);
-    memcpy(pal, s->pal[i], 8ull * s->P[i]);
+    uint64_t* pal = (uint64_t*)malloc(8ull * (s->P[i] ? s->P[i] : 1));
+    for (uint32_t k = 0; k < s->P[i]; ++k) pal[k] = pal_entry(s, i, k);
     or_decode_brick(pal, s->P[i], nib, (ns + 1) / 2, s->b, lod, dst);
     free(pal);
     free(nib);
 }
 
-int or_serve_step(or_server* s, const uint32_t* sess, const double* views_in, uint32_t n, uint64_t* out_label,
-                  float* out_depth, uint32_t* stats) {
-    if (n == 0 || n > OR_MAXV) return -1;
-    const uint32_t nb = s->nb, b = s->b;
-    memset(stats, 0, sizeof(uint32_t) * OR_SERVE_STATS);
-    /* directions normalised as the view's forward (camera.js:63) */
-    double views[OR_MAXV * 6];
-    for (uint32_t k = 0; k < n; ++k) {
-        const double* v = views_in + 6 * k;
-        double len = sqrt(v[3] * v[3] + v[4] * v[4] + v[5] * v[5]);
-        if (len == 0.0) len = 1.0;
-        views[6 * k + 0] = v[0];
-        views[6 * k + 1] = v[1];
-        views[6 * k + 2] = v[2];
-        views[6 * k + 3] = v[3] / len;
-        views[6 * k + 4] = v[4] / len;
-        views[6 * k + 5] = v[5] / len;
+static uint8_t need_mask(const or_server* s, uint32_t i, const uint8_t* open) {
+    uint8_t m = 0;
+    if (s->uni[i]) return 0;
+    for (int k = 0; k < OR_MAX_SESSIONS; ++k) {
+        if (!open[k]) continue;
+        const uint8_t w = s->want[k][i];
+        if (w != OR_NONE && w > 0) m |= (uint8_t)(1u << w);
     }
-    const int plan = views_moved(s, sess, views, n);
-    if (plan) {
-        s->planned_once = 1;
-        s->n_last = n;
-        for (uint32_t k = 0; k < n; ++k) {
-            s->last_sess[k] = sess[k];
-            memcpy(s->last_view[k], views + 6 * k, sizeof(double) * 6);
+    return m;
+}
+
+static void plan(or_server* s, const uint8_t* open, uint32_t* stats) {
+    const uint32_t nb = s->nb, b = s->b;
+    /* wants of every open session with its planned view */
+    for (int k = 0; k < OR_MAX_SESSIONS; ++k) {
+        if (!open[k]) {
+            memset(s->want[k], OR_NONE, nb + 1);
+            continue;
         }
-        uint8_t* want = (uint8_t*)malloc(nb + 1);
-        uint32_t A[OR_MAXV] = {0}, Wn[OR_MAXV] = {0};
         for (uint32_t i = 0; i < nb; ++i) {
             uint8_t w = OR_NONE;
             if (s->has[i]) {
@@ -306,99 +305,138 @@ int or_serve_step(or_server* s, const uint32_t* sess, const double* views_in, ui
                 or_demorton3(s->id[i], &x, &y, &z);
                 const double c[3] = {(double)x * (double)b + s->half, (double)y * (double)b + s->half,
                                      (double)z * (double)b + s->half};
-                for (uint32_t k = 0; k < n; ++k) {
-                    if (!brick_in_cone(s, c, views + 6 * k)) continue;
-                    const uint32_t l = or_brick_lod(c, (double)b, views + 6 * k, s->focal, s->max_lod);
-                    if (w == OR_NONE || l > w) w = (uint8_t)l;
-                }
+                if (brick_in_cone(s, c, s->pview[k]))
+                    w = (uint8_t)or_brick_lod(c, (double)b, s->pview[k], s->focal, s->max_lod);
             }
-            want[i] = w;
-            if (w != OR_NONE) stats[OR_ST_VISIBLE]++;
-            const int cached = w != OR_NONE && w > 0 && !s->uni[i];
-            const int keep = cached && s->res_lod[i] == w;
-            if (s->res_lod[i] != OR_NONE && !keep) { /* free: push in brick order */
-                const uint32_t l = s->res_lod[i];
-                s->stack[l][s->top[l]++] = s->res_off[i];
-                s->res_lod[i] = OR_NONE;
+            s->want[k][i] = w;
+        }
+    }
+    uint32_t A[OR_LODS] = {0};
+    for (uint32_t i = 0; i < nb; ++i) {
+        int vis = 0;
+        for (int k = 0; k < OR_MAX_SESSIONS; ++k) vis |= open[k] && s->want[k][i] != OR_NONE;
+        stats[OR_ST_VISIBLE] += vis;
+        const uint8_t need = need_mask(s, i, open);
+        const uint8_t fr = s->res[i] & (uint8_t)~need;
+        for (uint32_t l = 1; l <= s->max_lod; ++l) /* frees: pushed in brick order */
+            if (fr & (1u << l)) {
+                s->stack[l][s->top[l]++] = s->off[(size_t)i * OR_LODS + l];
                 stats[OR_ST_FREED]++;
             }
-            if (cached && !keep) A[w]++;
-            if (cached) Wn[w]++;
-        }
-        uint64_t need = 0;
+        s->res[i] &= need;
+        const uint8_t al = need & (uint8_t)~s->res[i];
+        for (uint32_t l = 1; l <= s->max_lod; ++l) A[l] += (al >> l) & 1u;
+    }
+    uint64_t fresh = 0;
+    for (uint32_t l = 1; l <= s->max_lod; ++l)
+        if (A[l] > s->top[l]) fresh += (uint64_t)(A[l] - s->top[l]) << (3 * l);
+    uint32_t* adm = (uint32_t*)malloc(sizeof(uint32_t) * ((size_t)nb * OR_LODS + 1));
+    uint32_t n_adm = 0;
+    if (s->bump + fresh <= s->cap) {
         for (uint32_t l = 1; l <= s->max_lod; ++l)
-            if (A[l] > s->top[l]) need += (uint64_t)(A[l] - s->top[l]) << (3 * l);
-        uint32_t* admitted = (uint32_t*)malloc(sizeof(uint32_t) * (nb + 1));
-        uint32_t n_adm = 0;
-        if (s->bump + need <= s->cap) {
-            for (uint32_t l = 1; l <= s->max_lod; ++l)
-                for (uint32_t i = 0; i < nb; ++i) {
-                    const int cached = want[i] == l && !s->uni[i];
-                    if (!cached || s->res_lod[i] == l) continue;
-                    uint64_t off;
-                    if (s->top[l] > 0) off = s->stack[l][--s->top[l]];
-                    else {
-                        off = s->bump;
-                        s->bump += 1ull << (3 * l);
-                    }
-                    s->res_lod[i] = (uint8_t)l;
-                    s->res_off[i] = off;
-                    admitted[n_adm++] = i;
+            for (uint32_t i = 0; i < nb; ++i) {
+                const uint8_t need = need_mask(s, i, open);
+                if (!((need >> l) & 1u) || ((s->res[i] >> l) & 1u)) continue;
+                uint64_t o;
+                if (s->top[l] > 0) o = s->stack[l][--s->top[l]];
+                else {
+                    o = s->bump;
+                    s->bump += 1ull << (3 * l);
                 }
-        } else {
-            stats[OR_ST_REBUILT] = 1;
-            for (uint32_t i = 0; i < nb; ++i) s->res_lod[i] = OR_NONE;
-            for (uint32_t l = 0; l < OR_MAXV; ++l) s->top[l] = 0;
-            s->bump = 0;
-            for (uint32_t l = 1; l <= s->max_lod; ++l)
-                for (uint32_t i = 0; i < nb; ++i) {
-                    if (want[i] != l || s->uni[i]) continue;
-                    const uint64_t sz = 1ull << (3 * l);
-                    if (s->bump + sz > s->cap) continue;
-                    s->res_lod[i] = (uint8_t)l;
-                    s->res_off[i] = s->bump;
-                    s->bump += sz;
-                    admitted[n_adm++] = i;
-                }
-        }
-        uint64_t vox = 0;
-        for (uint32_t k = 0; k < n_adm; ++k) {
-            const uint32_t i = admitted[k];
-            decode_into(s, i, s->res_lod[i], s->cache + s->pal_region + s->res_off[i]);
-            vox += 1ull << (3 * s->res_lod[i]);
-        }
-        stats[OR_ST_DECODED] = n_adm;
-        stats[OR_ST_VOX_LO] = (uint32_t)vox;
-        stats[OR_ST_VOX_HI] = (uint32_t)(vox >> 32);
-        /* slot table */
+                s->res[i] |= (uint8_t)(1u << l);
+                s->off[(size_t)i * OR_LODS + l] = o;
+                adm[n_adm++] = i * OR_LODS + l;
+            }
+    } else {
+        stats[OR_ST_REBUILT] = 1;
+        memset(s->res, 0, nb + 1);
+        for (uint32_t l = 0; l < OR_LODS; ++l) s->top[l] = 0;
+        s->bump = 0;
+        for (uint32_t l = 1; l <= s->max_lod; ++l)
+            for (uint32_t i = 0; i < nb; ++i) {
+                if (!((need_mask(s, i, open) >> l) & 1u)) continue;
+                const uint64_t sz = 1ull << (3 * l);
+                if (s->bump + sz > s->cap) continue;
+                s->res[i] |= (uint8_t)(1u << l);
+                s->off[(size_t)i * OR_LODS + l] = s->bump;
+                s->bump += sz;
+                adm[n_adm++] = i * OR_LODS + l;
+            }
+    }
+    uint64_t vox = 0;
+    for (uint32_t k = 0; k < n_adm; ++k) {
+        const uint32_t i = adm[k] / OR_LODS, l = adm[k] % OR_LODS;
+        decode_into(s, i, l, s->cache + s->pal_region + s->off[(size_t)i * OR_LODS + l]);
+        vox += 1ull << (3 * l);
+    }
+    free(adm);
+    stats[OR_ST_DECODED] = n_adm;
+    stats[OR_ST_VOX_LO] = (uint32_t)vox;
+    stats[OR_ST_VOX_HI] = (uint32_t)(vox >> 32);
+    /* slot tables of the open sessions */
+    for (int k = 0; k < OR_MAX_SESSIONS; ++k) {
+        if (!open[k]) continue;
         for (uint32_t i = 0; i < nb; ++i) {
+            const uint8_t w = s->want[k][i];
             or_slot sl = {0, 0, 0};
             if (!s->has[i]) sl.flags = 1u;
-            else if (s->res_lod[i] != OR_NONE) {
-                sl.offset = s->pal_region + s->res_off[i];
-                sl.lod = s->res_lod[i];
-            } else if (s->uni[i] || want[i] == 0) {
-                sl.offset = i;
+            else if (s->uni[i] || w == 0) sl.offset = i;
+            else if (w != OR_NONE && ((s->res[i] >> w) & 1u)) {
+                sl.offset = s->pal_region + s->off[(size_t)i * OR_LODS + w];
+                sl.lod = w;
             } else sl.flags = 2u;
-            s->slots[s->id[i]] = sl;
+            s->slots[k][s->id[i]] = sl;
         }
-        free(admitted);
-        free(want);
-        stats[OR_ST_PLANNED] = 1;
     }
-    for (uint32_t i = 0; i < nb; ++i) stats[OR_ST_RESIDENT] += s->res_lod[i] != OR_NONE;
-    /* render every view; request words as brickRequests, union over the views */
+    stats[OR_ST_PLANNED] = 1;
+}
+
+int or_serve_step(or_server* s, const uint32_t* sess, const double* views_in, const uint8_t* render, uint32_t n,
+                  uint64_t* out_label, float* out_depth, uint32_t* stats) {
+    if (n > OR_MAX_SESSIONS) return -1;
+    memset(stats, 0, sizeof(uint32_t) * OR_SERVE_STATS);
+    uint8_t open[OR_MAX_SESSIONS] = {0};
+    int changed = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        const uint32_t id = sess[k];
+        if (id >= OR_MAX_SESSIONS || open[id]) return -1;
+        open[id] = 1;
+        const double* v = views_in + 6 * k;
+        double len = sqrt(v[3] * v[3] + v[4] * v[4] + v[5] * v[5]);
+        if (len == 0.0) len = 1.0;
+        const double u[6] = {v[0], v[1], v[2], v[3] / len, v[4] / len, v[5] / len};
+        if (!s->planned[id] || view_moved(u, s->pview[id])) {
+            memcpy(s->pview[id], u, sizeof u);
+            s->planned[id] = 1;
+            changed = 1;
+        }
+    }
+    for (int k = 0; k < OR_MAX_SESSIONS; ++k) {
+        if (open[k] != s->last_open[k]) changed = 1;
+        if (!open[k]) s->planned[k] = 0;
+    }
+    if (changed) {
+        plan(s, open, stats);
+        memcpy(s->last_open, open, sizeof open);
+    }
+    for (uint32_t i = 0; i < s->nb; ++i)
+        for (uint32_t l = 1; l <= s->max_lod; ++l) stats[OR_ST_RESIDENT] += (s->res[i] >> l) & 1u;
+    /* render the sessions that submitted a frame; request words as brickRequests */
     uint32_t* req = (uint32_t*)calloc(s->n_slots, 4);
     const size_t px = (size_t)s->W * s->H;
+    uint32_t j = 0;
     for (uint32_t k = 0; k < n; ++k) {
+        if (!render[k]) continue;
         float cam[16];
         or_camera_uniform(views_in + 6 * k, views_in + 6 * k + 3, s->fov, cam);
-        or_render_rows(cam, s->W, s->H, 0, 1, (float)(s->bpa * b), b, s->bpa, s->slots, s->n_slots, s->cache,
-                       s->hidden, s->n_hidden, out_label + k * px, out_depth + k * px, NULL, req);
-    }
-    for (uint64_t m = 0; m < s->n_slots; ++m) {
-        if (req[m]) stats[OR_ST_ENTERED]++;
-        if (req[m] == 3u) stats[OR_ST_MISSING]++;
+        memset(req, 0, s->n_slots * 4);
+        or_render_rows(cam, s->W, s->H, 0, 1, (float)(s->bpa * s->b), s->b, s->bpa, s->slots[sess[k]], s->n_slots,
+                       s->cache, s->hidden, s->n_hidden, out_label + j * px, out_depth + j * px, NULL, req);
+        for (uint64_t m = 0; m < s->n_slots; ++m) {
+            if (req[m]) stats[OR_ST_SESSION + 2 * j]++;
+            if (req[m] == 3u) stats[OR_ST_SESSION + 2 * j + 1]++;
+        }
+        ++j;
     }
     free(req);
     return 0;

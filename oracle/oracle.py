@@ -70,14 +70,14 @@ class Oracle:
         L.or_serve_new.restype = C.c_void_p
         L.or_serve_new.argtypes = [_u8p, C.c_size_t, C.c_uint32, C.c_uint32, C.c_double, C.c_uint32, C.c_uint64,
                                    _u64p, C.c_uint32]
-        L.or_serve_step.argtypes = [C.c_void_p, _u32p, C.POINTER(C.c_double), C.c_uint32, _u64p,
+        L.or_serve_step.argtypes = [C.c_void_p, _u32p, C.POINTER(C.c_double), _u8p, C.c_uint32, _u64p,
                                     C.POINTER(C.c_float), _u32p]
         L.or_serve_n_slots.restype = C.c_uint64
         L.or_serve_n_slots.argtypes = [C.c_void_p]
         L.or_serve_bricks_per_axis.restype = C.c_uint32
         L.or_serve_bricks_per_axis.argtypes = [C.c_void_p]
         L.or_serve_slots.restype = C.c_void_p
-        L.or_serve_slots.argtypes = [C.c_void_p]
+        L.or_serve_slots.argtypes = [C.c_void_p, C.c_uint32]
         L.or_serve_cache.restype = C.c_void_p
         L.or_serve_cache.argtypes = [C.c_void_p]
         L.or_serve_free.argtypes = [C.c_void_p]
@@ -199,7 +199,8 @@ class Oracle:
         return int(nops[0]), ls, ck[:4 * int(nck[0])].reshape(-1, 4), st
 
 
-SERVE_STATS = ["planned", "visible", "decoded", "freed", "resident", "rebuilt", "entered", "missing"]
+SERVE_STATS = ["planned", "visible", "decoded", "freed", "resident", "rebuilt"]
+SERVE_NSTATS = 8 + 2 * 8
 SLOT_DTYPE = np.dtype([("offset", "<u8"), ("lod", "<u4"), ("flags", "<u4")])
 
 
@@ -226,24 +227,34 @@ class OracleServer:
         self.n_slots = int(self.lib.or_serve_n_slots(self.h))
         self.bpa = int(self.lib.or_serve_bricks_per_axis(self.h))
 
-    def step(self, sessions, views):
-        """views: per session (position[3], direction[3]); returns labels (n, H, W), depth (n, H, W), stats dict."""
+    def step(self, sessions, views, render=None):
+        """sessions: the open sessions (ascending ids); views: their latest (position[3], direction[3]);
+        render: per session, whether it submitted a frame (default all).  Returns labels (r, H, W) and
+        depth (r, H, W) of the r rendered sessions, and the stats dict (entered/missing: lists per rendered
+        session)."""
         n = len(sessions)
+        render = [1] * n if render is None else [1 if r else 0 for r in render]
+        r = sum(render)
         ss = np.ascontiguousarray(sessions, np.uint32)
-        vv = np.ascontiguousarray([list(p) + list(d) for p, d in views], np.float64)
-        lab = np.zeros(n * self.W * self.H, np.uint64)
-        dep = np.zeros(n * self.W * self.H, np.float32)
-        st = np.zeros(10, np.uint32)
-        rc = self.lib.or_serve_step(self.h, _ptr(ss, _u32p), vv.ctypes.data_as(C.POINTER(C.c_double)), n,
-                                    _ptr(lab, _u64p), dep.ctypes.data_as(C.POINTER(C.c_float)), _ptr(st, _u32p))
+        vv = np.ascontiguousarray([list(p) + list(d) for p, d in views] or [[0.0] * 6], np.float64)
+        rr = np.ascontiguousarray(render or [0], np.uint8)
+        lab = np.zeros(max(1, r) * self.W * self.H, np.uint64)
+        dep = np.zeros(max(1, r) * self.W * self.H, np.float32)
+        st = np.zeros(SERVE_NSTATS, np.uint32)
+        rc = self.lib.or_serve_step(self.h, _ptr(ss, _u32p), vv.ctypes.data_as(C.POINTER(C.c_double)),
+                                    _ptr(rr, _u8p), n, _ptr(lab, _u64p), dep.ctypes.data_as(C.POINTER(C.c_float)),
+                                    _ptr(st, _u32p))
         if rc:
             raise ValueError("or_serve_step failed")
         stats = {k: int(st[i]) for i, k in enumerate(SERVE_STATS)}
-        stats["decoded_voxels"] = int(st[8]) | (int(st[9]) << 32)
-        return lab.reshape(n, self.H, self.W), dep.reshape(n, self.H, self.W), stats
+        stats["decoded_voxels"] = int(st[6]) | (int(st[7]) << 32)
+        stats["entered"] = [int(st[8 + 2 * j]) for j in range(r)]
+        stats["missing"] = [int(st[9 + 2 * j]) for j in range(r)]
+        return lab[: r * self.W * self.H].reshape(r, self.H, self.W), \
+            dep[: r * self.W * self.H].reshape(r, self.H, self.W), stats
 
-    def slots(self) -> np.ndarray:
-        buf = (C.c_uint8 * (16 * self.n_slots)).from_address(self.lib.or_serve_slots(self.h))
+    def slots(self, session: int = 0) -> np.ndarray:
+        buf = (C.c_uint8 * (16 * self.n_slots)).from_address(self.lib.or_serve_slots(self.h, session))
         return np.frombuffer(bytes(buf), SLOT_DTYPE)
 
     def cache(self, n: int) -> np.ndarray:

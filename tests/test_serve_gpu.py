@@ -43,11 +43,13 @@ def _orbit_views(center, n, r0, r1, yaw0=0.2, pitch=0.25):
     return out
 
 
-def _run_pair(codec, oracle, img, steps, cache_bytes, cone, sessions=1, hidden=None):
-    """steps: list of per-step lists of (session, (pos, dir)); compares GPU and oracle after every step."""
+def _run_pair(codec, oracle, img, steps, cache_bytes, cone, sessions=1, hidden=None, leave=None, keep=None):
+    """steps: per step, the list of (session, (pos, dir)) that submit a frame; leave: {step: [sessions]} closed
+    before that step.  Compares GPU and oracle after every step; keep collects each session's images."""
     import torch
     from csvb200 import Server
     from oracle import SLOT_DTYPE, OracleServer, camera_uniform
+    leave = leave or {}
     ds = codec.open(img)
     srv = Server(codec, ds, W, H, FOV, cache_bytes=cache_bytes, max_sessions=sessions, cone=cone, hidden=hidden)
     ref = OracleServer(oracle, img, W, H, FOV, cone, cache_bytes, hidden=hidden)
@@ -56,37 +58,51 @@ def _run_pair(codec, oracle, img, steps, cache_bytes, cone, sessions=1, hidden=N
     info = srv.info()
     assert info.n_slots == ref.n_slots and info.bricks_per_axis == ref.bpa
     seen = {"rebuilt": 0, "freed": 0, "planned0": 0}
+    latest = {}
     for k, step in enumerate(steps):
+        for s in leave.get(k, []):
+            srv.leave(s)
+            latest.pop(s, None)
         for s, (pos, d) in step:
             srv.submit(s, pos, d, labs[s], deps[s])
+            latest[s] = (pos, d)
             assert np.array_equal(srv.camera(pos, d), camera_uniform(oracle, pos, d, FOV))
         sid = srv.step()
         frames = srv.poll(wait=True)
+        subm = sorted(s for s, _ in step)
         assert [f["step"] for f in frames] == [sid] * len(step)
-        rl, rd, rst = ref.step([s for s, _ in step], [v for _, v in step])
-        got = frames[0]
-        for key in ["planned", "visible", "decoded", "freed", "resident", "rebuilt", "entered", "missing",
-                    "decoded_voxels"]:
-            assert got[key] == rst[key], (k, key, got[key], rst[key])
-        slots = srv.slots_tensor().cpu().numpy().view(SLOT_DTYPE)
-        assert np.array_equal(slots, ref.slots()), k
-        if got["planned"] and got["decoded"]:
-            assert int(_status(srv, got["decoded"]).max()) == 0
-        for j, (s, _) in enumerate(step):
+        assert [f["session"] for f in frames] == subm
+        open_ = sorted(latest)
+        rl, rd, rst = ref.step(open_, [latest[s] for s in open_], [s in subm for s in open_])
+        for key in ["planned", "visible", "decoded", "freed", "resident", "rebuilt", "decoded_voxels"]:
+            assert all(f[key] == rst[key] for f in frames), (k, key, frames[0][key], rst[key])
+        assert [f["entered"] for f in frames] == rst["entered"], k
+        assert [f["missing"] for f in frames] == rst["missing"], k
+        for s in open_:
+            slots = srv.slots_tensor(s).cpu().numpy().view(SLOT_DTYPE)
+            assert np.array_equal(slots, ref.slots(s)), (k, s)
+        if frames and frames[0]["planned"] and frames[0]["decoded"]:
+            assert int(_status(srv, frames[0]["decoded"]).max()) == 0
+        for j, s in enumerate(subm):
             gl = labs[s].cpu().numpy().view(np.uint64).reshape(H, W)
             gd = deps[s].cpu().numpy().reshape(H, W)
             assert np.array_equal(gl, rl[j]), (k, s, int((gl != rl[j]).sum()))
             assert np.array_equal(gd.view(np.uint32), rd[j].view(np.uint32)), (k, s)
-        seen["rebuilt"] += got["rebuilt"]
-        seen["freed"] += got["freed"]
-        seen["planned0"] += got["planned"] == 0
+            if keep is not None:
+                keep.setdefault(s, []).append((gl.copy(), gd.copy()))
+        if frames:
+            seen["rebuilt"] += frames[0]["rebuilt"]
+            seen["freed"] += frames[0]["freed"]
+            seen["planned0"] += frames[0]["planned"] == 0
     # the resident labels equal the oracle's cache wherever a slot points
     cache = srv.cache_tensor().cpu().numpy().view(np.uint64)
     rc = ref.cache(len(cache))
-    for sl in slots[(slots["flags"] == 0)]:
-        n = 8 ** int(sl["lod"]) if sl["offset"] >= info.palette_table else 1
-        o = int(sl["offset"])
-        assert np.array_equal(cache[o:o + n], rc[o:o + n])
+    for s in sorted(latest):
+        slots = ref.slots(s)
+        for sl in slots[(slots["flags"] == 0)]:
+            n = 8 ** int(sl["lod"]) if sl["offset"] >= info.palette_table else 1
+            o = int(sl["offset"])
+            assert np.array_equal(cache[o:o + n], rc[o:o + n])
     srv.close()
     ref.close()
     ds.close()
@@ -122,8 +138,33 @@ def test_serve_two_sessions_one_step(codec, oracle, cube16):
     a = _orbit_views((64.0, 64.0, 64.0), 5, 160.0, 100.0)
     b = _orbit_views((64.0, 64.0, 64.0), 5, 120.0, 200.0, yaw0=2.5, pitch=-0.3)
     steps = [[(0, a[k]), (1, b[k])] for k in range(5)]
-    steps.insert(2, [(1, b[1])])  # one session alone: the session set changed, so the step re-plans
+    steps.insert(2, [(1, b[1])])  # session 0 open without a new frame
     _run_pair(codec, oracle, cube16, steps, 8 << 20, 1, sessions=2)
+
+
+def test_serve_each_session_same_alone_and_in_the_mix(codec, oracle, cube16):
+    """Continuous batching: session 1 joins while session 0 is served, skips a frame, leaves; session 2 joins
+    later.  Every session's images equal the ones it gets served alone, bit for bit."""
+    a = _orbit_views((64.0, 64.0, 64.0), 9, 170.0, 70.0)
+    b = _orbit_views((64.0, 64.0, 64.0), 9, 60.0, 190.0, yaw0=2.0, pitch=-0.4)
+    c = _orbit_views((64.0, 64.0, 64.0), 9, 110.0, 110.0, yaw0=4.0, pitch=0.6)
+    steps = []
+    for f in range(9):
+        st = [(0, a[f])]
+        if 2 <= f <= 6 and f != 4:
+            st.append((1, b[f]))
+        if f >= 5:
+            st.append((2, c[f]))
+        steps.append(st)
+    mix = {}
+    _run_pair(codec, oracle, cube16, steps, 64 << 20, 1, sessions=3, leave={7: [1]}, keep=mix)
+    for s in range(3):
+        alone = {}
+        solo = [[(0, v)] for st in steps for (q, v) in st if q == s]
+        _run_pair(codec, oracle, cube16, solo, 64 << 20, 1, sessions=1, keep=alone)
+        assert len(alone[0]) == len(mix[s])
+        for (l1, d1), (l2, d2) in zip(alone[0], mix[s]):
+            assert np.array_equal(l1, l2) and np.array_equal(d1.view(np.uint32), d2.view(np.uint32))
 
 
 def test_serve_hidden_labels(codec, oracle, cube16):
