@@ -40,6 +40,9 @@ MIXED = dict(name="mixed1024", shape=(1024, 1024, 1024), kind=2, n_cells=2000, n
 # The same generator at 1/8 of the volume (cells and tubes scaled with it): the small case for profiler captures.
 MIXED512 = dict(MIXED, name="mixed512", shape=(512, 512, 512), n_cells=250, n_tubes=625, split_x=256)
 WORKLOADS = {w["name"]: w for w in (MIXED, MIXED512)}
+SERVE = dict(name="serve2048", shape=(2048, 2048, 2048), brick=64, kind=1, n_cells=20000, n_tubes=8000, r_min=2.0,
+             r_max=12.0, zero_frac=0.15, seed=5, width=1920, height=1080, frames=600, cache_gib=24,
+             fov=1.0471975511965976)  # pi/3 (camera.js:19)
 NEURITE = dict(name="neurite512", shape=(512, 512, 512), brick=64, kind=1, n_cells=3000, n_tubes=400, r_min=2.0,
                r_max=12.0, zero_frac=0.15, seed=2)
 FALLBACK_HBM_GBS = 6650.0
@@ -290,6 +293,12 @@ def run_b200(args):
     # ---- neurite512: encode vs the reference encoder on this host, and its decode
     neur = neurite512(codec, dev, args, rank == 0 and world == 1 and not args.no_cpu)
 
+    # ---- serve2048: the frame loop (plan, cache, decode, render) over a 600-frame orbit
+    graph.close()
+    del out, vol, flush
+    torch.cuda.empty_cache()
+    serve = None if args.no_serve else serve2048(codec, dev, args)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_decode_sample(img_left, img_right, bl, br)
@@ -318,15 +327,97 @@ def run_b200(args):
             "encode": {"value": round(nvox / ((enc_ms_left + enc_ms_right) * 1e-3) / 1e6, 1), "unit": "Mvox/s",
                        "ms": round(enc_ms_left + enc_ms_right, 3), "workload": W["name"]},
             "neurite512": neur,
+            "serve2048": serve,
             "checks": {"decode_equals_source": check, "e2e_equals_device": e2e_ok},
         }
         print(json.dumps(line))
-    graph.close()
     cat.close()
     ds_left.close()
     ds_right.close()
     if pg is not None:
         pg.destroy_process_group()
+
+
+def orbit_path(n, center, seed):
+    """Seeded orbit with zoom (orbitController.js:100-123 camera placement): two turns, pitch swinging
+    +-0.35 rad, radius 1600..3600 voxels, small seeded jitter on every frame."""
+    import math
+    from csvb200.camera import orbit
+    rng = np.random.default_rng(seed)
+    jit = rng.normal(0.0, 1.0, (n, 3))
+    views = []
+    for f in range(n):
+        t = f / n
+        yaw = 2 * math.pi * 2 * t + 0.01 * jit[f, 0]
+        pitch = 0.35 * math.sin(2 * math.pi * 3 * t) + 0.01 * jit[f, 1]
+        radius = 2600.0 + 1000.0 * math.cos(2 * math.pi * 1.5 * t) + 10.0 * jit[f, 2]
+        views.append(orbit(center, radius, yaw, pitch))
+    return views
+
+
+def serve2048(codec, dev, args):
+    """On-demand decode + render at 1920x1080 over a 2048^3 volume with a 24 GiB decoded-brick cache."""
+    import math
+
+    import torch
+    from csvb200 import CONE_SCREEN, Server
+    S = SERVE
+    vol = torch.empty(S["shape"], dtype=torch.int64, device=dev)
+    codec.synth_volume(vol, S["kind"], S["n_cells"], S["n_tubes"], S["r_min"], S["r_max"], S["zero_frac"], S["seed"])
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    img_len = codec.encode_device(vol, S["brick"])
+    e1.record(st)
+    torch.cuda.synchronize()
+    enc_ms = e0.elapsed_time(e1)
+    ds = codec.open_encoded()
+    del vol
+    torch.cuda.empty_cache()
+    Wp, Hp = S["width"], S["height"]
+    srv = Server(codec, ds, Wp, Hp, S["fov"], cache_bytes=S["cache_gib"] << 30, cone=CONE_SCREEN)
+    lab = torch.empty(Wp * Hp, dtype=torch.int64, device=dev)
+    dep = torch.empty(Wp * Hp, dtype=torch.float32, device=dev)
+    c = [v / 2.0 for v in S["shape"][::-1]]
+    views = orbit_path(S["frames"], c, S["seed"])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    b0.record(st)
+    for pos, d in views:
+        srv.submit(0, pos, d, lab, dep)
+        srv.step(st)
+    b1.record(st)
+    frames = srv.poll(wait=True, max_frames=len(views) + 8)
+    wall = time.perf_counter() - t0
+    total_ms = b0.elapsed_time(b1)
+    ms = np.array([f["ms"] for f in frames])
+    dec = np.array([f["decoded"] for f in frames])
+    vox = np.array([f["decoded_voxels"] for f in frames])
+    out = {
+        "workload": S["name"], "volume": list(S["shape"][::-1]), "brick": S["brick"],
+        "bricks": ds.num_bricks, "tubes": S["n_tubes"], "voronoi_cells": S["n_cells"],
+        "radius": [S["r_min"], S["r_max"]], "zero_frac": S["zero_frac"], "seed": S["seed"],
+        "image_bytes": int(img_len), "encode_ms": round(enc_ms, 2),
+        "resolution": [Wp, Hp], "frames": len(frames), "cache_gib": S["cache_gib"], "cone": "screen",
+        "path": "seeded orbit with zoom, radius 1600-3600, 2 turns",
+        "p50_ms": round(float(np.percentile(ms, 50)), 3), "p99_ms": round(float(np.percentile(ms, 99)), 3),
+        "max_ms": round(float(ms.max()), 3), "first_frame_ms": round(float(ms[0]), 3),
+        "mean_ms": round(float(ms.mean()), 3), "loop_ms": round(total_ms, 2),
+        "host_wall_s": round(wall, 3),
+        "decoded_bricks": int(dec.sum()), "decoded_bricks_per_s": round(float(dec.sum()) / (ms.sum() * 1e-3), 1),
+        "decoded_gvox": round(float(vox.sum()) / 1e9, 3),
+        "missing_entered": int(sum(f["missing"] for f in frames)),
+        "rebuilds": int(sum(f["rebuilt"] for f in frames)),
+        "resident_blocks_last": int(frames[-1]["resident"]),
+        "entered_bricks_mean": round(float(np.mean([f["entered"] for f in frames])), 1),
+        "hit_pixels_last_frame": round(float((lab != 0).float().mean()), 4),
+        "timing": "device time per step (CUDA events around plan, cache, decode, render, census)",
+    }
+    srv.close()
+    ds.close()
+    torch.cuda.empty_cache()
+    return out
 
 
 def neurite512(codec, dev, args, with_cpu):
@@ -493,6 +584,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline legs")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop leg")
     ap.add_argument("--workload", default="mixed1024", choices=sorted(WORKLOADS),
                     help="mixed1024: the headline; mixed512: the same generator at 1/8 size (profiler captures)")
     args = ap.parse_args()
