@@ -1,6 +1,7 @@
 // csv_internal.h -- shared device/host definitions of the B200 CSV codec.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -124,6 +125,11 @@ cudaError_t launch_render(const csv_camera& cam, uint32_t W, uint32_t H, float g
                           const csv_brick_slot* slots, uint64_t n_slots, const uint64_t* labels, const uint64_t* hidden,
                           uint32_t n_hidden, uint64_t* out_label, float* out_depth, uint32_t* requests,
                           cudaStream_t st);
+
+size_t gemm_smem_bytes();
+cudaError_t launch_gemm_bf16(const __nv_bfloat16* A, const __nv_bfloat16* B, uint32_t M, uint32_t N, uint32_t K,
+                             const float* bias, const __nv_bfloat16* mask, uint32_t relu, float* C,
+                             __nv_bfloat16* Cb, __nv_bfloat16* CbT, float* CT, uint32_t* err, cudaStream_t st);
 
 cudaError_t synth_volume(uint64_t* d_vol, uint32_t W, uint32_t H, uint32_t D, int kind, uint32_t n_cells,
                          uint32_t n_tubes, float r_min, float r_max, float zero_frac, uint64_t seed,

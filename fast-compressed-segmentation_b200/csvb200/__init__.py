@@ -21,6 +21,7 @@ streams).  There is no CPU fallback: a missing library or GPU raises.
 from __future__ import annotations
 
 import ctypes as C
+import ctypes as C_MOD
 import os
 from dataclasses import dataclass
 
@@ -148,8 +149,15 @@ def load_library() -> C.CDLL:
     L.csv_serve_state.argtypes = [vp, C.c_uint32, C.POINTER(ServeInfo)]
     L.csv_serve_close.argtypes = [vp, C.c_uint32]
     L.csv_serve_destroy.argtypes = [vp]
+    L.csv_gemm_bf16.argtypes = [vp, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, C.c_uint32, vp, vp, vp, vp,
+                                vp, vp]
     _lib = L
     return L
+
+
+def _vp(t):
+    """Device pointer of a tensor (or NULL for None) as a ctypes void pointer."""
+    return C.c_void_p(t.data_ptr() if t is not None else None)
 
 
 def _stream_handle(stream) -> int | None:
@@ -385,6 +393,16 @@ class Codec:
             C.c_void_p(d_depth_out.data_ptr()),
             C.c_void_p(d_requests.data_ptr() if d_requests is not None else None),
             C.c_void_p(_stream_handle(stream))))
+
+    # ---- tensor-core dense layer ------------------------------------------
+    def gemm_bf16(self, A, B, bias=None, mask=None, relu=False, C=None, Cb=None, CbT=None, CT=None, err=None,
+                  stream=None):
+        """C = epilogue(A . B^T) on the tensor cores (csv_gemm_bf16); A [M][K], B [N][K] bf16 device tensors."""
+        M, K = A.shape
+        N = B.shape[0]
+        self._check(self.lib.csv_gemm_bf16(self.handle, _vp(A), _vp(B), M, N, K, _vp(bias), _vp(mask),
+                                           1 if relu else 0, _vp(C), _vp(Cb), _vp(CbT), _vp(CT), _vp(err),
+                                           C_MOD.c_void_p(_stream_handle(stream))))
 
     # ---- workload generator ---------------------------------------------
     def synth_volume(self, d_volume, kind: int, n_cells: int, n_tubes: int = 0, r_min: float = 0.0,

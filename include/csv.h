@@ -318,6 +318,18 @@ int csv_serve_camera(const csv_server* srv, const csv_view* view, csv_camera* ou
 int csv_serve_state(const csv_server* srv, uint32_t session, csv_serve_info* info);
 int csv_serve_destroy(csv_server* srv);
 
+/* ---- learned mode / table selector (no reference counterpart) ---------
+ * Dense layer on the tensor cores (tcgen05, accumulator in tensor memory):
+ * C[M][N] = epilogue(A[M][K] . B[N][K]^T), A and B bf16 row-major (K
+ * contiguous), fp32 accumulation.  Epilogue, in order: + d_bias[n] (if not
+ * NULL), max(0, .) (if relu), * (d_mask[m][n] > 0) (if d_mask, bf16 [M][N]: the
+ * ReLU gradient); outputs (each optional): d_C fp32 [M][N], d_Cb bf16 [M][N],
+ * d_CbT bf16 [N][M], d_CT fp32 [N][M].  M % 128 == 0, N % 16 == 0, K % 64 == 0.
+ * d_err (optional) is set to 1 if a bounded wait gave up. */
+int csv_gemm_bf16(csv_ctx* ctx, const void* d_A, const void* d_B, uint32_t M, uint32_t N, uint32_t K,
+                  const float* d_bias, const void* d_mask, uint32_t relu, float* d_C, void* d_Cb, void* d_CbT,
+                  float* d_CT, uint32_t* d_err, void* stream);
+
 /* ---- workload generator (no reference counterpart) --------------------
  * Seeded synthetic label volume on the device, x fastest: kind 0 = Voronoi
  * (n_cells cells, then a random half-space slab of label 0 covering about
