@@ -61,21 +61,25 @@ uint32_t rd32(const uint8_t* p) {
     return v;
 }
 
-// Host view of a .csbd v1 image (fileIO.cpp:25-96, datasetLoader.js:39-146).
+// Host view of a .csbd image: version 1 (fileIO.cpp:25-96, datasetLoader.js:39-146),
+// or version 2, which carries up to 16 shared rANS tables (28-byte header, then
+// freq[16] and cum[16] per table) and, after each brick's ID, a u32 naming the
+// brick's table (bits 4..7) and encoding mode (bits 0..3).
 struct ImageView {
-    uint32_t nb = 0, b = 0, total = 0;
-    uint32_t freq[16], cum[16];
+    uint32_t version = 1, nb = 0, b = 0, total = 0, n_tables = 1;
+    uint32_t freq[16][16], cum[16][16];
     struct Rec {
         size_t pal_at, enc_at;
-        uint32_t id, P, E, nsym;
+        uint32_t id, P, E, nsym, sel;
     };
     std::vector<Rec> recs;
 };
 
 int parse_image(csv_ctx* ctx, const uint8_t* img, size_t len, ImageView& v) {
-    if (!img || len < kHeaderBytes) return fail(ctx, CSV_EFORMAT, "image shorter than the 152-byte header");
+    if (!img || len < 28) return fail(ctx, CSV_EFORMAT, "image shorter than its header");
     if (rd32(img) != kMagic) return fail(ctx, CSV_EFORMAT, "Invalid file format (bad magic)");
-    if (rd32(img + 4) != 1) return fail(ctx, CSV_EFORMAT, "unsupported .csbd version");
+    v.version = rd32(img + 4);
+    if (v.version != 1 && v.version != 2) return fail(ctx, CSV_EFORMAT, "unsupported .csbd version");
     v.nb = rd32(img + 8);
     v.b = rd32(img + 12);
     if (v.b < 2 || v.b > 64 || (v.b & (v.b - 1)))
@@ -83,17 +87,42 @@ int parse_image(csv_ctx* ctx, const uint8_t* img, size_t len, ImageView& v) {
     if (rd32(img + 16) != 16) return fail(ctx, CSV_EFORMAT, "symbol count must be 16");
     v.total = rd32(img + 20);
     if (v.total != kTot) return fail(ctx, CSV_EFORMAT, "total frequency must be 4096");
-    for (int i = 0; i < 16; ++i) {
-        v.freq[i] = rd32(img + 24 + 4 * i);
-        v.cum[i] = rd32(img + 88 + 4 * i);
-        if (v.freq[i] > kTot || v.cum[i] >= kTot) return fail(ctx, CSV_EFORMAT, "rANS model entry out of range");
+    size_t o;
+    if (v.version == 1) {
+        if (len < kHeaderBytes) return fail(ctx, CSV_EFORMAT, "image shorter than the 152-byte header");
+        v.n_tables = 1;
+        for (int i = 0; i < 16; ++i) {
+            v.freq[0][i] = rd32(img + 24 + 4 * i);
+            v.cum[0][i] = rd32(img + 88 + 4 * i);
+        }
+        o = kHeaderBytes;
+    } else {
+        v.n_tables = rd32(img + 24);
+        if (v.n_tables == 0 || v.n_tables > 16) return fail(ctx, CSV_EFORMAT, "version 2: 1..16 tables");
+        o = 28 + 128ull * v.n_tables;
+        if (len < o) return fail(ctx, CSV_EFORMAT, "truncated table header");
+        for (uint32_t t = 0; t < v.n_tables; ++t)
+            for (int i = 0; i < 16; ++i) {
+                v.freq[t][i] = rd32(img + 28 + 128 * t + 4 * i);
+                v.cum[t][i] = rd32(img + 28 + 128 * t + 64 + 4 * i);
+            }
     }
+    for (uint32_t t = 0; t < v.n_tables; ++t)
+        for (int i = 0; i < 16; ++i)
+            if (v.freq[t][i] > kTot || v.cum[t][i] >= kTot)
+                return fail(ctx, CSV_EFORMAT, "rANS model entry out of range");
     v.recs.resize(v.nb);
-    size_t o = kHeaderBytes;
     for (uint32_t i = 0; i < v.nb; ++i) {
         ImageView::Rec& r = v.recs[i];
+        r.sel = 0;
         if (o + 8 > len) return fail(ctx, CSV_EFORMAT, "truncated brick header");
         r.id = rd32(img + o);
+        if (v.version == 2) {
+            r.sel = rd32(img + o + 4);
+            if (((r.sel >> 4) & 15u) >= v.n_tables) return fail(ctx, CSV_EFORMAT, "brick names a missing table");
+            o += 4;
+            if (o + 8 > len) return fail(ctx, CSV_EFORMAT, "truncated brick header");
+        }
         r.P = rd32(img + o + 4);
         if (r.P == 0 || r.P > kMaxPalette) return fail(ctx, CSV_EFORMAT, "palette size out of range");
         r.pal_at = o + 8;
@@ -128,8 +157,9 @@ int stage_dataset(csv_ctx* ctx, const uint8_t* img, const ImageView& v, DeviceDa
     d.L = levels_of(v.b);
     d.S = kOpsPerCheckpoint;
     d.total = v.total;
-    memcpy(d.freq, v.freq, sizeof d.freq);
-    memcpy(d.cum, v.cum, sizeof d.cum);
+    memcpy(d.freq, v.freq[0], sizeof d.freq);
+    memcpy(d.cum, v.cum[0], sizeof d.cum);
+    d.n_models = v.n_tables;
     std::vector<BrickDesc> desc(v.nb);
     uint64_t pal_n = 0, enc_n = 0, ck_n = 0;
     d.h_ids = (uint32_t*)malloc(sizeof(uint32_t) * std::max<uint32_t>(1, v.nb));
@@ -146,7 +176,7 @@ int stage_dataset(csv_ctx* ctx, const uint8_t* img, const ImageView& v, DeviceDa
         b.id = r.id;
         b.ck_off = (uint32_t)ck_n;
         b.ck_cap = (r.nsym + d.S - 1) / d.S + 1;
-        b.flags = BF_NOINDEX | (d.L << BF_LEVELS_SHIFT);
+        b.flags = BF_NOINDEX | (d.L << BF_LEVELS_SHIFT) | (((r.sel >> 4) & 15u) << BF_MODEL_SHIFT);
         d.h_ids[i] = r.id;
         d.h_cost[i] = r.nsym;
         pal_n += r.P;
@@ -169,20 +199,21 @@ int stage_dataset(csv_ctx* ctx, const uint8_t* img, const ImageView& v, DeviceDa
         memcpy(pal.data() + desc[i].pal_off, img + r.pal_at, 8ull * r.P);
         memcpy(enc.data() + desc[i].enc_off, img + r.enc_at, r.E);
     }
-    uint32_t lut[kTot];
-    build_lut(v.freq, v.cum, lut);
+    std::vector<uint32_t> lut((size_t)kTot * v.n_tables);
+    for (uint32_t t = 0; t < v.n_tables; ++t) build_lut(v.freq[t], v.cum[t], &lut[(size_t)t * kTot]);
     cudaError_t e;
     if ((e = cudaMalloc(&d.d_bricks, sizeof(BrickDesc) * std::max<uint32_t>(1, v.nb))) != cudaSuccess ||
         (e = cudaMalloc(&d.d_pal, 8 * pal.size())) != cudaSuccess ||
         (e = cudaMalloc(&d.d_enc, enc.size())) != cudaSuccess ||
         (e = cudaMalloc(&d.d_ck, sizeof(Checkpoint) * std::max<uint64_t>(1, ck_n))) != cudaSuccess ||
-        (e = cudaMalloc(&d.d_lut, sizeof lut)) != cudaSuccess)
+        (e = cudaMalloc(&d.d_lut, sizeof(uint32_t) * lut.size())) != cudaSuccess)
         return fail(ctx, CSV_ENOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
     if ((e = cudaMemcpyAsync(d.d_bricks, desc.data(), sizeof(BrickDesc) * v.nb, cudaMemcpyHostToDevice, st)) !=
             cudaSuccess ||
         (e = cudaMemcpyAsync(d.d_pal, pal.data(), 8 * pal.size(), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
         (e = cudaMemcpyAsync(d.d_enc, enc.data(), enc.size(), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(d.d_lut, lut, sizeof lut, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        (e = cudaMemcpyAsync(d.d_lut, lut.data(), sizeof(uint32_t) * lut.size(), cudaMemcpyHostToDevice, st)) !=
+            cudaSuccess)
         return cuda_fail(ctx, e, "staging copy");
     // the host vectors go out of scope: finish the copies first
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "staging copy");
@@ -494,6 +525,7 @@ int csv_dataset_concat(csv_ctx* ctx, const csv_dataset* const* parts, uint32_t n
         }
         memcpy(d.h_ids + id_base, p.h_ids, sizeof(uint32_t) * p.nb);
         memcpy(d.h_cost + id_base, p.h_cost, sizeof(uint32_t) * p.nb);
+        if (k > 0 && p.b != d.b) d.mixed_b = 1;
         d.b = std::max(d.b, p.b);
         d.L = std::max(d.L, p.L);
         d.max_P = std::max(d.max_P, p.max_P);

@@ -75,7 +75,8 @@ struct DeviceDataset {
     uint32_t freq[16] = {}, cum[16] = {}, total = 0;
     uint64_t stream_bytes = 0, palette_entries = 0, ck_entries = 0;
     uint32_t max_nsym = 0, max_P = 0;
-    uint32_t n_models = 1;  // LUTs at d_lut (a concatenation of datasets keeps each part's model)
+    uint32_t n_models = 1;  // LUTs at d_lut (a version-2 image's tables; a concatenation keeps each part's)
+    uint32_t mixed_b = 0;   // a concatenation of different brick sizes
     uint64_t enc_pool_bytes = 0, pal_pool_entries = 0;  // sizes of d_enc and d_pal
     uint32_t* h_cost = nullptr;  // per brick: decode work estimate (nSymbols), for scheduling
     BrickDesc* d_bricks = nullptr;
@@ -113,8 +114,16 @@ cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, ui
 struct EncoderState;
 EncoderState* encoder_state_new();
 void encoder_state_free(EncoderState* s);
+// Per-brick mode / shared-table choice for an encode (version-2 image).
+struct EncodeSelection {
+    uint32_t n_tables = 0;           // 0: version 1, one model from the sampled bricks' histogram
+    uint32_t freq[16][16] = {};      // each table's frequencies (each >= 1, sum 4096)
+    const uint8_t* d_sel = nullptr;  // per brick, device: mode | table << 4 (null: mode 0, table 0)
+};
 int encode_device(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W, uint64_t H, uint64_t D, uint32_t b,
-                  cudaStream_t st, std::string& err);
+                  cudaStream_t st, std::string& err, const EncodeSelection* sel = nullptr);
+int encode_stats(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W, uint64_t H, uint64_t D, uint32_t b,
+                 uint32_t* d_hist, cudaStream_t st, std::string& err);
 int encoder_to_dataset(EncoderState* s, DeviceDataset& d, std::string& err);
 const uint8_t* encoder_image(EncoderState* s, size_t* len);
 

@@ -151,13 +151,17 @@ __device__ __forceinline__ uint32_t rans_step(uint32_t& x, uint32_t& pos, const 
 __global__ void __launch_bounds__(32) build_index_kernel(BrickDesc* __restrict__ bricks, uint32_t nb,
                                                          const uint8_t* __restrict__ enc_pool,
                                                          const uint32_t* __restrict__ g_lut,
-                                                         Checkpoint* __restrict__ ck, uint32_t L, uint32_t S) {
-    __shared__ uint32_t lut[kTot];
-    for (uint32_t i = threadIdx.x; i < kTot; i += blockDim.x) lut[i] = g_lut[i];
+                                                         Checkpoint* __restrict__ ck, uint32_t L, uint32_t S,
+                                                         uint32_t n_models) {
+    __shared__ uint32_t lut0[kTot];
+    for (uint32_t i = threadIdx.x; i < kTot; i += blockDim.x) lut0[i] = g_lut[i];
     __syncthreads();
     uint32_t bi = blockIdx.x * blockDim.x + threadIdx.x;
     if (bi >= nb) return;
     BrickDesc br = bricks[bi];
+    // a version-2 image names a shared table per brick; other tables are read through the cache
+    const uint32_t model = min((br.flags >> BF_MODEL_SHIFT) & 255u, n_models - 1);
+    const uint32_t* lut = model == 0 ? lut0 : g_lut + (size_t)model * kTot;
     uint32_t ls[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) ls[k] = 0;
@@ -226,7 +230,8 @@ cudaError_t launch_build_index(DeviceDataset& ds, cudaStream_t st) {
     if (ds.nb == 0) return cudaSuccess;
     // one warp per block spreads the serial chains over as many SMs as possible
     uint32_t blocks = (ds.nb + 31) / 32;
-    build_index_kernel<<<blocks, 32, 0, st>>>(ds.d_bricks, ds.nb, ds.d_enc, ds.d_lut, ds.d_ck, ds.L, ds.S);
+    build_index_kernel<<<blocks, 32, 0, st>>>(ds.d_bricks, ds.nb, ds.d_enc, ds.d_lut, ds.d_ck, ds.L, ds.S,
+                                              ds.n_models ? ds.n_models : 1u);
     return cudaGetLastError();
 }
 

@@ -42,12 +42,16 @@ constexpr uint32_t kEncSmemLevels = 5;  // levels 0..4 in shared memory
 constexpr uint32_t kEncSmemNodes = 4681;
 constexpr uint32_t OP_PALNEED = 7;  // placeholder code until the palette walk decides P0 / Pd / Pa
 constexpr uint32_t EF_UNIFORM = 1u, EF_OVERFLOW = 2u;
+constexpr uint32_t kModes = 12;
+constexpr uint32_t kMaxTables = 16;
+constexpr uint32_t kModelWords = 65;  // freq[16] cum[16] total M[16] shift[16]
 
 struct EncMeta {
     uint64_t nib_off, pal_off, enc_off;
     uint32_t P, nsym, nbytes, n_ops;
     uint32_t id, flags, n_ck, E;
     uint32_t level_start[8];
+    uint32_t sel, pad;  // mode | table << 4
 };
 
 struct EncoderState {
@@ -75,6 +79,9 @@ struct EncoderState {
     uint8_t* d_image = nullptr;
     size_t image_cap = 0, image_len = 0;
     uint32_t freq[16] = {}, cum[17] = {};
+    uint32_t n_tables = 1;                       // rANS models of the last image
+    uint32_t tab_freq[16][16] = {}, tab_cum[16][16] = {};
+    bool v2 = false;
     std::vector<EncMeta> h_meta;
     bool valid = false;
 };
@@ -178,6 +185,7 @@ struct EncArgs {
     uint64_t pal_cap;
     Checkpoint* ck;
     unsigned long long* misc;
+    const uint8_t* sel;  // per brick: mode | table << 4 (null: mode 0, table 0)
 };
 
 struct EncShared {
@@ -214,14 +222,25 @@ __device__ __forceinline__ bool node_const(const BrickCtx& B, uint32_t l, uint32
     return B.cst_g[m] != 0;
 }
 
+// Decoder-transparent encoding modes.  Where several ops reproduce a child's
+// label, bestOperation (brickEncoding.hpp:198-282) takes Rp, then Rx, Ry, Rz,
+// then a palette op.  A mode keeps the grammar and changes that preference:
+// mode % 6 picks the order of the three neighbour axes, and modes >= 6 try the
+// neighbours before the parent.  The decoder replays any of them unchanged;
+// mode 0 is the reference's order.
+__constant__ uint8_t kAxisOrder[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+
 // Rp / Rx / Ry / Rz for child n on level lc (bestOperation, brickEncoding.hpp:198-282),
 // or OP_PALNEED when only a palette op can express it.
 __device__ __forceinline__ uint32_t choose_reuse(const BrickCtx& B, uint32_t lc, uint32_t n, uint64_t Lc,
-                                                 uint64_t parent) {
-    if (parent == Lc) return OP_RP;
+                                                 uint64_t parent, uint32_t mode) {
+    const bool nfirst = mode >= 6;
+    if (!nfirst && parent == Lc) return OP_RP;
+    const uint32_t ord = nfirst ? mode - 6 : mode;
     const uint32_t lvlmask = (1u << (3 * lc)) - 1u;
 #pragma unroll
-    for (uint32_t a = 0; a < 3; ++a) {
+    for (uint32_t k = 0; k < 3; ++k) {
+        const uint32_t a = kAxisOrder[ord][k];
         const uint32_t m = (0x09249249u << a) & lvlmask, bit = 1u << a;
         if (n & bit) {  // +1 side: later in Morton order -> the neighbour's parent (:265-272)
             if ((n & m) == m) continue;
@@ -233,28 +252,179 @@ __device__ __forceinline__ uint32_t choose_reuse(const BrickCtx& B, uint32_t lc,
             if (node_label(B, lc, N) == Lc) return OP_RX + a;
         }
     }
+    if (nfirst && parent == Lc) return OP_RP;
     return OP_PALNEED;
 }
 
-__global__ void __launch_bounds__(kEncThreads) enc_bricks_kernel(EncArgs A) {
-    __shared__ EncShared S;
-    const uint32_t tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5;
+// Per-CTA scratch carved from the context's encoder scratch.
+struct EncScratch {
+    uint64_t* lab_g;  // level L-2 labels when that level does not fit in shared memory
+    uint8_t* cst_g;
+    uint8_t* ops;     // code | stop << 3 | delta << 4
+    uint64_t* pal_lab;
+    uint8_t* nib;
+    uint64_t* pal_out;
+};
+
+__device__ __forceinline__ EncScratch enc_scratch(const EncArgs& A) {
     const uint64_t max_ops = ((1ull << (3 * A.L)) - 8) / 7;
     uint8_t* scr = A.scratch + (uint64_t)blockIdx.x * A.scratch_per_cta;
     auto align = [](uint64_t v) { return (v + 255) & ~255ull; };
     const uint32_t n_g = A.L >= kEncSmemLevels + 2 ? (1u << (3 * (A.L - 2))) : 0;  // level L-2 when it is big
+    EncScratch X;
     uint64_t o = 0;
-    uint64_t* lab_g = reinterpret_cast<uint64_t*>(scr + o);
+    X.lab_g = reinterpret_cast<uint64_t*>(scr + o);
     o = align(o + 8ull * n_g);
-    uint8_t* cst_g = scr + o;
+    X.cst_g = scr + o;
     o = align(o + n_g);
-    uint8_t* ops = scr + o;
+    X.ops = scr + o;
     o = align(o + max_ops);
-    uint64_t* pal_lab = reinterpret_cast<uint64_t*>(scr + o);
+    X.pal_lab = reinterpret_cast<uint64_t*>(scr + o);
     o = align(o + 8 * max_ops);
-    uint8_t* nib = scr + o;
+    X.nib = scr + o;
     o = align(o + 2 * max_ops + 2);
-    uint64_t* pal_out = reinterpret_cast<uint64_t*>(scr + o);
+    X.pal_out = reinterpret_cast<uint64_t*>(scr + o);
+    return X;
+}
+
+// The majority pyramid of one brick (Brick::build, brick.hpp:78-123): level L-2
+// straight from the voxels (x fastest for coalescing), then the coarser levels.
+__device__ void build_pyramid(const BrickCtx& B) {
+    const EncArgs& A = *B.A;
+    EncShared& S = *B.S;
+    const uint32_t tid = threadIdx.x, T = blockDim.x, L = A.L;
+    {
+        const uint32_t s = A.b >> 1, cnt = s * s * s;
+        const uint32_t lvl = L - 2;
+        for (uint32_t k = tid; k < cnt; k += T) {
+            uint32_t x = k % s, y = (k / s) % s, z = k / (s * s);
+            uint64_t v[8];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) v[c] = voxel(B, 2 * x + (c & 1), 2 * y + ((c >> 1) & 1), 2 * z + (c >> 2));
+            uint64_t maj = majority8(v);
+            bool same = true;
+#pragma unroll
+            for (int c = 0; c < 8; ++c) same &= (v[c] == maj);
+            uint32_t m = morton3(x, y, z);
+            if (lvl < kEncSmemLevels) {
+                S.lab[((1u << (3 * lvl)) - 1) / 7 + m] = maj;
+                S.cst[((1u << (3 * lvl)) - 1) / 7 + m] = same;
+            } else {
+                B.lab_g[m] = maj;
+                B.cst_g[m] = same;
+            }
+        }
+        __syncthreads();
+    }
+    for (int l = (int)L - 3; l >= 0; --l) {  // buildLevel (brick.hpp:92-123)
+        const uint32_t cnt = 1u << (3 * l);
+        for (uint32_t m = tid; m < cnt; m += T) {
+            uint64_t v[8];
+            bool cc = true;
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                v[c] = node_label(B, l + 1, 8 * m + c);
+                cc &= node_const(B, l + 1, 8 * m + c);
+            }
+            uint64_t maj = majority8(v);
+            bool same = cc;
+#pragma unroll
+            for (int c = 0; c < 8; ++c) same &= (v[c] == maj);
+            S.lab[((1u << (3 * l)) - 1) / 7 + m] = maj;
+            S.cst[((1u << (3 * l)) - 1) / 7 + m] = same;
+        }
+        __syncthreads();
+    }
+}
+
+// Reuse ops, level by level in stream order (encodeBrick, :372-433); returns the
+// op count and the first op of every level in ls.
+__device__ uint32_t gen_reuse_ops(const BrickCtx& B, uint32_t mode, bool root_const, uint8_t* ops, uint64_t* pal_lab,
+                                  uint32_t ls[8]) {
+    const uint32_t tid = threadIdx.x, T = blockDim.x, L = B.A->L;
+    uint32_t base = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) ls[k] = 0;
+    if (!root_const) {
+        for (uint32_t l = 0; l + 1 < L; ++l) {
+            const uint32_t np = 1u << (3 * l), per = (np + T - 1) / T;
+            const uint32_t p0 = min(np, tid * per), p1 = min(np, p0 + per);
+            uint32_t cnt = 0;
+            for (uint32_t p = p0; p < p1; ++p) cnt += node_const(B, l, p) ? 0u : 1u;
+            uint32_t A_l;
+            uint32_t r = block_exclusive<uint32_t>(cnt, B.S->sh32, &A_l);
+            ls[l] = base;
+            for (uint32_t p = p0; p < p1; ++p) {
+                if (node_const(B, l, p)) continue;
+                const uint64_t plab = node_label(B, l, p);
+#pragma unroll 1
+                for (uint32_t c = 0; c < 8; ++c) {
+                    const uint32_t n = 8 * p + c, j = base + 8 * r + c;
+                    const uint64_t Lc = node_label(B, l + 1, n);
+                    const uint32_t code = choose_reuse(B, l + 1, n, Lc, plab, mode);
+                    ops[j] = (uint8_t)(code | (node_const(B, l + 1, n) ? 8u : 0u));
+                    if (code == OP_PALNEED) pal_lab[j] = Lc;
+                }
+                ++r;
+            }
+            base += 8 * A_l;
+            __syncthreads();
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        if ((uint32_t)k >= L - 1) ls[k] = base;
+    return base;
+}
+
+// Palette ops: one warp walks the ops in stream order with a 17-entry window of
+// the most recent palette entries (reverse find only matters up to distance 16:
+// farther or absent means Pa).  Leaves the palette size in S.P.
+__device__ void palette_walk(const BrickCtx& B, uint64_t root, uint8_t* ops, const uint64_t* pal_lab, uint64_t* pal_out,
+                             uint32_t n_ops) {
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (warp == 0) {
+        uint64_t w = lane == 0 ? root : 0;
+        uint32_t P = 1;
+        if (lane == 0 && pal_out) pal_out[0] = root;
+        for (uint32_t j0 = 0; j0 < n_ops; j0 += 32) {
+            const uint32_t j = j0 + lane;
+            const uint32_t op = j < n_ops ? ops[j] : 0u;
+            const bool need = j < n_ops && (op & 7u) == OP_PALNEED;
+            uint32_t mask = __ballot_sync(0xffffffffu, need);
+            const uint64_t mine = need ? pal_lab[j] : 0ull;
+            while (mask) {
+                const int src = __ffs(mask) - 1;
+                mask &= mask - 1;
+                const uint64_t Lv = __shfl_sync(0xffffffffu, mine, src);
+                const uint32_t hit = __ballot_sync(0xffffffffu, lane < min(P, 17u) && w == Lv);
+                uint32_t code, delta = 0;
+                if (hit) {
+                    const int k = __ffs(hit) - 1;  // distance from the last entry
+                    code = k == 0 ? OP_P0 : OP_PD;
+                    delta = k == 0 ? 0u : (uint32_t)(k - 1);
+                } else {
+                    code = OP_PA;
+                    const uint64_t up = __shfl_up_sync(0xffffffffu, w, 1);
+                    w = lane == 0 ? Lv : up;
+                    if (lane == 0 && pal_out) pal_out[P] = Lv;
+                    ++P;
+                }
+                if (lane == src) ops[j] = (uint8_t)(code | (op & 8u) | (delta << 4));
+            }
+        }
+        if (lane == 0) B.S->P = P;
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kEncThreads) enc_bricks_kernel(EncArgs A) {
+    __shared__ EncShared S;
+    const uint32_t tid = threadIdx.x, T = blockDim.x;
+    const EncScratch X = enc_scratch(A);
+    uint8_t* ops = X.ops;
+    uint8_t* nib = X.nib;
+    uint64_t* pal_out = X.pal_out;
 
     for (;;) {
         if (tid == 0) S.work = atomicAdd(reinterpret_cast<unsigned int*>(A.misc + 18), 1u);
@@ -264,126 +434,14 @@ __global__ void __launch_bounds__(kEncThreads) enc_bricks_kernel(EncArgs A) {
         if (i >= A.nb) break;
         // split order: bx outer, bz inner (brick.hpp:152-154)
         const uint32_t bz = i % A.nbz, by = (i / A.nbz) % A.nby, bx = i / (A.nbz * A.nby);
-        BrickCtx B{&A, &S, (uint64_t)bx * A.b, (uint64_t)by * A.b, (uint64_t)bz * A.b, lab_g, cst_g};
-        const uint32_t L = A.L;
-
-        // ---- pyramid level L-2 straight from the voxels, x fastest for coalescing
-        {
-            const uint32_t s = A.b >> 1, cnt = s * s * s;
-            const uint32_t lvl = L - 2;
-            for (uint32_t k = tid; k < cnt; k += T) {
-                uint32_t x = k % s, y = (k / s) % s, z = k / (s * s);
-                uint64_t v[8];
-#pragma unroll
-                for (int c = 0; c < 8; ++c) v[c] = voxel(B, 2 * x + (c & 1), 2 * y + ((c >> 1) & 1), 2 * z + (c >> 2));
-                uint64_t maj = majority8(v);
-                bool same = true;
-#pragma unroll
-                for (int c = 0; c < 8; ++c) same &= (v[c] == maj);
-                uint32_t m = morton3(x, y, z);
-                if (lvl < kEncSmemLevels) {
-                    S.lab[((1u << (3 * lvl)) - 1) / 7 + m] = maj;
-                    S.cst[((1u << (3 * lvl)) - 1) / 7 + m] = same;
-                } else {
-                    lab_g[m] = maj;
-                    cst_g[m] = same;
-                }
-            }
-            __syncthreads();
-        }
-        // ---- coarser levels (buildLevel, brick.hpp:92-123)
-        for (int l = (int)L - 3; l >= 0; --l) {
-            const uint32_t cnt = 1u << (3 * l);
-            for (uint32_t m = tid; m < cnt; m += T) {
-                uint64_t v[8];
-                bool cc = true;
-#pragma unroll
-                for (int c = 0; c < 8; ++c) {
-                    v[c] = node_label(B, l + 1, 8 * m + c);
-                    cc &= node_const(B, l + 1, 8 * m + c);
-                }
-                uint64_t maj = majority8(v);
-                bool same = cc;
-#pragma unroll
-                for (int c = 0; c < 8; ++c) same &= (v[c] == maj);
-                S.lab[((1u << (3 * l)) - 1) / 7 + m] = maj;
-                S.cst[((1u << (3 * l)) - 1) / 7 + m] = same;
-            }
-            __syncthreads();
-        }
+        BrickCtx B{&A, &S, (uint64_t)bx * A.b, (uint64_t)by * A.b, (uint64_t)bz * A.b, X.lab_g, X.cst_g};
+        const uint32_t sel = A.sel ? A.sel[i] : 0u;
+        build_pyramid(B);
         const uint64_t root = node_label(B, 0, 0);
         const bool root_const = node_const(B, 0, 0);
-
-        // ---- reuse ops, level by level in stream order (encodeBrick, :372-433)
         uint32_t ls[8];
-        uint32_t base = 0;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) ls[k] = 0;
-        if (!root_const) {
-            for (uint32_t l = 0; l + 1 < L; ++l) {
-                const uint32_t np = 1u << (3 * l), per = (np + T - 1) / T;
-                const uint32_t p0 = min(np, tid * per), p1 = min(np, p0 + per);
-                uint32_t cnt = 0;
-                for (uint32_t p = p0; p < p1; ++p) cnt += node_const(B, l, p) ? 0u : 1u;
-                uint32_t A_l;
-                uint32_t r = block_exclusive<uint32_t>(cnt, S.sh32, &A_l);
-                ls[l] = base;
-                for (uint32_t p = p0; p < p1; ++p) {
-                    if (node_const(B, l, p)) continue;
-                    const uint64_t plab = node_label(B, l, p);
-#pragma unroll 1
-                    for (uint32_t c = 0; c < 8; ++c) {
-                        const uint32_t n = 8 * p + c, j = base + 8 * r + c;
-                        const uint64_t Lc = node_label(B, l + 1, n);
-                        const uint32_t code = choose_reuse(B, l + 1, n, Lc, plab);
-                        ops[j] = (uint8_t)(code | (node_const(B, l + 1, n) ? 8u : 0u));
-                        if (code == OP_PALNEED) pal_lab[j] = Lc;
-                    }
-                    ++r;
-                }
-                base += 8 * A_l;
-                __syncthreads();
-            }
-        }
-        const uint32_t n_ops = base;
-#pragma unroll
-        for (int k = 0; k < 8; ++k)
-            if ((uint32_t)k >= L - 1) ls[k] = n_ops;
-
-        // ---- palette ops: one warp in stream order with a 17-entry window
-        if (warp == 0) {
-            uint64_t w = lane == 0 ? root : 0;
-            uint32_t P = 1;
-            if (lane == 0) pal_out[0] = root;
-            for (uint32_t j0 = 0; j0 < n_ops; j0 += 32) {
-                const uint32_t j = j0 + lane;
-                const uint32_t op = j < n_ops ? ops[j] : 0u;
-                const bool need = j < n_ops && (op & 7u) == OP_PALNEED;
-                uint32_t mask = __ballot_sync(0xffffffffu, need);
-                const uint64_t mine = need ? pal_lab[j] : 0ull;
-                while (mask) {
-                    const int src = __ffs(mask) - 1;
-                    mask &= mask - 1;
-                    const uint64_t Lv = __shfl_sync(0xffffffffu, mine, src);
-                    const uint32_t hit = __ballot_sync(0xffffffffu, lane < min(P, 17u) && w == Lv);
-                    uint32_t code, delta = 0;
-                    if (hit) {
-                        const int k = __ffs(hit) - 1;  // distance from the last entry
-                        code = k == 0 ? OP_P0 : OP_PD;
-                        delta = k == 0 ? 0u : (uint32_t)(k - 1);
-                    } else {
-                        code = OP_PA;
-                        const uint64_t up = __shfl_up_sync(0xffffffffu, w, 1);
-                        w = lane == 0 ? Lv : up;
-                        if (lane == 0) pal_out[P] = Lv;
-                        ++P;
-                    }
-                    if (lane == src) ops[j] = (uint8_t)(code | (op & 8u) | (delta << 4));
-                }
-            }
-            if (lane == 0) S.P = P;
-        }
-        __syncthreads();
+        const uint32_t n_ops = gen_reuse_ops(B, sel & 15u, root_const, ops, X.pal_lab, ls);
+        palette_walk(B, root, ops, X.pal_lab, pal_out, n_ops);
         const uint32_t P = S.P;
 
         // ---- nibble layout (packOperationsToNibbles) and seek checkpoints
@@ -444,12 +502,56 @@ __global__ void __launch_bounds__(kEncThreads) enc_bricks_kernel(EncArgs A) {
                 m.flags = (root_const ? EF_UNIFORM : 0u) | (ok ? 0u : EF_OVERFLOW);
                 m.n_ck = (n_ops + A.S - 1) / A.S;
                 m.E = 0;
+                m.sel = sel;
+                m.pad = 0;
 #pragma unroll
                 for (int k = 0; k < 8; ++k) m.level_start[k] = ls[k];
                 A.meta[i] = m;
             }
         }
         __syncthreads();
+    }
+}
+
+// Exhaustive statistics for the mode / table choice: per brick and mode, the
+// histogram of the 16 nibble values the rANS coder would see (root nibble, op
+// nibbles, Pd offsets and the pad nibble of an odd count).
+__global__ void __launch_bounds__(kEncThreads) enc_stats_kernel(EncArgs A, uint32_t* __restrict__ hist_out) {
+    __shared__ EncShared S;
+    const uint32_t tid = threadIdx.x, T = blockDim.x;
+    const EncScratch X = enc_scratch(A);
+    for (;;) {
+        if (tid == 0) S.work = atomicAdd(reinterpret_cast<unsigned int*>(A.misc + 18), 1u);
+        __syncthreads();
+        const uint32_t i = S.work;
+        if (i >= A.nb) break;
+        const uint32_t bz = i % A.nbz, by = (i / A.nbz) % A.nby, bx = i / (A.nbz * A.nby);
+        BrickCtx B{&A, &S, (uint64_t)bx * A.b, (uint64_t)by * A.b, (uint64_t)bz * A.b, X.lab_g, X.cst_g};
+        build_pyramid(B);
+        const uint64_t root = node_label(B, 0, 0);
+        const bool root_const = node_const(B, 0, 0);
+        for (uint32_t mode = 0; mode < kModes; ++mode) {
+            if (tid < 16) S.hist[tid] = 0;
+            uint32_t ls[8];
+            const uint32_t n_ops = gen_reuse_ops(B, mode, root_const, X.ops, X.pal_lab, ls);
+            palette_walk(B, root, X.ops, X.pal_lab, nullptr, n_ops);
+            uint32_t nc = 0;
+            for (uint32_t j = tid; j < n_ops; j += T) {
+                const uint32_t op = X.ops[j], c = op & 7u;
+                atomicAdd(&S.hist[(c << 1) | ((op >> 3) & 1u)], 1u);
+                if (c == OP_PD) atomicAdd(&S.hist[op >> 4], 1u);
+                nc += c == OP_PD ? 2u : 1u;
+            }
+            uint32_t NC;
+            block_exclusive<uint32_t>(nc, S.sh32, &NC);
+            if (tid == 0) {
+                atomicAdd(&S.hist[(OP_PA << 1) | (root_const ? 1u : 0u)], 1u);  // root nibble
+                if (((1 + NC) & 1u) != 0) atomicAdd(&S.hist[0], 1u);             // pad nibble
+            }
+            __syncthreads();
+            if (tid < 16) hist_out[((size_t)i * kModes + mode) * 16 + tid] = S.hist[tid];
+            __syncthreads();
+        }
     }
 }
 
@@ -521,18 +623,21 @@ __global__ void __launch_bounds__(32) enc_rans_kernel(EncMeta* __restrict__ meta
                                                       const uint8_t* __restrict__ nib_pool,
                                                       const uint64_t* __restrict__ enc_off,
                                                       uint8_t* __restrict__ enc_pool, const uint32_t* __restrict__ model,
-                                                      Checkpoint* __restrict__ ck_all, uint32_t ck_cap) {
-    __shared__ uint64_t tab[16];
-    if (threadIdx.x < 16) {
-        const uint32_t s = threadIdx.x;
-        tab[s] = (uint64_t)model[s] | ((uint64_t)model[16 + s] << 13) | ((uint64_t)model[49 + s] << 25) |
-                 ((uint64_t)model[33 + s] << 32);
+                                                      uint32_t n_tables, Checkpoint* __restrict__ ck_all,
+                                                      uint32_t ck_cap) {
+    __shared__ uint64_t tabs[kMaxTables * 16];
+    for (uint32_t k = threadIdx.x; k < 16 * n_tables; k += blockDim.x) {
+        const uint32_t* md = model + (k >> 4) * kModelWords;
+        const uint32_t s = k & 15u;
+        tabs[k] = (uint64_t)md[s] | ((uint64_t)md[16 + s] << 13) | ((uint64_t)md[49 + s] << 25) |
+                  ((uint64_t)md[33 + s] << 32);
     }
     __syncthreads();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nb) return;
     const EncMeta m = meta[i];
     if (m.flags & EF_OVERFLOW) return;
+    const uint64_t* tab = tabs + 16 * min((m.sel >> 4) & 15u, n_tables - 1);
     // the packed nibbles of a brick start 16-byte aligned and are padded to 16
     const uint4* src4 = reinterpret_cast<const uint4*>(nib_pool + m.nib_off);
     uint8_t* out = enc_pool + enc_off[i];
@@ -577,24 +682,27 @@ __global__ void __launch_bounds__(32) enc_rans_kernel(EncMeta* __restrict__ meta
 
 // ------------------------------------------------------------ K4 serialize
 // One block per brick record: ID, P, palette, E, stream, nSymbols (fileIO.cpp:57-96).
+// Version 2 adds a u32 after the ID: the brick's table (bits 4..7) and mode (bits 0..3).
 __global__ void serialize_kernel(const EncMeta* __restrict__ meta, const uint64_t* __restrict__ rec_off,
                                  const uint64_t* __restrict__ pal_pool, const uint8_t* __restrict__ enc_pool,
-                                 const uint64_t* __restrict__ enc_off, uint8_t* __restrict__ image) {
+                                 const uint64_t* __restrict__ enc_off, uint8_t* __restrict__ image, uint32_t v2) {
     const uint32_t i = blockIdx.x;
     const EncMeta m = meta[i];
     uint8_t* dst = image + rec_off[i];
     const uint8_t* pal = reinterpret_cast<const uint8_t*>(pal_pool + m.pal_off);
     const uint8_t* enc = enc_pool + enc_off[i];
     const uint64_t pb = 8ull * m.P;
-    const uint64_t total = 16 + pb + m.E;
+    const uint64_t h = v2 ? 12 : 8;  // ID [, sel], P
+    const uint64_t total = h + 8 + pb + m.E;
     for (uint64_t k = threadIdx.x; k < total; k += blockDim.x) {
         uint8_t v;
         if (k < 4) v = (uint8_t)(m.id >> (8 * k));
-        else if (k < 8) v = (uint8_t)(m.P >> (8 * (k - 4)));
-        else if (k < 8 + pb) v = pal[k - 8];
-        else if (k < 12 + pb) v = (uint8_t)(m.E >> (8 * (k - 8 - pb)));
-        else if (k < 12 + pb + m.E) v = enc[k - 12 - pb];
-        else v = (uint8_t)(m.nsym >> (8 * (k - 12 - pb - m.E)));
+        else if (k < h - 4) v = (uint8_t)((m.sel & 0xFFu) >> (8 * (k - 4)));
+        else if (k < h) v = (uint8_t)(m.P >> (8 * (k - (h - 4))));
+        else if (k < h + pb) v = pal[k - h];
+        else if (k < h + 4 + pb) v = (uint8_t)(m.E >> (8 * (k - h - pb)));
+        else if (k < h + 4 + pb + m.E) v = enc[k - h - 4 - pb];
+        else v = (uint8_t)(m.nsym >> (8 * (k - h - 4 - pb - m.E)));
         dst[k] = v;
     }
 }
@@ -637,8 +745,88 @@ uint32_t enc_grid(int device) {
 }  // namespace
 
 // Runs K1..K4 on a device volume; leaves the image in s->d_image.
+// buildRansModel's per-symbol encoder constants for a given normalised table
+// (the host side of model_kernel).
+void table_model(const uint32_t* freq, uint32_t* model) {
+    uint32_t acc = 0;
+    for (int i = 0; i < 16; ++i) {
+        model[i] = freq[i];
+        model[16 + i] = acc;
+        acc += freq[i];
+        uint32_t s = 0;
+        while ((1u << s) < freq[i]) ++s;
+        const uint64_t M = ((1ull << (31 + s)) + freq[i] - 1) / freq[i];
+        model[33 + i] = (uint32_t)M;
+        model[49 + i] = 31 + s;
+    }
+    model[32] = acc;
+}
+
+int check_tables(const EncodeSelection* sel, std::string& err) {
+    if (!sel || sel->n_tables == 0) return CSV_OK;
+    if (sel->n_tables > kMaxTables) {
+        err = "at most 16 shared rANS tables";
+        return CSV_ERANGE;
+    }
+    for (uint32_t t = 0; t < sel->n_tables; ++t) {
+        uint32_t sum = 0;
+        for (int k = 0; k < 16; ++k) {
+            if (sel->freq[t][k] == 0) {
+                err = "a table frequency is 0";
+                return CSV_EINVAL;
+            }
+            sum += sel->freq[t][k];
+        }
+        if (sum != kTot) {
+            err = "a table's frequencies do not sum to 4096";
+            return CSV_EINVAL;
+        }
+    }
+    return CSV_OK;
+}
+
+// Per brick and mode, the 16-bin nibble histogram (the exhaustive search's statistics).
+int encode_stats(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W, uint64_t H, uint64_t D, uint32_t b,
+                 uint32_t* d_hist, cudaStream_t st, std::string& err) {
+    const uint64_t nbx = (W + b - 1) / b, nby = (H + b - 1) / b, nbz = (D + b - 1) / b;
+    if (nbx > 1024 || nby > 1024 || nbz > 1024) {
+        err = "volume needs more than 1024 bricks along an axis";
+        return CSV_ERANGE;
+    }
+    const uint32_t nb = (uint32_t)(nbx * nby * nbz);
+    cudaError_t e;
+    if (!s->d_misc && (e = cudaMalloc(&s->d_misc, 32 * sizeof(unsigned long long))) != cudaSuccess) {
+        err = cudaGetErrorString(e);
+        return CSV_ECUDA;
+    }
+    const uint32_t grid = std::min<uint32_t>(enc_grid(device), std::max<uint32_t>(nb, 1));
+    const size_t per_cta = enc_scratch_per_cta(b);
+    if ((e = grow(&s->d_scratch, &s->scratch_cap, per_cta * grid)) != cudaSuccess ||
+        (e = cudaMemsetAsync(s->d_misc, 0, 32 * sizeof(unsigned long long), st)) != cudaSuccess) {
+        err = cudaGetErrorString(e);
+        return CSV_ECUDA;
+    }
+    EncArgs A;
+    memset(&A, 0, sizeof A);
+    A.vol = d_vol;
+    A.W = W; A.H = H; A.D = D;
+    A.b = b; A.L = levels_of(b);
+    A.nbx = (uint32_t)nbx; A.nby = (uint32_t)nby; A.nbz = (uint32_t)nbz;
+    A.nb = nb;
+    A.S = s->S;
+    A.scratch = s->d_scratch;
+    A.scratch_per_cta = per_cta;
+    A.misc = s->d_misc;
+    if (nb) enc_stats_kernel<<<grid, kEncThreads, 0, st>>>(A, d_hist);
+    if ((e = cudaGetLastError()) != cudaSuccess) {
+        err = cudaGetErrorString(e);
+        return CSV_ECUDA;
+    }
+    return CSV_OK;
+}
+
 int encode_device(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W, uint64_t H, uint64_t D, uint32_t b,
-                  cudaStream_t st, std::string& err) {
+                  cudaStream_t st, std::string& err, const EncodeSelection* sel) {
     s->valid = false;
     s->device = device;
     s->b = b;
@@ -662,9 +850,15 @@ int encode_device(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W
             return CSV_ECUDA;                                              \
         }                                                                  \
     } while (0)
+    {
+        int rc = check_tables(sel, err);
+        if (rc) return rc;
+    }
+    const uint32_t n_tables = sel ? sel->n_tables : 0;
+    const bool v2 = n_tables > 0;
     CK(grow(&s->d_meta, &s->meta_cap, nb));
     CK(grow(&s->d_ck, &s->ck_cap_total, (size_t)nb * s->ck_cap));
-    if (!s->d_model) CK(cudaMalloc(&s->d_model, 128 * sizeof(uint32_t)));
+    if (!s->d_model) CK(cudaMalloc(&s->d_model, kMaxTables * kModelWords * sizeof(uint32_t)));
     {
         static_assert(sizeof(unsigned long long) == 8, "");
         if (!s->d_misc) CK(cudaMalloc(&s->d_misc, 32 * sizeof(unsigned long long)));
@@ -695,6 +889,7 @@ int encode_device(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W
         A.pal_cap = s->pal_cap;
         A.ck = s->d_ck;
         A.misc = s->d_misc;
+        A.sel = sel ? sel->d_sel : nullptr;
         if (nb > 0) {
             enc_bricks_kernel<<<grid, kEncThreads, 0, st>>>(A);
             CK(cudaGetLastError());
@@ -710,13 +905,28 @@ int encode_device(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W
         nib_need = heads[0];
         pal_need = heads[1];
     }
-    model_kernel<<<1, 1, 0, st>>>(s->d_misc + 2, s->d_model);
-    CK(cudaGetLastError());
+    std::vector<uint32_t> models(kMaxTables * kModelWords, 0);
+    if (v2) {  // the caller's shared tables
+        for (uint32_t t = 0; t < n_tables; ++t) table_model(sel->freq[t], &models[t * kModelWords]);
+        CK(cudaMemcpyAsync(s->d_model, models.data(), n_tables * kModelWords * sizeof(uint32_t),
+                           cudaMemcpyHostToDevice, st));
+    } else {  // one model from the sampled bricks' histogram (brickEncoding.hpp:481-482)
+        model_kernel<<<1, 1, 0, st>>>(s->d_misc + 2, s->d_model);
+        CK(cudaGetLastError());
+    }
     s->h_meta.resize(nb);
     if (nb) CK(cudaMemcpyAsync(s->h_meta.data(), s->d_meta, sizeof(EncMeta) * nb, cudaMemcpyDeviceToHost, st));
-    uint32_t model[128];
-    CK(cudaMemcpyAsync(model, s->d_model, sizeof model, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(models.data(), s->d_model, kModelWords * sizeof(uint32_t) * std::max<uint32_t>(1, n_tables),
+                       cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    const uint32_t* model = models.data();
+    s->n_tables = std::max<uint32_t>(1, n_tables);
+    for (uint32_t t = 0; t < s->n_tables; ++t)
+        for (int k = 0; k < 16; ++k) {
+            s->tab_freq[t][k] = models[t * kModelWords + k];
+            s->tab_cum[t][k] = models[t * kModelWords + 16 + k];
+        }
+    s->v2 = v2;
     std::vector<uint64_t> enc_off(std::max<uint32_t>(nb, 1)), rec_off(std::max<uint32_t>(nb, 1));
     uint64_t eo = 0;
     for (uint32_t i = 0; i < nb; ++i) {
@@ -729,36 +939,50 @@ int encode_device(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W
     CK(cudaMemcpyAsync(s->d_enc_off, enc_off.data(), 8ull * nb, cudaMemcpyHostToDevice, st));
     if (nb) {
         enc_rans_kernel<<<(nb + 31) / 32, 32, 0, st>>>(s->d_meta, nb, s->d_nib, s->d_enc_off, s->d_enc, s->d_model,
-                                                       s->d_ck, s->ck_cap);
+                                                       s->n_tables, s->d_ck, s->ck_cap);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(s->h_meta.data(), s->d_meta, sizeof(EncMeta) * nb, cudaMemcpyDeviceToHost, st));
     }
     CK(cudaStreamSynchronize(st));
-    uint64_t ro = kHeaderBytes;
+    // version 1: 152-byte header (fileIO.cpp:25-49); version 2: 28 bytes + 128 per table
+    const uint64_t hdr_bytes = v2 ? 28 + 128ull * n_tables : kHeaderBytes;
+    uint64_t ro = hdr_bytes;
     for (uint32_t i = 0; i < nb; ++i) {
         s->h_meta[i].enc_off = enc_off[i];
         rec_off[i] = ro;
-        ro += 16 + 8ull * s->h_meta[i].P + s->h_meta[i].E;
+        ro += (v2 ? 20 : 16) + 8ull * s->h_meta[i].P + s->h_meta[i].E;
     }
     CK(grow(&s->d_image, &s->image_cap, ro));
     CK(cudaMemcpyAsync(s->d_rec_off, rec_off.data(), 8ull * nb, cudaMemcpyHostToDevice, st));
-    uint32_t hdr[38];
+    std::vector<uint32_t> hdr(hdr_bytes / 4);
     hdr[0] = kMagic;
-    hdr[1] = 1;
+    hdr[1] = v2 ? 2 : 1;
     hdr[2] = nb;
     hdr[3] = b;  // the reference always writes BRICK_SIZE here (fileIO.cpp:28)
     hdr[4] = 16;
     hdr[5] = model[32];
+    if (!v2) {
+        for (int k = 0; k < 16; ++k) {
+            hdr[6 + k] = model[k];
+            hdr[22 + k] = model[16 + k];
+        }
+    } else {
+        hdr[6] = n_tables;
+        for (uint32_t t = 0; t < n_tables; ++t)
+            for (int k = 0; k < 16; ++k) {
+                hdr[7 + 32 * t + k] = models[t * kModelWords + k];
+                hdr[7 + 32 * t + 16 + k] = models[t * kModelWords + 16 + k];
+            }
+    }
     for (int k = 0; k < 16; ++k) {
-        hdr[6 + k] = model[k];
-        hdr[22 + k] = model[16 + k];
         s->freq[k] = model[k];
         s->cum[k] = model[16 + k];
     }
     s->cum[16] = model[32];
-    CK(cudaMemcpyAsync(s->d_image, hdr, kHeaderBytes, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(s->d_image, hdr.data(), hdr_bytes, cudaMemcpyHostToDevice, st));
     if (nb) {
-        serialize_kernel<<<nb, 256, 0, st>>>(s->d_meta, s->d_rec_off, s->d_pal, s->d_enc, s->d_enc_off, s->d_image);
+        serialize_kernel<<<nb, 256, 0, st>>>(s->d_meta, s->d_rec_off, s->d_pal, s->d_enc, s->d_enc_off, s->d_image,
+                                             v2 ? 1u : 0u);
         CK(cudaGetLastError());
     }
     CK(cudaStreamSynchronize(st));
@@ -800,7 +1024,8 @@ int encoder_to_dataset(EncoderState* s, DeviceDataset& d, std::string& err) {
         bd.ck_off = (uint32_t)((uint64_t)i * s->ck_cap);
         bd.ck_cap = s->ck_cap;
         bd.n_ops = m.n_ops;
-        bd.flags = ((m.flags & EF_UNIFORM) ? BF_UNIFORM : 0u) | (s->L << BF_LEVELS_SHIFT);
+        bd.flags = ((m.flags & EF_UNIFORM) ? BF_UNIFORM : 0u) | (s->L << BF_LEVELS_SHIFT) |
+                   ((s->v2 ? std::min((m.sel >> 4) & 15u, s->n_tables - 1) : 0u) << BF_MODEL_SHIFT);
         for (int k = 0; k < 8; ++k) bd.level_start[k] = m.level_start[k];
         d.h_ids[i] = m.id;
         d.h_cost[i] = m.nsym;
@@ -814,14 +1039,15 @@ int encoder_to_dataset(EncoderState* s, DeviceDataset& d, std::string& err) {
     d.ck_entries = (uint64_t)nb * s->ck_cap;
     d.enc_pool_bytes = std::max<uint64_t>(16, enc_n);
     d.pal_pool_entries = std::max<uint64_t>(1, pal_n);
-    uint32_t lut[kTot];
-    build_lut(s->freq, s->cum, lut);
+    d.n_models = s->n_tables;
+    std::vector<uint32_t> lut((size_t)kTot * s->n_tables);
+    for (uint32_t t = 0; t < s->n_tables; ++t) build_lut(s->tab_freq[t], s->tab_cum[t], &lut[(size_t)t * kTot]);
     cudaError_t e;
     if ((e = cudaMalloc(&d.d_bricks, sizeof(BrickDesc) * std::max<uint32_t>(1, nb))) != cudaSuccess ||
         (e = cudaMalloc(&d.d_pal, 8 * std::max<uint64_t>(1, pal_n))) != cudaSuccess ||
         (e = cudaMalloc(&d.d_enc, std::max<uint64_t>(16, enc_n))) != cudaSuccess ||
         (e = cudaMalloc(&d.d_ck, sizeof(Checkpoint) * std::max<uint64_t>(1, d.ck_entries))) != cudaSuccess ||
-        (e = cudaMalloc(&d.d_lut, sizeof lut)) != cudaSuccess) {
+        (e = cudaMalloc(&d.d_lut, sizeof(uint32_t) * lut.size())) != cudaSuccess) {
         err = std::string("device allocation: ") + cudaGetErrorString(e);
         return CSV_ENOMEM;
     }
@@ -830,7 +1056,8 @@ int encoder_to_dataset(EncoderState* s, DeviceDataset& d, std::string& err) {
         (e = cudaMemcpy(d.d_enc, s->d_enc, enc_n, cudaMemcpyDeviceToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(d.d_ck, s->d_ck, sizeof(Checkpoint) * d.ck_entries, cudaMemcpyDeviceToDevice)) !=
             cudaSuccess ||
-        (e = cudaMemcpy(d.d_lut, lut, sizeof lut, cudaMemcpyHostToDevice)) != cudaSuccess) {
+        (e = cudaMemcpy(d.d_lut, lut.data(), sizeof(uint32_t) * lut.size(), cudaMemcpyHostToDevice)) !=
+            cudaSuccess) {
         err = std::string("dataset copy: ") + cudaGetErrorString(e);
         return CSV_ECUDA;
     }

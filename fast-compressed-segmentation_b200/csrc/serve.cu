@@ -642,7 +642,7 @@ int csv_serve_create(csv_ctx* ctx, const csv_dataset* ds, const csv_serve_config
         return fail(ctx, CSV_EINVAL, "serve: viewport and field of view must be positive");
     const uint32_t ms = cfg->max_sessions ? cfg->max_sessions : 1u;
     if (ms > kMaxViews) return fail(ctx, CSV_ERANGE, "serve: at most 8 sessions per server");
-    if (ds->d.n_models > 1) return fail(ctx, CSV_EINVAL, "serve: one brick size per server (not a concatenation)");
+    if (ds->d.mixed_b) return fail(ctx, CSV_EINVAL, "serve: one brick size per server");
     if (n_hidden && !hidden) return fail(ctx, CSV_EINVAL, "serve: hidden labels pointer is null");
     DeviceGuard g(ctx->device);
     const DeviceDataset& d = ds->d;
