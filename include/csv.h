@@ -330,6 +330,71 @@ int csv_gemm_bf16(csv_ctx* ctx, const void* d_A, const void* d_B, uint32_t M, ui
                   const float* d_bias, const void* d_mask, uint32_t relu, float* d_C, void* d_Cb, void* d_CbT,
                   float* d_CT, uint32_t* d_err, void* stream);
 
+/* Encoding modes: where several ops reproduce a child's label, the reference
+ * takes Rp, then Rx, Ry, Rz, then a palette op (brickEncoding.hpp:198-282).
+ * Mode m keeps that grammar and changes the preference: m % 6 picks the order
+ * of the neighbour axes (xyz, xzy, yxz, yzx, zxy, zyx), m >= 6 tries the
+ * neighbours before the parent.  Mode 0 is the reference's order.  Decoding
+ * does not depend on the mode.
+ *
+ * Version-2 images (`.csbd` version 2): a 28-byte header (magic, version 2,
+ * numBricks, brickSize, 16, 4096, n_tables), n_tables x (freq[16], cum[16])
+ * shared rANS tables, and brick records with a u32 after the ID naming the
+ * brick's table (bits 4..7) and mode (bits 0..3).  csv_open reads both
+ * versions. */
+#define CSV_MODES 12
+#define CSV_MAX_TABLES 16
+#define CSV_FEATURES 32
+/* Per brick (split order) and mode: the 16-bin histogram of the nibbles the
+ * rANS coder would code (d_hist: numBricks x 12 x 16 u32). */
+int csv_encode_stats(csv_ctx* ctx, const uint64_t* d_volume, uint32_t W, uint32_t H, uint32_t D, uint32_t brick_size,
+                     uint32_t* d_hist, void* stream);
+/* Exhaustive choice: per brick the (mode, table) with the fewest estimated
+ * bits, sum_s hist[mode][s] * -log2(freq[table][s] / 4096), ties to the lower
+ * mode then table.  tables: host, n_tables x 16 frequencies.  d_sel: per brick
+ * mode | table << 4.  d_cost (optional): numBricks x 12 x n_tables estimated
+ * bits in 16.16 fixed point. */
+int csv_select_exhaustive(csv_ctx* ctx, const uint32_t* d_hist, uint32_t n_bricks, const uint32_t* tables,
+                          uint32_t n_tables, uint8_t* d_sel, uint64_t* d_cost, void* stream);
+/* csv_encode_device with a per-brick mode and shared table (d_sel, device, one
+ * byte per brick: mode | table << 4; NULL = mode 0, table 0).  n_tables > 0
+ * writes a version-2 image with these tables (host, n_tables x 16
+ * frequencies, each >= 1, summing to 4096); n_tables == 0 writes version 1. */
+int csv_encode_device_sel(csv_ctx* ctx, const uint64_t* d_volume, uint32_t W, uint32_t H, uint32_t D,
+                          uint32_t brick_size, const uint32_t* tables, uint32_t n_tables, const uint8_t* d_sel,
+                          void* stream, size_t* image_len);
+/* 32 cheap statistics per brick (d_features: numBricks x 32 fp32): distinct
+ * labels of an 8^3 sample, label equality of neighbours at distance 1 and 4
+ * per axis, the fraction of label 0, the histogram of run lengths along x, the
+ * run count, and the op-nibble histogram of the 8^3 sample encoded as a brick. */
+int csv_brick_features(csv_ctx* ctx, const uint64_t* d_volume, uint32_t W, uint32_t H, uint32_t D,
+                       uint32_t brick_size, float* d_features, void* stream);
+
+/* The selector network: 32 features -> 256 -> 256 (ReLU) -> 12 mode logits
+ * and 16 table logits, bf16 weights with fp32 masters, fp32 accumulation on
+ * the tensor cores (csv_gemm_bf16).  params (host, CSV_MLP_PARAMS floats):
+ * W1 [256][64] (columns 32..63 unused), b1 [256], W2 [256][256], b2 [256],
+ * W3 [32][256] (rows 28..31 unused), b3 [32]. */
+#define CSV_MLP_PARAMS (256 * 64 + 256 + 256 * 256 + 256 + 32 * 256 + 32)
+typedef struct csv_mlp csv_mlp;
+int csv_mlp_create(csv_ctx* ctx, const float* params, csv_mlp** out);
+void csv_mlp_destroy(csv_mlp* net);
+/* Host copies of the parameters and of the last gradients (either may be NULL). */
+int csv_mlp_params(const csv_mlp* net, float* params, float* grads);
+/* Logits (d_logits: count x 32 fp32, optional) and the argmax choice per brick
+ * (d_sel: mode | table << 4, optional) for count feature rows. */
+int csv_mlp_forward(csv_mlp* net, const float* d_features, uint32_t count, float* d_logits, uint8_t* d_sel,
+                    void* stream);
+/* Forward and backward of the mean cross-entropy of both heads against
+ * d_label (mode | table << 4 per row); gradients stay in the network; *loss
+ * (host, optional) receives the loss. */
+int csv_mlp_grad(csv_mlp* net, const float* d_features, const uint8_t* d_label, uint32_t count, float* loss,
+                 void* stream);
+/* One Adam step (Kingma & Ba) with the last gradients. */
+int csv_mlp_adam(csv_mlp* net, float lr, float beta1, float beta2, float eps, void* stream);
+/* CSV_OK, or CSV_ECUDA when a tensor-core wait gave up since creation. */
+int csv_mlp_status(const csv_mlp* net);
+
 /* ---- workload generator (no reference counterpart) --------------------
  * Seeded synthetic label volume on the device, x fastest: kind 0 = Voronoi
  * (n_cells cells, then a random half-space slab of label 0 covering about
