@@ -151,6 +151,19 @@ def load_library() -> C.CDLL:
     L.csv_serve_destroy.argtypes = [vp]
     L.csv_gemm_bf16.argtypes = [vp, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, C.c_uint32, vp, vp, vp, vp,
                                 vp, vp]
+    L.csv_encode_stats.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp]
+    L.csv_select_exhaustive.argtypes = [vp, vp, C.c_uint32, u32p, C.c_uint32, vp, vp, vp]
+    L.csv_encode_device_sel.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, u32p, C.c_uint32,
+                                        vp, vp, C.POINTER(C.c_size_t)]
+    L.csv_brick_features.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp]
+    L.csv_mlp_create.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(vp)]
+    L.csv_mlp_destroy.argtypes = [vp]
+    L.csv_mlp_destroy.restype = None
+    L.csv_mlp_params.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    L.csv_mlp_forward.argtypes = [vp, vp, C.c_uint32, vp, vp, vp]
+    L.csv_mlp_grad.argtypes = [vp, vp, vp, C.c_uint32, C.POINTER(C.c_float), vp]
+    L.csv_mlp_adam.argtypes = [vp, C.c_float, C.c_float, C.c_float, C.c_float, vp]
+    L.csv_mlp_status.argtypes = [vp]
     _lib = L
     return L
 
@@ -404,6 +417,37 @@ class Codec:
                                            1 if relu else 0, _vp(C), _vp(Cb), _vp(CbT), _vp(CT), _vp(err),
                                            C_MOD.c_void_p(_stream_handle(stream))))
 
+    # ---- mode / table selector -----------------------------------------------
+    def encode_stats(self, d_volume, brick_size: int, d_hist, stream=None):
+        """Per brick and encoding mode, the 16-bin nibble histogram (d_hist: int32 tensor nb x 12 x 16)."""
+        D, H, W = d_volume.shape
+        self._check(self.lib.csv_encode_stats(self.handle, _vp(d_volume), W, H, D, brick_size, _vp(d_hist),
+                                              C.c_void_p(_stream_handle(stream))))
+
+    def select_exhaustive(self, d_hist, tables, d_sel, d_cost=None, stream=None):
+        """Per brick the (mode, table) with the fewest estimated bits -> d_sel (uint8: mode | table << 4)."""
+        t = np.ascontiguousarray(tables, np.uint32).reshape(-1, 16)
+        self._check(self.lib.csv_select_exhaustive(self.handle, _vp(d_hist), d_hist.shape[0],
+                                                   t.ctypes.data_as(C.POINTER(C.c_uint32)), len(t), _vp(d_sel),
+                                                   _vp(d_cost), C.c_void_p(_stream_handle(stream))))
+
+    def encode_device_sel(self, d_volume, brick_size: int, tables=None, d_sel=None, stream=None) -> int:
+        """Encode with per-brick modes and shared tables (version 2 when tables are given); returns the length."""
+        D, H, W = d_volume.shape
+        t = None if tables is None else np.ascontiguousarray(tables, np.uint32).reshape(-1, 16)
+        n = C.c_size_t()
+        self._check(self.lib.csv_encode_device_sel(
+            self.handle, _vp(d_volume), W, H, D, brick_size,
+            None if t is None else t.ctypes.data_as(C.POINTER(C.c_uint32)), 0 if t is None else len(t),
+            _vp(d_sel), C.c_void_p(_stream_handle(stream)), C.byref(n)))
+        return n.value
+
+    def brick_features(self, d_volume, brick_size: int, d_features, stream=None):
+        """32 statistics per brick (d_features: float32 tensor nb x 32)."""
+        D, H, W = d_volume.shape
+        self._check(self.lib.csv_brick_features(self.handle, _vp(d_volume), W, H, D, brick_size, _vp(d_features),
+                                                C.c_void_p(_stream_handle(stream))))
+
     # ---- workload generator ---------------------------------------------
     def synth_volume(self, d_volume, kind: int, n_cells: int, n_tubes: int = 0, r_min: float = 0.0,
                      r_max: float = 0.0, zero_frac: float = 0.0, seed: int = 0, stream=None):
@@ -500,6 +544,73 @@ def _device_view(ptr: int, n: int, typestr: str, device: int):
         __cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False), "version": 2}
 
     return torch.as_tensor(_View(), device=f"cuda:{device}")
+
+
+MLP_PARAMS = 256 * 64 + 256 + 256 * 256 + 256 + 32 * 256 + 32
+
+
+class SelectorNet:
+    """The mode / table selector network on the device (csv_mlp_*)."""
+
+    def __init__(self, codec: Codec, params: np.ndarray):
+        self.codec, self.lib = codec, codec.lib
+        p = np.ascontiguousarray(params, np.float32)
+        assert p.size == MLP_PARAMS
+        h = C.c_void_p()
+        codec._check(self.lib.csv_mlp_create(codec.handle, p.ctypes.data_as(C.POINTER(C.c_float)), C.byref(h)))
+        self.handle = h
+
+    @staticmethod
+    def init_params(seed: int = 0) -> np.ndarray:
+        """He-uniform weights (unused input columns and output rows zero), zero biases."""
+        rng = np.random.default_rng(seed)
+        p = np.zeros(MLP_PARAMS, np.float32)
+        o = 0
+        for rows, cols, fan in [(256, 64, 32), (256, 256, 256), (32, 256, 256)]:
+            w = rng.uniform(-1, 1, (rows, cols)) * np.sqrt(6.0 / fan)
+            if cols == 64:
+                w[:, 32:] = 0
+            if rows == 32:
+                w[28:, :] = 0
+            p[o:o + rows * cols] = w.ravel()
+            o += rows * cols + rows
+        return p
+
+    def params(self, grads: bool = False):
+        p = np.zeros(MLP_PARAMS, np.float32)
+        g = np.zeros(MLP_PARAMS, np.float32) if grads else None
+        fp = C.POINTER(C.c_float)
+        self.codec._check(self.lib.csv_mlp_params(self.handle, p.ctypes.data_as(fp),
+                                                  g.ctypes.data_as(fp) if grads else None))
+        return (p, g) if grads else p
+
+    def forward(self, d_features, d_logits=None, d_sel=None, stream=None):
+        self.codec._check(self.lib.csv_mlp_forward(self.handle, _vp(d_features), d_features.shape[0], _vp(d_logits),
+                                                   _vp(d_sel), C.c_void_p(_stream_handle(stream))))
+
+    def grad(self, d_features, d_label, stream=None) -> float:
+        loss = C.c_float()
+        self.codec._check(self.lib.csv_mlp_grad(self.handle, _vp(d_features), _vp(d_label), d_features.shape[0],
+                                                C.byref(loss), C.c_void_p(_stream_handle(stream))))
+        return float(loss.value)
+
+    def adam(self, lr: float, beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-8, stream=None):
+        self.codec._check(self.lib.csv_mlp_adam(self.handle, lr, beta1, beta2, eps,
+                                                C.c_void_p(_stream_handle(stream))))
+
+    def status(self) -> int:
+        return self.lib.csv_mlp_status(self.handle)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.csv_mlp_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def requests(bricks, lods, dsts) -> np.ndarray:

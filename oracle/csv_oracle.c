@@ -167,17 +167,25 @@ static void push_pal(enc_t* e, uint64_t v) {
     e->pal[e->np++] = v;
 }
 
+/* Encoding modes (no reference counterpart): mode % 6 orders the neighbour
+ * axes, modes >= 6 try the neighbours before the parent; mode 0 is the
+ * reference's order (Rp, Rx, Ry, Rz: brickEncoding.hpp:202-203, 277-282). */
+static const int AXIS_ORDER[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+
 /* bestOperation (brickEncoding.hpp:188-318) for child `n` (Morton) at coarse
- * level lc = l+1 with parent level l. */
-static int best_op(const uint64_t* lab, uint32_t lc, uint32_t n, uint64_t parent_label, enc_t* e, uint8_t* delta) {
+ * level lc = l+1 with parent level l, under encoding mode `mode`. */
+static int best_op(const uint64_t* lab, uint32_t lc, uint32_t n, uint64_t parent_label, enc_t* e, uint8_t* delta,
+                   uint32_t mode) {
     const uint64_t* C = lab + level_off(lc);
     const uint64_t* P = lab + level_off(lc - 1);
     uint64_t L = C[n];
-    if (parent_label == L) return OP_RP; /* :202-203 */
+    const int nfirst = mode >= 6;
+    if (!nfirst && parent_label == L) return OP_RP; /* :202-203 */
     uint32_t x, y, z;
     or_demorton3(n, &x, &y, &z);
     int size = 1 << lc;
-    for (int axis = 0; axis < 3; ++axis) { /* X, Y, Z order: :277-282 */
+    for (int k = 0; k < 3; ++k) { /* X, Y, Z order in mode 0: :277-282 */
+        const int axis = AXIS_ORDER[nfirst ? mode - 6 : mode][k];
         int c[3] = {(int)x, (int)y, (int)z};
         c[axis] += (c[axis] & 1) ? 1 : -1; /* outside the sibling block: :224-240 */
         if (c[axis] < 0 || c[axis] >= size) continue; /* :244-246 */
@@ -190,6 +198,7 @@ static int best_op(const uint64_t* lab, uint32_t lc, uint32_t n, uint64_t parent
                 return OP_RX + axis;
         }
     }
+    if (nfirst && parent_label == L) return OP_RP;
     /* palette reverse find (:288-317) */
     for (int64_t i = (int64_t)e->np - 1; i >= 0; --i) {
         if (e->pal[i] == L) {
@@ -205,7 +214,7 @@ static int best_op(const uint64_t* lab, uint32_t lc, uint32_t n, uint64_t parent
 
 /* encodeBrick (brickEncoding.hpp:348-447) + packOperationsToNibbles
  * (brickEncoding.cpp:11-91): nibbles in emission order. */
-static void encode_brick(uint32_t b, const uint64_t* lab, const uint8_t* cst, enc_t* e) {
+static void encode_brick(uint32_t b, const uint64_t* lab, const uint8_t* cst, enc_t* e, uint32_t mode) {
     uint32_t L = levels_of(b);
     e->np = 0; e->nn = 0;
     push_pal(e, lab[0]);
@@ -221,7 +230,7 @@ static void encode_brick(uint32_t b, const uint64_t* lab, const uint8_t* cst, en
             for (uint32_t c = 0; c < 8; ++c) {
                 uint32_t n = (uint32_t)(8 * m + c); /* child Morton = 8m + c (utils.cpp:45-68) */
                 uint8_t delta = 0;
-                int op = best_op(lab, l + 1, n, P[m], e, &delta);
+                int op = best_op(lab, l + 1, n, P[m], e, &delta, mode);
                 if (op == OP_PA) push_pal(e, C[n]); /* :423 */
                 push_nib(e, (uint8_t)((op << 1) | (CC[n] ? 1 : 0)));
                 if (op == OP_PD) push_nib(e, delta);
@@ -283,6 +292,13 @@ static void rans_encode(const uint8_t* nib, uint32_t nn, const uint32_t* freq, c
 /* compressDataset (brickEncoding.hpp:466-531) + saveDatasetToFile
  * (fileIO.cpp:15-99). */
 int or_encode(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b, uint8_t** out, size_t* out_len) {
+    return or_encode_sel(vol, W, H, D, b, NULL, NULL, 0, out, out_len);
+}
+
+/* The same with a per-brick mode and table (sel: mode | table << 4, or NULL);
+ * n_tables > 0 writes version 2 with those tables (freq, n_tables x 16). */
+int or_encode_sel(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b, const uint8_t* sel,
+                  const uint32_t* tables, uint32_t n_tables, uint8_t** out, size_t* out_len) {
     if (b < 2 || (b & (b - 1)) || b > 1024) return -1;
     size_t nbx = (W + b - 1) / b, nby = (H + b - 1) / b, nbz = (D + b - 1) / b;
     size_t nb = nbx * nby * nbz;
@@ -304,7 +320,7 @@ int or_encode(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b, uin
             for (size_t bz = 0; bz < nbz; ++bz, ++i) {
                 cut_brick(vol, W, H, D, b, bx, by, bz, lab + level_off(L - 1));
                 build_pyramid(b, lab, cst);
-                encode_brick(b, lab, cst, &e);
+                encode_brick(b, lab, cst, &e, sel ? (sel[i] & 15u) : 0u);
                 ids[i] = or_morton3((uint32_t)bx, (uint32_t)by, (uint32_t)bz);
                 pals[i] = (uint64_t*)malloc(8 * (size_t)e.np);
                 memcpy(pals[i], e.pal, 8 * (size_t)e.np);
@@ -317,22 +333,41 @@ int or_encode(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b, uin
                     if (e.nn & 1) hist[0]++; /* the pad nibble of the last byte */
                 }
             }
-    uint32_t freq[16], cum[17];
-    or_build_model(hist, freq, cum);
+    uint32_t tf[16][16], tc[16][17];
+    const uint32_t nt = n_tables ? n_tables : 1;
+    if (n_tables == 0) {
+        or_build_model(hist, tf[0], tc[0]);
+    } else {
+        for (uint32_t t = 0; t < n_tables; ++t) {
+            uint32_t acc = 0;
+            for (int k = 0; k < 16; ++k) {
+                tf[t][k] = tables[16 * t + k];
+                tc[t][k] = acc;
+                acc += tf[t][k];
+            }
+            tc[t][16] = acc;
+        }
+    }
     buf_t o = {0};
     bput32(&o, 0x43534244u);
-    bput32(&o, 1);
+    bput32(&o, n_tables ? 2 : 1);
     bput32(&o, (uint32_t)nb);
     bput32(&o, b); /* the reference stores BRICK_SIZE (fileIO.cpp:28); see DESIGN */
     bput32(&o, 16);
     bput32(&o, TOT);
-    bput(&o, freq, 64);
-    bput(&o, cum, 64);
+    if (n_tables) bput32(&o, n_tables);
+    for (uint32_t t = 0; t < nt; ++t) {
+        bput(&o, tf[t], 64);
+        bput(&o, tc[t], 64);
+    }
     buf_t r = {0};
     for (i = 0; i < nb; ++i) {
+        const uint32_t s = sel ? sel[i] : 0u;
+        const uint32_t t = n_tables ? ((s >> 4) & 15u) : 0u;
         r.n = 0;
-        rans_encode(nibs[i], nnib[i], freq, cum, &r);
+        rans_encode(nibs[i], nnib[i], tf[t < nt ? t : 0], tc[t < nt ? t : 0], &r);
         bput32(&o, ids[i]);
+        if (n_tables) bput32(&o, s & 0xFFu);
         bput32(&o, npal[i]);
         bput(&o, pals[i], 8 * (size_t)npal[i]);
         bput32(&o, (uint32_t)r.n);
@@ -473,32 +508,61 @@ int or_decode_brick(const uint64_t* palette, uint32_t P, const uint8_t* nib, uin
 
 /* ----------------------------------------------------------- .csbd read */
 typedef struct {
-    uint32_t nb, b, total;
-    uint32_t freq[16], cum[16];
-    size_t* off; /* byte offset of each brick record */
+    uint32_t nb, b, total, version, n_tables;
+    uint32_t freq[16][16], cum[16][16];
+    size_t* off;  /* per brick: offset such that P is at off + 4 (after the ID, and the table word of v2) */
+    uint8_t* tab; /* each brick's table */
 } img_t;
 
+static int parse_fail(img_t* I) {
+    free(I->off);
+    free(I->tab);
+    return -1;
+}
+
 static int parse_image(const uint8_t* img, size_t len, img_t* I) {
-    /* layout: fileIO.cpp:25-96 */
-    if (len < 152) return -1;
-    uint32_t h[6];
-    memcpy(h, img, 24);
-    if (h[0] != 0x43534244u || h[4] != 16) return -1;
-    I->nb = h[2]; I->b = h[3]; I->total = h[5];
-    memcpy(I->freq, img + 24, 64);
-    memcpy(I->cum, img + 88, 64);
+    /* layout: fileIO.cpp:25-96 (version 1); version 2 adds the table header and a word per brick */
+    if (len < 28) return -1;
+    uint32_t h[7];
+    memcpy(h, img, 28);
+    if (h[0] != 0x43534244u || h[4] != 16 || (h[1] != 1 && h[1] != 2)) return -1;
+    I->version = h[1]; I->nb = h[2]; I->b = h[3]; I->total = h[5];
+    size_t o;
+    if (I->version == 1) {
+        if (len < 152) return -1;
+        I->n_tables = 1;
+        memcpy(I->freq[0], img + 24, 64);
+        memcpy(I->cum[0], img + 88, 64);
+        o = 152;
+    } else {
+        I->n_tables = h[6];
+        if (I->n_tables == 0 || I->n_tables > 16 || len < 28 + 128 * (size_t)I->n_tables) return -1;
+        for (uint32_t t = 0; t < I->n_tables; ++t) {
+            memcpy(I->freq[t], img + 28 + 128 * t, 64);
+            memcpy(I->cum[t], img + 28 + 128 * t + 64, 64);
+        }
+        o = 28 + 128 * (size_t)I->n_tables;
+    }
     I->off = (size_t*)malloc(sizeof(size_t) * (I->nb + 1));
-    size_t o = 152;
+    I->tab = (uint8_t*)calloc(I->nb + 1, 1);
     for (uint32_t i = 0; i < I->nb; ++i) {
-        I->off[i] = o;
         uint32_t P, E;
-        if (o + 8 > len) { free(I->off); return -1; }
+        if (I->version == 2) {
+            uint32_t s;
+            if (o + 8 > len) return parse_fail(I);
+            memcpy(&s, img + o + 4, 4);
+            I->tab[i] = (uint8_t)((s >> 4) & 15u);
+            if (I->tab[i] >= I->n_tables) return parse_fail(I);
+            o += 4;
+        }
+        I->off[i] = o;
+        if (o + 8 > len) return parse_fail(I);
         memcpy(&P, img + o + 4, 4);
         o += 8 + 8 * (size_t)P;
-        if (o + 4 > len) { free(I->off); return -1; }
+        if (o + 4 > len) return parse_fail(I);
         memcpy(&E, img + o, 4);
         o += 4 + E + 4;
-        if (o > len) { free(I->off); return -1; }
+        if (o > len) return parse_fail(I);
     }
     I->off[I->nb] = o;
     return 0;
@@ -522,13 +586,14 @@ int or_decode_image(const uint8_t* img, size_t len, uint32_t t, uint64_t* out, u
         uint32_t nbytes = (ns + 1) / 2;
         uint8_t* nib = (uint8_t*)calloc(nbytes + 1, 1);
         int st = 0;
-        if (or_rans_decode(I.freq, I.cum, I.total, enc, E, ns, nib)) st = 16;
+        if (or_rans_decode(I.freq[I.tab[i]], I.cum[I.tab[i]], I.total, enc, E, ns, nib)) st = 16;
         else st = or_decode_brick(palc, P, nib, nbytes, I.b, t, out + per * i);
         if (status) status[i] = (uint32_t)st;
         free(nib);
         free(palc);
     }
     free(I.off);
+    free(I.tab);
     return (int)I.nb;
 }
 

@@ -115,6 +115,21 @@ const or_slot* or_serve_slots(const or_server* s, uint32_t session);
 const uint64_t* or_serve_cache(const or_server* s);
 void or_serve_free(or_server* s);
 
+/* Encode with a per-brick mode and table (sel: mode | table << 4, or NULL);
+ * n_tables > 0 writes a version-2 image with those tables (n_tables x 16
+ * frequencies); n_tables == 0 writes version 1 with the dataset's model. */
+int or_encode_sel(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b, const uint8_t* sel,
+                  const uint32_t* tables, uint32_t n_tables, uint8_t** out, size_t* out_len);
+
+/* The mode / table selector (csv_oracle_select.c). */
+int or_encode_stats(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b, uint32_t* hist);
+void or_table_lengths(const uint32_t* tables, uint32_t n_tables, uint32_t* len);
+void or_select_exhaustive(const uint32_t* hist, uint32_t nb, const uint32_t* tables, uint32_t n_tables, uint8_t* sel,
+                          uint64_t* cost);
+int or_brick_features(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b, float* feat);
+void or_mlp_forward(const float* params, const float* feat, uint32_t n, float* logits);
+float or_mlp_grad(const float* params, const float* feat, const uint8_t* label, uint32_t n, float* grads);
+
 void or_free(void* p);
 
 #ifdef __cplusplus

@@ -63,6 +63,15 @@ class Oracle:
         L.or_brick_lod.argtypes = [C.POINTER(C.c_double), C.c_double, C.POINTER(C.c_double), C.c_double, C.c_uint32]
         L.or_render.argtypes = [C.POINTER(C.c_float), C.c_uint32, C.c_uint32, C.c_float, C.c_uint32, C.c_uint32,
                                 C.c_void_p, C.c_uint64, _u64p, _u64p, C.c_uint32, _u64p, C.POINTER(C.c_float), _u32p]
+        fp = C.POINTER(C.c_float)
+        L.or_encode_sel.argtypes = [_u64p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_uint32, _u8p, _u32p, C.c_uint32,
+                                    C.POINTER(_u8p), C.POINTER(C.c_size_t)]
+        L.or_encode_stats.argtypes = [_u64p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_uint32, _u32p]
+        L.or_select_exhaustive.argtypes = [_u32p, C.c_uint32, _u32p, C.c_uint32, _u8p, _u64p]
+        L.or_brick_features.argtypes = [_u64p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_uint32, fp]
+        L.or_mlp_forward.argtypes = [fp, fp, C.c_uint32, fp]
+        L.or_mlp_grad.restype = C.c_float
+        L.or_mlp_grad.argtypes = [fp, fp, _u8p, C.c_uint32, fp]
         L.or_camera_uniform.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double,
                                         C.POINTER(C.c_float)]
         L.or_serve_constants.argtypes = [C.c_uint32, C.c_uint32, C.c_double, C.c_uint32, C.c_uint32,
@@ -115,6 +124,70 @@ class Oracle:
 
     def morton3(self, x, y, z) -> int:
         return self.lib.or_morton3(x, y, z)
+
+    # ---- mode / table selector
+    def encode_sel(self, vol: np.ndarray, brick: int, sel=None, tables=None) -> bytes:
+        """Per-brick mode | table << 4 (sel) and shared tables (n x 16 frequencies) -> version-2 image
+        (version 1 when tables is None)."""
+        v = np.ascontiguousarray(vol, dtype=np.uint64)
+        D, H, W = v.shape
+        s = None if sel is None else np.ascontiguousarray(sel, np.uint8)
+        t = None if tables is None else np.ascontiguousarray(tables, np.uint32).reshape(-1, 16)
+        out = _u8p()
+        n = C.c_size_t()
+        rc = self.lib.or_encode_sel(_ptr(v, _u64p), W, H, D, brick, None if s is None else _ptr(s, _u8p),
+                                    None if t is None else _ptr(t, _u32p), 0 if t is None else len(t),
+                                    C.byref(out), C.byref(n))
+        if rc:
+            raise RuntimeError("oracle encode_sel failed")
+        data = C.string_at(out, n.value)
+        self.lib.or_free(out)
+        return data
+
+    def encode_stats(self, vol: np.ndarray, brick: int) -> np.ndarray:
+        v = np.ascontiguousarray(vol, dtype=np.uint64)
+        D, H, W = v.shape
+        nb = -(-W // brick) * -(-H // brick) * -(-D // brick)
+        h = np.zeros((nb, 12, 16), np.uint32)
+        if self.lib.or_encode_stats(_ptr(v, _u64p), W, H, D, brick, _ptr(h, _u32p)):
+            raise RuntimeError("oracle encode_stats failed")
+        return h
+
+    def select_exhaustive(self, hist: np.ndarray, tables):
+        h = np.ascontiguousarray(hist, np.uint32)
+        t = np.ascontiguousarray(tables, np.uint32).reshape(-1, 16)
+        nb = h.shape[0]
+        sel = np.zeros(nb, np.uint8)
+        cost = np.zeros((nb, 12, len(t)), np.uint64)
+        self.lib.or_select_exhaustive(_ptr(h, _u32p), nb, _ptr(t, _u32p), len(t), _ptr(sel, _u8p), _ptr(cost, _u64p))
+        return sel, cost
+
+    def brick_features(self, vol: np.ndarray, brick: int) -> np.ndarray:
+        v = np.ascontiguousarray(vol, dtype=np.uint64)
+        D, H, W = v.shape
+        nb = -(-W // brick) * -(-H // brick) * -(-D // brick)
+        f = np.zeros((nb, 32), np.float32)
+        if self.lib.or_brick_features(_ptr(v, _u64p), W, H, D, brick, f.ctypes.data_as(C.POINTER(C.c_float))):
+            raise RuntimeError("oracle features failed")
+        return f
+
+    def mlp_forward(self, params: np.ndarray, feat: np.ndarray) -> np.ndarray:
+        p = np.ascontiguousarray(params, np.float32)
+        f = np.ascontiguousarray(feat, np.float32)
+        z = np.zeros((len(f), 32), np.float32)
+        fp = C.POINTER(C.c_float)
+        self.lib.or_mlp_forward(p.ctypes.data_as(fp), f.ctypes.data_as(fp), len(f), z.ctypes.data_as(fp))
+        return z
+
+    def mlp_grad(self, params: np.ndarray, feat: np.ndarray, label: np.ndarray):
+        p = np.ascontiguousarray(params, np.float32)
+        f = np.ascontiguousarray(feat, np.float32)
+        lab = np.ascontiguousarray(label, np.uint8)
+        g = np.zeros_like(p)
+        fp = C.POINTER(C.c_float)
+        loss = self.lib.or_mlp_grad(p.ctypes.data_as(fp), f.ctypes.data_as(fp), _ptr(lab, _u8p), len(f),
+                                    g.ctypes.data_as(fp))
+        return float(loss), g
 
     def majority8(self, labels) -> int:
         a = np.ascontiguousarray(labels, dtype=np.uint64)
