@@ -43,6 +43,7 @@ WORKLOADS = {w["name"]: w for w in (MIXED, MIXED512)}
 SERVE = dict(name="serve2048", shape=(2048, 2048, 2048), brick=64, kind=1, n_cells=20000, n_tubes=8000, r_min=2.0,
              r_max=12.0, zero_frac=0.15, seed=5, width=1920, height=1080, frames=600, cache_gib=24,
              fov=1.0471975511965976)  # pi/3 (camera.js:19)
+SELECTOR = dict(train_volumes=40, steps=1200, seed=700)  # 40 x 512 bricks of 64^3 = 20,480 training bricks
 NEURITE = dict(name="neurite512", shape=(512, 512, 512), brick=64, kind=1, n_cells=3000, n_tubes=400, r_min=2.0,
                r_max=12.0, zero_frac=0.15, seed=2)
 FALLBACK_HBM_GBS = 6650.0
@@ -298,6 +299,8 @@ def run_b200(args):
     del out, vol, flush
     torch.cuda.empty_cache()
     serve = None if args.no_serve else serve2048(codec, dev, args)
+    torch.cuda.empty_cache()
+    selector = None if args.no_selector else selector1024(codec, dev, args)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -328,6 +331,7 @@ def run_b200(args):
                        "ms": round(enc_ms_left + enc_ms_right, 3), "workload": W["name"]},
             "neurite512": neur,
             "serve2048": serve,
+            "selector1024": selector,
             "checks": {"decode_equals_source": check, "e2e_equals_device": e2e_ok},
         }
         print(json.dumps(line))
@@ -336,6 +340,107 @@ def run_b200(args):
     ds_right.close()
     if pg is not None:
         pg.destroy_process_group()
+
+
+def selector1024(codec, dev, args):
+    """Learned mode / table selector: trained on ~20,000 64^3 bricks of seeded neurite-like volumes (512^3,
+    the neurite512 generator), evaluated on a held-out 1024^3 volume of the same kind against the exhaustive
+    search (every mode's statistics) and the plain encoder."""
+    import torch
+    from csvb200 import SelectorNet
+    from csvb200.selector import exhaustive_choice, features, fit_tables, learned_choice, train
+    N = NEURITE
+    st = torch.cuda.current_stream()
+
+    def ev():
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(st)
+        return e
+
+    t0 = time.perf_counter()
+    feats, hists = [], []
+    vol = torch.empty(N["shape"], dtype=torch.int64, device=dev)
+    for k in range(SELECTOR["train_volumes"]):
+        codec.synth_volume(vol, N["kind"], N["n_cells"], N["n_tubes"], N["r_min"], N["r_max"], N["zero_frac"],
+                           SELECTOR["seed"] + k)
+        feats.append(features(codec, vol, 64))
+        h = torch.empty((feats[-1].shape[0], 12, 16), dtype=torch.int32, device=dev)
+        codec.encode_stats(vol, 64, h)
+        hists.append(h)
+    del vol
+    tables = fit_tables(torch.cat(hists).cpu().numpy().astype(np.uint64), 16, iters=8)
+    labels = []
+    for h in hists:
+        sel = torch.empty(h.shape[0], dtype=torch.uint8, device=dev)
+        codec.select_exhaustive(h, tables, sel)
+        labels.append(sel)
+    data_s = time.perf_counter() - t0
+    e0 = ev()
+    net, losses = train(codec, torch.cat(feats), torch.cat(labels), steps=SELECTOR["steps"], batch=2048)
+    e1 = ev()
+    torch.cuda.synchronize()
+    train_ms = e0.elapsed_time(e1)
+    # held-out 1024^3
+    held = torch.empty((1024, 1024, 1024), dtype=torch.int64, device=dev)
+    codec.synth_volume(held, N["kind"], N["n_cells"] * 8, N["n_tubes"] * 8, N["r_min"], N["r_max"], N["zero_frac"],
+                       SELECTOR["seed"] + 1000)
+    nvox = held.numel()
+    res = {}
+    for rep in range(2):  # warm, then timed
+        a = ev()
+        codec.encode_device_sel(held, 64)
+        b = ev()
+        plain = codec.encoded_image()[1]
+        c = ev()
+        sel_x, _ = exhaustive_choice(codec, held, 64, tables)
+        codec.encode_device_sel(held, 64, tables, sel_x)
+        d = ev()
+        exh = codec.encoded_image()[1]
+        e = ev()
+        sel_l = learned_choice(net, features(codec, held, 64))
+        codec.encode_device_sel(held, 64, tables, sel_l)
+        f = ev()
+        learned = codec.encoded_image()[1]
+        torch.cuda.synchronize()
+        res = {"plain_ms": a.elapsed_time(b), "exhaustive_ms": c.elapsed_time(d), "learned_ms": e.elapsed_time(f)}
+    agree = float((sel_x == sel_l).float().mean())
+    # the network alone on the tensor cores: one forward pass over 1 Mi feature rows
+    rows = 1 << 20
+    big = torch.rand((rows, 32), device=dev)
+    logits = torch.empty((rows, 32), device=dev)
+    net.forward(big, d_logits=logits)
+    g0 = ev()
+    for _ in range(5):
+        net.forward(big, d_logits=logits)
+    g1 = ev()
+    torch.cuda.synchronize()
+    fwd_ms = g0.elapsed_time(g1) / 5
+    flops = 2.0 * rows * (64 * 256 + 256 * 256 + 256 * 32)
+    peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("bf16_tflops") if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else 1590.0
+    out = {
+        "train": {"volumes": SELECTOR["train_volumes"], "bricks": int(sum(f.shape[0] for f in feats)),
+                  "volume": list(N["shape"][::-1]), "generator": "neurite512 (400 tubes r 2-12, 3000 cells, 15 % 0)",
+                  "tables": 16, "modes": 12, "steps": SELECTOR["steps"], "batch": 2048, "train_ms": round(train_ms, 1),
+                  "loss_first": round(losses[0], 4), "loss_last": round(float(np.mean(losses[-20:])), 4),
+                  "data_s": round(data_s, 2)},
+        "held_out": {"volume": [1024, 1024, 1024], "bricks": int(sel_x.numel()), "seed": SELECTOR["seed"] + 1000,
+                     "generator": "neurite512 scaled x8 (3200 tubes, 24000 cells)"},
+        "bytes": {"plain": int(plain), "exhaustive": int(exh), "learned": int(learned)},
+        "size_loss_vs_exhaustive": round(learned / exh - 1.0, 5),
+        "size_vs_plain": round(learned / plain - 1.0, 5),
+        "choice_agreement": round(agree, 4),
+        "encode_ms": {k: round(v, 2) for k, v in res.items()},
+        "encode_mvox_s": {k[:-3]: round(nvox / (v * 1e-3) / 1e6, 1) for k, v in res.items()},
+        "speedup_vs_exhaustive": round(res["exhaustive_ms"] / res["learned_ms"], 2),
+        "mlp_forward": {"rows": rows, "ms": round(fwd_ms, 3), "tflops": round(flops / (fwd_ms * 1e-3) / 1e12, 1),
+                        "frac_of_bf16_peak": round(flops / (fwd_ms * 1e-3) / 1e12 / peak, 4)},
+        "decode": "version-2 image decodes to the same labels as the plain image (tests)",
+    }
+    net.close()
+    del held
+    torch.cuda.empty_cache()
+    return out
 
 
 def orbit_path(n, center, seed):
@@ -585,6 +690,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline legs")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop leg")
+    ap.add_argument("--no-selector", action="store_true", help="skip the learned-selector leg")
     ap.add_argument("--workload", default="mixed1024", choices=sorted(WORKLOADS),
                     help="mixed1024: the headline; mixed512: the same generator at 1/8 size (profiler captures)")
     args = ap.parse_args()
