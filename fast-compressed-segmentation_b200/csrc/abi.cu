@@ -33,9 +33,10 @@ int abi_ensure_scratch(csv_ctx* ctx, uint32_t b) {
     if (ctx->scr.base && ctx->scr_b >= b) return CSV_OK;
     size_t per = decode_scratch_per_cta(b);
     uint32_t ctas = decode_grid(ctx->device, 0xFFFFFFFFu);
+    const size_t bytes = decode_scratch_bytes(ctx->device, b);
     cudaFree(ctx->scr.base);
     ctx->scr.base = nullptr;
-    cudaError_t e = cudaMalloc(&ctx->scr.base, per * ctas);
+    cudaError_t e = cudaMalloc(&ctx->scr.base, bytes);
     if (e != cudaSuccess) return abi_fail(ctx, CSV_ENOMEM, std::string("decode scratch: ") + cudaGetErrorString(e));
     if (!ctx->scr.d_queue) {
         e = cudaMalloc(&ctx->scr.d_queue, 64);
@@ -43,6 +44,7 @@ int abi_ensure_scratch(csv_ctx* ctx, uint32_t b) {
     }
     ctx->scr.per_cta = per;
     ctx->scr.ctas = ctas;
+    ctx->scr.bytes = bytes;
     ctx->scr_b = b;
     return CSV_OK;
 }
@@ -565,9 +567,13 @@ struct csv_graph {
 
 namespace {
 
-// Largest-first order of the requests: estimated work = nSymbols of the brick
-// (rANS + replay) + a quarter of the labels written.
-int lpt_order(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_reqs, uint32_t n, uint32_t** d_order) {
+// The graph's schedule.  Requests above LOD 5 (64^3 outputs) go to the decode
+// kernel's large variant, the rest to its small-footprint variant with twice
+// the CTAs per SM; each part keeps the request order, or with `lpt` runs
+// largest first (estimated work = nSymbols of the brick, rANS + replay, plus a
+// quarter of the labels written).  ord = [large part | small part].
+int graph_schedule(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_reqs, uint32_t n, bool lpt,
+                   std::vector<uint32_t>& ord, uint32_t& n_large) {
     std::vector<csv_request> h(n);
     cudaError_t e = cudaMemcpy(h.data(), d_reqs, sizeof(csv_request) * n, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "request copy");
@@ -577,13 +583,17 @@ int lpt_order(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_reqs, ui
         if (h[i].brick < ds->d.nb && h[i].lod < 8) c = ds->d.h_cost[h[i].brick] + ((1ull << (3 * h[i].lod)) >> 2);
         cost[i] = c;
     }
-    std::vector<uint32_t> ord(n);
-    for (uint32_t i = 0; i < n; ++i) ord[i] = i;
-    std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
-    if ((e = cudaMalloc(d_order, sizeof(uint32_t) * std::max<uint32_t>(1, n))) != cudaSuccess)
-        return fail(ctx, CSV_ENOMEM, "order allocation");
-    if ((e = cudaMemcpy(*d_order, ord.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice)) != cudaSuccess)
-        return cuda_fail(ctx, e, "order copy");
+    ord.clear();
+    for (uint32_t i = 0; i < n; ++i)
+        if (h[i].lod > kSmallLod) ord.push_back(i);
+    n_large = (uint32_t)ord.size();
+    for (uint32_t i = 0; i < n; ++i)
+        if (h[i].lod <= kSmallLod) ord.push_back(i);
+    if (lpt) {
+        auto by_cost = [&](uint32_t a, uint32_t b) { return cost[a] > cost[b]; };
+        std::stable_sort(ord.begin(), ord.begin() + n_large, by_cost);
+        std::stable_sort(ord.begin() + n_large, ord.end(), by_cost);
+    }
     return CSV_OK;
 }
 
@@ -608,8 +618,17 @@ int csv_decode_graph_create(csv_ctx* ctx, const csv_dataset* ds, const csv_reque
         dc.ctas_per_sm = cfg->ctas_per_sm;
         dc.stage = cfg->stage;
     }
-    if (cfg && cfg->lpt && n) {
-        rc = lpt_order(ctx, ds, d_reqs, n, &gr->d_order);
+    // a dataset with 64^3 bricks: split the requests by output size (two launches), else one launch
+    const bool split = ds->d.L > kSmallLod + 1 && n;
+    uint32_t n_large = n;
+    if (split || (cfg && cfg->lpt && n)) {
+        std::vector<uint32_t> ord;
+        rc = graph_schedule(ctx, ds, d_reqs, n, cfg && cfg->lpt, ord, n_large);
+        if (!rc && !split) n_large = n;  // one part: all of them, in the scheduled order
+        cudaError_t e = rc ? cudaSuccess : cudaMalloc(&gr->d_order, sizeof(uint32_t) * n);
+        if (!rc && e != cudaSuccess) rc = fail(ctx, CSV_ENOMEM, "order allocation");
+        if (!rc && (e = cudaMemcpy(gr->d_order, ord.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice)) != cudaSuccess)
+            rc = cuda_fail(ctx, e, "order copy");
         if (rc) {
             csv_graph_destroy(gr);
             return rc;
@@ -624,7 +643,19 @@ int csv_decode_graph_create(csv_ctx* ctx, const csv_dataset* ds, const csv_reque
     }
     e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        cudaError_t le = launch_decode(ds->d, d_reqs, n, d_out, d_status, ctx->scr, s, &dc);
+        cudaError_t le = cudaSuccess;
+        if (!split) {
+            le = launch_decode(ds->d, d_reqs, n, d_out, d_status, ctx->scr, s, &dc);
+        } else {
+            // the large outputs first (longest bricks), then the small ones at twice the occupancy
+            DecodeConfig part = dc;
+            part.n_order = n_large;
+            if (n_large) le = launch_decode(ds->d, d_reqs, n, d_out, d_status, ctx->scr, s, &part);
+            part.order = gr->d_order + n_large;
+            part.n_order = n - n_large;
+            part.small_only = true;
+            if (le == cudaSuccess && n > n_large) le = launch_decode(ds->d, d_reqs, n, d_out, d_status, ctx->scr, s, &part);
+        }
         e = cudaStreamEndCapture(s, &gr->graph);
         if (le != cudaSuccess) e = le;
     }

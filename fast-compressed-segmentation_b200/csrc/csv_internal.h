@@ -93,18 +93,25 @@ cudaError_t launch_build_index(DeviceDataset& ds, cudaStream_t st);
 
 struct DecodeScratch {
     uint8_t* base = nullptr;
-    size_t per_cta = 0;
+    size_t per_cta = 0;   // per-CTA scratch of the largest brick size it was sized for
     uint32_t ctas = 0;
+    size_t bytes = 0;     // total; a launch runs at most bytes / (its per-CTA scratch) CTAs
     uint32_t* d_queue = nullptr;
 };
 size_t decode_scratch_per_cta(uint32_t b);
+size_t decode_scratch_bytes(int device, uint32_t b);
 uint32_t decode_grid(int device, uint32_t n);
+// Requests at this LOD (32^3 labels) or coarser can run in the decode kernel's
+// small-footprint variant (four CTAs per SM instead of two).
+constexpr uint32_t kSmallLod = 5;
 // Launch knobs the autotuner chooses (defaults: occupancy-limited grid, staging on, request order).
 struct DecodeConfig {
     uint32_t ctas_per_sm = 0;         // 0: as many as fit
     uint32_t stage = 1;               // stage brick streams in shared memory
-    const uint32_t* order = nullptr;  // device permutation of the requests, or null
-    const uint32_t* n_dev = nullptr;  // device-resident request count (<= n), or null
+    const uint32_t* order = nullptr;  // device list of request indices to decode, in this order, or null
+    uint32_t n_order = 0;             // entries of order (0: n)
+    const uint32_t* n_dev = nullptr;  // device-resident queue length (<= n or n_order), or null
+    bool small_only = false;          // every queued request is at LOD 5 (32^3) or coarser
 };
 cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, uint32_t n, uint64_t* d_out,
                           uint32_t* d_status, const DecodeScratch& scr, cudaStream_t st,

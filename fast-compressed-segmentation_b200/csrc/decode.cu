@@ -50,18 +50,25 @@ __host__ __device__ constexpr uint32_t voff(uint32_t l) { return (lvl_off(l) + 7
 // Activity bitmask words of level l at mask + moff(l).
 __host__ __device__ constexpr uint32_t mwords(uint32_t l) { return l < 2 ? 1u : (1u << (3 * l)) / 32; }
 __host__ __device__ constexpr uint32_t moff(uint32_t l) { return l == 0 ? 0u : moff(l - 1) + mwords(l - 1); }
-constexpr uint32_t kValEntries = voff(kDecLevels);   // 37456
-constexpr uint32_t kMaskWords = moff(kDecLevels);    // 1172
+// Shared memory holds the node values of parent levels 0..KL-1: KL = 6 serves
+// bricks up to 64^3 (two CTAs per SM), KL = 5 bricks up to 32^3 (four CTAs per
+// SM: their level arrays are an eighth of the size).
+constexpr uint32_t kSmallLevels = kSmallLod;
+template <uint32_t KL>
+struct LevelDims {
+    static constexpr uint32_t val = voff(KL);   // 37456 for KL 6, 4688 for KL 5
+    static constexpr uint32_t mask = moff(KL);  // 1172 for KL 6, 148 for KL 5
+};
 
-template <class V>
+template <class V, uint32_t KL>
 struct DecShared {
     uint32_t lut[kTot];
     // During the rANS phase the level arrays (val, mask, pre: contiguous) are
     // idle: the brick's compressed stream is staged over them by one bulk
     // (TMA) copy when it fits (stage_cap bytes).
-    alignas(16) V val[kValEntries];
-    uint32_t mask[kMaskWords];
-    uint16_t pre[kMaskWords];
+    alignas(16) V val[LevelDims<KL>::val];
+    uint32_t mask[LevelDims<KL>::mask];
+    uint16_t pre[LevelDims<KL>::mask];
     uint64_t pal[kPalCache];
     uint32_t warp_sums[kDecThreads / 32 + 1];
     BrickDesc br;
@@ -69,11 +76,12 @@ struct DecShared {
     uint32_t work, status;
     alignas(8) uint64_t bar;  // mbarrier of the stream copy
 };
-template <class V>
+template <class V, uint32_t KL>
 __host__ __device__ constexpr uint32_t stage_cap() {
-    return (uint32_t)(sizeof(V) * kValEntries + 6 * kMaskWords) & ~15u;
+    return (uint32_t)(sizeof(V) * LevelDims<KL>::val + 6 * LevelDims<KL>::mask) & ~15u;
 }
-static_assert((sizeof(uint16_t) * kValEntries) % 16 == 0, "mask follows val without padding");
+static_assert((sizeof(uint16_t) * LevelDims<kDecLevels>::val) % 16 == 0, "mask follows val without padding");
+static_assert((sizeof(uint16_t) * LevelDims<kSmallLevels>::val) % 16 == 0, "mask follows val without padding");
 
 // ---- bulk copy global -> shared with an mbarrier (cp.async.bulk, sm_90+)
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -248,9 +256,10 @@ struct DecodeArgs {
     uint8_t* scratch;
     uint64_t scratch_per_cta;
     uint32_t* queue;
-    uint32_t nb, L, S, n;
-    const uint32_t* order;  // optional processing order of the requests
-    const uint32_t* n_dev;  // optional device-resident request count (at most n)
+    uint32_t nb, L, S, n;   // n: queue length (requests, or entries of order)
+    uint32_t n_reqs;        // requests at reqs (and statuses at status)
+    const uint32_t* order;  // optional processing order: queue slot -> request
+    const uint32_t* n_dev;  // optional device-resident queue length (at most n)
     uint32_t stage_cap;     // largest stream staged in shared memory (0: never)
     uint32_t n_models;      // LUTs at lut, kTot entries each
 };
@@ -433,10 +442,10 @@ __device__ __forceinline__ void decode_segments(const DecodeArgs& A, const Brick
 
 // V = uint16_t when every palette of the dataset has fewer than 65535 entries
 // (value 0xFFFF stands for "label 0"), else uint32_t (one CTA per SM).
-template <class V>
-__global__ void __launch_bounds__(kDecThreads) decode_kernel(DecodeArgs A) {
+template <class V, uint32_t KL>
+__global__ void __launch_bounds__(kDecThreads, KL == kDecLevels ? 2 : 4) decode_kernel(DecodeArgs A) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
-    DecShared<V>& S = *reinterpret_cast<DecShared<V>*>(smem_raw);
+    DecShared<V, KL>& S = *reinterpret_cast<DecShared<V, KL>*>(smem_raw);
     const uint32_t tid = threadIdx.x, T = blockDim.x;
     constexpr uint32_t LABEL0 = sizeof(V) == 2 ? 0xFFFFu : PIDX_LABEL0;
 
@@ -458,23 +467,31 @@ __global__ void __launch_bounds__(kDecThreads) decode_kernel(DecodeArgs A) {
     for (;;) {
         if (tid == 0) {
             const uint32_t k = atomicAdd(A.queue, 1u);
-            // an optional schedule (e.g. longest brick first) maps queue slots to requests
-            S.work = (k < n_req && A.order) ? A.order[k] : k;
+            // an optional schedule (longest brick first, or one part of a
+            // split by output size) maps queue slots to requests
+            uint32_t wk = 0xFFFFFFFFu;  // past the end of the queue
+            if (k < n_req) wk = A.order ? min(A.order[k], 0xFFFFFFFEu) : k;
+            S.work = wk;
             S.status = 0;
-            if (k >= n_req) S.work = 0xFFFFFFFFu;
-            if (S.work < n_req) {
-                S.req = A.reqs[S.work];
+            if (wk < A.n_reqs) {
+                S.req = A.reqs[wk];
                 if (S.req.brick < A.nb) S.br = A.bricks[S.req.brick];
             }
         }
         __syncthreads();
         const uint32_t w = S.work;
-        if (w >= n_req) break;
+        if (w == 0xFFFFFFFFu) break;
+        if (w >= A.n_reqs) {  // an order entry naming no request: nothing to decode or report
+            __syncthreads();
+            continue;
+        }
         const csv_request req = S.req;
         const uint32_t t = req.lod;
-        // bricks of a concatenated dataset carry their own level count and model
+        // bricks of a concatenated dataset carry their own level count and model;
+        // a request at LOD t needs parent levels 0..t-1 in shared memory and the
+        // op records of levels 1..t in scratch, both sized for A.L levels
         const uint32_t Lb = (S.br.flags >> BF_LEVELS_SHIFT) & 15u, model = (S.br.flags >> BF_MODEL_SHIFT) & 255u;
-        if (req.brick >= A.nb || t >= Lb || Lb > A.L || model >= A.n_models) {
+        if (req.brick >= A.nb || t >= Lb || t >= A.L || model >= A.n_models) {
             if (tid == 0) A.status[w] = CSV_BRICK_BADREQ;
             __syncthreads();
             continue;
@@ -656,16 +673,17 @@ size_t decode_scratch_per_cta(uint32_t b) {
     return (size_t)((rec_bytes + act_bytes + 255) & ~255ull);
 }
 
-static int g_dec_occ[2][64] = {{0}};
+static int g_dec_occ[4][64] = {{0}};
 
-template <class V>
+template <class V, uint32_t KL>
 static int occupancy(int device) {
-    int& occ = g_dec_occ[sizeof(V) == 2 ? 0 : 1][device & 63];
+    int& occ = g_dec_occ[(sizeof(V) == 2 ? 0 : 1) + (KL == kDecLevels ? 0 : 2)][device & 63];
     if (occ == 0) {
-        cudaFuncSetAttribute(decode_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(DecShared<V>));
+        cudaFuncSetAttribute(decode_kernel<V, KL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(DecShared<V, KL>));
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, decode_kernel<V>, kDecThreads, sizeof(DecShared<V>));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, decode_kernel<V, KL>, kDecThreads,
+                                                      sizeof(DecShared<V, KL>));
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         occ = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
@@ -674,8 +692,39 @@ static int occupancy(int device) {
 }
 
 uint32_t decode_grid(int device, uint32_t n) {
-    uint32_t occ = (uint32_t)std::max(occupancy<uint16_t>(device), occupancy<uint32_t>(device));
+    uint32_t occ = (uint32_t)std::max(occupancy<uint16_t, kDecLevels>(device), occupancy<uint32_t, kDecLevels>(device));
     return n < occ ? n : occ;
+}
+
+// Scratch for every variant a dataset of bricks up to b^3 can use: the 64^3
+// variant's CTAs at b's size, or the 32^3 variant's CTAs at min(b, 32)'s size.
+size_t decode_scratch_bytes(int device, uint32_t b) {
+    const size_t big = decode_scratch_per_cta(b) * (size_t)decode_grid(device, 0xFFFFFFFFu);
+    const size_t small = decode_scratch_per_cta(std::min<uint32_t>(b, 32)) *
+                         (size_t)std::max(occupancy<uint16_t, kSmallLevels>(device),
+                                          occupancy<uint32_t, kSmallLevels>(device));
+    return std::max(big, small);
+}
+
+template <class V, uint32_t KL>
+static cudaError_t launch_variant(const DecodeArgs& A0, const DecodeScratch& scr, cudaStream_t st,
+                                  const DecodeConfig* cfg, int device) {
+    DecodeArgs A = A0;
+    uint32_t grid = (uint32_t)occupancy<V, KL>(device);
+    if (cfg && cfg->ctas_per_sm) {
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        const uint32_t per_sm = KL == kDecLevels ? cfg->ctas_per_sm : 2 * cfg->ctas_per_sm;
+        grid = std::min<uint32_t>(grid, per_sm * (uint32_t)std::max(sms, 1));
+    }
+    A.scratch_per_cta = decode_scratch_per_cta(1u << (A.L - 1));
+    const uint64_t cap = scr.bytes / A.scratch_per_cta;
+    if (grid > A.n) grid = A.n;
+    if (grid > cap) grid = (uint32_t)cap;
+    if (grid == 0) return cudaErrorInvalidValue;
+    A.stage_cap = (cfg && !cfg->stage) ? 0u : stage_cap<V, KL>();
+    decode_kernel<V, KL><<<grid, kDecThreads, sizeof(DecShared<V, KL>), st>>>(A);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, uint32_t n, uint64_t* d_out,
@@ -683,14 +732,8 @@ cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, ui
     if (n == 0) return cudaSuccess;
     if (ds.L > kDecLevels + 1) return cudaErrorInvalidValue;  // bricks up to 64^3
     const bool narrow = ds.max_P < 0xFFFFu;
-    uint32_t grid = (uint32_t)(narrow ? occupancy<uint16_t>(ds.device) : occupancy<uint32_t>(ds.device));
-    if (cfg && cfg->ctas_per_sm) {
-        int sms = 0;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ds.device);
-        grid = std::min<uint32_t>(grid, cfg->ctas_per_sm * (uint32_t)std::max(sms, 1));
-    }
-    if (grid > n) grid = n;
-    if (grid > scr.ctas) grid = scr.ctas;
+    // the 32^3 variant when every requested brick fits it: the whole dataset, or the caller says so
+    const bool small = ds.L <= kSmallLevels + 1 || (cfg && cfg->small_only);
     cudaError_t e = cudaMemsetAsync(scr.d_queue, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
     DecodeArgs A;
@@ -706,16 +749,22 @@ cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, ui
     A.scratch_per_cta = scr.per_cta;
     A.queue = scr.d_queue;
     A.nb = ds.nb;
-    A.L = ds.L;
+    // levels of the largest output this launch decodes (a request above it is refused with
+    // CSV_BRICK_BADREQ), so the per-CTA scratch can be laid out for that size
+    A.L = small ? std::min<uint32_t>(ds.L, kSmallLevels + 1) : ds.L;
     A.S = ds.S;
-    A.n = n;
+    A.n_reqs = n;
+    A.n = (cfg && cfg->order && cfg->n_order) ? cfg->n_order : n;
     A.order = cfg ? cfg->order : nullptr;
     A.n_dev = cfg ? cfg->n_dev : nullptr;
-    A.stage_cap = (cfg && !cfg->stage) ? 0u : (narrow ? stage_cap<uint16_t>() : stage_cap<uint32_t>());
+    A.stage_cap = 0;
     A.n_models = ds.n_models ? ds.n_models : 1u;
-    if (narrow) decode_kernel<uint16_t><<<grid, kDecThreads, sizeof(DecShared<uint16_t>), st>>>(A);
-    else decode_kernel<uint32_t><<<grid, kDecThreads, sizeof(DecShared<uint32_t>), st>>>(A);
-    return cudaGetLastError();
+    if (small) {
+        if (narrow) return launch_variant<uint16_t, kSmallLevels>(A, scr, st, cfg, ds.device);
+        return launch_variant<uint32_t, kSmallLevels>(A, scr, st, cfg, ds.device);
+    }
+    if (narrow) return launch_variant<uint16_t, kDecLevels>(A, scr, st, cfg, ds.device);
+    return launch_variant<uint32_t, kDecLevels>(A, scr, st, cfg, ds.device);
 }
 
 }  // namespace csv

@@ -64,6 +64,7 @@ int decode_batch_static(int device, const DeviceDataset& ds, const csv_request* 
     scr.base = base + kQueueBytes;
     scr.per_cta = per;
     scr.ctas = (uint32_t)((CSV_STATIC_SCRATCH_BYTES - kQueueBytes) / per);
+    scr.bytes = CSV_STATIC_SCRATCH_BYTES - kQueueBytes;
     e = launch_decode(ds, d_reqs, n, d_out, d_status, scr, st);
     if (e != cudaSuccess) {
         err = std::string("decode launch: ") + cudaGetErrorString(e);

@@ -131,3 +131,75 @@ def test_autotune_returns_a_working_config(codec, mixed):
     torch.cuda.synchronize()
     _check(out.cpu().numpy().view(np.uint64), bricks, lods, dst, parts_ref, offsets)
     g.close()
+
+
+def _graph_run(codec, cat, reqs, total):
+    import torch
+    from csvb200 import requests_tensor
+    out = torch.full((max(total, 1),), -3, dtype=torch.int64, device="cuda")
+    st = torch.full((len(reqs),), -1, dtype=torch.int32, device="cuda")
+    g = codec.decode_graph(cat, requests_tensor(reqs), out, st)
+    g.launch()
+    torch.cuda.synchronize()
+    g.close()
+    return out.cpu().numpy().view(np.uint64), st.cpu().numpy()
+
+
+@pytest.mark.parametrize("part", ["coarse_only", "full64_only", "mix_with_bad"])
+def test_graph_split_by_output_size(codec, mixed, part):
+    """A dataset with 64^3 bricks is decoded by two launches (outputs above 32^3, then the rest at twice the
+    occupancy); either part may be empty, and a refused request in either part leaves the others intact."""
+    from csvb200 import CSV_BRICK_BADREQ, requests
+    cat, dss, sizes_b, offsets, parts_ref = mixed
+    rng = np.random.default_rng(8)
+    brick_b = np.concatenate([[b] * n for n, b in sizes_b])
+    if part == "coarse_only":
+        bricks = np.arange(len(brick_b))
+        lods = np.array([int(rng.integers(0, min(6, int(b).bit_length()))) for b in brick_b])
+    elif part == "full64_only":
+        bricks = np.nonzero(brick_b == 64)[0]
+        lods = np.full(len(bricks), 6)
+    else:
+        bricks = np.concatenate([np.arange(len(brick_b)), [0, len(brick_b) + 5, offsets[1]]])
+        lods = np.concatenate([[int(b).bit_length() - 1 for b in brick_b], [6, 2, 5]])
+    sizes = 8 ** lods.astype(np.uint64)
+    dst = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.uint64)
+    out, st = _graph_run(codec, cat, requests(bricks, lods, dst), int(sizes.sum()))
+    bad = np.zeros(len(bricks), bool)
+    if part == "mix_with_bad":
+        bad[-3:-1] = True  # a 32^3 brick at LOD 6, a brick past the end
+        assert st[bad].tolist() == [CSV_BRICK_BADREQ, CSV_BRICK_BADREQ]
+    assert int(np.abs(st[~bad]).max()) == 0
+    keep = np.nonzero(~bad)[0]
+    _check(out, bricks[keep], lods[keep], dst[keep], parts_ref, offsets)
+
+
+def test_wide_palettes_in_both_kernel_variants(codec, oracle):
+    """Bricks with more than 65535 palette entries (32-bit node values in shared memory), decoded at 64^3 by
+    the large variant and at 32^3 and coarser by the small one, in one graph and in one batch."""
+    import torch
+    from csvb200 import requests, requests_tensor
+    g = torch.Generator(device="cuda")
+    g.manual_seed(12)
+    vol = torch.randint(1, 1 << 40, (64, 64, 128), dtype=torch.int64, device="cuda", generator=g)
+    vol[:, :, :16] = 7  # a coarse region so that not every node is a new label
+    codec.encode_device(vol, 64)
+    img = bytes(codec.encoded_image_tensor().cpu().numpy())
+    ds = codec.open(img)
+    ref = {t: oracle.decode_image(img, t)[0] for t in range(7)}
+    bricks = np.array([0, 1, 0, 1, 1, 0])
+    lods = np.array([6, 5, 4, 6, 0, 5])
+    sizes = 8 ** lods.astype(np.uint64)
+    dst = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.uint64)
+    reqs = requests(bricks, lods, dst)
+    out, st = _graph_run(codec, ds, reqs, int(sizes.sum()))
+    out2 = torch.zeros(int(sizes.sum()), dtype=torch.int64, device="cuda")
+    st2 = torch.full((len(reqs),), -1, dtype=torch.int32, device="cuda")
+    codec.decode_batch(ds, requests_tensor(reqs), out2, st2)
+    torch.cuda.synchronize()
+    for o, s in ((out, st), (out2.cpu().numpy().view(np.uint64), st2.cpu().numpy())):
+        assert int(np.abs(s).max()) == 0
+        for k in range(len(bricks)):
+            r = ref[int(lods[k])][int(bricks[k])]
+            assert np.array_equal(o[int(dst[k]):int(dst[k]) + len(r)], r), k
+    ds.close()
