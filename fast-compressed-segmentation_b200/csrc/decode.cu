@@ -578,18 +578,42 @@ __global__ void __launch_bounds__(kDecThreads, KL == kDecLevels ? 2 : 4) decode_
                             }
                         }
                     }
-                    // children of active parents take their ops
-                    for (uint32_t r = tid; r < n_act; r += T) {
-                        const uint32_t p = act_l[r];
-                        uint32_t rec[8];
-                        get_rec8(Vw, r, rec);
-                        uint32_t bits = 0;
-#pragma unroll
-                        for (uint32_t c = 0; c < 8; ++c) {
-                            val_c[8 * p + c] = (V)resolve(Vw, rec[c], 8 * p + c, lc, &bad);
-                            bits |= ((rec[c] & 8u) ? 0u : 1u) << c;
+                    // children of active parents take their ops (the r-th active
+                    // parent's are records o + 8r .. o + 8r + 7).  With fewer
+                    // children than threads, one thread per child, so that the
+                    // record reads of neighbour chains overlap across lanes; lanes
+                    // 8k..8k+7 then hold one parent (T is a multiple of 32) and
+                    // merge their activity bits by ballot.  Otherwise one thread
+                    // per parent.  (Measured: per child pays on every level of the
+                    // 32^3 variant, on the 64^3 one only up to T children.)
+                    const uint32_t n_kids = 8 * n_act;
+                    if (n_kids <= (KL == kDecLevels ? T : 8 * T)) {
+                        for (uint32_t base = 0; base < n_kids; base += T) {
+                            const uint32_t i = base + tid;
+                            uint32_t p = 0, child_active = 0;
+                            if (i < n_kids) {
+                                p = act_l[i >> 3];
+                                const uint32_t rec = get_rec(Vw, Vw.o + i);
+                                const uint32_t node = 8 * p + (i & 7u);
+                                val_c[node] = (V)resolve(Vw, rec, node, lc, &bad);
+                                child_active = (rec & 8u) ? 0u : 1u;
+                            }
+                            const uint32_t bits = (__ballot_sync(0xFFFFFFFFu, child_active) >> (tid & 24u)) & 0xFFu;
+                            if (bits && (tid & 7u) == 0) atomicOr(mask_c + ((8 * p) >> 5), bits << ((8 * p) & 31));
                         }
-                        if (bits) atomicOr(mask_c + ((8 * p) >> 5), bits << ((8 * p) & 31));
+                    } else {
+                        for (uint32_t r = tid; r < n_act; r += T) {
+                            const uint32_t p = act_l[r];
+                            uint32_t rec[8];
+                            get_rec8(Vw, r, rec);
+                            uint32_t bits = 0;
+#pragma unroll
+                            for (uint32_t c = 0; c < 8; ++c) {
+                                val_c[8 * p + c] = (V)resolve(Vw, rec[c], 8 * p + c, lc, &bad);
+                                bits |= ((rec[c] & 8u) ? 0u : 1u) << c;
+                            }
+                            if (bits) atomicOr(mask_c + ((8 * p) >> 5), bits << ((8 * p) & 31));
+                        }
                     }
                     __syncthreads();
                     // ranks: active nodes before each mask word, then the compacted list

@@ -42,6 +42,10 @@ constexpr uint32_t kEncSmemLevels = 5;  // levels 0..4 in shared memory
 constexpr uint32_t kEncSmemNodes = 4681;
 constexpr uint32_t OP_PALNEED = 7;  // placeholder code until the palette walk decides P0 / Pd / Pa
 constexpr uint32_t EF_UNIFORM = 1u, EF_OVERFLOW = 2u;
+// Encoder counters (u64 words): 0 nibble pool head, 1 palette pool head,
+// 2..17 the sampled bricks' nibble histogram, 18 the brick work queue (low
+// 32 bits), 19 checkpoint pool head.
+constexpr uint32_t kMiscQueue = 18, kMiscCk = 19, kMiscWords = 32;
 constexpr uint32_t kModes = 12;
 constexpr uint32_t kMaxTables = 16;
 constexpr uint32_t kModelWords = 65;  // freq[16] cum[16] total M[16] shift[16]
@@ -51,12 +55,14 @@ struct EncMeta {
     uint32_t P, nsym, nbytes, n_ops;
     uint32_t id, flags, n_ck, E;
     uint32_t level_start[8];
-    uint32_t sel, pad;  // mode | table << 4
+    uint32_t sel;     // mode | table << 4
+    uint32_t ck_off;  // first of the brick's n_ck seek checkpoints in the checkpoint pool
 };
 
 struct EncoderState {
     int device = 0;
-    uint32_t b = 0, L = 0, nb = 0, S = kOpsPerCheckpoint, ck_cap = 0;
+    uint32_t b = 0, L = 0, nb = 0, S = kOpsPerCheckpoint;
+    uint64_t ck_used = 0;  // checkpoints of the last encode (pool entries in use)
     uint64_t W = 0, H = 0, D = 0;
     // buffers (grow-only)
     EncMeta* d_meta = nullptr;
@@ -175,7 +181,7 @@ __device__ __forceinline__ uint32_t morton3(uint32_t x, uint32_t y, uint32_t z) 
 struct EncArgs {
     const uint64_t* vol;
     uint64_t W, H, D;
-    uint32_t b, L, nbx, nby, nbz, nb, S, ck_cap;
+    uint32_t b, L, nbx, nby, nbz, nb, S;
     uint8_t* scratch;
     uint64_t scratch_per_cta;
     EncMeta* meta;
@@ -183,7 +189,8 @@ struct EncArgs {
     uint64_t nib_cap;
     uint64_t* pal_pool;
     uint64_t pal_cap;
-    Checkpoint* ck;
+    Checkpoint* ck;     // checkpoint pool, reserved per brick at misc[kMiscCk]
+    uint64_t ck_cap;    // pool entries
     unsigned long long* misc;
     const uint8_t* sel;  // per brick: mode | table << 4 (null: mode 0, table 0)
 };
@@ -194,7 +201,7 @@ struct EncShared {
     uint32_t sh32[kEncThreads / 32 + 1];
     uint32_t hist[16];
     uint32_t work, P;
-    uint64_t nib_off, pal_off;
+    uint64_t nib_off, pal_off, ck_off;
 };
 
 struct BrickCtx {
@@ -427,7 +434,7 @@ __global__ void __launch_bounds__(kEncThreads) enc_bricks_kernel(EncArgs A) {
     uint64_t* pal_out = X.pal_out;
 
     for (;;) {
-        if (tid == 0) S.work = atomicAdd(reinterpret_cast<unsigned int*>(A.misc + 18), 1u);
+        if (tid == 0) S.work = atomicAdd(reinterpret_cast<unsigned int*>(A.misc + kMiscQueue), 1u);
         if (tid < 16) S.hist[tid] = 0;
         __syncthreads();
         const uint32_t i = S.work;
@@ -454,13 +461,19 @@ __global__ void __launch_bounds__(kEncThreads) enc_bricks_kernel(EncArgs A) {
                 nc += c == OP_PD ? 2u : 1u;
                 pa += c == OP_PA ? 1u : 0u;
             }
+            // the brick's seek checkpoints (one per S ops) are reserved in the pool
+            const uint32_t n_ck = (n_ops + A.S - 1) / A.S;
+            if (tid == 0) S.ck_off = atomicAdd(A.misc + kMiscCk, (unsigned long long)n_ck);
             uint32_t NC, PA;
             uint32_t pos = 1 + block_exclusive<uint32_t>(nc, S.sh32, &NC);
             uint32_t ip = block_exclusive<uint32_t>(pa, S.sh32, &PA);
-            Checkpoint* ck = A.ck + (uint64_t)i * A.ck_cap;
+            __syncthreads();
+            const uint64_t ck_off = S.ck_off;
+            const bool ck_ok = ck_off + n_ck <= A.ck_cap;
+            Checkpoint* ck = A.ck + ck_off;
             for (uint32_t j = j0; j < j1; ++j) {
                 const uint32_t op = ops[j], c = op & 7u;
-                if (j % A.S == 0 && j / A.S < A.ck_cap) ck[j / A.S] = Checkpoint{0, 0, pos, ip};
+                if (j % A.S == 0 && ck_ok) ck[j / A.S] = Checkpoint{0, 0, pos, ip};
                 nib[pos++] = (uint8_t)((c << 1) | ((op >> 3) & 1u));
                 if (c == OP_PD) nib[pos++] = (uint8_t)(op >> 4);
                 if (c == OP_PA) ++ip;
@@ -475,7 +488,7 @@ __global__ void __launch_bounds__(kEncThreads) enc_bricks_kernel(EncArgs A) {
             __syncthreads();
             const uint64_t nib_off = S.nib_off, pal_off = S.pal_off;
             // the rANS kernel reads whole 16-byte chunks of the reservation
-            const bool ok = nib_off + ((nbytes + 15) & ~15u) <= A.nib_cap && pal_off + P <= A.pal_cap;
+            const bool ok = nib_off + ((nbytes + 15) & ~15u) <= A.nib_cap && pal_off + P <= A.pal_cap && ck_ok;
             const bool sample = (i % 512) == 0;  // brickEncoding.hpp:482
             for (uint32_t q = tid; q < nbytes; q += T) {
                 const uint32_t hi = nib[2 * q], lo = (2 * q + 1 < nsym) ? nib[2 * q + 1] : 0u;
@@ -500,10 +513,10 @@ __global__ void __launch_bounds__(kEncThreads) enc_bricks_kernel(EncArgs A) {
                 m.n_ops = n_ops;
                 m.id = morton3(bx, by, bz);
                 m.flags = (root_const ? EF_UNIFORM : 0u) | (ok ? 0u : EF_OVERFLOW);
-                m.n_ck = (n_ops + A.S - 1) / A.S;
+                m.n_ck = n_ck;
                 m.E = 0;
                 m.sel = sel;
-                m.pad = 0;
+                m.ck_off = ck_ok ? (uint32_t)ck_off : 0u;
 #pragma unroll
                 for (int k = 0; k < 8; ++k) m.level_start[k] = ls[k];
                 A.meta[i] = m;
@@ -521,7 +534,7 @@ __global__ void __launch_bounds__(kEncThreads) enc_stats_kernel(EncArgs A, uint3
     const uint32_t tid = threadIdx.x, T = blockDim.x;
     const EncScratch X = enc_scratch(A);
     for (;;) {
-        if (tid == 0) S.work = atomicAdd(reinterpret_cast<unsigned int*>(A.misc + 18), 1u);
+        if (tid == 0) S.work = atomicAdd(reinterpret_cast<unsigned int*>(A.misc + kMiscQueue), 1u);
         __syncthreads();
         const uint32_t i = S.work;
         if (i >= A.nb) break;
@@ -623,8 +636,7 @@ __global__ void __launch_bounds__(32) enc_rans_kernel(EncMeta* __restrict__ meta
                                                       const uint8_t* __restrict__ nib_pool,
                                                       const uint64_t* __restrict__ enc_off,
                                                       uint8_t* __restrict__ enc_pool, const uint32_t* __restrict__ model,
-                                                      uint32_t n_tables, Checkpoint* __restrict__ ck_all,
-                                                      uint32_t ck_cap) {
+                                                      uint32_t n_tables, Checkpoint* __restrict__ ck_all) {
     __shared__ uint64_t tabs[kMaxTables * 16];
     for (uint32_t k = threadIdx.x; k < 16 * n_tables; k += blockDim.x) {
         const uint32_t* md = model + (k >> 4) * kModelWords;
@@ -641,9 +653,12 @@ __global__ void __launch_bounds__(32) enc_rans_kernel(EncMeta* __restrict__ meta
     // the packed nibbles of a brick start 16-byte aligned and are padded to 16
     const uint4* src4 = reinterpret_cast<const uint4*>(nib_pool + m.nib_off);
     uint8_t* out = enc_pool + enc_off[i];
-    Checkpoint* ck = ck_all + (uint64_t)i * ck_cap;
-    int k = (int)min(m.n_ck, ck_cap) - 1;
+    Checkpoint* ck = ck_all + m.ck_off;
+    int k = (int)m.n_ck - 1;
+    // the next checkpoint's symbol index, and the one after it loaded a
+    // checkpoint ahead so that the load is off the serial chain
     uint32_t next = k >= 0 ? ck[k].sym : 0xFFFFFFFFu;
+    uint32_t after = k >= 1 ? ck[k - 1].sym : 0xFFFFFFFFu;
     uint32_t x = kRansL, emitted = 0;
     const int nchunk = (int)((m.nbytes + 15) / 16);
     uint4 cur = nchunk > 0 ? src4[nchunk - 1] : make_uint4(0, 0, 0, 0);
@@ -661,14 +676,16 @@ __global__ void __launch_bounds__(32) enc_rans_kernel(EncMeta* __restrict__ meta
                 ck[k].state = x;
                 ck[k].pos = emitted;
                 --k;
-                next = k >= 0 ? ck[k].sym : 0xFFFFFFFFu;
+                next = after;
+                after = k >= 1 ? ck[k - 1].sym : 0xFFFFFFFFu;
             }
             rans_enc_step(x, emitted, out, tab[byte >> 4]);
             if (2 * q == next) {
                 ck[k].state = x;
                 ck[k].pos = emitted;
                 --k;
-                next = k >= 0 ? ck[k].sym : 0xFFFFFFFFu;
+                next = after;
+                after = k >= 1 ? ck[k - 1].sym : 0xFFFFFFFFu;
             }
         }
         cur = nxt;
@@ -795,14 +812,14 @@ int encode_stats(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W,
     }
     const uint32_t nb = (uint32_t)(nbx * nby * nbz);
     cudaError_t e;
-    if (!s->d_misc && (e = cudaMalloc(&s->d_misc, 32 * sizeof(unsigned long long))) != cudaSuccess) {
+    if (!s->d_misc && (e = cudaMalloc(&s->d_misc, kMiscWords * sizeof(unsigned long long))) != cudaSuccess) {
         err = cudaGetErrorString(e);
         return CSV_ECUDA;
     }
     const uint32_t grid = std::min<uint32_t>(enc_grid(device), std::max<uint32_t>(nb, 1));
     const size_t per_cta = enc_scratch_per_cta(b);
     if ((e = grow(&s->d_scratch, &s->scratch_cap, per_cta * grid)) != cudaSuccess ||
-        (e = cudaMemsetAsync(s->d_misc, 0, 32 * sizeof(unsigned long long), st)) != cudaSuccess) {
+        (e = cudaMemsetAsync(s->d_misc, 0, kMiscWords * sizeof(unsigned long long), st)) != cudaSuccess) {
         err = cudaGetErrorString(e);
         return CSV_ECUDA;
     }
@@ -840,7 +857,6 @@ int encode_device(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W
     }
     const uint32_t nb = (uint32_t)nb64;
     s->nb = nb;
-    s->ck_cap = (uint32_t)((max_ops_of(b) + s->S - 1) / s->S + 1);
     const uint64_t nvox = W * H * D;
     cudaError_t e;
 #define CK(x)                                                              \
@@ -857,21 +873,27 @@ int encode_device(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W
     const uint32_t n_tables = sel ? sel->n_tables : 0;
     const bool v2 = n_tables > 0;
     CK(grow(&s->d_meta, &s->meta_cap, nb));
-    CK(grow(&s->d_ck, &s->ck_cap_total, (size_t)nb * s->ck_cap));
     if (!s->d_model) CK(cudaMalloc(&s->d_model, kMaxTables * kModelWords * sizeof(uint32_t)));
     {
         static_assert(sizeof(unsigned long long) == 8, "");
-        if (!s->d_misc) CK(cudaMalloc(&s->d_misc, 32 * sizeof(unsigned long long)));
+        if (!s->d_misc) CK(cudaMalloc(&s->d_misc, kMiscWords * sizeof(unsigned long long)));
     }
     const uint32_t grid = std::min<uint32_t>(enc_grid(device), std::max<uint32_t>(nb, 1));
     const size_t per_cta = enc_scratch_per_cta(b);
     CK(grow(&s->d_scratch, &s->scratch_cap, per_cta * grid));
     size_t nib_need = std::max<size_t>(1 << 20, nvox / 4 + 16ull * nb);
     size_t pal_need = std::max<size_t>(1 << 16, nvox / 256 + 64ull * nb);
+    // as many ops as the nibble estimate allows (a nibble or two each)
+    size_t ck_need = std::max<size_t>(1 << 12, nib_need * 2 / s->S + nb);
     for (int attempt = 0; attempt < 2; ++attempt) {
+        if (ck_need > 0xFFFFFFFFull) {  // checkpoint offsets are 32-bit
+            err = "volume needs more than 2^32 seek checkpoints";
+            return CSV_ERANGE;
+        }
         CK(grow(&s->d_nib, &s->nib_cap, nib_need));
         CK(grow(&s->d_pal, &s->pal_cap, pal_need));
-        CK(cudaMemsetAsync(s->d_misc, 0, 32 * sizeof(unsigned long long), st));
+        CK(grow(&s->d_ck, &s->ck_cap_total, ck_need));
+        CK(cudaMemsetAsync(s->d_misc, 0, kMiscWords * sizeof(unsigned long long), st));
         EncArgs A;
         A.vol = d_vol;
         A.W = W; A.H = H; A.D = D;
@@ -879,7 +901,6 @@ int encode_device(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W
         A.nbx = (uint32_t)nbx; A.nby = (uint32_t)nby; A.nbz = (uint32_t)nbz;
         A.nb = nb;
         A.S = s->S;
-        A.ck_cap = s->ck_cap;
         A.scratch = s->d_scratch;
         A.scratch_per_cta = per_cta;
         A.meta = s->d_meta;
@@ -888,22 +909,25 @@ int encode_device(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W
         A.pal_pool = s->d_pal;
         A.pal_cap = s->pal_cap;
         A.ck = s->d_ck;
+        A.ck_cap = s->ck_cap_total;
         A.misc = s->d_misc;
         A.sel = sel ? sel->d_sel : nullptr;
         if (nb > 0) {
             enc_bricks_kernel<<<grid, kEncThreads, 0, st>>>(A);
             CK(cudaGetLastError());
         }
-        unsigned long long heads[2];
-        CK(cudaMemcpyAsync(heads, s->d_misc, sizeof heads, cudaMemcpyDeviceToHost, st));
+        unsigned long long misc[kMiscWords];
+        CK(cudaMemcpyAsync(misc, s->d_misc, sizeof misc, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
-        if (heads[0] <= s->nib_cap && heads[1] <= s->pal_cap) break;
+        s->ck_used = misc[kMiscCk];
+        if (misc[0] <= s->nib_cap && misc[1] <= s->pal_cap && misc[kMiscCk] <= s->ck_cap_total) break;
         if (attempt == 1) {
             err = "encoder pools overflowed twice";
             return CSV_ENOMEM;
         }
-        nib_need = heads[0];
-        pal_need = heads[1];
+        nib_need = std::max<size_t>(nib_need, misc[0]);
+        pal_need = std::max<size_t>(pal_need, misc[1]);
+        ck_need = std::max<size_t>(ck_need, misc[kMiscCk]);
     }
     std::vector<uint32_t> models(kMaxTables * kModelWords, 0);
     if (v2) {  // the caller's shared tables
@@ -939,7 +963,7 @@ int encode_device(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W
     CK(cudaMemcpyAsync(s->d_enc_off, enc_off.data(), 8ull * nb, cudaMemcpyHostToDevice, st));
     if (nb) {
         enc_rans_kernel<<<(nb + 31) / 32, 32, 0, st>>>(s->d_meta, nb, s->d_nib, s->d_enc_off, s->d_enc, s->d_model,
-                                                       s->n_tables, s->d_ck, s->ck_cap);
+                                                       s->n_tables, s->d_ck);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(s->h_meta.data(), s->d_meta, sizeof(EncMeta) * nb, cudaMemcpyDeviceToHost, st));
     }
@@ -1021,8 +1045,8 @@ int encoder_to_dataset(EncoderState* s, DeviceDataset& d, std::string& err) {
         bd.E = m.E;
         bd.nsym = m.nsym;
         bd.id = m.id;
-        bd.ck_off = (uint32_t)((uint64_t)i * s->ck_cap);
-        bd.ck_cap = s->ck_cap;
+        bd.ck_off = m.ck_off;
+        bd.ck_cap = m.n_ck;
         bd.n_ops = m.n_ops;
         bd.flags = ((m.flags & EF_UNIFORM) ? BF_UNIFORM : 0u) | (s->L << BF_LEVELS_SHIFT) |
                    ((s->v2 ? std::min((m.sel >> 4) & 15u, s->n_tables - 1) : 0u) << BF_MODEL_SHIFT);
@@ -1036,7 +1060,7 @@ int encoder_to_dataset(EncoderState* s, DeviceDataset& d, std::string& err) {
         d.max_nsym = std::max(d.max_nsym, m.nsym);
         d.max_P = std::max(d.max_P, m.P);
     }
-    d.ck_entries = (uint64_t)nb * s->ck_cap;
+    d.ck_entries = s->ck_used;
     d.enc_pool_bytes = std::max<uint64_t>(16, enc_n);
     d.pal_pool_entries = std::max<uint64_t>(1, pal_n);
     d.n_models = s->n_tables;
