@@ -253,6 +253,12 @@ void csv_destroy(csv_ctx* ctx) {
     DeviceGuard g(ctx->device);
     cudaFree(ctx->scr.base);
     cudaFree(ctx->scr.d_queue);
+    for (int i = 0; i < 2; ++i) {
+        cudaFree(ctx->chunk_buf[i]);
+        if (ctx->pipe_stream[i]) cudaStreamDestroy(ctx->pipe_stream[i]);
+    }
+    for (cudaEvent_t ev : ctx->pipe_event)
+        if (ev) cudaEventDestroy(ev);
     encoder_state_free(ctx->enc);
     delete ctx;
 }
@@ -335,6 +341,9 @@ int csv_decode_batch_static(csv_ctx* ctx, const csv_dataset* ds, const csv_reque
     return rc ? fail(ctx, rc, err) : CSV_OK;
 }
 
+// Labels per csv_decode_image chunk: two such device buffers per context.
+constexpr uint64_t kImageChunkBytes = 256ull << 20;
+
 int csv_decode_image(csv_ctx* ctx, const uint8_t* image, size_t len, uint32_t lod, uint64_t* out, uint32_t* status) {
     if (!ctx || !out) return CSV_EINVAL;
     DeviceGuard g(ctx->device);
@@ -345,40 +354,76 @@ int csv_decode_image(csv_ctx* ctx, const uint8_t* image, size_t len, uint32_t lo
         csv_close(ds);
         return fail(ctx, CSV_EINVAL, "lod beyond log2(brick size)");
     }
-    uint32_t nb = ds->d.nb;
-    uint64_t per = 1ull << (3 * lod);
+    const uint32_t nb = ds->d.nb;
+    const uint64_t per = 1ull << (3 * lod);
+    // chunks of whole bricks, at most kImageChunkBytes of labels each (at least one brick):
+    // chunk k decodes into buffer k % 2 while chunk k - 1 drains to the host
+    const uint64_t brick_bytes = 8 * per;
+    const uint32_t per_chunk = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(nb, kImageChunkBytes / brick_bytes));
     std::vector<csv_request> reqs(nb);
-    for (uint32_t i = 0; i < nb; ++i) reqs[i] = csv_request{i, lod, per * i};
+    for (uint32_t i = 0; i < nb; ++i) reqs[i] = csv_request{i, lod, per * (i % per_chunk)};
     csv_request* d_reqs = nullptr;
-    uint64_t* d_out = nullptr;
     uint32_t* d_st = nullptr;
-    cudaError_t e;
-    cudaStream_t st = 0;
-    if ((e = cudaMalloc(&d_reqs, sizeof(csv_request) * std::max<uint32_t>(1, nb))) != cudaSuccess ||
-        (e = cudaMalloc(&d_out, 8 * per * std::max<uint32_t>(1, nb))) != cudaSuccess ||
-        (e = cudaMalloc(&d_st, 4 * std::max<uint32_t>(1, nb))) != cudaSuccess) {
+    cudaError_t e = cudaSuccess;
+    const size_t need = (size_t)per_chunk * brick_bytes;
+    if (!ctx->pipe_stream[0]) {
+        for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaStreamCreateWithFlags(&ctx->pipe_stream[i], cudaStreamNonBlocking);
+        for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&ctx->pipe_event[i], cudaEventDisableTiming);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "pipeline streams");
+    }
+    if (rc == CSV_OK && need > ctx->chunk_bytes) {
+        for (int i = 0; i < 2; ++i) {
+            cudaFree(ctx->chunk_buf[i]);
+            ctx->chunk_buf[i] = nullptr;
+        }
+        ctx->chunk_bytes = 0;
+        for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaMalloc(&ctx->chunk_buf[i], need);
+        if (e == cudaSuccess) ctx->chunk_bytes = need;
+        else rc = fail(ctx, CSV_ENOMEM, std::string("chunk buffers: ") + cudaGetErrorString(e));
+    }
+    cudaStream_t s_dec = ctx->pipe_stream[0], s_copy = ctx->pipe_stream[1];
+    if (rc == CSV_OK &&
+        ((e = cudaMalloc(&d_reqs, sizeof(csv_request) * std::max<uint32_t>(1, nb))) != cudaSuccess ||
+         (e = cudaMalloc(&d_st, 4 * std::max<uint32_t>(1, nb))) != cudaSuccess)) {
         rc = fail(ctx, CSV_ENOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
-    } else if ((e = cudaMemcpyAsync(d_reqs, reqs.data(), sizeof(csv_request) * nb, cudaMemcpyHostToDevice, st)) !=
-               cudaSuccess) {
+    } else if (rc == CSV_OK &&
+               (e = cudaMemcpyAsync(d_reqs, reqs.data(), sizeof(csv_request) * nb, cudaMemcpyHostToDevice, s_dec)) !=
+                   cudaSuccess) {
         rc = cuda_fail(ctx, e, "request copy");
-    } else {
-        rc = csv_decode_batch(ctx, ds, d_reqs, nb, d_out, d_st, st);
-        if (rc == CSV_OK) {
-            std::vector<uint32_t> hst(nb);
-            if ((e = cudaMemcpyAsync(out, d_out, 8 * per * nb, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
-                (e = cudaMemcpyAsync(hst.data(), d_st, 4 * nb, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
-                (e = cudaStreamSynchronize(st)) != cudaSuccess) {
-                rc = cuda_fail(ctx, e, "decode");
-            } else {
-                if (status) memcpy(status, hst.data(), 4 * nb);
-                for (uint32_t i = 0; i < nb && rc == CSV_OK; ++i)
-                    if (hst[i]) rc = fail(ctx, CSV_EBRICK, "brick " + std::to_string(i) + " status " +
-                                                               std::to_string(hst[i]));
-            }
+    }
+    for (uint32_t k0 = 0, c = 0; rc == CSV_OK && k0 < nb; k0 += per_chunk, ++c) {
+        const uint32_t cnt = std::min(per_chunk, nb - k0), b = c & 1u;
+        if (c >= 2 && (e = cudaStreamWaitEvent(s_dec, ctx->pipe_event[2 + b], 0)) != cudaSuccess) {
+            rc = cuda_fail(ctx, e, "pipeline wait");
+            break;
+        }
+        rc = csv_decode_batch(ctx, ds, d_reqs + k0, cnt, ctx->chunk_buf[b], d_st + k0, s_dec);
+        if (rc) break;
+        if ((e = cudaEventRecord(ctx->pipe_event[b], s_dec)) != cudaSuccess ||
+            (e = cudaStreamWaitEvent(s_copy, ctx->pipe_event[b], 0)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(out + (uint64_t)k0 * per, ctx->chunk_buf[b], cnt * brick_bytes, cudaMemcpyDeviceToHost,
+                                 s_copy)) != cudaSuccess ||
+            (e = cudaEventRecord(ctx->pipe_event[2 + b], s_copy)) != cudaSuccess)
+            rc = cuda_fail(ctx, e, "pipeline copy");
+    }
+    if (rc == CSV_OK) {
+        std::vector<uint32_t> hst(nb);
+        if ((e = cudaEventRecord(ctx->pipe_event[0], s_dec)) != cudaSuccess ||
+            (e = cudaStreamWaitEvent(s_copy, ctx->pipe_event[0], 0)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(hst.data(), d_st, 4 * nb, cudaMemcpyDeviceToHost, s_copy)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(s_copy)) != cudaSuccess) {
+            rc = cuda_fail(ctx, e, "decode");
+        } else {
+            if (status) memcpy(status, hst.data(), 4 * nb);
+            for (uint32_t i = 0; i < nb && rc == CSV_OK; ++i)
+                if (hst[i]) rc = fail(ctx, CSV_EBRICK, "brick " + std::to_string(i) + " status " +
+                                                           std::to_string(hst[i]));
         }
     }
+    // both streams idle before the request and status buffers go
+    cudaStreamSynchronize(s_dec);
+    cudaStreamSynchronize(s_copy);
     cudaFree(d_reqs);
-    cudaFree(d_out);
     cudaFree(d_st);
     csv_close(ds);
     return rc;
@@ -617,9 +662,10 @@ int csv_decode_graph_create(csv_ctx* ctx, const csv_dataset* ds, const csv_reque
     if (cfg) {
         dc.ctas_per_sm = cfg->ctas_per_sm;
         dc.stage = cfg->stage;
+        dc.layout = cfg->layout;
     }
     // a dataset with 64^3 bricks: split the requests by output size (two launches), else one launch
-    const bool split = ds->d.L > kSmallLod + 1 && n;
+    const bool split = ds->d.L > kSmallLod + 1 && n && dc.layout == 0;
     uint32_t n_large = n;
     if (split || (cfg && cfg->lpt && n)) {
         std::vector<uint32_t> ord;
@@ -700,10 +746,12 @@ int csv_decode_autotune(csv_ctx* ctx, const csv_dataset* ds, const csv_request* 
     csv_decode_config bestc{0, 1, 0, 0};
     int rc = CSV_OK;
     const uint32_t per_sm_options[] = {2, 1};
+    const uint32_t n_layouts = ds->d.L > kSmallLod + 1 ? 2 : 1;  // layout matters with 64^3 bricks only
+    for (uint32_t layout = 0; layout < n_layouts && rc == CSV_OK; ++layout)
     for (uint32_t ps : per_sm_options) {
         for (uint32_t stage = 0; stage <= 1 && rc == CSV_OK; ++stage) {
             for (uint32_t lpt = 0; lpt <= 1 && rc == CSV_OK; ++lpt) {
-                csv_decode_config c{ps, stage, lpt, 0};
+                csv_decode_config c{ps, stage, lpt, layout};
                 csv_graph* gr = nullptr;
                 rc = csv_decode_graph_create(ctx, ds, d_reqs, n, d_out, d_status, &c, &gr);
                 if (rc) break;

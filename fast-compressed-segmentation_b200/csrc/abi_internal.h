@@ -14,6 +14,12 @@ struct csv_ctx {
     csv::DecodeScratch scr;
     uint32_t scr_b = 0;
     csv::EncoderState* enc = nullptr;
+    // csv_decode_image's pipeline: two chunk buffers (decode one while the
+    // other drains to the host), its streams and events; created on first use
+    uint64_t* chunk_buf[2] = {nullptr, nullptr};
+    size_t chunk_bytes = 0;
+    cudaStream_t pipe_stream[2] = {nullptr, nullptr};  // decode, copy
+    cudaEvent_t pipe_event[4] = {nullptr, nullptr, nullptr, nullptr};  // decoded[2], drained[2]
 };
 
 struct csv_dataset {

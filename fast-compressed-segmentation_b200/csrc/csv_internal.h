@@ -98,7 +98,7 @@ struct DecodeScratch {
     size_t bytes = 0;     // total; a launch runs at most bytes / (its per-CTA scratch) CTAs
     uint32_t* d_queue = nullptr;
 };
-size_t decode_scratch_per_cta(uint32_t b);
+size_t decode_scratch_per_cta(uint32_t b, uint32_t kl = 6);
 size_t decode_scratch_bytes(int device, uint32_t b);
 uint32_t decode_grid(int device, uint32_t n);
 // Requests at this LOD (32^3 labels) or coarser can run in the decode kernel's
@@ -112,6 +112,7 @@ struct DecodeConfig {
     uint32_t n_order = 0;             // entries of order (0: n)
     const uint32_t* n_dev = nullptr;  // device-resident queue length (<= n or n_order), or null
     bool small_only = false;          // every queued request is at LOD 5 (32^3) or coarser
+    uint32_t layout = 0;              // 1: every request in the four-CTA-per-SM kernel
 };
 cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, uint32_t n, uint64_t* d_out,
                           uint32_t* d_status, const DecodeScratch& scr, cudaStream_t st,

@@ -39,7 +39,10 @@
 
 namespace csv {
 
-constexpr int kDecThreads = 512;
+constexpr int kDecThreads = 512;      // threads of the four-CTA-per-SM variant
+constexpr int kDecThreadsBig = 512;   // threads of the two-CTA-per-SM variant
+template <uint32_t KL>
+__host__ __device__ constexpr int dec_threads() { return KL == 6 ? kDecThreadsBig : kDecThreads; }
 constexpr uint32_t kDecLevels = 6;       // parent levels 0..5 (a 64^3 brick has 7 levels)
 constexpr uint32_t kPalCache = 1024;     // palettes up to this size are copied to shared memory
 constexpr uint32_t REC_MISSING = OP_RP | 8u;
@@ -50,14 +53,16 @@ __host__ __device__ constexpr uint32_t voff(uint32_t l) { return (lvl_off(l) + 7
 // Activity bitmask words of level l at mask + moff(l).
 __host__ __device__ constexpr uint32_t mwords(uint32_t l) { return l < 2 ? 1u : (1u << (3 * l)) / 32; }
 __host__ __device__ constexpr uint32_t moff(uint32_t l) { return l == 0 ? 0u : moff(l - 1) + mwords(l - 1); }
-// Shared memory holds the node values of parent levels 0..KL-1: KL = 6 serves
-// bricks up to 64^3 (two CTAs per SM), KL = 5 bricks up to 32^3 (four CTAs per
-// SM: their level arrays are an eighth of the size).
+// Shared memory holds the node values of parent levels 0..KL-1 and the
+// activity masks of all parent levels.  KL = 6: every level of a 64^3 brick
+// (two CTAs per SM).  KL = 5: an eighth of the value space (four CTAs per SM);
+// a 64^3 brick's level-5 values (its last parent level) then live in the CTA's
+// global scratch, where they stay in L2.
 constexpr uint32_t kSmallLevels = kSmallLod;
 template <uint32_t KL>
 struct LevelDims {
-    static constexpr uint32_t val = voff(KL);   // 37456 for KL 6, 4688 for KL 5
-    static constexpr uint32_t mask = moff(KL);  // 1172 for KL 6, 148 for KL 5
+    static constexpr uint32_t val = voff(KL);            // 37456 for KL 6, 4688 for KL 5
+    static constexpr uint32_t mask = moff(kDecLevels);   // 1172
 };
 
 template <class V, uint32_t KL>
@@ -70,7 +75,7 @@ struct DecShared {
     uint32_t mask[LevelDims<KL>::mask];
     uint16_t pre[LevelDims<KL>::mask];
     uint64_t pal[kPalCache];
-    uint32_t warp_sums[kDecThreads / 32 + 1];
+    uint32_t warp_sums[1024 / 32 + 1];
     BrickDesc br;
     csv_request req;
     uint32_t work, status;
@@ -156,15 +161,21 @@ __device__ __forceinline__ uint32_t rans_step(uint32_t& x, uint32_t& pos, const 
 // before every S-th op and the first op of every level.  Level l+1 has 8 ops
 // per op of level l with stop bit 0; level 1 has 8 unless the root's stop bit
 // is set (then the brick is one label).
-__global__ void __launch_bounds__(32) build_index_kernel(BrickDesc* __restrict__ bricks, uint32_t nb,
+__global__ void __launch_bounds__(128) build_index_kernel(BrickDesc* __restrict__ bricks, uint32_t nb,
                                                          const uint8_t* __restrict__ enc_pool,
                                                          const uint32_t* __restrict__ g_lut,
                                                          Checkpoint* __restrict__ ck, uint32_t L, uint32_t S,
-                                                         uint32_t n_models) {
+                                                         uint32_t n_models, uint32_t lanes) {
     __shared__ uint32_t lut0[kTot];
     for (uint32_t i = threadIdx.x; i < kTot; i += blockDim.x) lut0[i] = g_lut[i];
     __syncthreads();
-    uint32_t bi = blockIdx.x * blockDim.x + threadIdx.x;
+    // The pass is one dependent chain per brick.  Lanes of one warp on
+    // different bricks run the union of their branch paths every step, so a
+    // warp works on only `lanes` bricks (lanes 0 .. lanes-1) when there are
+    // few enough bricks to give the SMs' schedulers many warps to interleave.
+    const uint32_t lane = threadIdx.x & 31;
+    if (lane >= lanes) return;
+    uint32_t bi = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * lanes + lane;
     if (bi >= nb) return;
     BrickDesc br = bricks[bi];
     // a version-2 image names a shared table per brick; other tables are read through the cache
@@ -236,10 +247,18 @@ __global__ void __launch_bounds__(32) build_index_kernel(BrickDesc* __restrict__
 
 cudaError_t launch_build_index(DeviceDataset& ds, cudaStream_t st) {
     if (ds.nb == 0) return cudaSuccess;
-    // one warp per block spreads the serial chains over as many SMs as possible
-    uint32_t blocks = (ds.nb + 31) / 32;
-    build_index_kernel<<<blocks, 32, 0, st>>>(ds.d_bricks, ds.nb, ds.d_enc, ds.d_lut, ds.d_ck, ds.L, ds.S,
-                                              ds.n_models ? ds.n_models : 1u);
+    // bricks per warp: the fewest (a power of two) that keeps about 32 warps per SM
+    // or fewer (measured: one brick per warp pays for a few thousand 64^3 bricks,
+    // a few per warp for tens of thousands of 32^3 ones)
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ds.device);
+    const uint64_t warps_max = 32ull * (uint64_t)std::max(sms, 1);
+    uint32_t lanes = 1;
+    while (lanes < 32 && (ds.nb + lanes - 1) / lanes > warps_max) lanes <<= 1;
+    const uint32_t per_block = 4 * lanes;  // four warps per block share the LUT copy
+    const uint32_t blocks = (ds.nb + per_block - 1) / per_block;
+    build_index_kernel<<<blocks, 128, 0, st>>>(ds.d_bricks, ds.nb, ds.d_enc, ds.d_lut, ds.d_ck, ds.L, ds.S,
+                                              ds.n_models ? ds.n_models : 1u, lanes);
     return cudaGetLastError();
 }
 
@@ -443,7 +462,7 @@ __device__ __forceinline__ void decode_segments(const DecodeArgs& A, const Brick
 // V = uint16_t when every palette of the dataset has fewer than 65535 entries
 // (value 0xFFFF stands for "label 0"), else uint32_t (one CTA per SM).
 template <class V, uint32_t KL>
-__global__ void __launch_bounds__(kDecThreads, KL == kDecLevels ? 2 : 4) decode_kernel(DecodeArgs A) {
+__global__ void __launch_bounds__(dec_threads<KL>(), KL == kDecLevels ? 2 : 4) decode_kernel(DecodeArgs A) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     DecShared<V, KL>& S = *reinterpret_cast<DecShared<V, KL>*>(smem_raw);
     const uint32_t tid = threadIdx.x, T = blockDim.x;
@@ -459,6 +478,8 @@ __global__ void __launch_bounds__(kDecThreads, KL == kDecLevels ? 2 : 4) decode_
     uint32_t* recs = reinterpret_cast<uint32_t*>(scr);
     const uint64_t max_ops = ((1ull << (3 * A.L)) - 8) / 7;
     uint32_t* act = reinterpret_cast<uint32_t*>(scr + ((max_ops * 4 + 255) & ~255ull));
+    // parent level KL (if the launch's bricks have one) in scratch, after the active lists
+    V* spill = reinterpret_cast<V*>(reinterpret_cast<uint8_t*>(act) + ((4ull * lvl_off(A.L - 1) + 255) & ~255ull));
 
     // the request count: fixed at launch, or produced on the device by an
     // earlier kernel in the same stream (the serving loop's admission)
@@ -554,7 +575,7 @@ __global__ void __launch_bounds__(kDecThreads, KL == kDecLevels ? 2 : 4) decode_
             for (uint32_t l = 0; l < t; ++l) {
                 const uint32_t lc = l + 1;
                 LevelView<V> Vw;
-                Vw.val = S.val + voff(l);
+                Vw.val = l < KL ? S.val + voff(l) : spill;
                 Vw.mask = S.mask + moff(l);
                 Vw.pre = S.pre + moff(l);
                 Vw.rec = recs;
@@ -563,7 +584,7 @@ __global__ void __launch_bounds__(kDecThreads, KL == kDecLevels ? 2 : 4) decode_
                 const uint32_t* act_l = act + lvl_off(l);
                 const uint32_t n_par = 1u << (3 * l);
                 if (lc < t) {
-                    V* val_c = S.val + voff(lc);
+                    V* val_c = lc < KL ? S.val + voff(lc) : spill;
                     uint32_t* mask_c = S.mask + moff(lc);
                     // children of stop-filled parents inherit (16 bytes of u16 or 2 x 16 of u32)
                     for (uint32_t p = tid; p < n_par; p += T) {
@@ -654,12 +675,14 @@ __global__ void __launch_bounds__(kDecThreads, KL == kDecLevels ? 2 : 4) decode_
                             }
                         }
                     }
-                    // active parents: four lanes per parent, two children each
+                    // active parents: four lanes per parent, two children each.
+                    // The next parent's index and records are fetched before
+                    // this one is resolved, so that two global reads per lane
+                    // are in flight.
                     const uint32_t sub = tid & 3u;
-                    for (uint32_t g = tid >> 2; g < n_act; g += T >> 2) {
-                        const uint32_t p = act_l[g];
+                    auto fetch = [&](uint32_t g, uint32_t& p, uint32_t& r0, uint32_t& r1) {
+                        p = act_l[g];
                         const uint32_t i0 = Vw.o + 8 * g + 2 * sub;
-                        uint32_t r0, r1;
                         if ((i0 & 1u) == 0 && i0 + 2 <= Vw.n_rec) {
                             const uint2 rr = *reinterpret_cast<const uint2*>(Vw.rec + i0);
                             r0 = rr.x;
@@ -668,6 +691,12 @@ __global__ void __launch_bounds__(kDecThreads, KL == kDecLevels ? 2 : 4) decode_
                             r0 = get_rec(Vw, i0);
                             r1 = get_rec(Vw, i0 + 1);
                         }
+                    };
+                    uint32_t g = tid >> 2, p_next = 0, r0_next = 0, r1_next = 0;
+                    if (g < n_act) fetch(g, p_next, r0_next, r1_next);
+                    for (; g < n_act; g += T >> 2) {
+                        const uint32_t p = p_next, r0 = r0_next, r1 = r1_next;
+                        if (g + (T >> 2) < n_act) fetch(g + (T >> 2), p_next, r0_next, r1_next);
                         const uint32_t n0 = 8 * p + 2 * sub;
                         const uint64_t a = label_of(pal, resolve(Vw, r0, n0, lc, &bad), LABEL0);
                         const uint64_t b = label_of(pal, resolve(Vw, r1, n0 + 1, lc, &bad), LABEL0);
@@ -690,11 +719,13 @@ __global__ void __launch_bounds__(kDecThreads, KL == kDecLevels ? 2 : 4) decode_
     }
 }
 
-size_t decode_scratch_per_cta(uint32_t b) {
+size_t decode_scratch_per_cta(uint32_t b, uint32_t kl) {
     uint32_t L = levels_of(b);
     uint64_t rec_bytes = (max_ops_of(b) * 4 + 255) & ~255ull;
-    uint64_t act_bytes = 4ull * lvl_off(L - 1);  // active lists of levels 0 .. L-2
-    return (size_t)((rec_bytes + act_bytes + 255) & ~255ull);
+    uint64_t act_bytes = (4ull * lvl_off(L - 1) + 255) & ~255ull;  // active lists of levels 0 .. L-2
+    // node values of parent level kl when the brick has one (up to 32-bit entries)
+    uint64_t spill_bytes = L - 1 > kl ? 4ull << (3 * kl) : 0;
+    return (size_t)(rec_bytes + act_bytes + spill_bytes);
 }
 
 static int g_dec_occ[4][64] = {{0}};
@@ -706,7 +737,7 @@ static int occupancy(int device) {
         cudaFuncSetAttribute(decode_kernel<V, KL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(DecShared<V, KL>));
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, decode_kernel<V, KL>, kDecThreads,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, decode_kernel<V, KL>, dec_threads<KL>(),
                                                       sizeof(DecShared<V, KL>));
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -723,8 +754,8 @@ uint32_t decode_grid(int device, uint32_t n) {
 // Scratch for every variant a dataset of bricks up to b^3 can use: the 64^3
 // variant's CTAs at b's size, or the 32^3 variant's CTAs at min(b, 32)'s size.
 size_t decode_scratch_bytes(int device, uint32_t b) {
-    const size_t big = decode_scratch_per_cta(b) * (size_t)decode_grid(device, 0xFFFFFFFFu);
-    const size_t small = decode_scratch_per_cta(std::min<uint32_t>(b, 32)) *
+    const size_t big = decode_scratch_per_cta(b, kDecLevels) * (size_t)decode_grid(device, 0xFFFFFFFFu);
+    const size_t small = decode_scratch_per_cta(b, kSmallLevels) *
                          (size_t)std::max(occupancy<uint16_t, kSmallLevels>(device),
                                           occupancy<uint32_t, kSmallLevels>(device));
     return std::max(big, small);
@@ -741,13 +772,13 @@ static cudaError_t launch_variant(const DecodeArgs& A0, const DecodeScratch& scr
         const uint32_t per_sm = KL == kDecLevels ? cfg->ctas_per_sm : 2 * cfg->ctas_per_sm;
         grid = std::min<uint32_t>(grid, per_sm * (uint32_t)std::max(sms, 1));
     }
-    A.scratch_per_cta = decode_scratch_per_cta(1u << (A.L - 1));
+    A.scratch_per_cta = decode_scratch_per_cta(1u << (A.L - 1), KL);
     const uint64_t cap = scr.bytes / A.scratch_per_cta;
     if (grid > A.n) grid = A.n;
     if (grid > cap) grid = (uint32_t)cap;
     if (grid == 0) return cudaErrorInvalidValue;
     A.stage_cap = (cfg && !cfg->stage) ? 0u : stage_cap<V, KL>();
-    decode_kernel<V, KL><<<grid, kDecThreads, sizeof(DecShared<V, KL>), st>>>(A);
+    decode_kernel<V, KL><<<grid, dec_threads<KL>(), sizeof(DecShared<V, KL>), st>>>(A);
     return cudaGetLastError();
 }
 
@@ -756,8 +787,9 @@ cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, ui
     if (n == 0) return cudaSuccess;
     if (ds.L > kDecLevels + 1) return cudaErrorInvalidValue;  // bricks up to 64^3
     const bool narrow = ds.max_P < 0xFFFFu;
-    // the 32^3 variant when every requested brick fits it: the whole dataset, or the caller says so
-    const bool small = ds.L <= kSmallLevels + 1 || (cfg && cfg->small_only);
+    // the four-CTA variant when the dataset's bricks are 32^3 or smaller, when the caller
+    // says every request is at LOD 5 or coarser, or when asked to take every request
+    const bool small = ds.L <= kSmallLevels + 1 || (cfg && (cfg->small_only || cfg->layout == 1));
     cudaError_t e = cudaMemsetAsync(scr.d_queue, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
     DecodeArgs A;
@@ -775,7 +807,7 @@ cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, ui
     A.nb = ds.nb;
     // levels of the largest output this launch decodes (a request above it is refused with
     // CSV_BRICK_BADREQ), so the per-CTA scratch can be laid out for that size
-    A.L = small ? std::min<uint32_t>(ds.L, kSmallLevels + 1) : ds.L;
+    A.L = (cfg && cfg->small_only) ? std::min<uint32_t>(ds.L, kSmallLevels + 1) : ds.L;
     A.S = ds.S;
     A.n_reqs = n;
     A.n = (cfg && cfg->order && cfg->n_order) ? cfg->n_order : n;

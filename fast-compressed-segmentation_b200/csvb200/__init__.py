@@ -55,11 +55,12 @@ class _Info(C.Structure):
 
 
 class DecodeConfig(C.Structure):
-    """csv_decode_config: grid CTAs per SM (0 = all that fit), stream staging, largest-first order."""
-    _fields_ = [("ctas_per_sm", C.c_uint32), ("stage", C.c_uint32), ("lpt", C.c_uint32), ("reserved", C.c_uint32)]
+    """csv_decode_config: grid CTAs per SM (0 = all that fit), stream staging, largest-first order, and for
+    datasets with 64^3 bricks the kernel layout (0: split by output size over two kernels, 1: one kernel)."""
+    _fields_ = [("ctas_per_sm", C.c_uint32), ("stage", C.c_uint32), ("lpt", C.c_uint32), ("layout", C.c_uint32)]
 
     def as_dict(self):
-        return {"ctas_per_sm": self.ctas_per_sm, "stage": self.stage, "lpt": self.lpt}
+        return {"ctas_per_sm": self.ctas_per_sm, "stage": self.stage, "lpt": self.lpt, "layout": self.layout}
 
 
 CONE_REFERENCE = 0

@@ -160,12 +160,16 @@ int csv_dataset_concat(csv_ctx* ctx, const csv_dataset* const* parts, uint32_t n
  * by csv_graph_launch.  Knobs: ctas_per_sm (0 = as many as fit), stage (1 =
  * stage each brick's compressed stream in shared memory by a bulk copy), lpt
  * (1 = hand out the largest bricks first: a request permutation computed at
- * creation). */
+ * creation), layout (for datasets with 64^3 bricks: 0 = requests above LOD 5
+ * in the decode kernel that holds every level in shared memory, two CTAs per
+ * SM, then the rest in the four-CTA-per-SM kernel, as two launches; 1 = every
+ * request in the four-CTA kernel, which keeps a 64^3 brick's last parent
+ * level in its global scratch). */
 typedef struct csv_decode_config {
     uint32_t ctas_per_sm;
     uint32_t stage;
     uint32_t lpt;
-    uint32_t reserved;
+    uint32_t layout;
 } csv_decode_config;
 
 typedef struct csv_graph csv_graph;

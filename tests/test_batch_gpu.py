@@ -97,7 +97,7 @@ def test_concat_rejects_lod_beyond_its_brick(codec, mixed):
     assert st.cpu().numpy().tolist() == [CSV_BRICK_BADREQ, 0]
 
 
-@pytest.mark.parametrize("cfg", [(0, 1, 1), (1, 0, 0), (2, 1, 0), (1, 1, 1)])
+@pytest.mark.parametrize("cfg", [(0, 1, 1, 0), (1, 0, 0, 0), (2, 1, 0, 0), (1, 1, 1, 0), (0, 1, 1, 1), (2, 0, 0, 1)])
 def test_graph_replay_matches(codec, mixed, cfg):
     import torch
     from csvb200 import DecodeConfig, requests_tensor
@@ -105,7 +105,7 @@ def test_graph_replay_matches(codec, mixed, cfg):
     reqs, bricks, lods, dst, total = _mixed_requests(sizes_b, np.random.default_rng(5))
     out = torch.zeros(total, dtype=torch.int64, device="cuda")
     st = torch.full((len(reqs),), -1, dtype=torch.int32, device="cuda")
-    g = codec.decode_graph(cat, requests_tensor(reqs), out, st, DecodeConfig(*cfg, 0))
+    g = codec.decode_graph(cat, requests_tensor(reqs), out, st, DecodeConfig(*cfg))
     for _ in range(3):
         out.zero_()
         g.launch()
@@ -125,6 +125,7 @@ def test_autotune_returns_a_working_config(codec, mixed):
     st = torch.zeros(len(reqs), dtype=torch.int32, device="cuda")
     best, ms = codec.autotune(cat, d_reqs, out, st, reps=3)
     assert ms > 0 and best.ctas_per_sm in (1, 2) and best.stage in (0, 1) and best.lpt in (0, 1)
+    assert best.layout in (0, 1)
     out.zero_()
     g = codec.decode_graph(cat, d_reqs, out, st, best)
     g.launch()
@@ -133,22 +134,24 @@ def test_autotune_returns_a_working_config(codec, mixed):
     g.close()
 
 
-def _graph_run(codec, cat, reqs, total):
+def _graph_run(codec, cat, reqs, total, layout=0):
     import torch
-    from csvb200 import requests_tensor
+    from csvb200 import DecodeConfig, requests_tensor
     out = torch.full((max(total, 1),), -3, dtype=torch.int64, device="cuda")
     st = torch.full((len(reqs),), -1, dtype=torch.int32, device="cuda")
-    g = codec.decode_graph(cat, requests_tensor(reqs), out, st)
+    g = codec.decode_graph(cat, requests_tensor(reqs), out, st, DecodeConfig(0, 1, 0, layout))
     g.launch()
     torch.cuda.synchronize()
     g.close()
     return out.cpu().numpy().view(np.uint64), st.cpu().numpy()
 
 
+@pytest.mark.parametrize("layout", [0, 1])
 @pytest.mark.parametrize("part", ["coarse_only", "full64_only", "mix_with_bad"])
-def test_graph_split_by_output_size(codec, mixed, part):
+def test_graph_split_by_output_size(codec, mixed, part, layout):
     """A dataset with 64^3 bricks is decoded by two launches (outputs above 32^3, then the rest at twice the
-    occupancy); either part may be empty, and a refused request in either part leaves the others intact."""
+    occupancy; layout 0) or by the four-CTA kernel alone (layout 1); either part may be empty, and a refused
+    request in either part leaves the others intact."""
     from csvb200 import CSV_BRICK_BADREQ, requests
     cat, dss, sizes_b, offsets, parts_ref = mixed
     rng = np.random.default_rng(8)
@@ -164,7 +167,7 @@ def test_graph_split_by_output_size(codec, mixed, part):
         lods = np.concatenate([[int(b).bit_length() - 1 for b in brick_b], [6, 2, 5]])
     sizes = 8 ** lods.astype(np.uint64)
     dst = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.uint64)
-    out, st = _graph_run(codec, cat, requests(bricks, lods, dst), int(sizes.sum()))
+    out, st = _graph_run(codec, cat, requests(bricks, lods, dst), int(sizes.sum()), layout)
     bad = np.zeros(len(bricks), bool)
     if part == "mix_with_bad":
         bad[-3:-1] = True  # a 32^3 brick at LOD 6, a brick past the end
@@ -193,11 +196,12 @@ def test_wide_palettes_in_both_kernel_variants(codec, oracle):
     dst = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.uint64)
     reqs = requests(bricks, lods, dst)
     out, st = _graph_run(codec, ds, reqs, int(sizes.sum()))
+    out1, st1 = _graph_run(codec, ds, reqs, int(sizes.sum()), layout=1)  # 32-bit level 5 in scratch
     out2 = torch.zeros(int(sizes.sum()), dtype=torch.int64, device="cuda")
     st2 = torch.full((len(reqs),), -1, dtype=torch.int32, device="cuda")
     codec.decode_batch(ds, requests_tensor(reqs), out2, st2)
     torch.cuda.synchronize()
-    for o, s in ((out, st), (out2.cpu().numpy().view(np.uint64), st2.cpu().numpy())):
+    for o, s in ((out, st), (out1, st1), (out2.cpu().numpy().view(np.uint64), st2.cpu().numpy())):
         assert int(np.abs(s).max()) == 0
         for k in range(len(bricks)):
             r = ref[int(lods[k])][int(bricks[k])]

@@ -166,3 +166,34 @@ def test_truncated_stream_reports_truncation(codec):
     out, st = codec.decode_image(bad, 6, check=False)
     assert st[1] & CSV_BRICK_TRUNCATED
     assert st[0] == 0 and st[2] == 0
+
+
+@pytest.mark.parametrize("b", [32, 64])
+def test_decode_image_spans_several_chunks(codec, b):
+    """csv_decode_image decodes in chunks of at most 256 MiB of labels through two device buffers (one chunk
+    decodes while the previous one drains to the host).  A 384^3 volume (432 MiB of labels: two chunks, the
+    second partial) comes back equal, brick for brick, to one device-side batch decode of the same image, on
+    a first call and on a second one that reuses the buffers."""
+    import torch
+    from csvb200 import requests, requests_tensor
+    vol = torch.empty((384, 384, 384), dtype=torch.int64, device="cuda")
+    codec.synth_volume(vol, 1, 300, 40, 1.0, 5.0, 0.1, 77)
+    codec.encode_device(vol, b)
+    img = bytes(codec.encoded_image_tensor().cpu().numpy())
+    del vol
+    full = b.bit_length() - 1
+    ds = codec.open(img)
+    nb = ds.num_bricks
+    dev = torch.empty(nb * b ** 3, dtype=torch.int64, device="cuda")
+    st = torch.full((nb,), -1, dtype=torch.int32, device="cuda")
+    codec.decode_batch(ds, requests_tensor(requests(np.arange(nb), np.full(nb, full),
+                                                    np.arange(nb, dtype=np.uint64) * b ** 3)), dev, st)
+    torch.cuda.synchronize()
+    assert int(st.abs().max()) == 0
+    ref = dev.cpu().numpy().view(np.uint64).reshape(nb, -1)
+    del dev
+    ds.close()
+    for _ in range(2):
+        out, hst = codec.decode_image(img, full)
+        assert int(hst.max()) == 0
+        assert np.array_equal(out, ref)
