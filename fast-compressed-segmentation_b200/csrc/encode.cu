@@ -632,11 +632,12 @@ __device__ __forceinline__ void rans_enc_step(uint32_t& x, uint32_t& emitted, ui
     x = (qd << kTotBits) + (x - qd * f) + (((uint32_t)e >> 13) & 0xFFFu);
 }
 
-__global__ void __launch_bounds__(32) enc_rans_kernel(EncMeta* __restrict__ meta, uint32_t nb,
-                                                      const uint8_t* __restrict__ nib_pool,
-                                                      const uint64_t* __restrict__ enc_off,
-                                                      uint8_t* __restrict__ enc_pool, const uint32_t* __restrict__ model,
-                                                      uint32_t n_tables, Checkpoint* __restrict__ ck_all) {
+__global__ void __launch_bounds__(128) enc_rans_kernel(EncMeta* __restrict__ meta, uint32_t nb,
+                                                       const uint8_t* __restrict__ nib_pool,
+                                                       const uint64_t* __restrict__ enc_off,
+                                                       uint8_t* __restrict__ enc_pool, const uint32_t* __restrict__ model,
+                                                       uint32_t n_tables, Checkpoint* __restrict__ ck_all,
+                                                       uint32_t lanes) {
     __shared__ uint64_t tabs[kMaxTables * 16];
     for (uint32_t k = threadIdx.x; k < 16 * n_tables; k += blockDim.x) {
         const uint32_t* md = model + (k >> 4) * kModelWords;
@@ -645,7 +646,12 @@ __global__ void __launch_bounds__(32) enc_rans_kernel(EncMeta* __restrict__ meta
                   ((uint64_t)md[33 + s] << 32);
     }
     __syncthreads();
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    // One serial chain per brick; a warp takes only `lanes` bricks (lanes
+    // 0 .. lanes-1) when there are few bricks, so that lanes do not run the
+    // union of other bricks' branch paths and the SM interleaves many warps.
+    const uint32_t lane = threadIdx.x & 31;
+    if (lane >= lanes) return;
+    const uint32_t i = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * lanes + lane;
     if (i >= nb) return;
     const EncMeta m = meta[i];
     if (m.flags & EF_OVERFLOW) return;
@@ -962,8 +968,14 @@ int encode_device(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W
     CK(grow(&s->d_rec_off, &s->rec_cap, std::max<uint32_t>(nb, 1)));
     CK(cudaMemcpyAsync(s->d_enc_off, enc_off.data(), 8ull * nb, cudaMemcpyHostToDevice, st));
     if (nb) {
-        enc_rans_kernel<<<(nb + 31) / 32, 32, 0, st>>>(s->d_meta, nb, s->d_nib, s->d_enc_off, s->d_enc, s->d_model,
-                                                       s->n_tables, s->d_ck);
+        // bricks per warp: the fewest (a power of two) that keeps about 32 warps per SM or fewer
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        uint32_t lanes = 1;
+        while (lanes < 32 && (nb + lanes - 1) / lanes > 32ull * (uint64_t)std::max(sms, 1)) lanes <<= 1;
+        const uint32_t per_block = 4 * lanes;  // four warps per block share the tables
+        enc_rans_kernel<<<(nb + per_block - 1) / per_block, 128, 0, st>>>(
+            s->d_meta, nb, s->d_nib, s->d_enc_off, s->d_enc, s->d_model, s->n_tables, s->d_ck, lanes);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(s->h_meta.data(), s->d_meta, sizeof(EncMeta) * nb, cudaMemcpyDeviceToHost, st));
     }
