@@ -144,6 +144,13 @@ cudaError_t launch_render(const csv_camera& cam, uint32_t W, uint32_t H, float g
                           cudaStream_t st);
 
 size_t gemm_smem_bytes();
+// B [N][K] bf16 -> the tensor cores' no-swizzle K-major core-matrix tiling (K-chunks of 64).
+cudaError_t launch_tile_b(const __nv_bfloat16* B, uint32_t N, uint32_t K, __nv_bfloat16* T, cudaStream_t st);
+// The selector network's forward pass fused in one persistent kernel (mlp.cu): features [count][32]
+// -> logits [count][32] and/or sel (argmax of logits 0..11 | argmax of logits 12..27 << 4).
+cudaError_t launch_mlp_infer(const float* feat, uint32_t count, const __nv_bfloat16* W1t, const __nv_bfloat16* W2t,
+                             const __nv_bfloat16* W3t, const float* b1, const float* b2, const float* b3, float* logits,
+                             uint8_t* sel, uint32_t* err, int device, cudaStream_t st);
 cudaError_t launch_gemm_bf16(const __nv_bfloat16* A, const __nv_bfloat16* B, uint32_t M, uint32_t N, uint32_t K,
                              const float* bias, const __nv_bfloat16* mask, uint32_t relu, float* C,
                              __nv_bfloat16* Cb, __nv_bfloat16* CbT, float* CT, uint32_t* err, cudaStream_t st);

@@ -407,19 +407,6 @@ __global__ void refresh_kernel(const float* __restrict__ P, __nv_bfloat16* W1b, 
     }
 }
 
-// Argmax of each head (ties: the lower index) -> mode | table << 4.
-__global__ void argmax_kernel(const float* __restrict__ Z, uint32_t n, uint8_t* __restrict__ sel) {
-    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n) return;
-    const float* z = Z + (size_t)r * kOut;
-    uint32_t bm = 0, bt = 0;
-    for (uint32_t k = 1; k < kModesN; ++k)
-        if (z[k] > z[bm]) bm = k;
-    for (uint32_t k = 1; k < kTablesN; ++k)
-        if (z[kModesN + k] > z[kModesN + bt]) bt = k;
-    sel[r] = (uint8_t)(bm | (bt << 4));
-}
-
 }  // namespace
 }  // namespace csv
 
@@ -435,6 +422,7 @@ struct csv_mlp {
     float* Mm = nullptr;
     float* Vm = nullptr;
     __nv_bfloat16 *W1b = nullptr, *W2b = nullptr, *W2bT = nullptr, *W3b = nullptr, *W3bT = nullptr;
+    __nv_bfloat16 *W1t = nullptr, *W2t = nullptr, *W3t = nullptr;  // tiled for the fused forward
     __nv_bfloat16 *X = nullptr, *XT = nullptr, *H1 = nullptr, *H1T = nullptr, *H2 = nullptr, *H2T = nullptr;
     __nv_bfloat16 *dZ = nullptr, *dZT = nullptr, *dH2 = nullptr, *dH2T = nullptr, *dH1 = nullptr, *dH1T = nullptr;
     float* Z = nullptr;
@@ -481,7 +469,11 @@ cudaError_t mlp_reserve(csv_mlp* n, uint32_t rows) {
 
 cudaError_t mlp_refresh(csv_mlp* n, cudaStream_t st) {
     refresh_kernel<<<(kHid * kHid + 255) / 256, 256, 0, st>>>(n->P, n->W1b, n->W2b, n->W2bT, n->W3b, n->W3bT);
-    return cudaGetLastError();
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = launch_tile_b(n->W1b, kHid, kFeatPad, n->W1t, st);
+    if (e == cudaSuccess) e = launch_tile_b(n->W2b, kHid, kHid, n->W2t, st);
+    if (e == cudaSuccess) e = launch_tile_b(n->W3b, kOut, kHid, n->W3t, st);
+    return e;
 }
 
 // Forward pass on `rows` (padded) rows of which `cnt` hold features; Z holds the logits.
@@ -508,7 +500,8 @@ void csv_mlp_destroy(csv_mlp* n) {
     DeviceGuard g(n->ctx->device);
     mlp_free_acts(n);
     for (void* p : {(void*)n->P, (void*)n->G, (void*)n->Mm, (void*)n->Vm, (void*)n->W1b, (void*)n->W2b,
-                    (void*)n->W2bT, (void*)n->W3b, (void*)n->W3bT, (void*)n->loss, (void*)n->err})
+                    (void*)n->W2bT, (void*)n->W3b, (void*)n->W3bT, (void*)n->W1t, (void*)n->W2t, (void*)n->W3t,
+                    (void*)n->loss, (void*)n->err})
         cudaFree(p);
     delete n;
 }
@@ -533,6 +526,9 @@ int csv_mlp_create(csv_ctx* ctx, const float* params, csv_mlp** out) {
     al((void**)&n->W2bT, kHid * kHid * 2);
     al((void**)&n->W3b, kOut * kHid * 2);
     al((void**)&n->W3bT, kHid * kOutPad * 2);
+    al((void**)&n->W1t, kHid * kFeatPad * 2);
+    al((void**)&n->W2t, kHid * kHid * 2);
+    al((void**)&n->W3t, kOut * kHid * 2);
     al((void**)&n->loss, 4);
     al((void**)&n->err, 4);
     if (e == cudaSuccess) e = cudaMemcpy(n->P, params, N_PARAMS * 4, cudaMemcpyHostToDevice);
@@ -564,16 +560,12 @@ int csv_mlp_forward(csv_mlp* n, const float* d_feat, uint32_t count, float* d_lo
     if (!n || (count && !d_feat)) return CSV_EINVAL;
     if (count == 0) return CSV_OK;
     DeviceGuard g(n->ctx->device);
+    if ((reinterpret_cast<uintptr_t>(d_feat) | reinterpret_cast<uintptr_t>(d_logits)) & 15u)
+        return abi_fail(n->ctx, CSV_EINVAL, "mlp forward: features and logits must be 16-byte aligned");
     cudaStream_t st = (cudaStream_t)stream;
-    const uint32_t rows = (count + 127) / 128 * 128;
-    cudaError_t e = mlp_reserve(n, rows);
-    if (e == cudaSuccess) e = mlp_forward(n, d_feat, count, rows, st);
-    if (e == cudaSuccess && d_logits)
-        e = cudaMemcpyAsync(d_logits, n->Z, (size_t)count * kOut * 4, cudaMemcpyDeviceToDevice, st);
-    if (e == cudaSuccess && d_sel) {
-        argmax_kernel<<<(count + 255) / 256, 256, 0, st>>>(n->Z, count, d_sel);
-        e = cudaGetLastError();
-    }
+    // the fused forward: features in, logits / choices out, activations on chip
+    cudaError_t e = launch_mlp_infer(d_feat, count, n->W1t, n->W2t, n->W3t, n->P + OFF_B1, n->P + OFF_B2, n->P + OFF_B3,
+                                     d_logits, d_sel, n->err, n->ctx->device, st);
     if (e != cudaSuccess) return abi_cuda_fail(n->ctx, e, "mlp forward");
     return CSV_OK;
 }

@@ -386,7 +386,8 @@ void csv_mlp_destroy(csv_mlp* net);
 /* Host copies of the parameters and of the last gradients (either may be NULL). */
 int csv_mlp_params(const csv_mlp* net, float* params, float* grads);
 /* Logits (d_logits: count x 32 fp32, optional) and the argmax choice per brick
- * (d_sel: mode | table << 4, optional) for count feature rows. */
+ * (d_sel: mode | table << 4, optional) for count feature rows, in one fused
+ * kernel (activations stay on the SM).  d_features and d_logits 16-byte aligned. */
 int csv_mlp_forward(csv_mlp* net, const float* d_features, uint32_t count, float* d_logits, uint8_t* d_sel,
                     void* stream);
 /* Forward and backward of the mean cross-entropy of both heads against

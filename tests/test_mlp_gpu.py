@@ -58,3 +58,49 @@ def test_gemm_rejects_unaligned_shapes(codec):
     B = torch.zeros((32, 64), dtype=torch.bfloat16, device="cuda")
     with pytest.raises(CsvError):
         codec.gemm_bf16(A, B, C=torch.empty((100, 32), device="cuda"))
+
+
+@pytest.mark.parametrize("count", [1, 200, 128 * 148 + 77, 70000])
+def test_fused_forward_equals_layer_by_layer_gemms(codec, count):
+    """csv_mlp_forward runs the whole network in one persistent kernel (activations stay in tensor memory and
+    shared memory, the 256 x 256 weight streams through a two-slot ring).  It issues the MMAs of the three
+    layer GEMMs in the same shapes and K order, so its logits equal, bit for bit, those of three csv_gemm_bf16
+    launches with the same bf16 rounding points; its choice is the argmax of each head (ties: the lower
+    index).  Counts cover one partial tile, more tiles than SMs, and several tiles per CTA."""
+    import torch
+    from csvb200 import SelectorNet
+    p = SelectorNet.init_params(5)
+    p[256 * 64:256 * 64 + 256] = np.random.default_rng(1).normal(0, 0.1, 256)  # non-zero b1
+    net = SelectorNet(codec, p)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(count)
+    feat = torch.rand((count, 32), device="cuda", generator=g)
+    logits = torch.empty((count, 32), device="cuda")
+    sel = torch.empty(count, dtype=torch.uint8, device="cuda")
+    net.forward(feat, d_logits=logits, d_sel=sel)
+    # the layer-by-layer reference on the same tensor cores
+    rows = (count + 127) // 128 * 128
+    P = torch.from_numpy(p).cuda()
+    o = 0
+    W1 = P[o:o + 256 * 64].view(256, 64).to(torch.bfloat16).contiguous(); o += 256 * 64
+    b1 = P[o:o + 256].contiguous(); o += 256
+    W2 = P[o:o + 256 * 256].view(256, 256).to(torch.bfloat16).contiguous(); o += 256 * 256
+    b2 = P[o:o + 256].contiguous(); o += 256
+    W3 = P[o:o + 32 * 256].view(32, 256).to(torch.bfloat16).contiguous(); o += 32 * 256
+    b3 = P[o:o + 32].contiguous()
+    X = torch.zeros((rows, 64), dtype=torch.bfloat16, device="cuda")
+    X[:count, :32] = feat.to(torch.bfloat16)
+    H1 = torch.empty((rows, 256), dtype=torch.bfloat16, device="cuda")
+    H2 = torch.empty((rows, 256), dtype=torch.bfloat16, device="cuda")
+    Z = torch.empty((rows, 32), dtype=torch.float32, device="cuda")
+    codec.gemm_bf16(X, W1, bias=b1, relu=True, Cb=H1)
+    codec.gemm_bf16(H1, W2, bias=b2, relu=True, Cb=H2)
+    codec.gemm_bf16(H2, W3, bias=b3, C=Z)
+    torch.cuda.synchronize()
+    assert torch.equal(logits, Z[:count])
+    zm, zt = Z[:count, :12], Z[:count, 12:28]
+    ref_sel = (torch.argmax(zm, 1) | (torch.argmax(zt, 1) << 4)).to(torch.uint8)
+    # torch.argmax returns the first maximal index, as the kernel's strict comparison does
+    assert torch.equal(sel, ref_sel)
+    assert net.status() == 0
+    net.close()
