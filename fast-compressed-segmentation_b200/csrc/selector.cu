@@ -169,50 +169,95 @@ __global__ void __launch_bounds__(kFThreads) features_kernel(const uint64_t* __r
         S.sorted[k] = v;
     }
     __syncthreads();
-    // full-resolution counts: one warp per row along x
+    // full-resolution counts.  Warp w takes the rows y = w, w + 8, ... and walks
+    // z with rows z .. z+4 of its y in registers (the z-neighbours), loads rows
+    // (y+1, z) and (y+4, z) for the y-neighbours, and takes the x-neighbours and
+    // the run starts from other lanes (lane l holds x = l and x = l + 32): every
+    // voxel is read three times from the cache instead of eight.
     uint32_t c[15] = {};
-    for (uint32_t row = warp; row < b * b; row += kFThreads / 32) {
-        const uint32_t y = row % b, z = row / b;
-        for (uint32_t xb = 0; xb < b; xb += 32) {
-            const uint32_t x = xb + lane;
-            const bool in = x < b;
-            const uint64_t gx = x0 + x, gy = y0 + y, gz = z0 + z;
-            const uint64_t v = in ? vox(vol, W, H, D, gx, gy, gz) : 0ull;
-            if (in) {
-                if (x + 1 < b) c[0] += v == vox(vol, W, H, D, gx + 1, gy, gz);
-                if (y + 1 < b) c[1] += v == vox(vol, W, H, D, gx, gy + 1, gz);
-                if (z + 1 < b) c[2] += v == vox(vol, W, H, D, gx, gy, gz + 1);
-                if (x + 4 < b) c[3] += v == vox(vol, W, H, D, gx + 4, gy, gz);
-                if (y + 4 < b) c[4] += v == vox(vol, W, H, D, gx, gy + 4, gz);
-                if (z + 4 < b) c[5] += v == vox(vol, W, H, D, gx, gy, gz + 4);
-                c[6] += v == 0;
+    {
+        const uint32_t nch = (b + 31) / 32;  // values per lane: 1 or 2
+        const bool interior = x0 + b <= W && y0 + b <= H && z0 + b <= D;
+        auto row = [&](uint32_t y, uint32_t z, uint64_t out[2]) {
+            if (interior) {
+                const uint64_t* base = vol + x0 + W * (y0 + y + H * (z0 + z));
+#pragma unroll
+                for (uint32_t h = 0; h < 2; ++h) {
+                    const uint32_t x = lane + 32 * h;
+                    out[h] = (h < nch && x < b) ? __ldg(base + x) : 0ull;
+                }
+            } else {
+#pragma unroll
+                for (uint32_t h = 0; h < 2; ++h) {
+                    const uint32_t x = lane + 32 * h;
+                    out[h] = (h < nch && x < b) ? vox(vol, W, H, D, x0 + x, y0 + y, z0 + z) : 0ull;
+                }
             }
-            // runs along x: a run starts where the label differs from its left neighbour
-            const uint64_t left = (in && x > 0) ? vox(vol, W, H, D, gx - 1, gy, gz) : ~v;
-            const bool start = in && (x == 0 || left != v);
-            const uint32_t smask = __ballot_sync(0xffffffffu, start);
-            if (start) {
-                // the run ends at the next start in this 32-voxel chunk, else it runs on past the chunk
-                const uint32_t after = lane == 31 ? 0u : (smask >> (lane + 1));
-                uint32_t len;
-                if (after) {
-                    len = (uint32_t)__ffs(after);
-                } else {
-                    len = min(b, xb + 32) - x;
-                    for (uint32_t xe = xb + 32; xe < b; ++xe) {
-                        if (vox(vol, W, H, D, x0 + xe, gy, gz) != v) break;
-                        ++len;
+        };
+        for (uint32_t y = warp; y < b; y += kFThreads / 32) {
+            uint64_t r[5][2];
+#pragma unroll
+            for (uint32_t k = 0; k < 5; ++k) {
+                r[k][0] = r[k][1] = 0ull;
+                if (k < b) row(y, k, r[k]);
+            }
+            for (uint32_t z = 0; z < b; ++z) {
+                uint64_t ya[2] = {0ull, 0ull}, yd[2] = {0ull, 0ull};
+                if (y + 1 < b) row(y + 1, z, ya);
+                if (y + 4 < b) row(y + 4, z, yd);
+                uint32_t start_mask[2];
+#pragma unroll
+                for (uint32_t h = 0; h < 2; ++h) {
+                    const uint32_t x = lane + 32 * h;
+                    const bool in = h < nch && x < b;
+                    const uint64_t v = r[0][h];
+                    // x + 1, x + 4 and x - 1 from the lanes that hold them (all lanes shuffle)
+                    const uint64_t nx = h == 0 ? r[0][1] : 0ull;
+                    const uint64_t d1a = __shfl_down_sync(0xffffffffu, v, 1), d1b = __shfl_sync(0xffffffffu, nx, (lane + 1) & 31);
+                    const uint64_t d4a = __shfl_down_sync(0xffffffffu, v, 4), d4b = __shfl_sync(0xffffffffu, nx, (lane + 4) & 31);
+                    const uint64_t px = h == 1 ? r[0][0] : 0ull;
+                    const uint64_t lfa = __shfl_up_sync(0xffffffffu, v, 1), lfb = __shfl_sync(0xffffffffu, px, 31);
+                    const uint64_t x1 = lane + 1 < 32 ? d1a : d1b, x4 = lane + 4 < 32 ? d4a : d4b;
+                    const uint64_t left = lane > 0 ? lfa : lfb;
+                    if (in) {
+                        if (x + 1 < b) c[0] += v == x1;
+                        if (y + 1 < b) c[1] += v == ya[h];
+                        if (z + 1 < b) c[2] += v == r[1][h];
+                        if (x + 4 < b) c[3] += v == x4;
+                        if (y + 4 < b) c[4] += v == yd[h];
+                        if (z + 4 < b) c[5] += v == r[4][h];
+                        c[6] += v == 0;
+                    }
+                    // a run starts where the label differs from its left neighbour
+                    start_mask[h] = __ballot_sync(0xffffffffu, in && (x == 0 || left != v));
+                }
+                const uint64_t starts = (uint64_t)start_mask[0] | ((uint64_t)start_mask[1] << 32);
+#pragma unroll
+                for (uint32_t h = 0; h < 2; ++h) {
+                    const uint32_t x = lane + 32 * h;
+                    if ((starts >> x) & 1ull) {
+                        // the run ends at the next start in the row, or at its end
+                        const uint64_t after = x + 1 < 64 ? starts >> (x + 1) : 0ull;
+                        const uint32_t len = after ? (uint32_t)__ffsll((long long)after) : b - x;
+                        const uint32_t bucket = len <= 1    ? 0
+                                                : len == 2  ? 1
+                                                : len <= 4  ? 2
+                                                : len <= 8  ? 3
+                                                : len <= 16 ? 4
+                                                : len <= 32 ? 5
+                                                            : 6;
+#pragma unroll
+                        for (uint32_t k = 0; k < 7; ++k) c[7 + k] += bucket == k;  // (registers, not a local array)
+                        c[14]++;
                     }
                 }
-                const uint32_t bucket = len <= 1    ? 0
-                                        : len == 2  ? 1
-                                        : len <= 4  ? 2
-                                        : len <= 8  ? 3
-                                        : len <= 16 ? 4
-                                        : len <= 32 ? 5
-                                                    : 6;
-                c[7 + bucket]++;
-                c[14]++;
+#pragma unroll
+                for (uint32_t k = 0; k < 4; ++k) {
+                    r[k][0] = r[k + 1][0];
+                    r[k][1] = r[k + 1][1];
+                }
+                r[4][0] = r[4][1] = 0ull;
+                if (z + 5 < b) row(y, z + 5, r[4]);
             }
         }
     }
