@@ -425,7 +425,7 @@ __device__ void palette_walk(const BrickCtx& B, uint64_t root, uint8_t* ops, con
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kEncThreads) enc_bricks_kernel(EncArgs A) {
+__global__ void __launch_bounds__(kEncThreads, 2) enc_bricks_kernel(EncArgs A) {
     __shared__ EncShared S;
     const uint32_t tid = threadIdx.x, T = blockDim.x;
     const EncScratch X = enc_scratch(A);
@@ -529,7 +529,7 @@ __global__ void __launch_bounds__(kEncThreads) enc_bricks_kernel(EncArgs A) {
 // Exhaustive statistics for the mode / table choice: per brick and mode, the
 // histogram of the 16 nibble values the rANS coder would see (root nibble, op
 // nibbles, Pd offsets and the pad nibble of an odd count).
-__global__ void __launch_bounds__(kEncThreads) enc_stats_kernel(EncArgs A, uint32_t* __restrict__ hist_out) {
+__global__ void __launch_bounds__(kEncThreads, 2) enc_stats_kernel(EncArgs A, uint32_t* __restrict__ hist_out) {
     __shared__ EncShared S;
     const uint32_t tid = threadIdx.x, T = blockDim.x;
     const EncScratch X = enc_scratch(A);
