@@ -444,6 +444,35 @@ int csv_encode_device(csv_ctx* ctx, const uint64_t* d_volume, uint32_t W, uint32
     return img ? CSV_OK : fail(ctx, CSV_EINVAL, "encode produced no image");
 }
 
+int csv_encode_shard_bricks(csv_ctx* ctx, const uint64_t* d_slab, uint32_t W, uint32_t H, uint32_t D,
+                            uint32_t brick_size, uint32_t bx0, uint32_t index_base, uint64_t* hist, void* stream) {
+    if (!ctx || !hist) return CSV_EINVAL;
+    if (brick_size < 2 || brick_size > 64 || (brick_size & (brick_size - 1)))
+        return fail(ctx, CSV_EINVAL, "brick size must be a power of two in [2, 64]");
+    if ((uint64_t)W * H * D > 0 && !d_slab) return fail(ctx, CSV_EINVAL, "null volume");
+    if ((uint64_t)bx0 + (W + brick_size - 1) / brick_size > 1024)
+        return fail(ctx, CSV_ERANGE, "brick x beyond 1023 (10-bit Morton brick IDs, utils.cpp:10-14)");
+    DeviceGuard g(ctx->device);
+    if (!ctx->enc) ctx->enc = encoder_state_new();
+    std::string err;
+    EncodeShard sh;
+    sh.bx0 = bx0;
+    sh.index_base = index_base;
+    int rc = encode_device(ctx->enc, ctx->device, d_slab, W, H, D, brick_size, (cudaStream_t)stream, err, nullptr, &sh,
+                           hist);
+    return rc ? fail(ctx, rc, err) : CSV_OK;
+}
+
+int csv_encode_shard_finish(csv_ctx* ctx, const uint64_t* hist, void* stream, size_t* image_len) {
+    if (!ctx || !hist || !image_len) return CSV_EINVAL;
+    DeviceGuard g(ctx->device);
+    std::string err;
+    int rc = finish_encode_shard(ctx->enc, hist, (cudaStream_t)stream, err);
+    if (rc) return fail(ctx, rc, err);
+    const uint8_t* img = encoder_image(ctx->enc, image_len);
+    return img ? CSV_OK : fail(ctx, CSV_EINVAL, "encode produced no image");
+}
+
 int csv_encoded_image(csv_ctx* ctx, const uint8_t** d_image, size_t* len) {
     if (!ctx || !d_image || !len) return CSV_EINVAL;
     const uint8_t* p = encoder_image(ctx->enc, len);

@@ -128,8 +128,19 @@ struct EncodeSelection {
     uint32_t freq[16][16] = {};      // each table's frequencies (each >= 1, sum 4096)
     const uint8_t* d_sel = nullptr;  // per brick, device: mode | table << 4 (null: mode 0, table 0)
 };
+// One x-slab of a larger volume, encoded by one rank: brick x-offset (IDs) and
+// the file index of its first brick (the model's every-512th sample rule).
+struct EncodeShard {
+    uint32_t bx0 = 0;
+    uint32_t index_base = 0;
+};
+// With hist_out, stops after the brick pass and returns the 16-bin histogram of
+// the sampled bricks; finish_encode_shard then builds the image from the
+// histogram summed over every shard (version 1 only).
 int encode_device(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W, uint64_t H, uint64_t D, uint32_t b,
-                  cudaStream_t st, std::string& err, const EncodeSelection* sel = nullptr);
+                  cudaStream_t st, std::string& err, const EncodeSelection* sel = nullptr,
+                  const EncodeShard* shard = nullptr, uint64_t* hist_out = nullptr);
+int finish_encode_shard(EncoderState* s, const uint64_t hist[16], cudaStream_t st, std::string& err);
 int encode_stats(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W, uint64_t H, uint64_t D, uint32_t b,
                  uint32_t* d_hist, cudaStream_t st, std::string& err);
 int encoder_to_dataset(EncoderState* s, DeviceDataset& d, std::string& err);

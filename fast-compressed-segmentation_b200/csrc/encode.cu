@@ -63,6 +63,7 @@ struct EncoderState {
     int device = 0;
     uint32_t b = 0, L = 0, nb = 0, S = kOpsPerCheckpoint;
     uint64_t ck_used = 0;  // checkpoints of the last encode (pool entries in use)
+    bool bricks_done = false;  // a shard's K1 ran; finish_encode_shard completes the image
     uint64_t W = 0, H = 0, D = 0;
     // buffers (grow-only)
     EncMeta* d_meta = nullptr;
@@ -191,6 +192,8 @@ struct EncArgs {
     uint64_t pal_cap;
     Checkpoint* ck;     // checkpoint pool, reserved per brick at misc[kMiscCk]
     uint64_t ck_cap;    // pool entries
+    uint32_t bx0;         // brick-x offset of this volume in a larger one (brick IDs)
+    uint32_t index_base;  // file index of brick 0 in the larger volume (the model's sample rule)
     unsigned long long* misc;
     const uint8_t* sel;  // per brick: mode | table << 4 (null: mode 0, table 0)
 };
@@ -489,7 +492,7 @@ __global__ void __launch_bounds__(kEncThreads, 2) enc_bricks_kernel(EncArgs A) {
             const uint64_t nib_off = S.nib_off, pal_off = S.pal_off;
             // the rANS kernel reads whole 16-byte chunks of the reservation
             const bool ok = nib_off + ((nbytes + 15) & ~15u) <= A.nib_cap && pal_off + P <= A.pal_cap && ck_ok;
-            const bool sample = (i % 512) == 0;  // brickEncoding.hpp:482
+            const bool sample = ((A.index_base + i) % 512) == 0;  // brickEncoding.hpp:482
             for (uint32_t q = tid; q < nbytes; q += T) {
                 const uint32_t hi = nib[2 * q], lo = (2 * q + 1 < nsym) ? nib[2 * q + 1] : 0u;
                 if (ok) A.nib_pool[nib_off + q] = (uint8_t)((hi << 4) | lo);
@@ -511,7 +514,7 @@ __global__ void __launch_bounds__(kEncThreads, 2) enc_bricks_kernel(EncArgs A) {
                 m.nsym = nsym;
                 m.nbytes = nbytes;
                 m.n_ops = n_ops;
-                m.id = morton3(bx, by, bz);
+                m.id = morton3(bx + A.bx0, by, bz);
                 m.flags = (root_const ? EF_UNIFORM : 0u) | (ok ? 0u : EF_OVERFLOW);
                 m.n_ck = n_ck;
                 m.E = 0;
@@ -848,8 +851,21 @@ int encode_stats(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W,
     return CSV_OK;
 }
 
+#define CK(x)                                                              \
+    do {                                                                   \
+        if ((e = (x)) != cudaSuccess) {                                    \
+            err = std::string(#x) + ": " + cudaGetErrorString(e);          \
+            return CSV_ECUDA;                                              \
+        }                                                                  \
+    } while (0)
+
+// K3 + K4 (and the model) after K1: the model from the sample histogram in
+// misc[2..17] (or the selection's tables), then the rANS pass and the image.
+static int finish_encode(EncoderState* s, const EncodeSelection* sel, cudaStream_t st, std::string& err);
+
 int encode_device(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W, uint64_t H, uint64_t D, uint32_t b,
-                  cudaStream_t st, std::string& err, const EncodeSelection* sel) {
+                  cudaStream_t st, std::string& err, const EncodeSelection* sel, const EncodeShard* shard,
+                  uint64_t* hist_out) {
     s->valid = false;
     s->device = device;
     s->b = b;
@@ -865,19 +881,15 @@ int encode_device(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W
     s->nb = nb;
     const uint64_t nvox = W * H * D;
     cudaError_t e;
-#define CK(x)                                                              \
-    do {                                                                   \
-        if ((e = (x)) != cudaSuccess) {                                    \
-            err = std::string(#x) + ": " + cudaGetErrorString(e);          \
-            return CSV_ECUDA;                                              \
-        }                                                                  \
-    } while (0)
     {
         int rc = check_tables(sel, err);
         if (rc) return rc;
     }
-    const uint32_t n_tables = sel ? sel->n_tables : 0;
-    const bool v2 = n_tables > 0;
+    if (hist_out && sel && sel->n_tables) {
+        err = "a shard encodes version-1 images only";
+        return CSV_EINVAL;
+    }
+    s->bricks_done = false;
     CK(grow(&s->d_meta, &s->meta_cap, nb));
     if (!s->d_model) CK(cudaMalloc(&s->d_model, kMaxTables * kModelWords * sizeof(uint32_t)));
     {
@@ -918,6 +930,8 @@ int encode_device(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W
         A.ck_cap = s->ck_cap_total;
         A.misc = s->d_misc;
         A.sel = sel ? sel->d_sel : nullptr;
+        A.bx0 = shard ? shard->bx0 : 0u;
+        A.index_base = shard ? shard->index_base : 0u;
         if (nb > 0) {
             enc_bricks_kernel<<<grid, kEncThreads, 0, st>>>(A);
             CK(cudaGetLastError());
@@ -935,6 +949,36 @@ int encode_device(EncoderState* s, int device, const uint64_t* d_vol, uint64_t W
         pal_need = std::max<size_t>(pal_need, misc[1]);
         ck_need = std::max<size_t>(ck_need, misc[kMiscCk]);
     }
+    if (hist_out) {  // a shard: stop here with the sample histogram; finish_encode_shard completes it
+        unsigned long long h[16];
+        CK(cudaMemcpyAsync(h, s->d_misc + 2, sizeof h, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (int k = 0; k < 16; ++k) hist_out[k] = h[k];
+        s->bricks_done = true;
+        return CSV_OK;
+    }
+    return finish_encode(s, sel, st, err);
+}
+
+int finish_encode_shard(EncoderState* s, const uint64_t hist[16], cudaStream_t st, std::string& err) {
+    if (!s || !s->bricks_done) {
+        err = "no encoder shard waiting for its model on this context";
+        return CSV_EINVAL;
+    }
+    cudaError_t e;
+    unsigned long long h[16];
+    for (int k = 0; k < 16; ++k) h[k] = hist[k];
+    CK(cudaMemcpyAsync(s->d_misc + 2, h, sizeof h, cudaMemcpyHostToDevice, st));
+    s->bricks_done = false;
+    return finish_encode(s, nullptr, st, err);
+}
+
+static int finish_encode(EncoderState* s, const EncodeSelection* sel, cudaStream_t st, std::string& err) {
+    cudaError_t e;
+    const uint32_t nb = s->nb, b = s->b;
+    const uint32_t n_tables = sel ? sel->n_tables : 0;
+    const bool v2 = n_tables > 0;
+    const int device = s->device;
     std::vector<uint32_t> models(kMaxTables * kModelWords, 0);
     if (v2) {  // the caller's shared tables
         for (uint32_t t = 0; t < n_tables; ++t) table_model(sel->freq[t], &models[t * kModelWords]);

@@ -124,6 +124,9 @@ def load_library() -> C.CDLL:
     L.csv_encode_device.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, vp,
                                     C.POINTER(C.c_size_t)]
     L.csv_encoded_image.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_size_t)]
+    L.csv_encode_shard_bricks.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                          C.c_uint32, u64p, vp]
+    L.csv_encode_shard_finish.argtypes = [vp, u64p, vp, C.POINTER(C.c_size_t)]
     L.csv_open.argtypes = [vp, u8p, C.c_size_t, C.POINTER(vp)]
     L.csv_open_encoded.argtypes = [vp, C.POINTER(vp)]
     L.csv_dataset_info_get.argtypes = [vp, C.POINTER(_Info)]
@@ -300,6 +303,25 @@ class Codec:
         n = C.c_size_t()
         self._check(self.lib.csv_encode_device(self.handle, C.c_void_p(d_volume.data_ptr()), W, H, D, brick_size,
                                                C.c_void_p(_stream_handle(stream)), C.byref(n)))
+        return n.value
+
+    def encode_shard_bricks(self, d_slab, brick_size: int, bx0: int, index_base: int, stream=None) -> np.ndarray:
+        """First step of a sharded encode (csv_encode_shard_bricks): the slab's bricks; returns the 16-bin histogram
+        (uint64) of its bricks whose file index is a multiple of 512."""
+        D, H, W = d_slab.shape
+        hist = np.zeros(16, np.uint64)
+        self._check(self.lib.csv_encode_shard_bricks(self.handle, C.c_void_p(d_slab.data_ptr()), W, H, D, brick_size,
+                                                     bx0, index_base, hist.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                                     C.c_void_p(_stream_handle(stream))))
+        return hist
+
+    def encode_shard_finish(self, hist, stream=None) -> int:
+        """Second step (csv_encode_shard_finish): the model from the histogram summed over all shards, then this
+        shard's image (header + its records); returns the image length."""
+        h = np.ascontiguousarray(hist, np.uint64)
+        n = C.c_size_t()
+        self._check(self.lib.csv_encode_shard_finish(self.handle, h.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                                     C.c_void_p(_stream_handle(stream)), C.byref(n)))
         return n.value
 
     def encoded_image(self):

@@ -100,6 +100,25 @@ int csv_encode_device(csv_ctx* ctx, const uint64_t* d_volume, uint32_t W, uint32
                       uint32_t brick_size, void* stream, size_t* image_len);
 int csv_encoded_image(csv_ctx* ctx, const uint8_t** d_image, size_t* len);
 
+/* No counterpart in the reference: one rank's part of a volume split into
+ * x-slabs of whole bricks (the split order puts bx outermost, brick.hpp:152-154,
+ * so a slab is a contiguous range of file indices).  The only exchange step of
+ * the encoder is the rANS model: it comes from the bricks whose file index is a
+ * multiple of 512 (brickEncoding.hpp:481-482), wherever they live.
+ *   1. csv_encode_shard_bricks: the slab (d_slab: W x H x D, x fastest, W the
+ *      slab's width) with its first brick at x-brick bx0 of the whole volume and
+ *      file index index_base; returns hist[16], the nibble histogram of its
+ *      sampled bricks.
+ *   2. the caller sums hist over the ranks (an all-reduce);
+ *   3. csv_encode_shard_finish: the model from the summed histogram, then the
+ *      slab's image (header + its brick records, as csv_encode_device leaves it).
+ * The whole file is the header with numBricks set to the total, then every
+ * rank's records in rank order: byte-identical to csv_encode of the whole
+ * volume (csvb200/dist.py runs the protocol over torch.distributed). */
+int csv_encode_shard_bricks(csv_ctx* ctx, const uint64_t* d_slab, uint32_t W, uint32_t H, uint32_t D,
+                            uint32_t brick_size, uint32_t bx0, uint32_t index_base, uint64_t* hist, void* stream);
+int csv_encode_shard_finish(csv_ctx* ctx, const uint64_t* hist, void* stream, size_t* image_len);
+
 /* ---- dataset -----------------------------------------------------------
  * loadDatasetFromFile (fileIO.cpp:101-182) / loadDatasetFromArrayBuffer
  * (web/scripts/datasetLoader.js:39-146): parse a .csbd v1 image, stage

@@ -295,10 +295,16 @@ int or_encode(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b, uin
     return or_encode_sel(vol, W, H, D, b, NULL, NULL, 0, out, out_len);
 }
 
-/* The same with a per-brick mode and table (sel: mode | table << 4, or NULL);
- * n_tables > 0 writes version 2 with those tables (freq, n_tables x 16). */
-int or_encode_sel(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b, const uint8_t* sel,
-                  const uint32_t* tables, uint32_t n_tables, uint8_t** out, size_t* out_len) {
+/* The whole encoder with its options: per-brick mode and table (sel: mode |
+ * table << 4, or NULL; n_tables > 0 writes version 2 with those tables, freq,
+ * n_tables x 16), and the shard of a larger volume this volume is (its first
+ * brick at x-brick bx0 and file index index_base: brick IDs and the
+ * every-512th sample rule use the whole volume's numbering).  hist_out (or
+ * NULL) receives the sample histogram of these bricks; hist_in (or NULL)
+ * replaces it when the model is built (the histogram summed over all shards). */
+static int encode_core(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b, const uint8_t* sel,
+                       const uint32_t* tables, uint32_t n_tables, uint32_t bx0, uint32_t index_base,
+                       const uint64_t* hist_in, uint64_t* hist_out, uint8_t** out, size_t* out_len) {
     if (b < 2 || (b & (b - 1)) || b > 1024) return -1;
     size_t nbx = (W + b - 1) / b, nby = (H + b - 1) / b, nbz = (D + b - 1) / b;
     size_t nb = nbx * nby * nbz;
@@ -321,22 +327,23 @@ int or_encode_sel(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b,
                 cut_brick(vol, W, H, D, b, bx, by, bz, lab + level_off(L - 1));
                 build_pyramid(b, lab, cst);
                 encode_brick(b, lab, cst, &e, sel ? (sel[i] & 15u) : 0u);
-                ids[i] = or_morton3((uint32_t)bx, (uint32_t)by, (uint32_t)bz);
+                ids[i] = or_morton3((uint32_t)bx + bx0, (uint32_t)by, (uint32_t)bz);
                 pals[i] = (uint64_t*)malloc(8 * (size_t)e.np);
                 memcpy(pals[i], e.pal, 8 * (size_t)e.np);
                 npal[i] = e.np;
                 nibs[i] = (uint8_t*)malloc(e.nn + 1);
                 memcpy(nibs[i], e.nib, e.nn);
                 nnib[i] = e.nn;
-                if (i % 512 == 0) { /* brickEncoding.hpp:482, brickEncoding.cpp:131-143 */
+                if ((index_base + i) % 512 == 0) { /* brickEncoding.hpp:482, brickEncoding.cpp:131-143 */
                     for (uint32_t k = 0; k < e.nn; ++k) hist[e.nib[k]]++;
                     if (e.nn & 1) hist[0]++; /* the pad nibble of the last byte */
                 }
             }
     uint32_t tf[16][16], tc[16][17];
     const uint32_t nt = n_tables ? n_tables : 1;
+    if (hist_out) memcpy(hist_out, hist, sizeof hist);
     if (n_tables == 0) {
-        or_build_model(hist, tf[0], tc[0]);
+        or_build_model(hist_in ? hist_in : hist, tf[0], tc[0]);
     } else {
         for (uint32_t t = 0; t < n_tables; ++t) {
             uint32_t acc = 0;
@@ -382,6 +389,16 @@ int or_encode_sel(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b,
     *out = o.p;
     *out_len = o.n;
     return 0;
+}
+
+int or_encode_sel(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b, const uint8_t* sel,
+                  const uint32_t* tables, uint32_t n_tables, uint8_t** out, size_t* out_len) {
+    return encode_core(vol, W, H, D, b, sel, tables, n_tables, 0, 0, NULL, NULL, out, out_len);
+}
+
+int or_encode_shard(const uint64_t* slab, size_t W, size_t H, size_t D, uint32_t b, uint32_t bx0, uint32_t index_base,
+                    const uint64_t* hist_in, uint64_t* hist_out, uint8_t** out, size_t* out_len) {
+    return encode_core(slab, W, H, D, b, NULL, NULL, 0, bx0, index_base, hist_in, hist_out, out, out_len);
 }
 
 /* ------------------------------------------------------------- decoding */

@@ -120,6 +120,13 @@ void or_serve_free(or_server* s);
  * frequencies); n_tables == 0 writes version 1 with the dataset's model. */
 int or_encode_sel(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b, const uint8_t* sel,
                   const uint32_t* tables, uint32_t n_tables, uint8_t** out, size_t* out_len);
+/* One x-slab of a larger volume (first brick at x-brick bx0, file index
+ * index_base): hist_out receives the sample histogram of its bricks (the
+ * every-512th rule in whole-volume numbering); hist_in, when given, is the
+ * histogram the model is built from (summed over every slab).  The image holds
+ * the slab's bricks only. */
+int or_encode_shard(const uint64_t* slab, size_t W, size_t H, size_t D, uint32_t b, uint32_t bx0, uint32_t index_base,
+                    const uint64_t* hist_in, uint64_t* hist_out, uint8_t** out, size_t* out_len);
 
 /* The mode / table selector (csv_oracle_select.c). */
 int or_encode_stats(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b, uint32_t* hist);

@@ -51,6 +51,8 @@ class Oracle:
         L.or_build_model.argtypes = [_u64p, _u32p, _u32p]
         L.or_encode.argtypes = [_u64p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_uint32,
                                 C.POINTER(_u8p), C.POINTER(C.c_size_t)]
+        L.or_encode_shard.argtypes = [_u64p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_uint32, C.c_uint32, C.c_uint32,
+                                      _u64p, _u64p, C.POINTER(_u8p), C.POINTER(C.c_size_t)]
         L.or_pyramid.argtypes = [_u64p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_uint32, C.c_uint32,
                                  _u64p, _u8p]
         L.or_rans_decode.argtypes = [_u32p, _u32p, C.c_uint32, _u8p, C.c_uint32, C.c_uint32, _u8p]
@@ -199,6 +201,23 @@ class Oracle:
         c = np.zeros(17, np.uint32)
         self.lib.or_build_model(_ptr(raw, _u64p), _ptr(f, _u32p), _ptr(c, _u32p))
         return f, c
+
+    def encode_shard(self, slab: np.ndarray, brick: int, bx0: int, index_base: int, hist_in=None):
+        """One x-slab of a larger volume (or_encode_shard): (image of its bricks, sample histogram)."""
+        v = np.ascontiguousarray(slab, dtype=np.uint64)
+        D, H, W = v.shape
+        out = _u8p()
+        n = C.c_size_t()
+        h_out = np.zeros(16, np.uint64)
+        h_in = None if hist_in is None else np.ascontiguousarray(hist_in, np.uint64)
+        rc = self.lib.or_encode_shard(_ptr(v, _u64p), W, H, D, brick, bx0, index_base,
+                                      None if h_in is None else _ptr(h_in, _u64p), _ptr(h_out, _u64p),
+                                      C.byref(out), C.byref(n))
+        if rc:
+            raise RuntimeError("oracle shard encode failed")
+        data = C.string_at(out, n.value)
+        self.lib.or_free(out)
+        return data, h_out
 
     def encode(self, vol: np.ndarray, brick: int) -> bytes:
         """vol has shape (D, H, W) in C order, i.e. x fastest."""

@@ -101,3 +101,24 @@ def test_encoder_seek_index_decodes_every_lod(codec, oracle):
         assert (st.cpu().numpy() == 0).all()
         assert np.array_equal(out.cpu().numpy().view(np.uint64).reshape(nb, per), ref), t
     ds.close()
+
+
+@pytest.mark.parametrize("shards", [2, 3])
+def test_sharded_encode_on_the_device_equals_whole(codec, shards):
+    """csv_encode_shard_bricks / csv_encode_shard_finish, one context per x-slab (as one rank each would run
+    them): the slabs' records behind one header with the summed sample histogram's model are the whole-volume
+    image byte for byte (1536 bricks, so that the every-512th sample falls on several slabs)."""
+    from csvb200 import Codec
+    from csvb200.dist import DeviceShardEncoder, assemble, slab_of, slab_ranges
+    b = 8
+    vol = _device_volume(codec, (64, 64, 192), 1, n_cells=200, n_tubes=40, r_min=1.0, r_max=5.0, zero_frac=0.1,
+                         seed=91)
+    codec.encode_device(vol, b)
+    whole = bytes(codec.encoded_image_tensor().cpu().numpy())
+    D, H, W = vol.shape
+    nyz = -(-H // b) * -(-D // b)
+    encs = [DeviceShardEncoder(Codec(0)) for _ in range(shards)]
+    ranges = slab_ranges(W, b, shards)
+    hists = [e.bricks(slab_of(vol, b, bx0, bx1), b, bx0, bx0 * nyz) for e, (bx0, bx1) in zip(encs, ranges)]
+    total = np.sum(hists, axis=0).astype(np.uint64)
+    assert assemble([e.finish(total) for e in encs]) == whole
