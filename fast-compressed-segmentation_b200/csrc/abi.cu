@@ -10,6 +10,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <new>
 #include <string>
 #include <vector>
@@ -831,6 +832,86 @@ int csv_render(csv_ctx* ctx, const csv_camera* camera, uint32_t width, uint32_t 
     cudaError_t e = launch_render(*camera, width, height, grid_size, brick_size, bricks_per_axis, d_slots, n_slots,
                                   d_labels, d_hidden, n_hidden, d_label_out, d_depth_out, d_requests,
                                   (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "render launch");
+    return CSV_OK;
+}
+
+int csv_lighting_default(double light_angle_deg, csv_lighting* out) {
+    if (!out) return CSV_EINVAL;
+    // webgpuSetup.js:24-31 (defaults) and :205-219 (the uniform): the light on a
+    // west-east arc at a fixed elevation, ambient 0.5, diffuse 0.8
+    const double a = light_angle_deg * 3.14159265358979323846 / 180.0;
+    memset(out, 0, sizeof *out);
+    out->light_dir[0] = (float)sin(a);
+    out->light_dir[1] = 0.6f;
+    out->light_dir[2] = (float)-cos(a);
+    out->ambient = 0.5f;
+    out->diffuse = 0.8f;
+    return CSV_OK;
+}
+
+int csv_transfer_function(const csv_dataset* ds, const uint64_t* hidden, uint32_t n_hidden, uint64_t* keys,
+                          uint32_t* rgba, uint32_t cap, uint32_t* n_out) {
+    if (!ds || !n_out || (n_hidden && !hidden)) return CSV_EINVAL;
+    DeviceGuard g(ds->ctx->device);
+    // buildTransferFunctionBuffers (webgpuSetup.js:389-465): every distinct non-zero
+    // palette label of the dataset, ascending; entry i gets hue 137.5 i (golden
+    // angle), saturation, lightness and opacity cycling with i, HSL -> RGB
+    // (hslToRgb, :490-515), RGB scaled by 0.92 for lighting headroom
+    std::vector<uint64_t> pal(ds->d.pal_pool_entries);
+    if (!pal.empty()) {
+        cudaError_t e = cudaMemcpy(pal.data(), ds->d.d_pal, 8 * pal.size(), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_fail(ds->ctx, e, "palette copy");
+    }
+    std::sort(pal.begin(), pal.end());
+    pal.erase(std::unique(pal.begin(), pal.end()), pal.end());
+    if (!pal.empty() && pal[0] == 0) pal.erase(pal.begin());
+    *n_out = (uint32_t)pal.size();
+    if (pal.size() > cap || (!pal.empty() && (!keys || !rgba)))
+        return fail(ds->ctx, CSV_ERANGE, "transfer function: " + std::to_string(pal.size()) + " labels, room for " +
+                                             std::to_string(cap));
+    std::vector<uint64_t> hid(hidden, hidden + n_hidden);
+    std::sort(hid.begin(), hid.end());
+    auto js_round = [](double x) { return floor(x + 0.5); };  // Math.round
+    for (size_t i = 0; i < pal.size(); ++i) {
+        const double h = fmod((double)i * 137.5, 360.0);
+        const double sat = 0.55 + (double)(i % 3) * 0.08, lig = 0.35 + (double)(i % 4) * 0.05;
+        const double op = 0.25 + (double)(i % 5) * 0.08;
+        const double c = (1 - fabs(2 * lig - 1)) * sat;
+        const double x = c * (1 - fabs(fmod(h / 60, 2) - 1));
+        const double m = lig - c / 2;
+        double r, gg, b;
+        if (h < 60) { r = c; gg = x; b = 0; }
+        else if (h < 120) { r = x; gg = c; b = 0; }
+        else if (h < 180) { r = 0; gg = c; b = x; }
+        else if (h < 240) { r = 0; gg = x; b = c; }
+        else if (h < 300) { r = x; gg = 0; b = c; }
+        else { r = c; gg = 0; b = x; }
+        const double rr = js_round((r + m) * 255), rg = js_round((gg + m) * 255), rb = js_round((b + m) * 255);
+        const uint32_t R = (uint32_t)std::min(floor(rr * 0.92), 255.0), G = (uint32_t)std::min(floor(rg * 0.92), 255.0),
+                       B = (uint32_t)std::min(floor(rb * 0.92), 255.0), A = (uint32_t)floor(op * 255);
+        keys[i] = pal[i];
+        // a hidden label is transparent (rebuildLabelColors, webgpuSetup.js:826-834)
+        rgba[i] = std::binary_search(hid.begin(), hid.end(), pal[i]) ? 0u : (R | (G << 8) | (B << 16) | (A << 24));
+    }
+    return CSV_OK;
+}
+
+int csv_render_rgba(csv_ctx* ctx, const csv_camera* camera, uint32_t width, uint32_t height, float grid_size,
+                    uint32_t brick_size, uint32_t bricks_per_axis, const csv_brick_slot* d_slots, uint64_t n_slots,
+                    const uint64_t* d_labels, const uint64_t* d_tf_keys, const uint32_t* d_tf_rgba, uint32_t n_tf,
+                    const csv_lighting* lighting, uint32_t* d_rgba_out, uint32_t* d_requests, void* stream) {
+    if (!ctx || !camera || !lighting) return CSV_EINVAL;
+    if (width == 0 || height == 0) return CSV_OK;
+    if (!d_rgba_out || (n_slots && (!d_slots || !d_labels)) || (n_tf && (!d_tf_keys || !d_tf_rgba)))
+        return fail(ctx, CSV_EINVAL, "null render buffer");
+    if (brick_size < 1 || brick_size > 1024 || (brick_size & (brick_size - 1)))
+        return fail(ctx, CSV_EINVAL, "brick size must be a power of two");
+    if (bricks_per_axis > 1024) return fail(ctx, CSV_ERANGE, "more than 1024 bricks per axis");
+    DeviceGuard g(ctx->device);
+    cudaError_t e = launch_render_rgba(*camera, width, height, grid_size, brick_size, bricks_per_axis, d_slots, n_slots,
+                                       d_labels, d_tf_keys, d_tf_rgba, n_tf, lighting->light_dir, lighting->ambient,
+                                       lighting->diffuse, d_rgba_out, d_requests, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "render launch");
     return CSV_OK;
 }

@@ -153,6 +153,10 @@ cudaError_t launch_render(const csv_camera& cam, uint32_t W, uint32_t H, float g
                           const csv_brick_slot* slots, uint64_t n_slots, const uint64_t* labels, const uint64_t* hidden,
                           uint32_t n_hidden, uint64_t* out_label, float* out_depth, uint32_t* requests,
                           cudaStream_t st);
+cudaError_t launch_render_rgba(const csv_camera& cam, uint32_t W, uint32_t H, float grid, uint32_t bs, uint32_t bpa,
+                               const csv_brick_slot* slots, uint64_t n_slots, const uint64_t* labels,
+                               const uint64_t* tf_keys, const uint32_t* tf_rgba, uint32_t n_tf, const float* light,
+                               float ambient, float diffuse, uint32_t* out_rgba, uint32_t* requests, cudaStream_t st);
 
 size_t gemm_smem_bytes();
 // B [N][K] bf16 -> the tensor cores' no-swizzle K-major core-matrix tiling (K-chunks of 64).

@@ -143,6 +143,10 @@ def load_library() -> C.CDLL:
                                       C.POINTER(C.c_float)]
     L.csv_render.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_float, C.c_uint32, C.c_uint32, vp, C.c_uint64, vp,
                              vp, C.c_uint32, vp, vp, vp, vp]
+    L.csv_lighting_default.argtypes = [C.c_double, C.POINTER(Lighting)]
+    L.csv_transfer_function.argtypes = [vp, u64p, C.c_uint32, u64p, u32p, C.c_uint32, C.POINTER(C.c_uint32)]
+    L.csv_render_rgba.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_float, C.c_uint32, C.c_uint32, vp, C.c_uint64,
+                                  vp, vp, vp, C.c_uint32, C.POINTER(Lighting), vp, vp, vp]
     L.csv_synth_volume.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_uint32, C.c_uint32,
                                    C.c_float, C.c_float, C.c_float, C.c_uint64, vp]
     L.csv_serve_create.argtypes = [vp, vp, C.POINTER(ServeConfig), u64p, C.c_uint32, C.POINTER(vp)]
@@ -184,6 +188,14 @@ def _stream_handle(stream) -> int | None:
     if isinstance(stream, int):
         return stream
     return stream.cuda_stream
+
+
+class Lighting(C.Structure):
+    """csv_lighting: direction towards the light (unnormalised), ambient and diffuse strengths."""
+    _fields_ = [("light_dir", C.c_float * 3), ("ambient", C.c_float), ("diffuse", C.c_float), ("pad", C.c_float * 3)]
+
+    def as_array(self):
+        return np.array(list(self.light_dir) + [self.ambient, self.diffuse], np.float32)
 
 
 @dataclass
@@ -427,6 +439,43 @@ class Codec:
             C.c_void_p(d_hidden.data_ptr() if d_hidden is not None else None),
             0 if d_hidden is None else d_hidden.numel(), C.c_void_p(d_label_out.data_ptr()),
             C.c_void_p(d_depth_out.data_ptr()),
+            C.c_void_p(d_requests.data_ptr() if d_requests is not None else None),
+            C.c_void_p(_stream_handle(stream))))
+
+    def lighting(self, light_angle_deg: float = 25.0) -> Lighting:
+        """The viewer's default lighting for a light at this angle on its west-east arc (csv_lighting_default)."""
+        li = Lighting()
+        self._check(self.lib.csv_lighting_default(light_angle_deg, C.byref(li)))
+        return li
+
+    def transfer_function(self, ds, hidden=None):
+        """(keys uint64, rgba uint32) of the dataset's labels (csv_transfer_function); hidden labels transparent."""
+        hid = np.ascontiguousarray(hidden if hidden is not None else np.zeros(1, np.uint64), np.uint64)
+        nh = 0 if hidden is None else len(hidden)
+        n = C.c_uint32()
+        self.lib.csv_transfer_function(ds.handle, hid.ctypes.data_as(C.POINTER(C.c_uint64)), nh, None, None, 0,
+                                       C.byref(n))
+        keys = np.zeros(max(n.value, 1), np.uint64)
+        cols = np.zeros(max(n.value, 1), np.uint32)
+        self._check(self.lib.csv_transfer_function(ds.handle, hid.ctypes.data_as(C.POINTER(C.c_uint64)), nh,
+                                                   keys.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                                   cols.ctypes.data_as(C.POINTER(C.c_uint32)), n.value, C.byref(n)))
+        return keys[:n.value], cols[:n.value]
+
+    def render_rgba(self, cam16, width: int, height: int, grid_size: float, brick_size: int, bricks_per_axis: int,
+                    d_slots, d_labels, d_tf_keys, d_tf_rgba, lighting: Lighting, d_rgba_out, d_requests=None,
+                    stream=None):
+        """RGBA8 image (csv_render_rgba) through the transfer function (device tensors d_tf_keys uint64 /
+        d_tf_rgba int32 or uint32) with the given lighting."""
+        from .camera import camera_struct
+        cam = camera_struct(cam16)
+        n_slots = d_slots.numel() * d_slots.element_size() // 16
+        n_tf = d_tf_keys.numel() if d_tf_keys is not None else 0
+        self._check(self.lib.csv_render_rgba(
+            self.handle, C.byref(cam), width, height, grid_size, brick_size, bricks_per_axis,
+            C.c_void_p(d_slots.data_ptr()), n_slots, C.c_void_p(d_labels.data_ptr()),
+            C.c_void_p(d_tf_keys.data_ptr() if n_tf else None), C.c_void_p(d_tf_rgba.data_ptr() if n_tf else None),
+            n_tf, C.byref(lighting), C.c_void_p(d_rgba_out.data_ptr()),
             C.c_void_p(d_requests.data_ptr() if d_requests is not None else None),
             C.c_void_p(_stream_handle(stream))))
 

@@ -249,6 +249,40 @@ int csv_render(csv_ctx* ctx, const csv_camera* camera, uint32_t width, uint32_t 
                const uint64_t* d_labels, const uint64_t* d_hidden, uint32_t n_hidden, uint64_t* d_label_out,
                float* d_depth_out, uint32_t* d_requests, void* stream);
 
+/* The shader's colour path on the same traversal (rayTrace.wgsl:565-906 with
+ * getVoxelColor's colours): every sample's label is coloured by the transfer
+ * function (d_tf_keys sorted ascending with their RGBA8 d_tf_rgba, as
+ * csv_transfer_function builds them; a label not in it takes hashLabel's
+ * colour, decode.wgsl:135-172; label 0 is transparent), composited front to
+ * back with the LOD opacity correction, shaded above alpha 0.35 by the
+ * LOD-strided alpha gradient, the diffuse light and, above 0.4, a 64-step
+ * shadow ray; the ray stops at alpha 0.95.  d_rgba_out: width x height RGBA8
+ * (r | g << 8 | b << 16 | a << 24).  Differences from the shader: a brick at
+ * LOD 0 is coloured by the transfer function of its label (the shader reads
+ * the label's low bytes as a colour, rayTrace.wgsl:165-177), and samples in
+ * bricks that are not resident have alpha 0.  Floating point follows the
+ * CPU restatement's order without fused multiply-add; powf and expf are
+ * CUDA's, so images agree with it to rounding. */
+typedef struct csv_lighting {
+    float light_dir[3]; /* towards the light (unnormalised) */
+    float ambient;
+    float diffuse;
+    float pad[3];
+} csv_lighting;
+/* The viewer's default lighting (webgpuSetup.js:24-31, 205-219) for a light
+ * at angle `light_angle_deg` on its west-east arc (25 by default). */
+int csv_lighting_default(double light_angle_deg, csv_lighting* out);
+/* buildTransferFunctionBuffers (webgpuSetup.js:389-465) on a dataset: its
+ * distinct non-zero palette labels ascending (host keys) and their RGBA8
+ * (host rgba); labels in `hidden` (host, any order) get 0.  *n receives the
+ * count; CSV_ERANGE when it exceeds cap. */
+int csv_transfer_function(const csv_dataset* ds, const uint64_t* hidden, uint32_t n_hidden, uint64_t* keys,
+                          uint32_t* rgba, uint32_t cap, uint32_t* n);
+int csv_render_rgba(csv_ctx* ctx, const csv_camera* camera, uint32_t width, uint32_t height, float grid_size,
+                    uint32_t brick_size, uint32_t bricks_per_axis, const csv_brick_slot* d_slots, uint64_t n_slots,
+                    const uint64_t* d_labels, const uint64_t* d_tf_keys, const uint32_t* d_tf_rgba, uint32_t n_tf,
+                    const csv_lighting* lighting, uint32_t* d_rgba_out, uint32_t* d_requests, void* stream);
+
 /* ---- serving loop --------------------------------------------------------
  * The viewer's frame loop with its cache on the device.  Replaces the host
  * side of renderLoop.js:208-340 (frame), cacheProcessing.js:99-232

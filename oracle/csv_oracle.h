@@ -73,6 +73,19 @@ void or_render_rows(const float* cam, uint32_t W, uint32_t H, uint32_t y0, uint3
                     const uint64_t* labels, const uint64_t* hidden, uint32_t n_hidden, uint64_t* out_label,
                     float* out_depth, uint32_t* miss, uint32_t* requests);
 
+/* The colour path (csv_oracle_rgba.c).  Transfer function of n distinct
+ * labels ascending (buildTransferFunctionBuffers + hslToRgb,
+ * webgpuSetup.js:389-515), hidden ones transparent; hashLabel
+ * (decode.wgsl:135-172); the RGBA ray march for rows y0, y0 + ystep, ...
+ * (lighting: light_dir[3], ambient, diffuse). */
+void or_transfer_function(const uint64_t* labels, uint32_t n, const uint64_t* hidden, uint32_t n_hidden,
+                          uint32_t* rgba);
+uint32_t or_label_rgba(uint64_t v, const uint64_t* keys, const uint32_t* cols, uint32_t n_tf);
+void or_render_rgba_rows(const float* cam, uint32_t W, uint32_t H, uint32_t y0, uint32_t ystep, float grid,
+                         uint32_t bsz, uint32_t bpa, const or_slot* slots, uint64_t n_slots, const uint64_t* labels,
+                         const uint64_t* keys, const uint32_t* cols, uint32_t n_tf, const float* lighting,
+                         uint32_t* out_rgba);
+
 /* camera.js:61-77 (getUniformData): float32[16] from a double position,
  * direction and vertical field of view. */
 void or_camera_uniform(const double* pos, const double* dir, double fov, float* out16);

@@ -51,6 +51,12 @@ class Oracle:
         L.or_build_model.argtypes = [_u64p, _u32p, _u32p]
         L.or_encode.argtypes = [_u64p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_uint32,
                                 C.POINTER(_u8p), C.POINTER(C.c_size_t)]
+        L.or_transfer_function.argtypes = [_u64p, C.c_uint32, _u64p, C.c_uint32, _u32p]
+        L.or_label_rgba.restype = C.c_uint32
+        L.or_label_rgba.argtypes = [C.c_uint64, _u64p, _u32p, C.c_uint32]
+        L.or_render_rgba_rows.argtypes = [C.POINTER(C.c_float), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                          C.c_float, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint64, _u64p, _u64p,
+                                          _u32p, C.c_uint32, C.POINTER(C.c_float), _u32p]
         L.or_encode_shard.argtypes = [_u64p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_uint32, C.c_uint32, C.c_uint32,
                                       _u64p, _u64p, C.POINTER(_u8p), C.POINTER(C.c_size_t)]
         L.or_pyramid.argtypes = [_u64p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_uint32, C.c_uint32,
@@ -123,6 +129,36 @@ class Oracle:
         if with_requests:
             return out.reshape(H, W), dep.reshape(H, W), miss.reshape(H, W), req
         return out.reshape(H, W), dep.reshape(H, W), miss.reshape(H, W)
+
+    def transfer_function(self, labels: np.ndarray, hidden=None) -> np.ndarray:
+        """RGBA8 of distinct labels given ascending (buildTransferFunctionBuffers + hslToRgb)."""
+        lab = np.ascontiguousarray(labels, np.uint64)
+        hid = np.ascontiguousarray(hidden if hidden is not None else np.zeros(1, np.uint64), np.uint64)
+        out = np.zeros(max(len(lab), 1), np.uint32)
+        self.lib.or_transfer_function(_ptr(lab, _u64p), len(lab), _ptr(hid, _u64p),
+                                      0 if hidden is None else len(hidden), _ptr(out, _u32p))
+        return out[:len(lab)]
+
+    def label_rgba(self, v: int, keys: np.ndarray, cols: np.ndarray) -> int:
+        k = np.ascontiguousarray(keys, np.uint64)
+        c = np.ascontiguousarray(cols, np.uint32)
+        return int(self.lib.or_label_rgba(C.c_uint64(v), _ptr(k, _u64p), _ptr(c, _u32p), len(k)))
+
+    def render_rgba(self, cam16, W: int, H: int, grid: float, brick: int, bpa: int, slots, labels, keys, cols,
+                    lighting, rows=None) -> np.ndarray:
+        """The RGBA ray march (or_render_rgba_rows); lighting: light_dir[3], ambient, diffuse."""
+        cam = np.ascontiguousarray(cam16, np.float32)
+        lab = np.ascontiguousarray(labels, np.uint64)
+        k = np.ascontiguousarray(keys if len(keys) else np.zeros(1, np.uint64), np.uint64)
+        c = np.ascontiguousarray(cols if len(cols) else np.zeros(1, np.uint32), np.uint32)
+        li = np.ascontiguousarray(lighting, np.float32)
+        sl = np.ascontiguousarray(slots)
+        out = np.zeros(W * H, np.uint32)
+        y0, ystep = rows if rows is not None else (0, 1)
+        self.lib.or_render_rgba_rows(cam.ctypes.data_as(C.POINTER(C.c_float)), W, H, y0, ystep, grid, brick, bpa,
+                                     sl.ctypes.data, len(sl), _ptr(lab, _u64p), _ptr(k, _u64p), _ptr(c, _u32p), len(keys),
+                                     li.ctypes.data_as(C.POINTER(C.c_float)), _ptr(out, _u32p))
+        return out.reshape(H, W)
 
     def morton3(self, x, y, z) -> int:
         return self.lib.or_morton3(x, y, z)
