@@ -122,3 +122,24 @@ def test_sharded_encode_on_the_device_equals_whole(codec, shards):
     hists = [e.bricks(slab_of(vol, b, bx0, bx1), b, bx0, bx0 * nyz) for e, (bx0, bx1) in zip(encs, ranges)]
     total = np.sum(hists, axis=0).astype(np.uint64)
     assert assemble([e.finish(total) for e in encs]) == whole
+
+
+def test_real_bricks_encode_like_the_oracle(codec, oracle):
+    """Real segmentation: the MICrONS bricks of the shipped-file subset (tests/golden/shipped_subset.csbd,
+    the smallest, median and largest streams and a few spread over the file), decoded and laid side by side
+    along x as one volume, encode on the device to the oracle's bytes (the oracle matches the compiled
+    reference encoder on the whole 512^3 shipped volume, tests/test_npy_real_data.py)."""
+    import torch
+    from conftest import read_golden
+    img = read_golden("shipped_subset")
+    full, st = oracle.decode_image(img, 6)
+    assert int(st.max()) == 0
+    m = np.arange(64)
+    sp = np.zeros(64, np.int64)
+    for k in range(10):
+        sp |= ((m >> k) & 1) << (3 * k)
+    morton = sp[None, None, :] | (sp[None, :, None] << 1) | (sp[:, None, None] << 2)  # [z, y, x]
+    vol = np.concatenate([full[i][morton] for i in range(len(full))], axis=2)  # (64, 64, 64 n)
+    d = torch.from_numpy(vol.view(np.int64)).cuda()
+    codec.encode_device(d, 64)
+    assert bytes(codec.encoded_image_tensor().cpu().numpy()) == oracle.encode(vol, 64)
