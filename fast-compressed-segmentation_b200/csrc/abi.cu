@@ -775,7 +775,7 @@ int csv_decode_autotune(csv_ctx* ctx, const csv_dataset* ds, const csv_request* 
     float best_t = 1e30f;
     csv_decode_config bestc{0, 1, 0, 0};
     int rc = CSV_OK;
-    const uint32_t per_sm_options[] = {2, 1};
+    const uint32_t per_sm_options[] = {0, 2, 1};  // 0: as many CTAs as fit
     const uint32_t n_layouts = ds->d.L > kSmallLod + 1 ? 2 : 1;  // layout matters with 64^3 bricks only
     for (uint32_t layout = 0; layout < n_layouts && rc == CSV_OK; ++layout)
     for (uint32_t ps : per_sm_options) {

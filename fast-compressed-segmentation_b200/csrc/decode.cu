@@ -39,8 +39,10 @@
 
 namespace csv {
 
-constexpr int kDecThreads = 512;      // threads of the four-CTA-per-SM variant
-constexpr int kDecThreadsBig = 512;   // threads of the two-CTA-per-SM variant
+// Threads per CTA (measured on mixed1024: 768 / 384 against 512 / 512 took the
+// replay from 3.04 to 2.95 ms; fewer warps per brick wait at each phase barrier)
+constexpr int kDecThreads = 384;      // the 32^3 variant: up to five CTAs per SM
+constexpr int kDecThreadsBig = 768;   // the 64^3 variant: two CTAs per SM
 template <uint32_t KL>
 __host__ __device__ constexpr int dec_threads() { return KL == 6 ? kDecThreadsBig : kDecThreads; }
 constexpr uint32_t kDecLevels = 6;       // parent levels 0..5 (a 64^3 brick has 7 levels)
@@ -55,7 +57,7 @@ __host__ __device__ constexpr uint32_t mwords(uint32_t l) { return l < 2 ? 1u : 
 __host__ __device__ constexpr uint32_t moff(uint32_t l) { return l == 0 ? 0u : moff(l - 1) + mwords(l - 1); }
 // Shared memory holds the node values of parent levels 0..KL-1 and the
 // activity masks of all parent levels.  KL = 6: every level of a 64^3 brick
-// (two CTAs per SM).  KL = 5: an eighth of the value space (four CTAs per SM);
+// (two CTAs per SM).  KL = 5: an eighth of the value space (five CTAs per SM);
 // a 64^3 brick's level-5 values (its last parent level) then live in the CTA's
 // global scratch, where they stay in L2.
 constexpr uint32_t kSmallLevels = kSmallLod;
@@ -462,7 +464,7 @@ __device__ __forceinline__ void decode_segments(const DecodeArgs& A, const Brick
 // V = uint16_t when every palette of the dataset has fewer than 65535 entries
 // (value 0xFFFF stands for "label 0"), else uint32_t (one CTA per SM).
 template <class V, uint32_t KL>
-__global__ void __launch_bounds__(dec_threads<KL>(), KL == kDecLevels ? 2 : 4) decode_kernel(DecodeArgs A) {
+__global__ void __launch_bounds__(dec_threads<KL>(), KL == kDecLevels ? 2 : 5) decode_kernel(DecodeArgs A) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     DecShared<V, KL>& S = *reinterpret_cast<DecShared<V, KL>*>(smem_raw);
     const uint32_t tid = threadIdx.x, T = blockDim.x;

@@ -124,7 +124,7 @@ def test_autotune_returns_a_working_config(codec, mixed):
     out = torch.zeros(total, dtype=torch.int64, device="cuda")
     st = torch.zeros(len(reqs), dtype=torch.int32, device="cuda")
     best, ms = codec.autotune(cat, d_reqs, out, st, reps=3)
-    assert ms > 0 and best.ctas_per_sm in (1, 2) and best.stage in (0, 1) and best.lpt in (0, 1)
+    assert ms > 0 and best.ctas_per_sm in (0, 1, 2) and best.stage in (0, 1) and best.lpt in (0, 1)
     assert best.layout in (0, 1)
     out.zero_()
     g = codec.decode_graph(cat, d_reqs, out, st, best)
