@@ -638,6 +638,7 @@ struct csv_graph {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     uint32_t* d_order = nullptr;
+    uint32_t kernels = 0;  // decode kernels one replay launches
 };
 
 namespace {
@@ -722,15 +723,22 @@ int csv_decode_graph_create(csv_ctx* ctx, const csv_dataset* ds, const csv_reque
         cudaError_t le = cudaSuccess;
         if (!split) {
             le = launch_decode(ds->d, d_reqs, n, d_out, d_status, ctx->scr, s, &dc);
+            gr->kernels = n ? 1u : 0u;
         } else {
             // the large outputs first (longest bricks), then the small ones at twice the occupancy
             DecodeConfig part = dc;
             part.n_order = n_large;
-            if (n_large) le = launch_decode(ds->d, d_reqs, n, d_out, d_status, ctx->scr, s, &part);
+            if (n_large) {
+                le = launch_decode(ds->d, d_reqs, n, d_out, d_status, ctx->scr, s, &part);
+                ++gr->kernels;
+            }
             part.order = gr->d_order + n_large;
             part.n_order = n - n_large;
             part.small_only = true;
-            if (le == cudaSuccess && n > n_large) le = launch_decode(ds->d, d_reqs, n, d_out, d_status, ctx->scr, s, &part);
+            if (le == cudaSuccess && n > n_large) {
+                le = launch_decode(ds->d, d_reqs, n, d_out, d_status, ctx->scr, s, &part);
+                ++gr->kernels;
+            }
         }
         e = cudaStreamEndCapture(s, &gr->graph);
         if (le != cudaSuccess) e = le;
@@ -750,6 +758,12 @@ int csv_graph_launch(csv_graph* gr, void* stream) {
     DeviceGuard g(gr->ctx->device);
     cudaError_t e = cudaGraphLaunch(gr->exec, (cudaStream_t)stream);
     return e == cudaSuccess ? CSV_OK : cuda_fail(gr->ctx, e, "graph launch");
+}
+
+int csv_graph_kernels(const csv_graph* gr, uint32_t* n) {
+    if (!gr || !n) return CSV_EINVAL;
+    *n = gr->kernels;
+    return CSV_OK;
 }
 
 void csv_graph_destroy(csv_graph* gr) {

@@ -138,6 +138,7 @@ def load_library() -> C.CDLL:
     L.csv_dataset_concat.argtypes = [vp, C.POINTER(vp), C.c_uint32, C.POINTER(vp)]
     L.csv_decode_graph_create.argtypes = [vp, vp, vp, C.c_uint32, vp, vp, C.POINTER(DecodeConfig), C.POINTER(vp)]
     L.csv_graph_launch.argtypes = [vp, vp]
+    L.csv_graph_kernels.argtypes = [vp, C.POINTER(C.c_uint32)]
     L.csv_graph_destroy.argtypes = [vp]
     L.csv_decode_autotune.argtypes = [vp, vp, vp, C.c_uint32, vp, vp, C.c_uint32, C.POINTER(DecodeConfig),
                                       C.POINTER(C.c_float)]
@@ -255,6 +256,13 @@ class DecodeGraph:
 
     def launch(self, stream=None):
         self.codec._check(self.codec.lib.csv_graph_launch(self.handle, C.c_void_p(_stream_handle(stream))))
+
+    @property
+    def kernels(self) -> int:
+        """Decode kernels one replay launches (csv_graph_kernels)."""
+        n = C.c_uint32()
+        self.codec._check(self.codec.lib.csv_graph_kernels(self.handle, C.byref(n)))
+        return n.value
 
     def close(self):
         if self.handle:

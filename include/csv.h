@@ -196,6 +196,9 @@ typedef struct csv_graph csv_graph;
 int csv_decode_graph_create(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_reqs, uint32_t n,
                             uint64_t* d_out, uint32_t* d_status, const csv_decode_config* cfg, csv_graph** out);
 int csv_graph_launch(csv_graph* g, void* stream);
+/* Decode kernels one replay of the graph launches (1, or 2 when it splits the
+ * requests by output size; 0 for an empty batch). */
+int csv_graph_kernels(const csv_graph* g, uint32_t* n);
 void csv_graph_destroy(csv_graph* g);
 /* Times every candidate configuration on this batch (a captured graph each,
  * `reps` timed replays after one warm-up, median) and returns the fastest and

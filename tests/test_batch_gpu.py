@@ -207,3 +207,21 @@ def test_wide_palettes_in_both_kernel_variants(codec, oracle):
             r = ref[int(lods[k])][int(bricks[k])]
             assert np.array_equal(o[int(dst[k]):int(dst[k]) + len(r)], r), k
     ds.close()
+
+
+def test_graph_reports_its_kernels(codec, mixed):
+    """csv_graph_kernels: two decode kernels per replay when a dataset with 64^3 bricks is split by output
+    size (layout 0), one with layout 1, none for an empty batch."""
+    import torch
+    from csvb200 import DecodeConfig, requests_tensor
+    cat, dss, sizes_b, offsets, parts_ref = mixed
+    reqs, bricks, lods, dst, total = _mixed_requests(sizes_b, np.random.default_rng(5))
+    out = torch.zeros(total, dtype=torch.int64, device="cuda")
+    st = torch.zeros(len(reqs), dtype=torch.int32, device="cuda")
+    for layout, want in ((0, 2), (1, 1)):
+        g = codec.decode_graph(cat, requests_tensor(reqs), out, st, DecodeConfig(0, 1, 0, layout))
+        assert g.kernels == want
+        g.close()
+    g = codec.decode_graph(cat, requests_tensor(reqs), out, st, n=0)
+    assert g.kernels == 0
+    g.close()
