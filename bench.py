@@ -526,6 +526,23 @@ def serve2048(codec, dev, args):
         "timing": "device time per step (CUDA events around plan, cache, decode, render, census)",
     }
     srv.close()
+    # the same orbit with the viewer's RGBA frames (transfer function, shading, shadow rays), fresh cache
+    del lab, dep
+    torch.cuda.empty_cache()
+    srv = Server(codec, ds, Wp, Hp, S["fov"], cache_bytes=S["cache_gib"] << 30, cone=CONE_SCREEN)
+    rgba = torch.empty(Wp * Hp, dtype=torch.int32, device=dev)
+    for pos, d in views:
+        srv.submit_rgba(0, pos, d, rgba)
+        srv.step(st)
+    fr = srv.poll(wait=True, max_frames=len(views) + 8)
+    ms2 = np.array([f["ms"] for f in fr])
+    out["rgba"] = {"p50_ms": round(float(np.percentile(ms2, 50)), 3), "p99_ms": round(float(np.percentile(ms2, 99)), 3),
+                   "max_ms": round(float(ms2.max()), 3), "mean_ms": round(float(ms2.mean()), 3),
+                   "entered_bricks_mean": round(float(np.mean([f["entered"] for f in fr])), 1),
+                   "visible_pixels_last_frame": round(float(((rgba >> 24) != 0).float().mean()), 4),
+                   "lighting": "csv_lighting_default(25): ambient 0.5, diffuse 0.8",
+                   "timing": "device time per step, frames RGBA8 through csv_render_rgba's colour path"}
+    srv.close()
     ds.close()
     torch.cuda.empty_cache()
     return out
@@ -656,8 +673,9 @@ def run_reference(args):
         kind = "reference"
 
         def step():
-            assert R.decode_parallel(img_left, threads) == 0
-            assert R.decode_parallel(img_right, threads) == 0
+            # decodeBrick throws on a brick whose root stop bit is set (the whole brick one label): the
+            # reference decodes nothing there; such bricks are counted, not fatal
+            return R.decode_parallel(img_left, threads) + R.decode_parallel(img_right, threads)
     else:
         O = Oracle()
         kind, threads = "port", 1
@@ -665,12 +683,14 @@ def run_reference(args):
         def step():
             O.decode_image(img_left, bl.bit_length() - 1)
             O.decode_image(img_right, br.bit_length() - 1)
+            return 0
     for _ in range(min(args.warmup, 1)):
         step()
     times = []
+    thrown = 0
     for _ in range(min(args.steps, 3)):
         t0 = time.perf_counter()
-        step()
+        thrown = step()
         times.append(time.perf_counter() - t0)
     s = statistics.mean(times)
     nvox = D * H * Wd
@@ -680,7 +700,10 @@ def run_reference(args):
         "steps": len(times), "warmup": min(args.warmup, 1), "ms_per_step": round(s * 1e3, 2),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
         "config": {"workload": W["name"], "volume": [Wd, H, D], "bricks": {"32^3": nl, "64^3": nr},
-                   "lod": "full resolution"},
+                   "lod": "full resolution",
+                   "bricks_thrown": int(thrown),  # uniform bricks: decodeBrick throws, nothing decoded
+                   "note": "the reference C++ decoder throws on bricks that are one label (root stop bit); "
+                           "they are counted, and the GPU decoder fills them with palette[0]"},
         "cpu_baseline": {"value": round(v, 4), "unit": "Gvox/s", "cores": threads, "kind": kind,
                          "sample": f"every step decodes all {nl + nr} bricks of both images at full resolution "
                                    f"(decodeRansStream + decodeBrick<b>), bricks split over {threads} host threads"},

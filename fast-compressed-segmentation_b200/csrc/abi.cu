@@ -30,6 +30,49 @@ int abi_cuda_fail(csv_ctx* ctx, cudaError_t e, const char* where) {
     return abi_fail(ctx, CSV_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
 
+cudaError_t transfer_function(const DeviceDataset& d, const uint64_t* hidden, uint32_t n_hidden,
+                              std::vector<uint64_t>& keys, std::vector<uint32_t>& rgba) {
+    // buildTransferFunctionBuffers (webgpuSetup.js:389-465): every distinct non-zero
+    // palette label of the dataset, ascending; entry i gets hue 137.5 i (golden
+    // angle), saturation, lightness and opacity cycling with i, HSL -> RGB
+    // (hslToRgb, :490-515), RGB scaled by 0.92 for lighting headroom
+    std::vector<uint64_t> pal(d.pal_pool_entries);
+    if (!pal.empty()) {
+        cudaError_t e = cudaMemcpy(pal.data(), d.d_pal, 8 * pal.size(), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return e;
+    }
+    std::sort(pal.begin(), pal.end());
+    pal.erase(std::unique(pal.begin(), pal.end()), pal.end());
+    if (!pal.empty() && pal[0] == 0) pal.erase(pal.begin());
+    keys.resize(pal.size());
+    rgba.resize(pal.size());
+    std::vector<uint64_t> hid(hidden, hidden + n_hidden);
+    std::sort(hid.begin(), hid.end());
+    auto js_round = [](double x) { return floor(x + 0.5); };  // Math.round
+    for (size_t i = 0; i < pal.size(); ++i) {
+        const double h = fmod((double)i * 137.5, 360.0);
+        const double sat = 0.55 + (double)(i % 3) * 0.08, lig = 0.35 + (double)(i % 4) * 0.05;
+        const double op = 0.25 + (double)(i % 5) * 0.08;
+        const double c = (1 - fabs(2 * lig - 1)) * sat;
+        const double x = c * (1 - fabs(fmod(h / 60, 2) - 1));
+        const double m = lig - c / 2;
+        double r, gg, b;
+        if (h < 60) { r = c; gg = x; b = 0; }
+        else if (h < 120) { r = x; gg = c; b = 0; }
+        else if (h < 180) { r = 0; gg = c; b = x; }
+        else if (h < 240) { r = 0; gg = x; b = c; }
+        else if (h < 300) { r = x; gg = 0; b = c; }
+        else { r = c; gg = 0; b = x; }
+        const double rr = js_round((r + m) * 255), rg = js_round((gg + m) * 255), rb = js_round((b + m) * 255);
+        const uint32_t R = (uint32_t)std::min(floor(rr * 0.92), 255.0), G = (uint32_t)std::min(floor(rg * 0.92), 255.0),
+                       B = (uint32_t)std::min(floor(rb * 0.92), 255.0), A = (uint32_t)floor(op * 255);
+        keys[i] = pal[i];
+        // a hidden label is transparent (rebuildLabelColors, webgpuSetup.js:826-834)
+        rgba[i] = std::binary_search(hid.begin(), hid.end(), pal[i]) ? 0u : (R | (G << 8) | (B << 16) | (A << 24));
+    }
+    return cudaSuccess;
+}
+
 int abi_ensure_scratch(csv_ctx* ctx, uint32_t b) {
     if (ctx->scr.base && ctx->scr_b >= b) return CSV_OK;
     size_t per = decode_scratch_per_cta(b);
@@ -868,45 +911,17 @@ int csv_transfer_function(const csv_dataset* ds, const uint64_t* hidden, uint32_
                           uint32_t* rgba, uint32_t cap, uint32_t* n_out) {
     if (!ds || !n_out || (n_hidden && !hidden)) return CSV_EINVAL;
     DeviceGuard g(ds->ctx->device);
-    // buildTransferFunctionBuffers (webgpuSetup.js:389-465): every distinct non-zero
-    // palette label of the dataset, ascending; entry i gets hue 137.5 i (golden
-    // angle), saturation, lightness and opacity cycling with i, HSL -> RGB
-    // (hslToRgb, :490-515), RGB scaled by 0.92 for lighting headroom
-    std::vector<uint64_t> pal(ds->d.pal_pool_entries);
-    if (!pal.empty()) {
-        cudaError_t e = cudaMemcpy(pal.data(), ds->d.d_pal, 8 * pal.size(), cudaMemcpyDeviceToHost);
-        if (e != cudaSuccess) return cuda_fail(ds->ctx, e, "palette copy");
-    }
-    std::sort(pal.begin(), pal.end());
-    pal.erase(std::unique(pal.begin(), pal.end()), pal.end());
-    if (!pal.empty() && pal[0] == 0) pal.erase(pal.begin());
-    *n_out = (uint32_t)pal.size();
-    if (pal.size() > cap || (!pal.empty() && (!keys || !rgba)))
-        return fail(ds->ctx, CSV_ERANGE, "transfer function: " + std::to_string(pal.size()) + " labels, room for " +
+    std::vector<uint64_t> k;
+    std::vector<uint32_t> c;
+    cudaError_t e = transfer_function(ds->d, hidden, n_hidden, k, c);
+    if (e != cudaSuccess) return cuda_fail(ds->ctx, e, "palette copy");
+    *n_out = (uint32_t)k.size();
+    if (k.size() > cap || (!k.empty() && (!keys || !rgba)))
+        return fail(ds->ctx, CSV_ERANGE, "transfer function: " + std::to_string(k.size()) + " labels, room for " +
                                              std::to_string(cap));
-    std::vector<uint64_t> hid(hidden, hidden + n_hidden);
-    std::sort(hid.begin(), hid.end());
-    auto js_round = [](double x) { return floor(x + 0.5); };  // Math.round
-    for (size_t i = 0; i < pal.size(); ++i) {
-        const double h = fmod((double)i * 137.5, 360.0);
-        const double sat = 0.55 + (double)(i % 3) * 0.08, lig = 0.35 + (double)(i % 4) * 0.05;
-        const double op = 0.25 + (double)(i % 5) * 0.08;
-        const double c = (1 - fabs(2 * lig - 1)) * sat;
-        const double x = c * (1 - fabs(fmod(h / 60, 2) - 1));
-        const double m = lig - c / 2;
-        double r, gg, b;
-        if (h < 60) { r = c; gg = x; b = 0; }
-        else if (h < 120) { r = x; gg = c; b = 0; }
-        else if (h < 180) { r = 0; gg = c; b = x; }
-        else if (h < 240) { r = 0; gg = x; b = c; }
-        else if (h < 300) { r = x; gg = 0; b = c; }
-        else { r = c; gg = 0; b = x; }
-        const double rr = js_round((r + m) * 255), rg = js_round((gg + m) * 255), rb = js_round((b + m) * 255);
-        const uint32_t R = (uint32_t)std::min(floor(rr * 0.92), 255.0), G = (uint32_t)std::min(floor(rg * 0.92), 255.0),
-                       B = (uint32_t)std::min(floor(rb * 0.92), 255.0), A = (uint32_t)floor(op * 255);
-        keys[i] = pal[i];
-        // a hidden label is transparent (rebuildLabelColors, webgpuSetup.js:826-834)
-        rgba[i] = std::binary_search(hid.begin(), hid.end(), pal[i]) ? 0u : (R | (G << 8) | (B << 16) | (A << 24));
+    if (!k.empty()) {
+        memcpy(keys, k.data(), 8 * k.size());
+        memcpy(rgba, c.data(), 4 * c.size());
     }
     return CSV_OK;
 }

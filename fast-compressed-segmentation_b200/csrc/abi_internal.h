@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "csv_internal.h"
 
@@ -34,6 +35,10 @@ int abi_fail(csv_ctx* ctx, int code, const std::string& msg);
 int abi_cuda_fail(csv_ctx* ctx, cudaError_t e, const char* where);
 // Size the context's decode scratch for bricks of edge b (grows, never shrinks).
 int abi_ensure_scratch(csv_ctx* ctx, uint32_t b);
+// buildTransferFunctionBuffers (webgpuSetup.js:389-465) on a dataset: its distinct
+// non-zero palette labels ascending and their RGBA8, hidden labels transparent.
+cudaError_t transfer_function(const DeviceDataset& d, const uint64_t* hidden, uint32_t n_hidden,
+                              std::vector<uint64_t>& keys, std::vector<uint32_t>& rgba);
 
 // Makes `dev` current for the scope and restores the caller's device after.
 struct DeviceGuard {

@@ -499,6 +499,11 @@ struct csv_server {
     uint32_t* d_status = nullptr;
     uint64_t* d_hidden = nullptr;
     uint32_t n_hidden = 0;
+    // the colour path: the dataset's transfer function (hidden labels transparent) and the light
+    uint64_t* d_tf_keys = nullptr;
+    uint32_t* d_tf_rgba = nullptr;
+    uint32_t n_tf = 0;
+    csv_lighting light;
     StepStats* d_stats = nullptr;  // kRing slots
     StepStats* h_stats = nullptr;  // pinned mirror
     struct Session {
@@ -507,6 +512,7 @@ struct csv_server {
         double pv[6];     // camera of the session's last re-plan (unit direction)
         uint64_t* lab = nullptr;
         float* dep = nullptr;
+        uint32_t* rgba = nullptr;  // set: the frame is an RGBA8 image (csv_serve_submit_rgba)
     };
     std::vector<Session> ses;
     std::vector<uint32_t> last_open;  // open sessions at the last plan
@@ -526,6 +532,8 @@ int fail(csv_ctx* ctx, int code, const std::string& m) { return abi_fail(ctx, co
 int cfail(csv_ctx* ctx, cudaError_t e, const char* w) { return abi_cuda_fail(ctx, e, w); }
 
 void server_free(csv_server* s) {
+    cudaFree(s->d_tf_keys);
+    cudaFree(s->d_tf_rgba);
     cudaFree(s->d_cache);
     cudaFree(s->d_slots);
     cudaFree(s->d_req_words);
@@ -723,6 +731,17 @@ int csv_serve_create(csv_ctx* ctx, const csv_dataset* ds, const csv_serve_config
         e = cudaMemcpy(s->d_hidden, h.data(), 8ull * n_hidden, cudaMemcpyHostToDevice);
     }
     s->n_hidden = n_hidden;
+    if (e == cudaSuccess) {  // the transfer function of RGBA frames
+        std::vector<uint64_t> k;
+        std::vector<uint32_t> c;
+        e = transfer_function(d, hidden, n_hidden, k, c);
+        s->n_tf = (uint32_t)k.size();
+        if (e == cudaSuccess) e = cudaMalloc(&s->d_tf_keys, 8 * std::max<size_t>(1, k.size()));
+        if (e == cudaSuccess) e = cudaMalloc(&s->d_tf_rgba, 4 * std::max<size_t>(1, c.size()));
+        if (e == cudaSuccess && !k.empty()) e = cudaMemcpy(s->d_tf_keys, k.data(), 8 * k.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !c.empty()) e = cudaMemcpy(s->d_tf_rgba, c.data(), 4 * c.size(), cudaMemcpyHostToDevice);
+    }
+    csv_lighting_default(25.0, &s->light);
     ServeState st0;
     memset(&st0, 0, sizeof st0);
     st0.cap = s->total - s->pal_region;
@@ -765,6 +784,29 @@ int csv_serve_submit(csv_server* s, uint32_t session, const csv_view* view, uint
     }
     p.lab = d_label;
     p.dep = d_depth;
+    p.rgba = nullptr;
+    return CSV_OK;
+}
+
+int csv_serve_submit_rgba(csv_server* s, uint32_t session, const csv_view* view, uint32_t* d_rgba) {
+    if (!s || !view || !d_rgba) return CSV_EINVAL;
+    if (session >= s->max_sessions) return fail(s->ctx, CSV_ERANGE, "serve: session id beyond max_sessions");
+    auto& p = s->ses[session];
+    p.open = true;
+    p.pending = true;
+    for (int a = 0; a < 3; ++a) {
+        p.v[a] = view->position[a];
+        p.v[3 + a] = view->direction[a];
+    }
+    p.lab = nullptr;
+    p.dep = nullptr;
+    p.rgba = d_rgba;
+    return CSV_OK;
+}
+
+int csv_serve_set_lighting(csv_server* s, const csv_lighting* light) {
+    if (!s || !light) return CSV_EINVAL;
+    s->light = *light;  // used by the RGBA frames of the next steps
     return CSV_OK;
 }
 
@@ -871,10 +913,17 @@ int csv_serve_step(csv_server* s, void* stream, uint64_t* step_id) {
         const auto& p = s->ses[rendered[k]];
         csv_camera cam;
         camera_of(p.v, s->fov, &cam);
-        e = launch_render(cam, s->W, s->H, (float)(s->bpa * s->b), s->b, s->bpa,
-                          s->d_slots + (size_t)rendered[k] * s->n_slots, s->n_slots, s->d_cache,
-                          s->n_hidden ? s->d_hidden : nullptr, s->n_hidden, p.lab, p.dep,
-                          s->d_req_words + (size_t)rendered[k] * s->n_slots, st);
+        if (p.rgba)
+            e = launch_render_rgba(cam, s->W, s->H, (float)(s->bpa * s->b), s->b, s->bpa,
+                                   s->d_slots + (size_t)rendered[k] * s->n_slots, s->n_slots, s->d_cache,
+                                   s->n_tf ? s->d_tf_keys : nullptr, s->d_tf_rgba, s->n_tf, s->light.light_dir,
+                                   s->light.ambient, s->light.diffuse, p.rgba,
+                                   s->d_req_words + (size_t)rendered[k] * s->n_slots, st);
+        else
+            e = launch_render(cam, s->W, s->H, (float)(s->bpa * s->b), s->b, s->bpa,
+                              s->d_slots + (size_t)rendered[k] * s->n_slots, s->n_slots, s->d_cache,
+                              s->n_hidden ? s->d_hidden : nullptr, s->n_hidden, p.lab, p.dep,
+                              s->d_req_words + (size_t)rendered[k] * s->n_slots, st);
     }
     if (e == cudaSuccess && s->nb && !rendered.empty()) {
         CensusArgs A;

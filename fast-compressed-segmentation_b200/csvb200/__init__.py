@@ -152,6 +152,8 @@ def load_library() -> C.CDLL:
                                    C.c_float, C.c_float, C.c_float, C.c_uint64, vp]
     L.csv_serve_create.argtypes = [vp, vp, C.POINTER(ServeConfig), u64p, C.c_uint32, C.POINTER(vp)]
     L.csv_serve_submit.argtypes = [vp, C.c_uint32, C.POINTER(View), vp, vp]
+    L.csv_serve_submit_rgba.argtypes = [vp, C.c_uint32, C.POINTER(View), vp]
+    L.csv_serve_set_lighting.argtypes = [vp, C.POINTER(Lighting)]
     L.csv_serve_step.argtypes = [vp, vp, C.POINTER(C.c_uint64)]
     L.csv_serve_poll.argtypes = [vp, C.POINTER(FrameStats), C.c_uint32, C.POINTER(C.c_uint32), C.c_int]
     L.csv_serve_camera.argtypes = [vp, C.POINTER(View), vp]
@@ -567,6 +569,17 @@ class Server:
         self._keep[session] = (d_label, d_depth)
         self.codec._check(self.lib.csv_serve_submit(self.handle, session, C.byref(v), C.c_void_p(d_label.data_ptr()),
                                                     C.c_void_p(d_depth.data_ptr())))
+
+    def submit_rgba(self, session: int, position, direction, d_rgba):
+        """A frame as the viewer shows it: an RGBA8 image (W*H int32/uint32 device tensor) through the dataset's
+        transfer function and the server's lighting (csv_serve_submit_rgba)."""
+        v = self.view(position, direction)
+        self._keep[session] = (d_rgba,)
+        self.codec._check(self.lib.csv_serve_submit_rgba(self.handle, session, C.byref(v),
+                                                         C.c_void_p(d_rgba.data_ptr())))
+
+    def set_lighting(self, lighting: "Lighting"):
+        self.codec._check(self.lib.csv_serve_set_lighting(self.handle, C.byref(lighting)))
 
     def step(self, stream=None) -> int:
         sid = C.c_uint64()

@@ -366,6 +366,12 @@ int csv_serve_create(csv_ctx* ctx, const csv_dataset* ds, const csv_serve_config
                      uint32_t n_hidden, csv_server** out);
 /* d_label (W*H u64) and d_depth (W*H f32) are device images the step writes. */
 int csv_serve_submit(csv_server* srv, uint32_t session, const csv_view* view, uint64_t* d_label, float* d_depth);
+/* The same frame as the viewer shows it: an RGBA8 image (W*H words, device)
+ * from csv_render_rgba's colour path through the dataset's transfer function
+ * (built at create; the hidden labels transparent) and the server's lighting
+ * (csv_lighting_default(25) until csv_serve_set_lighting). */
+int csv_serve_submit_rgba(csv_server* srv, uint32_t session, const csv_view* view, uint32_t* d_rgba);
+int csv_serve_set_lighting(csv_server* srv, const csv_lighting* light);
 int csv_serve_step(csv_server* srv, void* stream, uint64_t* step_id);
 /* Up to `max` finished frames (one per session of each finished step), oldest
  * first; wait != 0 blocks until every step enqueued so far has finished. */

@@ -219,3 +219,49 @@ def test_serve_many_steps_without_polling(codec, cube16):
     assert all(f["ms"] > 0 for f in frames)
     srv.close()
     ds.close()
+
+
+def test_serve_rgba_frames_are_the_colour_path(codec, cube16):
+    """A session that submits RGBA frames, beside one that submits label/depth frames, in the same steps: each
+    RGBA frame is csv_render_rgba of that step's cache and slot table through the dataset's transfer function
+    (hidden labels transparent) and the server's lighting, word for word; the label session's frames are its
+    label render.  RGBA rays run on past the first visible voxel (to alpha 0.95), so they enter at least the
+    bricks the label rays enter."""
+    import torch
+    from csvb200 import Server
+    ds = codec.open(cube16)
+    keys, cols = codec.transfer_function(ds)
+    hidden = keys[::3].copy()
+    keys, cols = codec.transfer_function(ds, hidden=hidden)
+    d_keys = torch.from_numpy(keys.view(np.int64).copy()).cuda()
+    d_cols = torch.from_numpy(cols.view(np.int32).copy()).cuda()
+    srv = Server(codec, ds, W, H, FOV, max_sessions=2, hidden=hidden)
+    light = codec.lighting(40.0)
+    srv.set_lighting(light)
+    rgba = torch.zeros(W * H, dtype=torch.int32, device="cuda")
+    lab = torch.zeros(W * H, dtype=torch.int64, device="cuda")
+    dep = torch.zeros(W * H, dtype=torch.float32, device="cuda")
+    info = srv.info()
+    for f, (pos, d) in enumerate(_orbit_views((64.0, 64.0, 64.0), 4, 260.0, 150.0)):
+        srv.submit_rgba(0, pos, d, rgba)
+        srv.submit(1, pos, d, lab, dep)
+        srv.step()
+        frames = srv.poll(wait=True)
+        assert sorted(fr["session"] for fr in frames) == [0, 1]
+        cam = srv.camera(pos, d)
+        want = torch.empty(W * H, dtype=torch.int32, device="cuda")
+        codec.render_rgba(cam, W, H, float(info.bricks_per_axis * 16), 16, info.bricks_per_axis, srv.slots_tensor(0),
+                          srv.cache_tensor(), d_keys, d_cols, light, want)
+        l2 = torch.empty(W * H, dtype=torch.int64, device="cuda")
+        d2 = torch.empty(W * H, dtype=torch.float32, device="cuda")
+        d_hid = torch.from_numpy(np.sort(hidden).view(np.int64).copy()).cuda()
+        codec.render(cam, W, H, float(info.bricks_per_axis * 16), 16, info.bricks_per_axis, srv.slots_tensor(1),
+                     srv.cache_tensor(), l2, d2, d_hidden=d_hid)
+        torch.cuda.synchronize()
+        assert torch.equal(rgba, want), f
+        assert torch.equal(lab, l2) and torch.equal(dep.view(torch.int32), d2.view(torch.int32)), f
+        assert (rgba >> 24).any()
+        by = {fr["session"]: fr for fr in frames}
+        assert by[0]["entered"] >= by[1]["entered"]
+    srv.close()
+    ds.close()
