@@ -275,26 +275,37 @@ def run_b200(args):
     h_outs = [torch.empty((nb_, b_ ** 3), dtype=torch.int64, pin_memory=True) for _, b_, nb_ in per_img]
     h_st = [np.zeros(nb_, np.uint32) for _, _, nb_ in per_img]
     host_imgs = [np.frombuffer(im, np.uint8) for im, _, _ in per_img]
+    # one host thread and one context per file (ctypes releases the GIL): one file's open and seek-index
+    # pass overlaps the other's copy to the host, as a viewer loading both halves would run them
+    from concurrent.futures import ThreadPoolExecutor
+    ctxs = [codec, Codec(local)]
+
+    def decode_file(j):
+        im, b_, nb_ = per_img[j]
+        c = ctxs[j]
+        rc = c.lib.csv_decode_image(c.handle, host_imgs[j].ctypes.data_as(C.POINTER(C.c_uint8)), len(im),
+                                    b_.bit_length() - 1, C.cast(h_outs[j].data_ptr(), C.POINTER(C.c_uint64)),
+                                    h_st[j].ctypes.data_as(C.POINTER(C.c_uint32)))
+        assert rc == 0, c.lib.csv_last_error(c.handle)
+
     e2e_ms = []
-    for k in range(6):  # one warm-up, five timed: the median (host copies share the machine's PCIe and memory)
-        barrier(pg)
-        t0 = time.perf_counter()
-        for j, (im, b_, nb_) in enumerate(per_img):
-            rc = codec.lib.csv_decode_image(codec.handle, host_imgs[j].ctypes.data_as(C.POINTER(C.c_uint8)), len(im),
-                                            b_.bit_length() - 1, C.cast(h_outs[j].data_ptr(), C.POINTER(C.c_uint64)),
-                                            h_st[j].ctypes.data_as(C.POINTER(C.c_uint32)))
-            assert rc == 0, codec.lib.csv_last_error(codec.handle)
-        t1 = time.perf_counter()
-        if k > 0:
-            e2e_ms.append((t1 - t0) * 1e3)
+    with ThreadPoolExecutor(max_workers=len(per_img)) as ex:
+        for k in range(6):  # one warm-up, five timed: the median (host copies share the machine's PCIe and memory)
+            barrier(pg)
+            t0 = time.perf_counter()
+            list(ex.map(decode_file, range(len(per_img))))
+            t1 = time.perf_counter()
+            if k > 0:
+                e2e_ms.append((t1 - t0) * 1e3)
     e2e_t = max_over_ranks(statistics.median(e2e_ms), pg, dev)
     e2e_ok = bool(torch.equal(h_outs[0].view(-1).to(dev), out[: nl * bl ** 3]) and
                   torch.equal(h_outs[1].view(-1).to(dev), out[nl * bl ** 3:]))
     e2e = {"value": round(world * nvox / (e2e_t * 1e-3) / 1e9, 3), "unit": "Gvox/s",
            "h2d_bytes_per_step": len(img_left) + len(img_right), "d2h_bytes_per_step": 8 * nvox + 4 * n,
            "ms_per_step": round(e2e_t, 2), "ms_samples": [round(t, 1) for t in e2e_ms],
-           "path": "csv_decode_image per image: host .csbd -> open (H2D, seek index) -> decode -> D2H labels"}
-    del h_outs
+           "path": "csv_decode_image per image, the two images on two host threads and contexts: host .csbd -> "
+                   "open (H2D, seek index) -> decode -> D2H labels"}
+    del h_outs, ctxs
 
     # ---- neurite512: encode vs the reference encoder on this host, and its decode
     neur = neurite512(codec, dev, args, rank == 0 and world == 1 and not args.no_cpu)
