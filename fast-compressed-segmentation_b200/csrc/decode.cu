@@ -40,13 +40,17 @@
 namespace csv {
 
 // Threads per CTA (measured on mixed1024: 768 / 384 against 512 / 512 took the
-// replay from 3.04 to 2.95 ms; fewer warps per brick wait at each phase barrier)
-constexpr int kDecThreads = 384;      // the 32^3 variant: up to five CTAs per SM
+// replay from 3.04 to 2.95 ms, and 320 threads at six CTAs per SM -- with the
+// 32^3 variant's palette cache halved to fit -- from 2.68 to 2.61 ms: fewer warps
+// of a brick wait at each phase barrier, more bricks are in flight per SM)
+constexpr int kDecThreads = 320;      // the 32^3 variant: up to six CTAs per SM
 constexpr int kDecThreadsBig = 768;   // the 64^3 variant: two CTAs per SM
 template <uint32_t KL>
 __host__ __device__ constexpr int dec_threads() { return KL == 6 ? kDecThreadsBig : kDecThreads; }
 constexpr uint32_t kDecLevels = 6;       // parent levels 0..5 (a 64^3 brick has 7 levels)
 constexpr uint32_t kPalCache = 1024;     // palettes up to this size are copied to shared memory
+template <uint32_t KL>
+__host__ __device__ constexpr uint32_t pal_cache() { return KL == 6 ? kPalCache : 512u; }
 constexpr uint32_t REC_MISSING = OP_RP | 8u;
 
 // Node values of level l at val + voff(l): lvl_off rounded up to 8 entries (16 bytes for u16).
@@ -76,7 +80,7 @@ struct DecShared {
     alignas(16) V val[LevelDims<KL>::val];
     uint32_t mask[LevelDims<KL>::mask];
     uint16_t pre[LevelDims<KL>::mask];
-    uint64_t pal[kPalCache];
+    uint64_t pal[pal_cache<KL>()];
     uint32_t warp_sums[1024 / 32 + 1];
     BrickDesc br;
     csv_request req;
@@ -464,7 +468,7 @@ __device__ __forceinline__ void decode_segments(const DecodeArgs& A, const Brick
 // V = uint16_t when every palette of the dataset has fewer than 65535 entries
 // (value 0xFFFF stands for "label 0"), else uint32_t (one CTA per SM).
 template <class V, uint32_t KL>
-__global__ void __launch_bounds__(dec_threads<KL>(), KL == kDecLevels ? 2 : 5) decode_kernel(DecodeArgs A) {
+__global__ void __launch_bounds__(dec_threads<KL>(), KL == kDecLevels ? 2 : 6) decode_kernel(DecodeArgs A) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     DecShared<V, KL>& S = *reinterpret_cast<DecShared<V, KL>*>(smem_raw);
     const uint32_t tid = threadIdx.x, T = blockDim.x;
@@ -531,7 +535,7 @@ __global__ void __launch_bounds__(dec_threads<KL>(), KL == kDecLevels ? 2 : 5) d
         uint64_t* out = A.out + req.dst;
         const uint64_t* gpal = A.pal + br.pal_off;
         const uint64_t* pal = gpal;
-        if (br.P <= kPalCache) {
+        if (br.P <= pal_cache<KL>()) {
             for (uint32_t i = tid; i < br.P; i += T) S.pal[i] = gpal[i];
             pal = S.pal;
         }

@@ -181,8 +181,8 @@ int csv_dataset_concat(csv_ctx* ctx, const csv_dataset* const* parts, uint32_t n
  * (1 = hand out the largest bricks first: a request permutation computed at
  * creation), layout (for datasets with 64^3 bricks: 0 = requests above LOD 5
  * in the decode kernel that holds every level in shared memory, two CTAs per
- * SM, then the rest in the five-CTA-per-SM kernel, as two launches; 1 = every
- * request in the five-CTA kernel, which keeps a 64^3 brick's last parent
+ * SM, then the rest in the six-CTA-per-SM kernel, as two launches; 1 = every
+ * request in the six-CTA kernel, which keeps a 64^3 brick's last parent
  * level in its global scratch). */
 typedef struct csv_decode_config {
     uint32_t ctas_per_sm;
