@@ -102,7 +102,7 @@ size_t decode_scratch_per_cta(uint32_t b, uint32_t kl = 6);
 size_t decode_scratch_bytes(int device, uint32_t b);
 uint32_t decode_grid(int device, uint32_t n);
 // Requests at this LOD (32^3 labels) or coarser can run in the decode kernel's
-// small-footprint variant (four CTAs per SM instead of two).
+// small-footprint variant (six CTAs per SM instead of two).
 constexpr uint32_t kSmallLod = 5;
 // Launch knobs the autotuner chooses (defaults: occupancy-limited grid, staging on, request order).
 struct DecodeConfig {
@@ -112,7 +112,7 @@ struct DecodeConfig {
     uint32_t n_order = 0;             // entries of order (0: n)
     const uint32_t* n_dev = nullptr;  // device-resident queue length (<= n or n_order), or null
     bool small_only = false;          // every queued request is at LOD 5 (32^3) or coarser
-    uint32_t layout = 0;              // 1: every request in the four-CTA-per-SM kernel
+    uint32_t layout = 0;              // 1: every request in the small (six-CTA-per-SM) kernel
 };
 cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, uint32_t n, uint64_t* d_out,
                           uint32_t* d_status, const DecodeScratch& scr, cudaStream_t st,

@@ -61,7 +61,7 @@ __host__ __device__ constexpr uint32_t mwords(uint32_t l) { return l < 2 ? 1u : 
 __host__ __device__ constexpr uint32_t moff(uint32_t l) { return l == 0 ? 0u : moff(l - 1) + mwords(l - 1); }
 // Shared memory holds the node values of parent levels 0..KL-1 and the
 // activity masks of all parent levels.  KL = 6: every level of a 64^3 brick
-// (two CTAs per SM).  KL = 5: an eighth of the value space (five CTAs per SM);
+// (two CTAs per SM).  KL = 5: an eighth of the value space (six CTAs per SM);
 // a 64^3 brick's level-5 values (its last parent level) then live in the CTA's
 // global scratch, where they stay in L2.
 constexpr uint32_t kSmallLevels = kSmallLod;
@@ -793,7 +793,7 @@ cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, ui
     if (n == 0) return cudaSuccess;
     if (ds.L > kDecLevels + 1) return cudaErrorInvalidValue;  // bricks up to 64^3
     const bool narrow = ds.max_P < 0xFFFFu;
-    // the four-CTA variant when the dataset's bricks are 32^3 or smaller, when the caller
+    // the small variant when the dataset's bricks are 32^3 or smaller, when the caller
     // says every request is at LOD 5 or coarser, or when asked to take every request
     const bool small = ds.L <= kSmallLevels + 1 || (cfg && (cfg->small_only || cfg->layout == 1));
     cudaError_t e = cudaMemsetAsync(scr.d_queue, 0, sizeof(uint32_t), st);
