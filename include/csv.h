@@ -361,7 +361,9 @@ typedef struct csv_serve_info {
 } csv_serve_info;
 
 /* `hidden`: labels the transfer function hides (host array, any order); a
- * brick whose palette has no other non-zero label is empty. */
+ * brick whose palette has no other non-zero label is empty.  Creation also
+ * builds the dataset's transfer function for RGBA frames (csv_transfer_function:
+ * a host copy and sort of every palette label, once). */
 int csv_serve_create(csv_ctx* ctx, const csv_dataset* ds, const csv_serve_config* cfg, const uint64_t* hidden,
                      uint32_t n_hidden, csv_server** out);
 /* d_label (W*H u64) and d_depth (W*H f32) are device images the step writes. */
