@@ -20,7 +20,7 @@ constexpr uint32_t kHeaderBytes = 152;    // 16 B header + 136 B model (fileIO.c
 // Seek-index spacing: one decoder checkpoint (16 bytes) every this many ops.
 // Each checkpoint starts one independent rANS segment in the decoder, so the
 // spacing trades the serial segment length (latency) against index size.
-constexpr uint32_t kOpsPerCheckpoint = 32;
+constexpr uint32_t kOpsPerCheckpoint = 16;
 
 // Op codes (types.hpp:162-171) and nibble layout (op << 1 | stop, brickEncoding.cpp:66-67).
 enum : uint32_t { OP_RP = 0, OP_RX = 1, OP_RY = 2, OP_RZ = 3, OP_PA = 4, OP_P0 = 5, OP_PD = 6 };
