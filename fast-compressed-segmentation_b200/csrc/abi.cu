@@ -93,6 +93,22 @@ int abi_ensure_scratch(csv_ctx* ctx, uint32_t b) {
     return CSV_OK;
 }
 
+int abi_ensure_scratch_small(csv_ctx* ctx) {
+    if (ctx->scr_small.base) return CSV_OK;
+    const size_t bytes = decode_scratch_small_bytes(ctx->device);
+    cudaError_t e = cudaMalloc(&ctx->scr_small.base, bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->scr_small.d_queue, 64);
+    if (e != cudaSuccess) {
+        cudaFree(ctx->scr_small.base);
+        ctx->scr_small.base = nullptr;
+        return abi_fail(ctx, CSV_ENOMEM, std::string("decode scratch: ") + cudaGetErrorString(e));
+    }
+    ctx->scr_small.per_cta = decode_scratch_per_cta(1u << kSmallLod, kSmallLod);
+    ctx->scr_small.ctas = (uint32_t)(bytes / ctx->scr_small.per_cta);
+    ctx->scr_small.bytes = bytes;
+    return CSV_OK;
+}
+
 }  // namespace csv
 
 namespace {
@@ -297,6 +313,8 @@ void csv_destroy(csv_ctx* ctx) {
     DeviceGuard g(ctx->device);
     cudaFree(ctx->scr.base);
     cudaFree(ctx->scr.d_queue);
+    cudaFree(ctx->scr_small.base);
+    cudaFree(ctx->scr_small.d_queue);
     for (int i = 0; i < 2; ++i) {
         cudaFree(ctx->chunk_buf[i]);
         if (ctx->pipe_stream[i]) cudaStreamDestroy(ctx->pipe_stream[i]);
@@ -687,8 +705,8 @@ struct csv_graph {
 namespace {
 
 // The graph's schedule.  Requests above LOD 5 (64^3 outputs) go to the decode
-// kernel's large variant, the rest to its small-footprint variant with twice
-// the CTAs per SM; each part keeps the request order, or with `lpt` runs
+// kernel's large variant, the rest to its small-footprint variant with three
+// times the CTAs per SM; each part keeps the request order, or with `lpt` runs
 // largest first (estimated work = nSymbols of the brick, rANS + replay, plus a
 // quarter of the labels written).  ord = [large part | small part].
 int graph_schedule(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_reqs, uint32_t n, bool lpt,
@@ -729,6 +747,8 @@ int csv_decode_graph_create(csv_ctx* ctx, const csv_dataset* ds, const csv_reque
     int rc = ensure_scratch(ctx, ds->d.b);
     if (rc) return rc;
     decode_grid(ctx->device, 1);  // occupancy queries happen outside the capture
+    const bool split = ds->d.L > kSmallLod + 1 && n && !(cfg && cfg->layout != 0);
+    if (split && (rc = abi_ensure_scratch_small(ctx))) return rc;
     csv_graph* gr = new (std::nothrow) csv_graph();
     if (!gr) return fail(ctx, CSV_ENOMEM, "host allocation");
     gr->ctx = ctx;
@@ -739,7 +759,6 @@ int csv_decode_graph_create(csv_ctx* ctx, const csv_dataset* ds, const csv_reque
         dc.layout = cfg->layout;
     }
     // a dataset with 64^3 bricks: split the requests by output size (two launches), else one launch
-    const bool split = ds->d.L > kSmallLod + 1 && n && dc.layout == 0;
     uint32_t n_large = n;
     if (split || (cfg && cfg->lpt && n)) {
         std::vector<uint32_t> ord;
@@ -768,18 +787,24 @@ int csv_decode_graph_create(csv_ctx* ctx, const csv_dataset* ds, const csv_reque
             le = launch_decode(ds->d, d_reqs, n, d_out, d_status, ctx->scr, s, &dc);
             gr->kernels = n ? 1u : 0u;
         } else {
-            // the large outputs first (longest bricks), then the small ones at twice the occupancy
+            // the large outputs first (longest bricks), then the small ones at three times the
+            // occupancy.  With both parts present the second is a programmatic dependent of the
+            // first, with its own scratch and queue (reset before the first launch): its CTAs
+            // fill the SMs that the first launch's CTAs leave once its queue has run dry.
             DecodeConfig part = dc;
             part.n_order = n_large;
-            if (n_large) {
+            const bool both = n_large && n > n_large;
+            if (both) le = cudaMemsetAsync(ctx->scr_small.d_queue, 0, sizeof(uint32_t), s);
+            if (le == cudaSuccess && n_large) {
                 le = launch_decode(ds->d, d_reqs, n, d_out, d_status, ctx->scr, s, &part);
                 ++gr->kernels;
             }
             part.order = gr->d_order + n_large;
             part.n_order = n - n_large;
             part.small_only = true;
+            part.pdl = both;
             if (le == cudaSuccess && n > n_large) {
-                le = launch_decode(ds->d, d_reqs, n, d_out, d_status, ctx->scr, s, &part);
+                le = launch_decode(ds->d, d_reqs, n, d_out, d_status, both ? ctx->scr_small : ctx->scr, s, &part);
                 ++gr->kernels;
             }
         }

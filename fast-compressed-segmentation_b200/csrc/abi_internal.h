@@ -14,6 +14,9 @@ struct csv_ctx {
     std::string err;
     csv::DecodeScratch scr;
     uint32_t scr_b = 0;
+    // the second launch of a split graph (outputs of 32^3 and smaller) runs beside the first
+    // one's last CTAs, so it has scratch and a queue counter of its own; created on first use
+    csv::DecodeScratch scr_small;
     csv::EncoderState* enc = nullptr;
     // csv_decode_image's pipeline: two chunk buffers (decode one while the
     // other drains to the host), its streams and events; created on first use
@@ -35,6 +38,8 @@ int abi_fail(csv_ctx* ctx, int code, const std::string& msg);
 int abi_cuda_fail(csv_ctx* ctx, cudaError_t e, const char* where);
 // Size the context's decode scratch for bricks of edge b (grows, never shrinks).
 int abi_ensure_scratch(csv_ctx* ctx, uint32_t b);
+// Allocate the context's scratch for the small variant's part of a split schedule.
+int abi_ensure_scratch_small(csv_ctx* ctx);
 // buildTransferFunctionBuffers (webgpuSetup.js:389-465) on a dataset: its distinct
 // non-zero palette labels ascending and their RGBA8, hidden labels transparent.
 cudaError_t transfer_function(const DeviceDataset& d, const uint64_t* hidden, uint32_t n_hidden,

@@ -100,6 +100,8 @@ struct DecodeScratch {
 };
 size_t decode_scratch_per_cta(uint32_t b, uint32_t kl = 6);
 size_t decode_scratch_bytes(int device, uint32_t b);
+// Scratch for the small variant's CTAs at 32^3 outputs (the second part of a split schedule).
+size_t decode_scratch_small_bytes(int device);
 uint32_t decode_grid(int device, uint32_t n);
 // Requests at this LOD (32^3 labels) or coarser can run in the decode kernel's
 // small-footprint variant (six CTAs per SM instead of two).
@@ -113,6 +115,9 @@ struct DecodeConfig {
     const uint32_t* n_dev = nullptr;  // device-resident queue length (<= n or n_order), or null
     bool small_only = false;          // every queued request is at LOD 5 (32^3) or coarser
     uint32_t layout = 0;              // 1: every request in the small (six-CTA-per-SM) kernel
+    // launched as a programmatic dependent of the previous kernel in the stream: its CTAs
+    // start on the SMs that kernel's CTAs leave; the caller has reset scr.d_queue
+    bool pdl = false;
 };
 cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, uint32_t n, uint64_t* d_out,
                           uint32_t* d_status, const DecodeScratch& scr, cudaStream_t st,

@@ -472,6 +472,10 @@ __global__ void __launch_bounds__(dec_threads<KL>(), KL == kDecLevels ? 2 : 6) d
     extern __shared__ __align__(16) uint8_t smem_raw[];
     DecShared<V, KL>& S = *reinterpret_cast<DecShared<V, KL>*>(smem_raw);
     const uint32_t tid = threadIdx.x, T = blockDim.x;
+    // A kernel launched as this one's programmatic dependent (the second part of a
+    // split schedule: other requests, other scratch) may start on the SMs this
+    // grid's CTAs leave; without one this is a no-op.
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     constexpr uint32_t LABEL0 = sizeof(V) == 2 ? 0xFFFFu : PIDX_LABEL0;
 
     for (uint32_t i = tid; i < kTot; i += T) S.lut[i] = A.lut[i];
@@ -723,6 +727,10 @@ __global__ void __launch_bounds__(dec_threads<KL>(), KL == kDecLevels ? 2 : 6) d
         if (tid == 0) A.status[w] = S.status;
         __syncthreads();
     }
+    // Launched as a programmatic dependent: finish only after the kernel before
+    // this one has, so that work after this grid in the stream sees both grids'
+    // results.  Otherwise a no-op.
+    asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 size_t decode_scratch_per_cta(uint32_t b, uint32_t kl) {
@@ -767,6 +775,11 @@ size_t decode_scratch_bytes(int device, uint32_t b) {
     return std::max(big, small);
 }
 
+size_t decode_scratch_small_bytes(int device) {
+    return decode_scratch_per_cta(1u << kSmallLevels, kSmallLevels) *
+           (size_t)std::max(occupancy<uint16_t, kSmallLevels>(device), occupancy<uint32_t, kSmallLevels>(device));
+}
+
 template <class V, uint32_t KL>
 static cudaError_t launch_variant(const DecodeArgs& A0, const DecodeScratch& scr, cudaStream_t st,
                                   const DecodeConfig* cfg, int device) {
@@ -784,6 +797,19 @@ static cudaError_t launch_variant(const DecodeArgs& A0, const DecodeScratch& scr
     if (grid > cap) grid = (uint32_t)cap;
     if (grid == 0) return cudaErrorInvalidValue;
     A.stage_cap = (cfg && !cfg->stage) ? 0u : stage_cap<V, KL>();
+    if (cfg && cfg->pdl) {
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3(grid);
+        lc.blockDim = dim3(dec_threads<KL>());
+        lc.dynamicSmemBytes = sizeof(DecShared<V, KL>);
+        lc.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        lc.attrs = at;
+        lc.numAttrs = 1;
+        return cudaLaunchKernelEx(&lc, decode_kernel<V, KL>, A);
+    }
     decode_kernel<V, KL><<<grid, dec_threads<KL>(), sizeof(DecShared<V, KL>), st>>>(A);
     return cudaGetLastError();
 }
@@ -796,8 +822,10 @@ cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, ui
     // the small variant when the dataset's bricks are 32^3 or smaller, when the caller
     // says every request is at LOD 5 or coarser, or when asked to take every request
     const bool small = ds.L <= kSmallLevels + 1 || (cfg && (cfg->small_only || cfg->layout == 1));
-    cudaError_t e = cudaMemsetAsync(scr.d_queue, 0, sizeof(uint32_t), st);
-    if (e != cudaSuccess) return e;
+    if (!(cfg && cfg->pdl)) {  // a programmatic dependent follows a kernel, not this reset
+        cudaError_t e = cudaMemsetAsync(scr.d_queue, 0, sizeof(uint32_t), st);
+        if (e != cudaSuccess) return e;
+    }
     DecodeArgs A;
     A.bricks = ds.d_bricks;
     A.pal = ds.d_pal;

@@ -115,6 +115,32 @@ def test_graph_replay_matches(codec, mixed, cfg):
     g.close()
 
 
+def test_split_graph_finishes_before_later_stream_work(codec, mixed):
+    """In a split graph the second launch (the small outputs) may start while the first one's last CTAs
+    still run, and it ends only after the first one has: work queued after the graph on the same stream,
+    with no synchronisation between, reads every label of both launches."""
+    import torch
+    from csvb200 import DecodeConfig, requests_tensor
+    cat, dss, sizes_b, offsets, parts_ref = mixed
+    reqs, bricks, lods, dst, total = _mixed_requests(sizes_b, np.random.default_rng(9))
+    assert (lods > 5).any() and (lods <= 5).any()  # both launches have work
+    out = torch.zeros(total, dtype=torch.int64, device="cuda")
+    st = torch.full((len(reqs),), -1, dtype=torch.int32, device="cuda")
+    g = codec.decode_graph(cat, requests_tensor(reqs), out, st, DecodeConfig(0, 1, 0, 0))
+    assert g.kernels == 2
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        for _ in range(3):
+            out.fill_(-3)
+            g.launch(s)
+            got, got_st = out.clone(), st.clone()  # same stream, straight after the replay
+            s.synchronize()
+            assert int(got_st.abs().max()) == 0
+            _check(got.cpu().numpy().view(np.uint64), bricks, lods, dst, parts_ref, offsets)
+    g.close()
+
+
 def test_autotune_returns_a_working_config(codec, mixed):
     import torch
     from csvb200 import requests_tensor
