@@ -197,7 +197,11 @@ int csv_decode_graph_create(csv_ctx* ctx, const csv_dataset* ds, const csv_reque
                             uint64_t* d_out, uint32_t* d_status, const csv_decode_config* cfg, csv_graph** out);
 int csv_graph_launch(csv_graph* g, void* stream);
 /* Decode kernels one replay of the graph launches (1, or 2 when it splits the
- * requests by output size; 0 for an empty batch). */
+ * requests by output size; 0 for an empty batch).  In a split replay the second
+ * kernel may start while the first one's last bricks are still decoding; the
+ * replay as a whole still completes in stream order like any other graph launch.
+ * A split graph uses a second decode scratch of the context (allocated on the
+ * first split graph's creation), so graphs of one context replay one at a time. */
 int csv_graph_kernels(const csv_graph* g, uint32_t* n);
 void csv_graph_destroy(csv_graph* g);
 /* Times every candidate configuration on this batch (a captured graph each,
