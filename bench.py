@@ -290,7 +290,7 @@ def run_b200(args):
 
     e2e_ms = []
     with ThreadPoolExecutor(max_workers=len(per_img)) as ex:
-        for k in range(10):  # one warm-up, nine timed: the median (host copies share the machine's PCIe and memory)
+        for k in range(16):  # one warm-up, fifteen timed: the median (host copies share the machine's PCIe and memory)
             barrier(pg)
             t0 = time.perf_counter()
             list(ex.map(decode_file, range(len(per_img))))
