@@ -175,9 +175,9 @@ def _graph_run(codec, cat, reqs, total, layout=0):
 @pytest.mark.parametrize("layout", [0, 1])
 @pytest.mark.parametrize("part", ["coarse_only", "full64_only", "mix_with_bad"])
 def test_graph_split_by_output_size(codec, mixed, part, layout):
-    """A dataset with 64^3 bricks is decoded by two launches (outputs above 32^3, then the rest at twice the
-    occupancy; layout 0) or by the small kernel alone (layout 1); either part may be empty, and a refused
-    request in either part leaves the others intact."""
+    """A dataset with 64^3 bricks is decoded by two launches (outputs above 32^3, then the rest at three times
+    the occupancy, overlapping the first launch's tail; layout 0) or by the small kernel alone (layout 1);
+    either part may be empty, and a refused request in either part leaves the others intact."""
     from csvb200 import CSV_BRICK_BADREQ, requests
     cat, dss, sizes_b, offsets, parts_ref = mixed
     rng = np.random.default_rng(8)
