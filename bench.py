@@ -327,16 +327,10 @@ def run_b200(args):
             "metric": METRIC, "value": round(value, 3), "unit": "Gvox/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": W["name"], "volume": [Wd, H, D],
-                       "bricks": {"32^3": nl, "64^3": nr, "split_x": sx},
-                       "left": f"Voronoi {W['n_cells']} cells, 32^3 bricks",
-                       "right": f"{W['n_tubes']} tubes r {W['r_min']}-{W['r_max']} over it, 64^3 bricks",
-                       "lod": "full resolution", "seed": W["seed"], "launch": "one CUDA graph (csv_decode_graph)",
-                       "decode_config": best.as_dict(), "autotuned": not args.config,
-                       "autotune_ms": round(tune_ms, 4),
-                       "stream_bytes": info.stream_bytes, "image_bytes": [len(img_left), len(img_right)],
-                       "l2": "flushed between timed steps (256 MiB buffer)",
-                       "parallelism": f"weak x{world}, bricks independent, no collective"},
+            "config": workload_config(W, nl, nr, [img_left, img_right]),
+            "decode": {"launch": "one CUDA graph (csv_decode_graph)", "decode_config": best.as_dict(),
+                       "autotuned": not args.config, "autotune_ms": round(tune_ms, 4),
+                       "device_stream_bytes": info.stream_bytes},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                          "frac": round(achieved / hbm, 4), "traffic": load_traffic("decode_kernel", W["name"]),
                          "algorithmic_bytes": alg_bytes, "peak_kind": hbm_kind},
@@ -460,9 +454,10 @@ def selector1024(codec, dev, args):
     return out
 
 
-def orbit_path(n, center, seed):
+def orbit_path(n, center, seed, scale=1.0):
     """Seeded orbit with zoom (orbitController.js:100-123 camera placement): two turns, pitch swinging
-    +-0.35 rad, radius 1600..3600 voxels, small seeded jitter on every frame."""
+    +-0.35 rad, radius 1600..3600 voxels (times scale, for smaller volumes), small seeded jitter on every
+    frame."""
     import math
     from csvb200.camera import orbit
     rng = np.random.default_rng(seed)
@@ -472,7 +467,7 @@ def orbit_path(n, center, seed):
         t = f / n
         yaw = 2 * math.pi * 2 * t + 0.01 * jit[f, 0]
         pitch = 0.35 * math.sin(2 * math.pi * 3 * t) + 0.01 * jit[f, 1]
-        radius = 2600.0 + 1000.0 * math.cos(2 * math.pi * 1.5 * t) + 10.0 * jit[f, 2]
+        radius = scale * (2600.0 + 1000.0 * math.cos(2 * math.pi * 1.5 * t) + 10.0 * jit[f, 2])
         views.append(orbit(center, radius, yaw, pitch))
     return views
 
@@ -656,68 +651,122 @@ def load_traffic(kernel: str, workload: str):
     return d.get(kernel, {}).get(workload)
 
 
+def image_stats(img: bytes):
+    """Per brick of a .csbd v1 image: encoded stream bytes E and palette entries P."""
+    import struct
+    nb = struct.unpack_from("<I", img, 8)[0]
+    o, E, P = 152, [], []
+    for _ in range(nb):
+        p = struct.unpack_from("<I", img, o + 4)[0]
+        o += 8 + 8 * p
+        e = struct.unpack_from("<I", img, o)[0]
+        o += 8 + e
+        E.append(e)
+        P.append(p)
+    return np.array(E, np.int64), np.array(P, np.int64)
+
+
+def stream_histogram(images):
+    """Encoded stream sizes and palette sizes over the bricks of the given images: power-of-two bins of E."""
+    E = np.concatenate([image_stats(im)[0] for im in images])
+    P = np.concatenate([image_stats(im)[1] for im in images])
+    edges = [0, 64, 256, 1024, 4096, 16384, 65536, 131072, 262144, 1 << 40]
+    names = ["<64B", "64-256B", "256B-1K", "1-4K", "4-16K", "16-64K", "64-128K", "128-256K", ">=256K"]
+    cnt = np.histogram(E, bins=edges)[0]
+    return {"bricks_by_stream_bytes": {k: int(c) for k, c in zip(names, cnt)},
+            "stream_bytes_min": int(E.min()), "stream_bytes_median": int(np.median(E)), "stream_bytes_max": int(E.max()),
+            "palette_max": int(P.max()), "palette_median": int(np.median(P))}
+
+
+def workload_config(W, nl, nr, images):
+    """The config object both arms print: the workload, its sizes and the measured stream-size distribution."""
+    D, H, Wd = W["shape"]
+    return {"workload": W["name"], "volume": [Wd, H, D],
+            "bricks": {"32^3": nl, "64^3": nr, "split_x": W["split_x"]},
+            "left": f"Voronoi {W['n_cells']} cells, {W['brick_left']}^3 bricks",
+            "right": f"{W['n_tubes']} tubes r {W['r_min']}-{W['r_max']} over it, {W['brick_right']}^3 bricks",
+            "lod": "full resolution", "seed": W["seed"],
+            "stream_bytes": int(sum(int(image_stats(im)[0].sum()) for im in images)),
+            "image_bytes": [len(im) for im in images],
+            "streams": stream_histogram(images),
+            "l2": "flushed between timed steps (256 MiB buffer); inputs and outputs larger than L2",
+            "parallelism": "bricks independent, no collective"}
+
+
 def run_reference(args):
-    """The reference's own CPU decoder (oracle/_ref: decodeRansStream + decodeBrick<b>) on every host thread."""
+    """The reference's own CPU decoder (oracle/_ref: decodeRansStream + decodeBrick<b>) on every host thread.
+
+    The input images are built without the product library: the workload generator restated on the CPU
+    (oracle or_synth_volume, the same volume as csv_synth_volume) and encoded by the oracle's threaded
+    encoder (the same bytes as the reference encoder and the GPU encoder).  Only oracle/ libraries load."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import torch
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    from csvb200 import Codec
     from oracle import REF_SO, Oracle, Reference
     W = WORKLOADS[args.workload]
     D, H, Wd = W["shape"]
     sx = W["split_x"]
     bl, br = W["brick_left"], W["brick_right"]
-    codec = Codec(0)
-    vol = torch.empty(W["shape"], dtype=torch.int64, device="cuda")
-    codec.synth_volume(vol, W["kind"], W["n_cells"], W["n_tubes"], W["r_min"], W["r_max"], W["zero_frac"], W["seed"])
-    # the input images: the reference encoder's bytes equal the GPU encoder's (tests/test_encode_gpu.py)
-    img_left = encode_to_host(codec, vol[:, :, :sx].contiguous(), bl)
-    img_right = encode_to_host(codec, vol[:, :, sx:].contiguous(), br)
+    O = Oracle()
+    t0 = time.perf_counter()
+    vol = O.synth_volume(W["shape"], W["kind"], W["n_cells"], W["n_tubes"], W["r_min"], W["r_max"], W["zero_frac"],
+                         W["seed"])
+    img_left = O.encode_threads(np.ascontiguousarray(vol[:, :, :sx]), bl)
+    img_right = O.encode_threads(np.ascontiguousarray(vol[:, :, sx:]), br)
     del vol
+    prep_s = time.perf_counter() - t0
     nl, nr = image_bricks(img_left)[0], image_bricks(img_right)[0]
     threads = os.cpu_count() or 1
     if os.path.exists(REF_SO):
         R = Reference()
         kind = "reference"
 
-        def step():
+        def step(stride):
             # decodeBrick throws on a brick whose root stop bit is set (the whole brick one label): the
             # reference decodes nothing there; such bricks are counted, not fatal
-            return R.decode_parallel(img_left, threads) + R.decode_parallel(img_right, threads)
+            return R.decode_parallel(img_left, threads, stride=stride) + \
+                R.decode_parallel(img_right, threads, stride=stride)
     else:
-        O = Oracle()
         kind, threads = "port", 1
 
-        def step():
+        def step(stride):
             O.decode_image(img_left, bl.bit_length() - 1)
             O.decode_image(img_right, br.bit_length() - 1)
             return 0
-    for _ in range(min(args.warmup, 1)):
-        step()
+    # the first warm-up step sizes the sample: every stride-th brick, so that the remaining warm-up and
+    # timed steps take about a minute in all
+    t1 = time.perf_counter()
+    step(1)
+    full_s = time.perf_counter() - t1
+    budget_s = 60.0
+    stride = max(1, int(np.ceil(full_s * (args.steps + args.warmup - 1) / budget_s)))
+    for _ in range(args.warmup - 1):
+        step(stride)
     times = []
     thrown = 0
-    for _ in range(min(args.steps, 3)):
-        t0 = time.perf_counter()
-        thrown = step()
-        times.append(time.perf_counter() - t0)
+    for _ in range(args.steps):
+        t1 = time.perf_counter()
+        thrown = step(stride)
+        times.append(time.perf_counter() - t1)
     s = statistics.mean(times)
-    nvox = D * H * Wd
+    nvox = len(range(0, nl, stride)) * bl ** 3 + len(range(0, nr, stride)) * br ** 3
     v = nvox / s / 1e9
+    sample = (f"every step decodes {'all' if stride == 1 else f'every {stride}th of the'} {nl + nr} bricks of both "
+              f"images at full resolution ({nvox} voxels; decodeRansStream + decodeBrick<b>), bricks split over "
+              f"{threads} host threads")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": "Gvox/s", "n_gpus": world,
-        "steps": len(times), "warmup": min(args.warmup, 1), "ms_per_step": round(s * 1e3, 2),
+        "steps": len(times), "warmup": args.warmup, "ms_per_step": round(s * 1e3, 2),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": {"workload": W["name"], "volume": [Wd, H, D], "bricks": {"32^3": nl, "64^3": nr},
-                   "lod": "full resolution",
-                   "bricks_thrown": int(thrown),  # uniform bricks: decodeBrick throws, nothing decoded
-                   "note": "the reference C++ decoder throws on bricks that are one label (root stop bit); "
-                           "they are counted, and the GPU decoder fills them with palette[0]"},
-        "cpu_baseline": {"value": round(v, 4), "unit": "Gvox/s", "cores": threads, "kind": kind,
-                         "sample": f"every step decodes all {nl + nr} bricks of both images at full resolution "
-                                   f"(decodeRansStream + decodeBrick<b>), bricks split over {threads} host threads"},
+        "config": workload_config(W, nl, nr, [img_left, img_right]),
+        "reference": {"bricks_thrown_per_step": int(thrown), "stride": stride, "input_build_s": round(prep_s, 1),
+                      "inputs": "oracle CPU generator (= csv_synth_volume) + oracle threaded encoder (= the "
+                                "reference encoder's bytes); no product library in this process",
+                      "note": "the reference C++ decoder throws on bricks that are one label (root stop bit); "
+                              "they are counted, and the GPU decoder fills them with palette[0]"},
+        "cpu_baseline": {"value": round(v, 4), "unit": "Gvox/s", "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": round(v, 4), "unit": "Gvox/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 

@@ -85,6 +85,9 @@ struct DecShared {
     BrickDesc br;
     csv_request req;
     uint32_t work, status;
+    // the stream copy's bounded waits: rewait is set when the first wait gave up (one more wait before the
+    // staging region is reused); drained when the second gave up too (the CTA decodes nothing more)
+    uint32_t rewait, drained;
     alignas(8) uint64_t bar;  // mbarrier of the stream copy
 };
 template <class V, uint32_t KL>
@@ -479,9 +482,16 @@ __global__ void __launch_bounds__(dec_threads<KL>(), KL == kDecLevels ? 2 : 6) d
     constexpr uint32_t LABEL0 = sizeof(V) == 2 ? 0xFFFFu : PIDX_LABEL0;
 
     for (uint32_t i = tid; i < kTot; i += T) S.lut[i] = A.lut[i];
-    if (tid == 0) mbar_init(&S.bar);
+    if (tid == 0) {
+        mbar_init(&S.bar);
+        S.rewait = 0;
+        // Set when a copy into the staging region was still unconfirmed after two
+        // bounded waits.  The region is then never touched again: every request the
+        // CTA takes from then on is reported CSV_BRICK_TIMEOUT without output.
+        S.drained = 0;
+    }
     uint32_t phase = 0;     // parity of the stream-copy barrier
-    bool stage_ok = true;   // cleared if a copy ever fails to land
+    bool stage_ok = true;   // cleared if a copy ever fails to land in time
 
     // per-CTA scratch: op records | active-node lists of every parent level
     uint8_t* scr = A.scratch + (uint64_t)blockIdx.x * A.scratch_per_cta;
@@ -527,6 +537,11 @@ __global__ void __launch_bounds__(dec_threads<KL>(), KL == kDecLevels ? 2 : 6) d
             __syncthreads();
             continue;
         }
+        if (S.drained) {  // the staging region may still receive a lost copy: decode nothing
+            if (tid == 0) A.status[w] = CSV_BRICK_TIMEOUT;
+            __syncthreads();
+            continue;
+        }
         if (model != cur_model) {  // made visible by the barrier after the palette copy
             for (uint32_t i = tid; i < kTot; i += T) S.lut[i] = A.lut[(size_t)model * kTot + i];
             cur_model = model;
@@ -557,11 +572,14 @@ __global__ void __launch_bounds__(dec_threads<KL>(), KL == kDecLevels ? 2 : 6) d
             const uint32_t nseg = (n_need + A.S - 1) / A.S;
             bool staged = false;
             if (stage) {
-                staged = mbar_wait(&S.bar, phase);
-                phase ^= 1u;
-                if (!staged) {  // the copy did not land in time: read this brick from global memory
+                // one decision for the whole CTA: staged only if every thread saw the copy land
+                staged = __syncthreads_and(mbar_wait(&S.bar, phase)) != 0;
+                if (staged) {
+                    phase ^= 1u;
+                } else {  // the copy did not land in time: read this brick from global memory
                     st |= CSV_BRICK_TIMEOUT;
-                    stage_ok = false;
+                    stage_ok = false;  // and stage nothing more
+                    if (tid == 0) S.rewait = 1;  // read after the barrier that ends the rANS phase
                 }
             }
             if (staged)
@@ -570,6 +588,22 @@ __global__ void __launch_bounds__(dec_threads<KL>(), KL == kDecLevels ? 2 : 6) d
             else
                 decode_segments<true>(A, br, A.enc + br.enc_off, S.lut, n_need, nseg, recs, st, LABEL0);
             __syncthreads();  // the staged stream is dead: its space becomes the level arrays
+            if (S.rewait) {
+                // The late copy must land before the staging region is written: a second
+                // bounded wait on the same phase.  If it gives up too, this brick is
+                // reported without output and the CTA decodes nothing more (drained).
+                const bool landed = __syncthreads_and(mbar_wait(&S.bar, phase)) != 0;
+                if (landed) phase ^= 1u;
+                if (tid == 0) {
+                    S.rewait = 0;
+                    if (!landed) {
+                        S.drained = 1;
+                        A.status[w] = st | CSV_BRICK_TIMEOUT;
+                    }
+                }
+                __syncthreads();
+                if (!landed) continue;
+            }
             // level 0: the root, value palette[0], active; clear the other masks
             for (uint32_t i = tid; i < moff(t); i += T) S.mask[i] = i == 0 ? 1u : 0u;
             if (tid == 0) {

@@ -130,7 +130,7 @@ __global__ void voronoi_kernel(uint64_t* __restrict__ vol, VoronoiArgs a) {
         }
         uint64_t lab = a.ids[besti];
         if (a.zero_cell && a.zero_cell[besti]) lab = 0;
-        if (px * a.nx + py * a.ny + pz * a.nz >= a.thr) lab = 0;
+        if (__fadd_rn(__fadd_rn(__fmul_rn(px, a.nx), __fmul_rn(py, a.ny)), __fmul_rn(pz, a.nz)) >= a.thr) lab = 0;
         vol[x + (uint64_t)a.W * (y + (uint64_t)a.H * z)] = lab;
     }
 }
@@ -141,23 +141,30 @@ struct Piece {
     int lo[3], hi[3];
 };
 
+__device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(ax, bx), __fmul_rn(ay, by)), __fmul_rn(az, bz));
+}
+
 // One block per straight piece of a tube: voxels within r of the piece get the
 // highest tube number that covers them (atomicMax makes overlaps deterministic).
 __global__ void tube_kernel(uint32_t* __restrict__ owner, const Piece* __restrict__ pieces, uint32_t W, uint32_t H) {
     Piece p = pieces[blockIdx.x];
     int ex = p.hi[0] - p.lo[0], ey = p.hi[1] - p.lo[1], ez = p.hi[2] - p.lo[2];
     if (ex <= 0 || ey <= 0 || ez <= 0) return;
+    // every product and sum rounded on its own (no contracted multiply-adds), so that
+    // a CPU restatement with the same operation order gives the same volume
     float abx = p.bx - p.ax, aby = p.by - p.ay, abz = p.bz - p.az;
-    float den = fmaxf(abx * abx + aby * aby + abz * abz, 1e-12f);
-    float r2 = p.r * p.r;
+    float den = fmaxf(dot3(abx, aby, abz, abx, aby, abz), 1e-12f);
+    float r2 = __fmul_rn(p.r, p.r);
     uint32_t n = (uint32_t)ex * ey * ez;
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
         int x = p.lo[0] + (int)(i % ex), y = p.lo[1] + (int)((i / ex) % ey), z = p.lo[2] + (int)(i / (ex * ey));
-        float qx = x + 0.5f - p.ax, qy = y + 0.5f - p.ay, qz = z + 0.5f - p.az;
-        float s = (qx * abx + qy * aby + qz * abz) / den;
+        float qx = (x + 0.5f) - p.ax, qy = (y + 0.5f) - p.ay, qz = (z + 0.5f) - p.az;
+        float s = __fdiv_rn(dot3(qx, qy, qz, abx, aby, abz), den);
         s = fminf(1.f, fmaxf(0.f, s));
-        float dx = qx - s * abx, dy = qy - s * aby, dz = qz - s * abz;
-        if (dx * dx + dy * dy + dz * dz < r2) atomicMax(owner + x + (uint64_t)W * (y + (uint64_t)H * z), p.tube + 1);
+        float dx = __fsub_rn(qx, __fmul_rn(s, abx)), dy = __fsub_rn(qy, __fmul_rn(s, aby)),
+              dz = __fsub_rn(qz, __fmul_rn(s, abz));
+        if (dot3(dx, dy, dz, dx, dy, dz) < r2) atomicMax(owner + x + (uint64_t)W * (y + (uint64_t)H * z), p.tube + 1);
     }
 }
 
@@ -210,7 +217,12 @@ cudaError_t synth_volume(uint64_t* d_vol, uint32_t W, uint32_t H, uint32_t D, in
         double nn = sqrt(nx * nx + ny * ny + nz * nz) + 1e-12;
         nx /= nn; ny /= nn; nz /= nn;
         std::vector<double> d(65536);
-        for (auto& v : d) v = (rng.uniform() * W) * nx + (rng.uniform() * H) * ny + (rng.uniform() * D) * nz;
+        for (auto& v : d) {  // the three draws in a fixed order
+            const double a = rng.uniform() * W;
+            const double b = rng.uniform() * H;
+            const double c = rng.uniform() * D;
+            v = a * nx + b * ny + c * nz;
+        }
         std::sort(d.begin(), d.end());
         size_t q = (size_t)((1.0 - zero_frac) * (d.size() - 1));
         a.nx = (float)nx; a.ny = (float)ny; a.nz = (float)nz;

@@ -12,8 +12,9 @@
  */
 #include "csv_oracle.h"
 
-#include <stdlib.h>
 #include <math.h>
+#include <pthread.h>
+#include <stdlib.h>
 #include <string.h>
 
 #define EMPTY_LABEL UINT64_MAX /* types.hpp:19 */
@@ -394,6 +395,125 @@ static int encode_core(const uint64_t* vol, size_t W, size_t H, size_t D, uint32
 int or_encode_sel(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b, const uint8_t* sel,
                   const uint32_t* tables, uint32_t n_tables, uint8_t** out, size_t* out_len) {
     return encode_core(vol, W, H, D, b, sel, tables, n_tables, 0, 0, NULL, NULL, out, out_len);
+}
+
+/* or_encode with the per-brick work on `threads` threads: the same steps in the
+ * same order per brick (split, pyramid, encodeBrick, packing; rANS with the one
+ * model of the every-512th sample), so the bytes equal or_encode's.  Phase 1
+ * builds each brick's palette and nibbles, the sample histogram is summed in
+ * file order, phase 2 runs each brick's rANS, and the records are written in
+ * file order. */
+typedef struct {
+    const uint64_t* vol;
+    size_t W, H, D, nby, nbz;
+    uint32_t b, L;
+    size_t i0, i1;
+    uint64_t** pals; uint32_t* npal;
+    uint8_t** nibs; uint32_t* nnib;
+    uint8_t** rans; uint32_t* nrans;
+    const uint32_t* freq; const uint32_t* cum;
+    int phase;
+} encjob_t;
+
+static void* encode_range(void* arg) {
+    encjob_t* j = (encjob_t*)arg;
+    if (j->phase == 1) {
+        size_t ntot = level_off(j->L);
+        uint64_t* lab = (uint64_t*)malloc(ntot * 8);
+        uint8_t* cst = (uint8_t*)malloc(ntot);
+        enc_t e = {0};
+        for (size_t i = j->i0; i < j->i1; ++i) {
+            size_t bz = i % j->nbz, by = (i / j->nbz) % j->nby, bx = i / (j->nbz * j->nby);
+            cut_brick(j->vol, j->W, j->H, j->D, j->b, bx, by, bz, lab + level_off(j->L - 1));
+            build_pyramid(j->b, lab, cst);
+            encode_brick(j->b, lab, cst, &e, 0u);
+            j->pals[i] = (uint64_t*)malloc(8 * (size_t)e.np);
+            memcpy(j->pals[i], e.pal, 8 * (size_t)e.np);
+            j->npal[i] = e.np;
+            j->nibs[i] = (uint8_t*)malloc(e.nn + 1);
+            memcpy(j->nibs[i], e.nib, e.nn);
+            j->nnib[i] = e.nn;
+        }
+        free(e.pal); free(e.nib); free(lab); free(cst);
+    } else {
+        buf_t r = {0};
+        for (size_t i = j->i0; i < j->i1; ++i) {
+            r.n = 0;
+            rans_encode(j->nibs[i], j->nnib[i], j->freq, j->cum, &r);
+            j->rans[i] = (uint8_t*)malloc(r.n ? r.n : 1);
+            memcpy(j->rans[i], r.p, r.n);
+            j->nrans[i] = (uint32_t)r.n;
+        }
+        free(r.p);
+    }
+    return NULL;
+}
+
+int or_encode_threads(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b, uint32_t threads,
+                      uint8_t** out, size_t* out_len) {
+    if (b < 2 || (b & (b - 1)) || b > 1024) return -1;
+    size_t nbx = (W + b - 1) / b, nby = (H + b - 1) / b, nbz = (D + b - 1) / b;
+    size_t nb = nbx * nby * nbz;
+    if (threads < 1) threads = 1;
+    if (threads > nb) threads = nb ? (uint32_t)nb : 1u;
+    encjob_t proto = {0};
+    proto.vol = vol; proto.W = W; proto.H = H; proto.D = D; proto.nby = nby; proto.nbz = nbz;
+    proto.b = b; proto.L = levels_of(b);
+    proto.pals = (uint64_t**)calloc(nb, sizeof(void*));
+    proto.npal = (uint32_t*)calloc(nb, 4);
+    proto.nibs = (uint8_t**)calloc(nb, sizeof(void*));
+    proto.nnib = (uint32_t*)calloc(nb, 4);
+    proto.rans = (uint8_t**)calloc(nb, sizeof(void*));
+    proto.nrans = (uint32_t*)calloc(nb, 4);
+    pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * threads);
+    encjob_t* jobs = (encjob_t*)malloc(sizeof(encjob_t) * threads);
+    uint32_t freq[16], cum[17];
+    for (int phase = 1; phase <= 2; ++phase) {
+        if (phase == 2) {
+            uint64_t hist[16] = {0};
+            for (size_t i = 0; i < nb; i += 512) { /* brickEncoding.hpp:482 */
+                for (uint32_t k = 0; k < proto.nnib[i]; ++k) hist[proto.nibs[i][k]]++;
+                if (proto.nnib[i] & 1) hist[0]++;
+            }
+            or_build_model(hist, freq, cum);
+            proto.freq = freq;
+            proto.cum = cum;
+        }
+        for (uint32_t t = 0; t < threads; ++t) {
+            jobs[t] = proto;
+            jobs[t].phase = phase;
+            jobs[t].i0 = nb * t / threads;
+            jobs[t].i1 = nb * (t + 1) / threads;
+            pthread_create(&th[t], NULL, encode_range, &jobs[t]);
+        }
+        for (uint32_t t = 0; t < threads; ++t) pthread_join(th[t], NULL);
+    }
+    buf_t o = {0};
+    bput32(&o, 0x43534244u);
+    bput32(&o, 1);
+    bput32(&o, (uint32_t)nb);
+    bput32(&o, b);
+    bput32(&o, 16);
+    bput32(&o, TOT);
+    bput(&o, freq, 64);
+    bput(&o, cum, 64);
+    size_t i = 0;
+    for (size_t bx = 0; bx < nbx; ++bx)
+        for (size_t by = 0; by < nby; ++by)
+            for (size_t bz = 0; bz < nbz; ++bz, ++i) {
+                bput32(&o, or_morton3((uint32_t)bx, (uint32_t)by, (uint32_t)bz));
+                bput32(&o, proto.npal[i]);
+                bput(&o, proto.pals[i], 8 * (size_t)proto.npal[i]);
+                bput32(&o, proto.nrans[i]);
+                bput(&o, proto.rans[i], proto.nrans[i]);
+                bput32(&o, proto.nnib[i]);
+                free(proto.pals[i]); free(proto.nibs[i]); free(proto.rans[i]);
+            }
+    free(proto.pals); free(proto.npal); free(proto.nibs); free(proto.nnib); free(proto.rans); free(proto.nrans);
+    free(th); free(jobs);
+    *out = o.p;
+    *out_len = o.n;
+    return 0;
 }
 
 int or_encode_shard(const uint64_t* slab, size_t W, size_t H, size_t D, uint32_t b, uint32_t bx0, uint32_t index_base,

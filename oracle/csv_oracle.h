@@ -150,6 +150,15 @@ int or_brick_features(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_
 void or_mlp_forward(const float* params, const float* feat, uint32_t n, float* logits);
 float or_mlp_grad(const float* params, const float* feat, const uint8_t* label, uint32_t n, float* grads);
 
+/* or_encode with the bricks spread over `threads` threads (the same bytes). */
+int or_encode_threads(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_t b, uint32_t threads,
+                      uint8_t** out, size_t* out_len);
+/* The native library's seeded synthetic volume (csv_synth_volume, kinds 0-2),
+ * restated on the CPU with the same draws and float operations; vol is W*H*D
+ * u64, x fastest (csv_oracle_synth.c). */
+int or_synth_volume(uint64_t* vol, uint32_t W, uint32_t H, uint32_t D, int kind, uint32_t n_cells, uint32_t n_tubes,
+                    float r_min, float r_max, float zero_frac, uint64_t seed, uint32_t threads);
+
 void or_free(void* p);
 
 #ifdef __cplusplus

@@ -19,7 +19,11 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "libcsvoracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libcsvref.so")
-REF_SRC = "/root/reference/encoder/CSVEncoder/src"
+# The reference project's root: CSV_REFERENCE_ROOT, else where this machine keeps it.  Only the build recipe
+# (build(), oracle/Makefile) and fixture generation read it; nothing that runs on a GPU machine needs it.
+REF_ROOT = os.environ.get("CSV_REFERENCE_ROOT", "/root/reference")
+REF_SRC = os.path.join(REF_ROOT, "encoder", "CSVEncoder", "src")
+REF_SHIPPED = os.path.join(REF_ROOT, "encoder", "CSVEncoder", "compressed_dataset.csbd")
 
 _u8p = C.POINTER(C.c_uint8)
 _u32p = C.POINTER(C.c_uint32)
@@ -36,7 +40,7 @@ def build(ref: bool | None = None) -> None:
     if ref is None:
         ref = os.path.isdir(REF_SRC)
     if ref:
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_SRC={REF_SRC}"], check=True)
 
 
 class Oracle:
@@ -57,6 +61,10 @@ class Oracle:
         L.or_render_rgba_rows.argtypes = [C.POINTER(C.c_float), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                           C.c_float, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint64, _u64p, _u64p,
                                           _u32p, C.c_uint32, C.POINTER(C.c_float), _u32p]
+        L.or_encode_threads.argtypes = [_u64p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_uint32, C.c_uint32,
+                                        C.POINTER(_u8p), C.POINTER(C.c_size_t)]
+        L.or_synth_volume.argtypes = [_u64p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_uint32, C.c_uint32,
+                                      C.c_float, C.c_float, C.c_float, C.c_uint64, C.c_uint32]
         L.or_encode_shard.argtypes = [_u64p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_uint32, C.c_uint32, C.c_uint32,
                                       _u64p, _u64p, C.POINTER(_u8p), C.POINTER(C.c_size_t)]
         L.or_pyramid.argtypes = [_u64p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_uint32, C.c_uint32,
@@ -268,6 +276,31 @@ class Oracle:
         self.lib.or_free(out)
         return data
 
+    def encode_threads(self, vol: np.ndarray, brick: int, threads: int = 0) -> bytes:
+        """encode() with the bricks spread over host threads (0: every core); the same bytes."""
+        v = np.ascontiguousarray(vol, dtype=np.uint64)
+        D, H, W = v.shape
+        out = _u8p()
+        n = C.c_size_t()
+        rc = self.lib.or_encode_threads(_ptr(v, _u64p), W, H, D, brick, threads or (os.cpu_count() or 1),
+                                        C.byref(out), C.byref(n))
+        if rc:
+            raise RuntimeError("oracle encode failed")
+        data = C.string_at(out, n.value)
+        self.lib.or_free(out)
+        return data
+
+    def synth_volume(self, shape, kind: int, n_cells: int, n_tubes: int, r_min: float, r_max: float,
+                     zero_frac: float, seed: int, threads: int = 0) -> np.ndarray:
+        """The native library's csv_synth_volume restated on the CPU: a (D, H, W) uint64 volume, x fastest."""
+        D, H, W = shape
+        vol = np.empty((D, H, W), np.uint64)
+        rc = self.lib.or_synth_volume(_ptr(vol, _u64p), W, H, D, kind, n_cells, n_tubes, r_min, r_max, zero_frac,
+                                      seed, threads or (os.cpu_count() or 1))
+        if rc:
+            raise RuntimeError("oracle synth failed")
+        return vol
+
     def pyramid(self, vol: np.ndarray, brick: int, index: int):
         v = np.ascontiguousarray(vol, dtype=np.uint64)
         D, H, W = v.shape
@@ -424,6 +457,7 @@ class Reference:
         L.ref_load.argtypes = [_u8p, C.c_size_t]
         L.ref_unload.argtypes = [C.c_void_p]
         L.ref_decode_range.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, _u64p]
+        L.ref_decode_strided.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, _u64p]
         L.ref_build_pyramid64.argtypes = [_u64p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_uint32, _u64p, _u8p]
         self.lib = L
 
@@ -468,9 +502,10 @@ class Reference:
             raise RuntimeError(self.error())
         return (out.reshape(nb, -1) if keep else None), st, {"rans_ms": tr.value, "replay_ms": tp.value}
 
-    def decode_parallel(self, img: bytes, threads: int, out: np.ndarray | None = None) -> int:
-        """Full-resolution decode of every brick, bricks split over `threads` host threads (ctypes releases
-        the GIL).  Returns the number of bricks where the reference threw."""
+    def decode_parallel(self, img: bytes, threads: int, out: np.ndarray | None = None, stride: int = 1) -> int:
+        """Full-resolution decode of bricks 0, stride, 2*stride, ... (every brick by default), split over
+        `threads` host threads (ctypes releases the GIL).  out (or None) receives the decoded bricks in that
+        order.  Returns the number of bricks where the reference threw."""
         from concurrent.futures import ThreadPoolExecutor
         a = np.frombuffer(img, np.uint8)
         h = self.lib.ref_load(_ptr(a, _u8p), len(img))
@@ -478,13 +513,15 @@ class Reference:
             raise RuntimeError(self.error())
         nb = int(np.frombuffer(img[8:12], np.uint32)[0])
         b = int(np.frombuffer(img[12:16], np.uint32)[0])
-        chunk = -(-nb // max(1, threads))
+        stride = max(1, int(stride))
+        m = len(range(0, nb, stride))
+        chunk = -(-m // max(1, threads))
 
         def run(k):
             s = k * chunk
-            c = max(0, min(chunk, nb - s))
+            c = max(0, min(chunk, m - s))
             p = None if out is None else out.reshape(-1)[s * b ** 3:].ctypes.data_as(_u64p)
-            return self.lib.ref_decode_range(h, s, c, p) if c else 0
+            return self.lib.ref_decode_strided(h, s * stride, c, stride, p) if c else 0
 
         with ThreadPoolExecutor(max_workers=threads) as ex:
             bad = sum(ex.map(run, range(threads)))

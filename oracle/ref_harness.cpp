@@ -224,13 +224,20 @@ void ref_unload(void* h) { delete static_cast<RefImage*>(h); }
 
 // decodeRansStream + decodeBrick<b>(., full) for bricks [start, start+count);
 // out (may be null) receives count * b^3 labels.  Returns bricks that threw.
+int ref_decode_strided(void* hv, uint32_t start, uint32_t count, uint32_t stride, uint64_t* out);
 int ref_decode_range(void* hv, uint32_t start, uint32_t count, uint64_t* out) {
+    return ref_decode_strided(hv, start, count, 1, out);
+}
+
+// The same over bricks start, start + stride, ... (count of them).
+int ref_decode_strided(void* hv, uint32_t start, uint32_t count, uint32_t stride, uint64_t* out) {
     auto* h = static_cast<RefImage*>(hv);
     int bad = 0;
     size_t vox = (size_t)h->b * h->b * h->b;
-    for (uint32_t k = 0; k < count && start + k < h->ds.bricks.size(); ++k) {
+    if (stride == 0) stride = 1;
+    for (uint32_t k = 0; k < count && start + (size_t)k * stride < h->ds.bricks.size(); ++k) {
         try {
-            Encoding::CompressedBrick cb = h->ds.bricks[start + k];
+            Encoding::CompressedBrick cb = h->ds.bricks[start + (size_t)k * stride];
             cb.encodedData = decodeRansStream(cb, h->ds.model);
             std::vector<LabelType> labels;
             switch (h->b) {

@@ -22,10 +22,10 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, os.path.join(ROOT, "fast-compressed-segmentation_b200"))
-from oracle import Oracle, Reference, build  # noqa: E402
+from oracle import REF_SHIPPED, Oracle, Reference, build  # noqa: E402
 from csvb200 import synth  # noqa: E402
 
-SHIPPED = "/root/reference/encoder/CSVEncoder/compressed_dataset.csbd"
+SHIPPED = REF_SHIPPED
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 

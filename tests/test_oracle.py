@@ -220,3 +220,30 @@ def test_scalar_dda_sees_the_volume(oracle):
     l, dep, miss = oracle.render(camera_uniform(pos, d, math.pi / 3), 32, 32, 32.0, 16, 2, slots, lab)
     assert (l == 7).sum() > 20 and set(np.unique(l)) <= {0, 7}
     assert np.isfinite(dep[l == 7]).all() and np.isinf(dep[l == 0]).all()
+
+
+@pytest.mark.parametrize("shape,b", [((32, 32, 96), 4), ((40, 70, 130), 16), ((72, 80, 96), 64)])
+def test_threaded_encode_equals_encode(oracle, shape, b):
+    """or_encode_threads (the bench reference arm's input builder) writes or_encode's bytes; with 4^3 bricks the
+    every-512th model sample spans several threads' ranges."""
+    from csvb200.synth import tubes_over_voronoi
+    vol = tubes_over_voronoi(shape, 40, 8, 1.0, 3.0, 5 + b, zero_frac=0.1)
+    one = oracle.encode(vol, b)
+    for threads in (1, 3, 7):
+        assert oracle.encode_threads(vol, b, threads) == one, threads
+
+
+def test_threaded_encode_equals_reference(oracle, reference):
+    vol = oracle.synth_volume((96, 80, 72), 2, 60, 30, 1.0, 4.0, 0.0, 4, threads=2)
+    assert oracle.encode_threads(vol, 32, 4) == reference.encode(vol, 32)
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2])
+def test_cpu_generator_is_deterministic(oracle, kind):
+    """or_synth_volume is a pure function of its arguments: any thread count gives the same volume."""
+    a = oracle.synth_volume((48, 40, 64), kind, 80, 12, 1.0, 5.0, 0.1, 9, threads=1)
+    b = oracle.synth_volume((48, 40, 64), kind, 80, 12, 1.0, 5.0, 0.1, 9, threads=5)
+    assert np.array_equal(a, b)
+    assert len(np.unique(a)) > 10
+    if kind == 0:
+        assert 0.05 < float((a == 0).mean()) < 0.15

@@ -50,6 +50,32 @@ def test_static_decode_matches_allocating_decode_twice(codec, name):
     ds.close()
 
 
+def test_static_decode_shipped_subset_golden_hashes(codec, golden):
+    """Every LOD of the shipped MICrONS bricks, decoded by the allocation-free entry point (twice, so that the
+    second call starts from the first call's scratch), hashed against the golden fixture: the reference
+    decoder's output at full resolution, the decode.wgsl restatement at coarser LODs."""
+    import hashlib
+
+    import torch
+    from csvb200 import requests, requests_tensor
+    img = read_golden("shipped_subset")
+    ds = codec.open(img)
+    nb = ds.num_bricks
+    for call in range(2):
+        for lod in range(ds.brick_size.bit_length()):
+            per = 8 ** lod
+            reqs = requests_tensor(requests(np.arange(nb), np.full(nb, lod), np.arange(nb, dtype=np.uint64) * per))
+            out = torch.full((nb * per,), -1, dtype=torch.int64, device="cuda")
+            st = torch.full((nb,), -1, dtype=torch.int32, device="cuda")
+            codec.decode_batch_static(ds, reqs, out, st)
+            torch.cuda.synchronize()
+            assert int(st.abs().max()) == 0, (call, lod)
+            h = out.cpu().numpy().view(np.uint64).reshape(nb, per)
+            got = [hashlib.sha256(np.ascontiguousarray(h[k]).tobytes()).hexdigest() for k in range(nb)]
+            assert got == golden["shipped_subset"]["lod"][str(lod)], (call, lod)
+    ds.close()
+
+
 def test_static_decode_encoder_dataset_full_resolution(codec):
     """A 64^3-brick dataset from the encoder: 256 bricks through the 47 concurrent slots of the array."""
     import torch
