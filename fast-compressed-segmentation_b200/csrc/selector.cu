@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
+#include <stdio.h>
 #include <string.h>
 
 #include <algorithm>
@@ -760,6 +761,107 @@ int csv_encode_device_sel(csv_ctx* ctx, const uint64_t* d_volume, uint32_t W, ui
     encoder_image(ctx->enc, &len);
     if (image_len) *image_len = len;
     return CSV_OK;
+}
+
+// ---- selector files: the fitted tables and the trained network, so that a
+// learned encode needs no training run.  Little-endian: u32 magic "CSVS"
+// (0x53565343), u32 version 1, u32 CSV_MLP_PARAMS, u32 n_tables (1..16), u32
+// tables[n_tables][16], f32 params[CSV_MLP_PARAMS], u32 FNV-1a of every byte
+// before it.
+static uint32_t fnv1a(const uint8_t* p, size_t n, uint32_t h = 2166136261u) {
+    for (size_t i = 0; i < n; ++i) h = (h ^ p[i]) * 16777619u;
+    return h;
+}
+static bool tables_ok(const uint32_t* t, uint32_t n) {
+    if (n == 0 || n > kTablesN) return false;
+    for (uint32_t k = 0; k < n; ++k) {
+        uint32_t sum = 0;
+        for (int s = 0; s < 16; ++s) {
+            if (t[k * 16 + s] == 0) return false;
+            sum += t[k * 16 + s];
+        }
+        if (sum != kTot) return false;
+    }
+    return true;
+}
+constexpr uint32_t kSelMagic = 0x53565343u;
+
+int csv_selector_write(const char* path, const float* params, const uint32_t* tables, uint32_t n_tables) {
+    if (!path || !params || !tables) return CSV_EINVAL;
+    if (!tables_ok(tables, n_tables)) return CSV_EINVAL;
+    std::vector<uint8_t> buf;
+    auto put = [&](const void* p, size_t n) {
+        const uint8_t* b = (const uint8_t*)p;
+        buf.insert(buf.end(), b, b + n);
+    };
+    const uint32_t head[4] = {kSelMagic, 1u, (uint32_t)N_PARAMS, n_tables};
+    put(head, sizeof head);
+    put(tables, 64ull * n_tables);
+    put(params, 4ull * N_PARAMS);
+    const uint32_t h = fnv1a(buf.data(), buf.size());
+    put(&h, 4);
+    FILE* f = fopen(path, "wb");
+    if (!f) return CSV_EIO;
+    const size_t w = fwrite(buf.data(), 1, buf.size(), f);
+    const int c = fclose(f);
+    return (w == buf.size() && c == 0) ? CSV_OK : CSV_EIO;
+}
+
+int csv_selector_read(const char* path, float* params, uint32_t* tables, uint32_t* n_tables) {
+    if (!path || !params || !tables || !n_tables) return CSV_EINVAL;
+    FILE* f = fopen(path, "rb");
+    if (!f) return CSV_EIO;
+    std::vector<uint8_t> buf;
+    uint8_t tmp[65536];
+    size_t r;
+    while ((r = fread(tmp, 1, sizeof tmp, f)) > 0) buf.insert(buf.end(), tmp, tmp + r);
+    fclose(f);
+    if (buf.size() < 20) return CSV_EFORMAT;
+    uint32_t head[4];
+    memcpy(head, buf.data(), sizeof head);
+    if (head[0] != kSelMagic || head[1] != 1u || head[2] != (uint32_t)N_PARAMS || head[3] == 0 || head[3] > kTablesN)
+        return CSV_EFORMAT;
+    const size_t need = 16 + 64ull * head[3] + 4ull * N_PARAMS + 4;
+    if (buf.size() != need) return CSV_EFORMAT;
+    uint32_t h;
+    memcpy(&h, buf.data() + need - 4, 4);
+    if (h != fnv1a(buf.data(), need - 4)) return CSV_EFORMAT;
+    if (!tables_ok(reinterpret_cast<const uint32_t*>(buf.data() + 16), head[3])) return CSV_EFORMAT;
+    memcpy(tables, buf.data() + 16, 64ull * head[3]);
+    memcpy(params, buf.data() + 16 + 64ull * head[3], 4ull * N_PARAMS);
+    *n_tables = head[3];
+    return CSV_OK;
+}
+
+// The learned encode in one call: features of every brick, the network's
+// choice, the encode with those choices into a version-2 image.
+int csv_encode_learned(csv_ctx* ctx, const uint64_t* d_volume, uint32_t W, uint32_t H, uint32_t D,
+                       uint32_t brick_size, csv_mlp* net, const uint32_t* tables, uint32_t n_tables, void* stream,
+                       size_t* image_len) {
+    if (!ctx || !d_volume || !net || !tables) return CSV_EINVAL;
+    if (!tables_ok(tables, n_tables)) return abi_fail(ctx, CSV_EINVAL, "learned encode: tables must sum to 4096");
+    if (brick_size < 8 || brick_size > 64 || (brick_size & (brick_size - 1)))
+        return abi_fail(ctx, CSV_EINVAL, "brick size must be a power of two in [8, 64]");
+    DeviceGuard g(ctx->device);
+    const uint64_t nb = (uint64_t)((W + brick_size - 1) / brick_size) * ((H + brick_size - 1) / brick_size) *
+                        ((D + brick_size - 1) / brick_size);
+    if (nb == 0 || nb > 0xFFFFFFFFull) return abi_fail(ctx, CSV_ERANGE, "learned encode: brick count");
+    float* d_feat = nullptr;
+    uint8_t* d_sel = nullptr;
+    cudaError_t e = cudaMalloc(&d_feat, nb * CSV_FEATURES * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&d_sel, nb);
+    if (e != cudaSuccess) {
+        cudaFree(d_feat);
+        return abi_cuda_fail(ctx, e, "learned encode");
+    }
+    int rc = csv_brick_features(ctx, d_volume, W, H, D, brick_size, d_feat, stream);
+    if (rc == CSV_OK) rc = csv_mlp_forward(net, d_feat, (uint32_t)nb, nullptr, d_sel, stream);
+    if (rc == CSV_OK)
+        rc = csv_encode_device_sel(ctx, d_volume, W, H, D, brick_size, tables, n_tables, d_sel, stream, image_len);
+    cudaStreamSynchronize((cudaStream_t)stream);
+    cudaFree(d_feat);
+    cudaFree(d_sel);
+    return rc;
 }
 
 }  // extern "C"

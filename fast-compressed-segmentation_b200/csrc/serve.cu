@@ -19,6 +19,12 @@
 //   census_kernel  per brick: bricks each session's rays entered, and how many
 //                  had no data
 //
+// Admission by rays (CSV_ADMIT_RAYS, the reference's switched-off useGPUCulling
+// path): the plan keeps only the bricks a session's last render entered (its
+// request words, which the census then leaves for the plan to consume).
+// Compaction (csv_serve_compact, CacheState.compact()) is a step whose plan is
+// the resident set itself, placed again as a rebuild places blocks.
+//
 // Sessions share the cache but not their LODs: a block is keyed by (brick,
 // LOD), each session's slot table points at the blocks of its own LODs, and a
 // session's plan uses the camera of its own last re-plan (it re-plans when it
@@ -95,6 +101,9 @@ struct PlanArgs {
     const uint32_t* ids;
     const uint8_t* bflag;
     const uint8_t* res;   // bit l: block at LOD l resident
+    uint32_t* req_words;  // [session][n_slots]: the last render's request words (admission by rays)
+    uint64_t n_slots;
+    uint32_t ready;       // bit s: view s has request words to apply (and consume)
     uint8_t* want;        // [session][brick]
     uint8_t* need;        // bit l: some open session needs LOD l of the brick
     uint32_t* cnt;        // [kCnt][n_cta]
@@ -182,6 +191,11 @@ __global__ void __launch_bounds__(kBlk) plan_kernel(PlanArgs A) {
         for (uint32_t s = 0; s < A.n_views; ++s) {
             uint32_t w = kNone;
             if ((bf & BK_HAS) && in_cone(A, c, A.v[s])) w = brick_lod(A, c, A.v[s]);
+            if ((A.ready >> s) & 1u) {  // admission by rays: only what the last render entered
+                uint32_t* rw = A.req_words + (size_t)A.sid[s] * A.n_slots + id;
+                if (*rw == 0u) w = kNone;
+                else *rw = 0u;  // consumed
+            }
             A.want[(size_t)A.sid[s] * A.nb + i] = (uint8_t)w;
             if (w != kNone) {
                 vis = true;
@@ -204,11 +218,33 @@ __global__ void __launch_bounds__(kBlk) plan_kernel(PlanArgs A) {
     if (tid == 0 && s_vis) atomicAdd(&A.stats->visible, s_vis);
 }
 
+// Compaction's plan: every brick needs exactly its resident blocks (no frees,
+// no admissions); the scan then places them all again as a rebuild does.
+__global__ void __launch_bounds__(kBlk) compact_plan_kernel(const uint8_t* __restrict__ res, uint8_t* __restrict__ need,
+                                                            uint32_t nb, uint32_t* __restrict__ cnt, uint32_t n_cta) {
+    __shared__ uint32_t s_wc[kWarps][kLods];
+    __shared__ uint32_t s_tot[kLods];
+    const uint32_t i = blockIdx.x * kBlk + threadIdx.x;
+    uint32_t r = 0;
+    if (i < nb) {
+        r = res[i];
+        need[i] = (uint8_t)r;
+    }
+    uint32_t rank[kLods];
+    cta_ranks(r, rank, s_wc, s_tot);
+    if (threadIdx.x < kLods) {
+        cnt[(CNT_FREE + threadIdx.x) * n_cta + blockIdx.x] = 0;
+        cnt[(CNT_ALLOC + threadIdx.x) * n_cta + blockIdx.x] = 0;
+        cnt[(CNT_NEED + threadIdx.x) * n_cta + blockIdx.x] = s_tot[threadIdx.x];
+    }
+}
+
 // One CTA: exclusive scans of the per-CTA counts (one warp per counter), then
 // the step's cache policy by thread 0.
 __global__ void __launch_bounds__(1024) scan_kernel(const uint32_t* __restrict__ cnt, uint32_t* __restrict__ base,
                                                     uint32_t n_cta, uint32_t max_lod, uint32_t nb,
-                                                    ServeState* __restrict__ S, StepStats* __restrict__ st) {
+                                                    ServeState* __restrict__ S, StepStats* __restrict__ st,
+                                                    uint32_t force_rebuild) {
     __shared__ uint32_t tot[kCnt];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     if (warp < kCnt) {
@@ -242,7 +278,7 @@ __global__ void __launch_bounds__(1024) scan_kernel(const uint32_t* __restrict__
         nfree += F;
         nalloc += A;
     }
-    if (S->bump + need > S->cap) rebuild = true;
+    if (S->bump + need > S->cap || force_rebuild) rebuild = true;
     uint64_t vox = 0;
     if (!rebuild) {
         uint64_t b = S->bump;
@@ -401,6 +437,7 @@ struct CensusArgs {
     uint64_t n_slots;
     const uint32_t* ids;
     uint32_t* req_words;  // [session][n_slots]
+    uint32_t keep;        // admission by rays: leave the words for the next plan
     const ServeState* S;
     StepStats* st;
 };
@@ -416,7 +453,7 @@ __global__ void __launch_bounds__(kBlk) census_kernel(CensusArgs A) {
         if (i < A.nb) {
             uint32_t* w = A.req_words + (size_t)A.sid[s] * A.n_slots + m;
             v = *w;
-            if (v) *w = 0;
+            if (v && !A.keep) *w = 0;
         }
         const uint32_t e = __popc(__ballot_sync(0xffffffffu, v != 0));
         const uint32_t ms = __popc(__ballot_sync(0xffffffffu, v == 3));
@@ -480,6 +517,7 @@ struct csv_server {
     csv_ctx* ctx = nullptr;
     const csv_dataset* ds = nullptr;
     uint32_t W = 0, H = 0, cone = 0, b = 0, max_lod = 0, nb = 0, bpa = 0, n_cta = 0, max_sessions = 1;
+    uint32_t admit = CSV_ADMIT_CONE;
     double fov = 0, focal = 0, cos_half = 0, radius = 0;
     uint64_t total = 0, pal_region = 0, n_slots = 0;
     uint64_t* d_cache = nullptr;
@@ -508,6 +546,7 @@ struct csv_server {
     StepStats* h_stats = nullptr;  // pinned mirror
     struct Session {
         bool open = false, pending = false, planned = false;
+        bool ready = false;  // admission by rays: rendered since the last plan (request words on the device)
         double v[6];      // latest submitted camera (raw direction)
         double pv[6];     // camera of the session's last re-plan (unit direction)
         uint64_t* lab = nullptr;
@@ -661,6 +700,11 @@ int csv_serve_create(csv_ctx* ctx, const csv_dataset* ds, const csv_serve_config
     s->W = cfg->width;
     s->H = cfg->height;
     s->cone = cfg->cone;
+    if (cfg->admit > CSV_ADMIT_RAYS) {
+        delete s;
+        return fail(ctx, CSV_EINVAL, "serve: unknown admission policy");
+    }
+    s->admit = cfg->admit;
     s->fov = cfg->fov;
     s->b = d.b;
     s->nb = d.nb;
@@ -838,6 +882,13 @@ int csv_serve_step(csv_server* s, void* stream, uint64_t* step_id) {
         }
     }
     if (open != s->last_open) changed = true;
+    uint32_t ready = 0;  // admission by rays: views (plan order) with request words to apply
+    if (s->admit == CSV_ADMIT_RAYS)
+        for (size_t k = 0; k < open.size(); ++k)
+            if (s->ses[open[k]].ready) {
+                ready |= 1u << k;
+                changed = true;
+            }
     if (rendered.empty() && !changed) return fail(s->ctx, CSV_EINVAL, "serve: no frame submitted since the last step");
     DeviceGuard g(s->ctx->device);
     // a full ring: wait for the oldest step and keep its counters for csv_serve_poll
@@ -850,6 +901,14 @@ int csv_serve_step(csv_server* s, void* stream, uint64_t* step_id) {
     StepStats* stats = s->d_stats + slot;
     cudaError_t e = cudaEventRecord(rec.e0, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(stats, 0, sizeof(StepStats), st);
+    // a session that left with request words not yet applied: drop them
+    for (uint32_t k = 0; k < s->max_sessions && e == cudaSuccess; ++k) {
+        auto& p = s->ses[k];
+        if (!p.open && p.ready) {
+            e = cudaMemsetAsync(s->d_req_words + (size_t)k * s->n_slots, 0, s->n_slots * 4, st);
+            p.ready = false;
+        }
+    }
     if (e == cudaSuccess && changed && s->nb) {
         PlanArgs P;
         memset(&P, 0, sizeof P);
@@ -873,12 +932,17 @@ int csv_serve_step(csv_server* s, void* stream, uint64_t* step_id) {
         P.ids = s->d_ids;
         P.bflag = s->d_bflag;
         P.res = s->d_res;
+        P.req_words = s->d_req_words;
+        P.n_slots = s->n_slots;
+        P.ready = (e == cudaSuccess) ? ready : 0u;
         P.want = s->d_want;
         P.need = s->d_need;
         P.cnt = s->d_cnt;
         P.stats = stats;
         plan_kernel<<<s->n_cta, kBlk, 0, st>>>(P);
-        scan_kernel<<<1, 1024, 0, st>>>(s->d_cnt, s->d_base, s->n_cta, s->max_lod, s->nb, s->d_state, stats);
+        scan_kernel<<<1, 1024, 0, st>>>(s->d_cnt, s->d_base, s->n_cta, s->max_lod, s->nb, s->d_state, stats, 0u);
+        for (size_t k = 0; k < open.size(); ++k)
+            if ((ready >> k) & 1u) s->ses[open[k]].ready = false;  // consumed by this plan
         CacheArgs C;
         memset(&C, 0, sizeof C);
         for (size_t k = 0; k < open.size(); ++k) C.sid[k] = open[k];
@@ -934,6 +998,7 @@ int csv_serve_step(csv_server* s, void* stream, uint64_t* step_id) {
         A.n_slots = s->n_slots;
         A.ids = s->d_ids;
         A.req_words = s->d_req_words;
+        A.keep = s->admit == CSV_ADMIT_RAYS ? 1u : 0u;
         A.S = s->d_state;
         A.st = stats;
         census_kernel<<<s->n_cta, kBlk, 0, st>>>(A);
@@ -947,7 +1012,67 @@ int csv_serve_step(csv_server* s, void* stream, uint64_t* step_id) {
     rec.rendered = rendered;
     if (step_id) *step_id = s->next_seq;
     ++s->next_seq;
-    for (uint32_t k : rendered) s->ses[k].pending = false;
+    for (uint32_t k : rendered) {
+        s->ses[k].pending = false;
+        if (s->admit == CSV_ADMIT_RAYS) s->ses[k].ready = true;
+    }
+    return CSV_OK;
+}
+
+int csv_serve_compact(csv_server* s, void* stream) {
+    if (!s) return CSV_EINVAL;
+    if (!s->nb) return CSV_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    DeviceGuard g(s->ctx->device);
+    if (s->next_seq - s->harvest_seq >= kRing) {
+        int rc = harvest(s, false, true);
+        if (rc) return rc;
+    }
+    const uint32_t slot = (uint32_t)(s->next_seq % kRing);
+    auto& rec = s->ring[slot];
+    StepStats* stats = s->d_stats + slot;
+    cudaError_t e = cudaEventRecord(rec.e0, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(stats, 0, sizeof(StepStats), st);
+    if (e == cudaSuccess) {
+        compact_plan_kernel<<<s->n_cta, kBlk, 0, st>>>(s->d_res, s->d_need, s->nb, s->d_cnt, s->n_cta);
+        scan_kernel<<<1, 1024, 0, st>>>(s->d_cnt, s->d_base, s->n_cta, s->max_lod, s->nb, s->d_state, stats, 1u);
+        CacheArgs C;
+        memset(&C, 0, sizeof C);
+        // the slot tables of the sessions open at the last plan, whose wants stand
+        for (size_t k = 0; k < s->last_open.size(); ++k) C.sid[k] = s->last_open[k];
+        C.n_views = (uint32_t)s->last_open.size();
+        C.nb = s->nb;
+        C.n_cta = s->n_cta;
+        C.max_lod = s->max_lod;
+        C.n_slots = s->n_slots;
+        C.bflag = s->d_bflag;
+        C.want = s->d_want;
+        C.need = s->d_need;
+        C.base = s->d_base;
+        C.ids = s->d_ids;
+        C.res = s->d_res;
+        C.off = s->d_off;
+        C.stack = s->d_stack;
+        C.S = s->d_state;
+        C.reqs = s->d_reqs;
+        C.slots = s->d_slots;
+        C.pal_region = s->pal_region;
+        push_kernel<<<s->n_cta, kBlk, 0, st>>>(C);
+        pop_kernel<<<s->n_cta, kBlk, 0, st>>>(C);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) {
+            DecodeConfig dc;
+            dc.n_dev = &s->d_state->n_req;
+            e = launch_decode(s->ds->d, s->d_reqs, s->nb * kLods, s->d_cache, s->d_status, s->ctx->scr, st, &dc);
+        }
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->h_stats + slot, stats, sizeof(StepStats), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaEventRecord(rec.e1, st);
+    if (e != cudaSuccess) return cfail(s->ctx, e, "serve compact");
+    rec.seq = s->next_seq;
+    rec.rendered.clear();  // no frame
+    ++s->next_seq;
     return CSV_OK;
 }
 

@@ -65,12 +65,14 @@ class DecodeConfig(C.Structure):
 
 CONE_REFERENCE = 0
 CONE_SCREEN = 1
+ADMIT_CONE = 0  # csv_serve_config.admit: the cone and LOD plan (the reference as it runs)
+ADMIT_RAYS = 1  # only the bricks the session's last render entered (the reference's useGPUCulling path)
 
 
 class ServeConfig(C.Structure):
     """csv_serve_config."""
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("max_sessions", C.c_uint32), ("cone", C.c_uint32),
-                ("fov", C.c_double), ("cache_bytes", C.c_uint64)]
+                ("fov", C.c_double), ("cache_bytes", C.c_uint64), ("admit", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class View(C.Structure):
@@ -159,6 +161,7 @@ def load_library() -> C.CDLL:
     L.csv_serve_camera.argtypes = [vp, C.POINTER(View), vp]
     L.csv_serve_state.argtypes = [vp, C.c_uint32, C.POINTER(ServeInfo)]
     L.csv_serve_close.argtypes = [vp, C.c_uint32]
+    L.csv_serve_compact.argtypes = [vp, vp]
     L.csv_serve_destroy.argtypes = [vp]
     L.csv_gemm_bf16.argtypes = [vp, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, C.c_uint32, vp, vp, vp, vp,
                                 vp, vp]
@@ -168,6 +171,10 @@ def load_library() -> C.CDLL:
                                         vp, vp, C.POINTER(C.c_size_t)]
     L.csv_brick_features.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp]
     L.csv_mlp_create.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(vp)]
+    L.csv_selector_write.argtypes = [C.c_char_p, C.POINTER(C.c_float), u32p, C.c_uint32]
+    L.csv_selector_read.argtypes = [C.c_char_p, C.POINTER(C.c_float), u32p, u32p]
+    L.csv_encode_learned.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, vp, u32p, C.c_uint32,
+                                     vp, C.POINTER(C.c_size_t)]
     L.csv_mlp_destroy.argtypes = [vp]
     L.csv_mlp_destroy.restype = None
     L.csv_mlp_params.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_float)]
@@ -524,6 +531,16 @@ class Codec:
             _vp(d_sel), C.c_void_p(_stream_handle(stream)), C.byref(n)))
         return n.value
 
+    def encode_learned(self, d_volume, brick_size: int, net: "SelectorNet", tables, stream=None) -> int:
+        """csv_encode_learned: features, the network's choices and the encode in one call; the image length."""
+        D, H, W = d_volume.shape
+        t = np.ascontiguousarray(tables, np.uint32)
+        n = C.c_size_t()
+        self._check(self.lib.csv_encode_learned(self.handle, C.c_void_p(d_volume.data_ptr()), W, H, D, brick_size,
+                                                net.handle, t.ctypes.data_as(C.POINTER(C.c_uint32)), t.shape[0],
+                                                C.c_void_p(_stream_handle(stream)), C.byref(n)))
+        return n.value
+
     def brick_features(self, d_volume, brick_size: int, d_features, stream=None):
         """32 statistics per brick (d_features: float32 tensor nb x 32)."""
         D, H, W = d_volume.shape
@@ -544,9 +561,9 @@ class Server:
     render on one stream; poll returns per-frame counters and step times."""
 
     def __init__(self, codec: Codec, dataset: Dataset, width: int, height: int, fov: float, cache_bytes: int = 0,
-                 max_sessions: int = 1, cone: int = CONE_SCREEN, hidden=None):
+                 max_sessions: int = 1, cone: int = CONE_SCREEN, hidden=None, admit: int = ADMIT_CONE):
         self.codec, self.dataset, self.lib = codec, dataset, codec.lib
-        cfg = ServeConfig(width, height, max_sessions, cone, fov, cache_bytes)
+        cfg = ServeConfig(width, height, max_sessions, cone, fov, cache_bytes, admit, 0)
         hid = np.ascontiguousarray(hidden if hidden is not None else np.zeros(1, np.uint64), np.uint64)
         h = C.c_void_p()
         codec._check(self.lib.csv_serve_create(codec.handle, dataset.handle, C.byref(cfg),
@@ -599,6 +616,10 @@ class Server:
         self.codec._check(self.lib.csv_serve_camera(self.handle, C.byref(v), cam))
         return np.array(cam[:], np.float32)
 
+    def compact(self, stream=None):
+        """CacheState.compact(): resident blocks packed from the start of the block space (csv_serve_compact)."""
+        self.codec._check(self.lib.csv_serve_compact(self.handle, C.c_void_p(_stream_handle(stream))))
+
     def leave(self, session: int):
         """The session closes; its cache blocks are released by the next step."""
         self.codec._check(self.lib.csv_serve_close(self.handle, session))
@@ -640,6 +661,27 @@ def _device_view(ptr: int, n: int, typestr: str, device: int):
 
 
 MLP_PARAMS = 256 * 64 + 256 + 256 * 256 + 256 + 32 * 256 + 32
+
+
+def write_selector(lib, path: str, params: np.ndarray, tables: np.ndarray):
+    p = np.ascontiguousarray(params, np.float32)
+    t = np.ascontiguousarray(tables, np.uint32)
+    rc = lib.csv_selector_write(os.fsencode(path), p.ctypes.data_as(C.POINTER(C.c_float)),
+                                t.ctypes.data_as(C.POINTER(C.c_uint32)), t.shape[0])
+    if rc:
+        raise CsvError(rc, f"csv_selector_write({path}) failed")
+
+
+def read_selector(lib, path: str):
+    """(params, tables) of a selector file; host only (no device needed)."""
+    p = np.zeros(MLP_PARAMS, np.float32)
+    t = np.zeros((16, 16), np.uint32)
+    n = C.c_uint32()
+    rc = lib.csv_selector_read(os.fsencode(path), p.ctypes.data_as(C.POINTER(C.c_float)),
+                               t.ctypes.data_as(C.POINTER(C.c_uint32)), C.byref(n))
+    if rc:
+        raise CsvError(rc, f"csv_selector_read({path}) failed")
+    return p, t[: n.value].copy()
 
 
 class SelectorNet:
@@ -693,6 +735,16 @@ class SelectorNet:
 
     def status(self) -> int:
         return self.lib.csv_mlp_status(self.handle)
+
+    def save(self, path: str, tables: np.ndarray):
+        """A selector file with these tables and this network's parameters (csv_selector_write)."""
+        write_selector(self.lib, path, self.params(), tables)
+
+    @classmethod
+    def load(cls, codec: Codec, path: str):
+        """(network, tables) from a selector file (csv_selector_read + csv_mlp_create)."""
+        params, tables = read_selector(codec.lib, path)
+        return cls(codec, params), tables
 
     def close(self):
         if getattr(self, "handle", None):

@@ -41,7 +41,8 @@ enum {
     CSV_ECUDA = -3,    /* a CUDA call failed */
     CSV_ENOMEM = -4,   /* device or host allocation failed */
     CSV_ERANGE = -5,   /* size beyond a documented limit */
-    CSV_EBRICK = -6    /* at least one brick reported a nonzero status */
+    CSV_EBRICK = -6,   /* at least one brick reported a nonzero status */
+    CSV_EIO = -7       /* a file could not be opened, read or written (fileIO.cpp:20-22, 105-107) */
 };
 
 /* Per-brick status bits written by the batched decoder (d_status).  The
@@ -319,12 +320,27 @@ typedef struct csv_server csv_server;
 #define CSV_CONE_REFERENCE 0u /* cone half-angle fov/2 (culling.js:132) */
 #define CSV_CONE_SCREEN 1u    /* cone half-angle to the screen corner: every brick a ray can reach */
 
+/* Admission policy (csv_serve_config.admit).  CONE: a session needs every
+ * brick its cone and LOD tests pass (the reference's loop as it runs,
+ * cacheProcessing.js:99-232).  RAYS: of those, only the bricks its rays entered
+ * in its last render (the request words of rayTrace.wgsl:682-686 driving
+ * admission and eviction: the reference's useGPUCulling path,
+ * cacheProcessing.js:134-164, which it ships switched off).  A session with no
+ * render since the last plan (its first frame) keeps the cone plan; a step
+ * re-plans when an open session rendered since the last plan, so bricks that
+ * rays stop reaching (hidden behind bricks that arrived) are released while
+ * the camera stands still. */
+#define CSV_ADMIT_CONE 0u
+#define CSV_ADMIT_RAYS 1u
+
 typedef struct csv_serve_config {
     uint32_t width, height;   /* viewport of every session (pixels) */
     uint32_t max_sessions;    /* sessions served together, 1..8 (0 = 1) */
     uint32_t cone;            /* CSV_CONE_* */
     double fov;               /* vertical field of view, radians (camera.js:19: pi/3) */
     uint64_t cache_bytes;     /* label cache incl. a palette-0 table of 8 B per brick; 0 = 24 GiB */
+    uint32_t admit;           /* CSV_ADMIT_* */
+    uint32_t reserved;        /* 0 */
 } csv_serve_config;
 
 typedef struct csv_view {
@@ -382,6 +398,16 @@ int csv_serve_step(csv_server* srv, void* stream, uint64_t* step_id);
 /* Up to `max` finished frames (one per session of each finished step), oldest
  * first; wait != 0 blocks until every step enqueued so far has finished. */
 int csv_serve_poll(csv_server* srv, csv_frame_stats* out, uint32_t max, uint32_t* n_out, int wait);
+/* Compaction (CacheState.compact(), cacheManager.js:170-211; the reference
+ * defines it and never calls it): every resident block is kept and placed
+ * again from the start of the block space, coarse LODs first and brick order
+ * within a LOD, the free stacks are emptied and fresh space starts after the
+ * last block, so that fragmented free blocks of one LOD become space for any.
+ * Enqueued on `stream` like a step (the blocks are decoded again into their new
+ * places, which costs what moving them would at the HBM rate, and needs no
+ * second buffer); every open session's slot table points at the new places
+ * when it completes.  Renders nothing and reports no frame. */
+int csv_serve_compact(csv_server* srv, void* stream);
 /* A session leaves: its cache blocks are released by the next step. */
 int csv_serve_close(csv_server* srv, uint32_t session);
 /* The float camera the server renders a view with (camera.js:61-77). */
@@ -467,6 +493,25 @@ int csv_mlp_grad(csv_mlp* net, const float* d_features, const uint8_t* d_label, 
 int csv_mlp_adam(csv_mlp* net, float lr, float beta1, float beta2, float eps, void* stream);
 /* CSV_OK, or CSV_ECUDA when a tensor-core wait gave up since creation. */
 int csv_mlp_status(const csv_mlp* net);
+
+/* Selector files (no reference counterpart): the shared tables and the
+ * network's parameters, so that a learned encode runs without a training run.
+ * Little-endian: u32 magic "CSVS" (0x53565343), u32 version 1, u32
+ * CSV_MLP_PARAMS, u32 n_tables (1..16), u32 tables[n_tables][16], f32
+ * params[CSV_MLP_PARAMS], u32 FNV-1a hash of every byte before it.  Host only:
+ * write takes params as csv_mlp_params returns them; read fills params
+ * (CSV_MLP_PARAMS floats), tables (room for 16 x 16) and *n_tables, and
+ * refuses a file whose size, header, hash or tables (each >= 1, summing to
+ * 4096) are wrong with CSV_EFORMAT, a missing file with CSV_EIO. */
+int csv_selector_write(const char* path, const float* params, const uint32_t* tables, uint32_t n_tables);
+int csv_selector_read(const char* path, float* params, uint32_t* tables, uint32_t* n_tables);
+/* The learned encode in one call: csv_brick_features, csv_mlp_forward's choice
+ * per brick, csv_encode_device_sel with those choices and tables (a version-2
+ * image, as csv_encode_device leaves it for csv_encoded_image).  Allocates the
+ * per-brick features and choices for the call. */
+int csv_encode_learned(csv_ctx* ctx, const uint64_t* d_volume, uint32_t W, uint32_t H, uint32_t D,
+                       uint32_t brick_size, csv_mlp* net, const uint32_t* tables, uint32_t n_tables, void* stream,
+                       size_t* image_len);
 
 /* ---- workload generator (no reference counterpart) --------------------
  * Seeded synthetic label volume on the device, x fastest: kind 0 = Voronoi

@@ -121,6 +121,11 @@ or_server* or_serve_new(const uint8_t* img, size_t len, uint32_t W, uint32_t H, 
  * plan.  stats: OR_SERVE_STATS words. */
 int or_serve_step(or_server* s, const uint32_t* sess, const double* views, const uint8_t* render, uint32_t n,
                   uint64_t* out_label, float* out_depth, uint32_t* stats);
+/* Admission policy: 0 the cone plan (the reference as it runs), 1 by the rays' requests (the reference's
+ * disabled useGPUCulling path). */
+void or_serve_set_admit(or_server* s, uint32_t admit);
+/* CacheState.compact(): resident blocks packed from offset 0, coarse LODs first, brick order. */
+int or_serve_compact(or_server* s);
 uint64_t or_serve_n_slots(const or_server* s);
 uint32_t or_serve_bricks_per_axis(const or_server* s);
 /* The slot table session `session` renders with. */

@@ -37,6 +37,21 @@
  *     the start of the cache (rayTrace.wgsl:167-178 reads palette[0] for LOD 0;
  *     a uniform brick decodes to palette[0] at every LOD, so the image is the
  *     one a decoded copy would give);
+ *   - admission by rays (or_serve_set_admit 1): the path the reference wrote
+ *     and left switched off (cacheProcessing.js:134-164, useGPUCulling; the
+ *     marcher's brickRequests words, rayTrace.wgsl:682-686).  A brick a session
+ *     needs by the cone and LOD tests is kept or admitted only if that
+ *     session's rays entered it in its last render; a session with no render
+ *     since the last plan (a new session) keeps the cone plan, the reference's
+ *     fallback while no requests are ready.  The plan consumes the words.  In
+ *     this mode a step also re-plans when an open session rendered since the
+ *     last plan (the requests change while the camera stands still, as bricks
+ *     arrive and hide the ones behind them);
+ *   - compaction (or_serve_compact, CacheState.compact(), cacheManager.js:
+ *     170-211): every resident block is kept and placed again from offset 0,
+ *     LOD by LOD (coarse first) in brick order, the free stacks are
+ *     emptied and fresh space starts after the last block; the blocks' labels
+ *     are those they held (decoded again into their new place);
  *   - the cone's margin sin(atan2(r, d)) is evaluated as r / sqrt(r^2 + d^2),
  *     the same number for d > 0 up to rounding; the half-angle is fov/2
  *     (cone 0, the reference) or the half-diagonal of the screen (cone 1), and
@@ -81,6 +96,10 @@ struct or_server {
     uint8_t planned[OR_MAX_SESSIONS];     /* the session has a planned view */
     double pview[OR_MAX_SESSIONS][6];     /* the view its plan used */
     uint8_t last_open[OR_MAX_SESSIONS];   /* open at the last plan */
+    /* admission by rays */
+    uint32_t admit;                       /* 0: cone plan, 1: rays' requests */
+    uint32_t* req[OR_MAX_SESSIONS];       /* request words of the session's last render, by Morton slot */
+    uint8_t ready[OR_MAX_SESSIONS];       /* the session rendered since the last plan */
 };
 
 static uint32_t rd32(const uint8_t* p) {
@@ -231,6 +250,7 @@ or_server* or_serve_new(const uint8_t* img, size_t len, uint32_t W, uint32_t H, 
     for (int k = 0; k < OR_MAX_SESSIONS; ++k) {
         s->slots[k] = (or_slot*)calloc(s->n_slots, sizeof(or_slot));
         for (uint64_t m = 0; m < s->n_slots; ++m) s->slots[k][m].flags = 1u;
+        s->req[k] = (uint32_t*)calloc(s->n_slots, 4);
     }
     const uint64_t total = cache_bytes / 8;
     s->pal_region = ((uint64_t)nb + 31) & ~31ull;
@@ -248,10 +268,13 @@ void or_serve_free(or_server* s) {
     for (int k = 0; k < OR_MAX_SESSIONS; ++k) {
         free(s->want[k]);
         free(s->slots[k]);
+        free(s->req[k]);
     }
     for (uint32_t l = 0; l < OR_LODS; ++l) free(s->stack[l]);
     free(s);
 }
+
+void or_serve_set_admit(or_server* s, uint32_t admit) { s->admit = admit; }
 
 uint64_t or_serve_n_slots(const or_server* s) { return s->n_slots; }
 uint32_t or_serve_bricks_per_axis(const or_server* s) { return s->bpa; }
@@ -307,8 +330,14 @@ static void plan(or_server* s, const uint8_t* open, uint32_t* stats) {
                                      (double)z * (double)b + s->half};
                 if (brick_in_cone(s, c, s->pview[k]))
                     w = (uint8_t)or_brick_lod(c, (double)b, s->pview[k], s->focal, s->max_lod);
+                /* admission by rays: only the bricks the session's last render entered */
+                if (s->admit && s->ready[k] && s->req[k][s->id[i]] == 0) w = OR_NONE;
             }
             s->want[k][i] = w;
+        }
+        if (s->admit && s->ready[k]) { /* the plan consumes the requests */
+            memset(s->req[k], 0, s->n_slots * 4);
+            s->ready[k] = 0;
         }
     }
     uint32_t A[OR_LODS] = {0};
@@ -413,23 +442,34 @@ int or_serve_step(or_server* s, const uint32_t* sess, const double* views_in, co
     }
     for (int k = 0; k < OR_MAX_SESSIONS; ++k) {
         if (open[k] != s->last_open[k]) changed = 1;
-        if (!open[k]) s->planned[k] = 0;
+        if (!open[k]) {
+            s->planned[k] = 0;
+            if (s->ready[k]) { /* a closed session's requests are dropped */
+                memset(s->req[k], 0, s->n_slots * 4);
+                s->ready[k] = 0;
+            }
+        }
     }
+    if (s->admit) /* admission by rays: new requests re-plan */
+        for (int k = 0; k < OR_MAX_SESSIONS; ++k) changed |= open[k] && s->ready[k];
     if (changed) {
         plan(s, open, stats);
         memcpy(s->last_open, open, sizeof open);
     }
     for (uint32_t i = 0; i < s->nb; ++i)
         for (uint32_t l = 1; l <= s->max_lod; ++l) stats[OR_ST_RESIDENT] += (s->res[i] >> l) & 1u;
-    /* render the sessions that submitted a frame; request words as brickRequests */
-    uint32_t* req = (uint32_t*)calloc(s->n_slots, 4);
+    /* render the sessions that submitted a frame; request words as brickRequests (kept for the next plan
+       when admission is by rays) */
+    uint32_t* tmp = (uint32_t*)calloc(s->n_slots, 4);
     const size_t px = (size_t)s->W * s->H;
     uint32_t j = 0;
     for (uint32_t k = 0; k < n; ++k) {
         if (!render[k]) continue;
         float cam[16];
         or_camera_uniform(views_in + 6 * k, views_in + 6 * k + 3, s->fov, cam);
+        uint32_t* req = s->admit ? s->req[sess[k]] : tmp;
         memset(req, 0, s->n_slots * 4);
+        if (s->admit) s->ready[sess[k]] = 1;
         or_render_rows(cam, s->W, s->H, 0, 1, (float)(s->bpa * s->b), s->b, s->bpa, s->slots[sess[k]], s->n_slots,
                        s->cache, s->hidden, s->n_hidden, out_label + j * px, out_depth + j * px, NULL, req);
         for (uint64_t m = 0; m < s->n_slots; ++m) {
@@ -438,6 +478,42 @@ int or_serve_step(or_server* s, const uint32_t* sess, const double* views_in, co
         }
         ++j;
     }
-    free(req);
+    free(tmp);
+    return 0;
+}
+
+/* CacheState.compact() (cacheManager.js:170-211) with the labels moved: every
+ * resident block placed again from offset 0, LOD by LOD (coarse first) in brick
+ * order; free stacks emptied; fresh space after the last block; the slot tables
+ * of the sessions open at the last plan point at the new places. */
+int or_serve_compact(or_server* s) {
+    const uint32_t nb = s->nb;
+    uint64_t* newoff = (uint64_t*)calloc((size_t)(nb + 1) * OR_LODS, 8);
+    uint64_t b = 0;
+    for (uint32_t l = 1; l <= s->max_lod; ++l)
+        for (uint32_t i = 0; i < nb; ++i) {
+            if (!((s->res[i] >> l) & 1u)) continue;
+            newoff[(size_t)i * OR_LODS + l] = b;
+            b += 1ull << (3 * l);
+        }
+    /* decode into the new places (the labels equal the old block's) */
+    for (uint32_t l = 1; l <= s->max_lod; ++l)
+        for (uint32_t i = 0; i < nb; ++i)
+            if ((s->res[i] >> l) & 1u) {
+                s->off[(size_t)i * OR_LODS + l] = newoff[(size_t)i * OR_LODS + l];
+                decode_into(s, i, l, s->cache + s->pal_region + newoff[(size_t)i * OR_LODS + l]);
+            }
+    free(newoff);
+    s->bump = b;
+    for (uint32_t l = 0; l < OR_LODS; ++l) s->top[l] = 0;
+    for (int k = 0; k < OR_MAX_SESSIONS; ++k) {
+        if (!s->last_open[k]) continue;
+        for (uint32_t i = 0; i < nb; ++i) {
+            const uint8_t w = s->want[k][i];
+            or_slot* sl = &s->slots[k][s->id[i]];
+            if (s->has[i] && !s->uni[i] && w != OR_NONE && w != 0 && ((s->res[i] >> w) & 1u))
+                sl->offset = s->pal_region + s->off[(size_t)i * OR_LODS + w];
+        }
+    }
     return 0;
 }

@@ -97,6 +97,9 @@ class Oracle:
                                    _u64p, C.c_uint32]
         L.or_serve_step.argtypes = [C.c_void_p, _u32p, C.POINTER(C.c_double), _u8p, C.c_uint32, _u64p,
                                     C.POINTER(C.c_float), _u32p]
+        L.or_serve_set_admit.argtypes = [C.c_void_p, C.c_uint32]
+        L.or_serve_compact.restype = C.c_int
+        L.or_serve_compact.argtypes = [C.c_void_p]
         L.or_serve_n_slots.restype = C.c_uint64
         L.or_serve_n_slots.argtypes = [C.c_void_p]
         L.or_serve_bricks_per_axis.restype = C.c_uint32
@@ -377,7 +380,7 @@ class OracleServer:
     """The viewer's frame loop restated on the CPU (csv_oracle_serve.c)."""
 
     def __init__(self, oracle: "Oracle", image: bytes, W: int, H: int, fov: float, cone: int, cache_bytes: int,
-                 hidden=None):
+                 hidden=None, admit: int = 0):
         self.lib, self.W, self.H = oracle.lib, W, H
         self._img = np.frombuffer(image, np.uint8).copy()
         hid = np.ascontiguousarray(np.sort(hidden) if hidden is not None else np.zeros(1, np.uint64), np.uint64)
@@ -385,6 +388,7 @@ class OracleServer:
                                        _ptr(hid, _u64p), 0 if hidden is None else len(hidden))
         if not self.h:
             raise ValueError("or_serve_new failed")
+        self.lib.or_serve_set_admit(self.h, admit)
         self.n_slots = int(self.lib.or_serve_n_slots(self.h))
         self.bpa = int(self.lib.or_serve_bricks_per_axis(self.h))
 
@@ -413,6 +417,10 @@ class OracleServer:
         stats["missing"] = [int(st[9 + 2 * j]) for j in range(r)]
         return lab[: r * self.W * self.H].reshape(r, self.H, self.W), \
             dep[: r * self.W * self.H].reshape(r, self.H, self.W), stats
+
+    def compact(self):
+        if self.lib.or_serve_compact(self.h):
+            raise ValueError("or_serve_compact failed")
 
     def slots(self, session: int = 0) -> np.ndarray:
         buf = (C.c_uint8 * (16 * self.n_slots)).from_address(self.lib.or_serve_slots(self.h, session))

@@ -44,3 +44,46 @@ def test_no_cpu_fallback_without_gpu():
         assert e.code == -3
     else:
         raise AssertionError("context created without a GPU")
+
+
+def test_selector_file_round_trip_and_refusals(tmp_path):
+    """Selector files (csv_selector_write / csv_selector_read) are host-only: tables and parameters come back
+    bit for bit; a flipped byte, a truncated file, tables that do not sum to 4096 and a missing file are
+    refused with their codes."""
+    import numpy as np
+    from csvb200 import MLP_PARAMS, CsvError, load_library, read_selector, write_selector
+    lib = load_library()
+    rng = np.random.default_rng(3)
+    params = rng.standard_normal(MLP_PARAMS).astype(np.float32)
+    tables = np.full((5, 16), 256, np.uint32)
+    tables[:, 0] += np.arange(5, dtype=np.uint32)
+    tables[:, 1] -= np.arange(5, dtype=np.uint32)
+    path = str(tmp_path / "sel.csvs")
+    write_selector(lib, path, params, tables)
+    p2, t2 = read_selector(lib, path)
+    assert np.array_equal(p2.view(np.uint32), params.view(np.uint32)) and np.array_equal(t2, tables)
+    raw = bytearray(open(path, "rb").read())
+    assert len(raw) == 16 + 64 * 5 + 4 * MLP_PARAMS + 4
+    for bad, code in [(raw[:-7], -2), (raw[:100] + bytes([raw[100] ^ 1]) + raw[101:], -2)]:
+        open(path, "wb").write(bytes(bad))
+        try:
+            read_selector(lib, path)
+        except CsvError as e:
+            assert e.code == code
+        else:
+            raise AssertionError("a damaged selector file was read")
+    bad_tables = tables.copy()
+    bad_tables[2, 3] += 1
+    for args, code in [((str(tmp_path / "x"), params, bad_tables), -1)]:
+        try:
+            write_selector(lib, *args)
+        except CsvError as e:
+            assert e.code == code
+        else:
+            raise AssertionError("tables that do not sum to 4096 were written")
+    try:
+        read_selector(lib, str(tmp_path / "absent.csvs"))
+    except CsvError as e:
+        assert e.code == -7
+    else:
+        raise AssertionError("a missing file was read")

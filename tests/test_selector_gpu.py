@@ -195,3 +195,35 @@ def test_learned_choice_near_exhaustive_and_faster(codec, oracle):
                           oracle.decode_image(oracle.encode(held.cpu().numpy().view(np.uint64), 64), 6)[0].ravel())
     assert net.status() == 0
     net.close()
+
+
+def test_selector_file_drives_a_learned_encode(codec, oracle, tmp_path):
+    """A trained selector saved to a file and loaded again (csv_selector_write / csv_selector_read) gives the
+    same network and tables, and csv_encode_learned with it writes the image that the step-by-step path
+    (features, the network's choice, csv_encode_device_sel) writes with the original network.  That image
+    decodes to the source."""
+    import torch
+    from csvb200 import SelectorNet
+    from csvb200.selector import exhaustive_choice, features, learned_choice, train
+    v = _vol(codec, (128, 128, 256), 71)
+    h = torch.empty((32, 12, 16), dtype=torch.int32, device="cuda")
+    codec.encode_stats(v, 64, h)
+    tables = _tables(h)
+    net, _ = train(codec, features(codec, v, 64), exhaustive_choice(codec, v, 64, tables)[0], steps=40, batch=32)
+    path = str(tmp_path / "selector.csvs")
+    net.save(path, tables)
+    net2, tables2 = SelectorNet.load(codec, path)
+    assert np.array_equal(tables2, tables)
+    assert np.array_equal(net2.params().view(np.uint32), net.params().view(np.uint32))
+    sel = learned_choice(net, features(codec, v, 64))
+    codec.encode_device_sel(v, 64, tables, sel)
+    step_by_step = _img(codec)
+    n = codec.encode_learned(v, 64, net2, tables2)
+    one_call = _img(codec)
+    assert len(one_call) == n and one_call == step_by_step
+    lab, st = codec.decode_image(one_call, 6)
+    assert int(st.max()) == 0
+    ref = oracle.decode_image(oracle.encode(v.cpu().numpy().view(np.uint64), 64), 6)[0]
+    assert np.array_equal(lab, ref)
+    net.close()
+    net2.close()

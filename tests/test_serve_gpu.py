@@ -43,23 +43,47 @@ def _orbit_views(center, n, r0, r1, yaw0=0.2, pitch=0.25):
     return out
 
 
-def _run_pair(codec, oracle, img, steps, cache_bytes, cone, sessions=1, hidden=None, leave=None, keep=None):
+def _compare_cache(srv, ref, info, sessions):
+    """Every resident block a session's slot table points at holds the oracle's labels."""
+    cache = srv.cache_tensor().cpu().numpy().view(np.uint64)
+    rc = ref.cache(len(cache))
+    for s in sessions:
+        slots = ref.slots(s)
+        for sl in slots[(slots["flags"] == 0)]:
+            n = 8 ** int(sl["lod"]) if sl["offset"] >= info.palette_table else 1
+            o = int(sl["offset"])
+            assert np.array_equal(cache[o:o + n], rc[o:o + n])
+
+
+def _run_pair(codec, oracle, img, steps, cache_bytes, cone, sessions=1, hidden=None, leave=None, keep=None,
+              admit=0, compact_before=()):
     """steps: per step, the list of (session, (pos, dir)) that submit a frame; leave: {step: [sessions]} closed
-    before that step.  Compares GPU and oracle after every step; keep collects each session's images."""
+    before that step; compact_before: steps before which both caches are compacted (and compared).  Compares GPU
+    and oracle after every step; keep collects each session's images."""
     import torch
     from csvb200 import Server
     from oracle import SLOT_DTYPE, OracleServer, camera_uniform
     leave = leave or {}
     ds = codec.open(img)
-    srv = Server(codec, ds, W, H, FOV, cache_bytes=cache_bytes, max_sessions=sessions, cone=cone, hidden=hidden)
-    ref = OracleServer(oracle, img, W, H, FOV, cone, cache_bytes, hidden=hidden)
+    srv = Server(codec, ds, W, H, FOV, cache_bytes=cache_bytes, max_sessions=sessions, cone=cone, hidden=hidden,
+                 admit=admit)
+    ref = OracleServer(oracle, img, W, H, FOV, cone, cache_bytes, hidden=hidden, admit=admit)
     labs = [torch.zeros(W * H, dtype=torch.int64, device="cuda") for _ in range(sessions)]
     deps = [torch.zeros(W * H, dtype=torch.float32, device="cuda") for _ in range(sessions)]
     info = srv.info()
     assert info.n_slots == ref.n_slots and info.bricks_per_axis == ref.bpa
-    seen = {"rebuilt": 0, "freed": 0, "planned0": 0}
+    seen = {"rebuilt": 0, "freed": 0, "planned0": 0, "resident": [], "decoded": []}
     latest = {}
     for k, step in enumerate(steps):
+        if k in compact_before:
+            srv.compact()
+            ref.compact()
+            torch.cuda.synchronize()
+            assert srv.poll(wait=True) == []  # a compaction reports no frame
+            for s in sorted(latest):
+                slots = srv.slots_tensor(s).cpu().numpy().view(SLOT_DTYPE)
+                assert np.array_equal(slots, ref.slots(s)), ("compact", k, s)
+            _compare_cache(srv, ref, info, sorted(latest))
         for s in leave.get(k, []):
             srv.leave(s)
             latest.pop(s, None)
@@ -94,15 +118,10 @@ def _run_pair(codec, oracle, img, steps, cache_bytes, cone, sessions=1, hidden=N
             seen["rebuilt"] += frames[0]["rebuilt"]
             seen["freed"] += frames[0]["freed"]
             seen["planned0"] += frames[0]["planned"] == 0
+            seen["resident"].append(frames[0]["resident"])
+            seen["decoded"].append(frames[0]["decoded"])
     # the resident labels equal the oracle's cache wherever a slot points
-    cache = srv.cache_tensor().cpu().numpy().view(np.uint64)
-    rc = ref.cache(len(cache))
-    for s in sorted(latest):
-        slots = ref.slots(s)
-        for sl in slots[(slots["flags"] == 0)]:
-            n = 8 ** int(sl["lod"]) if sl["offset"] >= info.palette_table else 1
-            o = int(sl["offset"])
-            assert np.array_equal(cache[o:o + n], rc[o:o + n])
+    _compare_cache(srv, ref, info, sorted(latest))
     srv.close()
     ref.close()
     ds.close()
@@ -173,6 +192,39 @@ def test_serve_hidden_labels(codec, oracle, cube16):
     hidden = vals[np.argsort(-counts)[:6]].astype(np.uint64)
     views = _orbit_views((64.0, 64.0, 64.0), 4, 160.0, 110.0)
     _run_pair(codec, oracle, cube16, [[(0, v)] for v in views], 64 << 20, 1, hidden=hidden)
+
+
+def test_serve_admission_by_rays(codec, oracle, cube16):
+    """CSV_ADMIT_RAYS (the reference's useGPUCulling path): the first frame plans by the cone, later frames keep
+    only the bricks the rays entered; bricks hidden behind others are released.  Step by step equal to the
+    oracle's frame loop in the same mode, and the plan differs from the cone plan's."""
+    views = _orbit_views((64.0, 64.0, 64.0), 6, 90.0, 60.0)
+    steps = [[(0, v)] for v in views]
+    steps.insert(2, [(0, views[1])])  # still camera: the new requests re-plan
+    rays = _run_pair(codec, oracle, cube16, steps, 64 << 20, 1, admit=1)
+    cone = _run_pair(codec, oracle, cube16, steps, 64 << 20, 1, admit=0)
+    assert rays["resident"][0] == cone["resident"][0]  # first frame: the cone plan
+    assert all(r <= c for r, c in zip(rays["resident"], cone["resident"]))
+    assert any(r < c for r, c in zip(rays["resident"], cone["resident"]))
+    assert rays["planned0"] == 0 and cone["planned0"] == 1
+
+
+def test_serve_admission_by_rays_two_sessions(codec, oracle, cube16):
+    a = _orbit_views((64.0, 64.0, 64.0), 5, 150.0, 80.0)
+    b = _orbit_views((64.0, 64.0, 64.0), 5, 80.0, 160.0, yaw0=2.5, pitch=-0.3)
+    steps = [[(0, a[k]), (1, b[k])] for k in range(5)]
+    steps.insert(2, [(1, b[1])])  # session 0 open without a new frame: it keeps its plan's inputs
+    _run_pair(codec, oracle, cube16, steps, 8 << 20, 1, sessions=2, admit=1, leave={4: [1]})
+
+
+@pytest.mark.parametrize("cache", [6 << 20, 64 << 20])
+def test_serve_compaction(codec, oracle, slab32, cache):
+    """csv_serve_compact (CacheState.compact()): after frees scattered over the stacks, the resident blocks are
+    packed from offset 0, coarse LODs first; slot tables, cache contents and the following steps equal the
+    oracle's."""
+    views = _orbit_views((128.0, 64.0, 48.0), 9, 260.0, 120.0, yaw0=1.0, pitch=0.4)
+    seen = _run_pair(codec, oracle, slab32, [[(0, v)] for v in views], cache, 1, compact_before=(4, 7))
+    assert seen["freed"] > 0
 
 
 def test_serve_newest_frame_wins_and_errors(codec, cube16):
