@@ -16,9 +16,10 @@ host (bytes compared), and that workload's decode throughput.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-Multi-GPU: one process per GPU (torchrun); every rank decodes its own copy of
-the workload (bricks are independent; no collective on the data path), so
-scaling is weak and value = all ranks' voxels / max-over-ranks time.
+Multi-GPU: one process per GPU (torchrun); every rank decodes its own
+contiguous range of the requests, about 1/N of the voxels (bricks are
+independent: no collective on the data path), so scaling is strong and value =
+the whole volume's voxels / max-over-ranks time.
 """
 from __future__ import annotations
 
@@ -241,6 +242,22 @@ def run_b200(args):
     assert int(status.abs().max()) == 0, "decode status"
     check = (check_against_volume(out, 0, left, bl) and check_against_volume(out, nl * bl ** 3, right, br))
     del left, right
+    # several GPUs: each rank decodes its own contiguous range of the requests, about 1/N of the voxels
+    # (strong scaling: the whole workload is fixed; bricks are independent, so no collective)
+    lo, hi = 0, n
+    if world > 1:
+        from csvb200.dist import voxel_ranges
+        lo, hi = voxel_ranges(sizes, world)[rank]
+        graph.close()
+        d_reqs_r = d_reqs.view(n, 16)[lo:hi].reshape(-1).contiguous()
+        status_r = status[lo:max(hi, lo + 1)]
+        if args.config:
+            best_r = best
+        else:
+            best_r, tune_ms = codec.autotune(cat, d_reqs_r, out, status_r, reps=3)
+        graph = codec.decode_graph(cat, d_reqs_r, out, status_r, best_r)
+        kernels_per_step = graph.kernels
+        best = best_r
 
     stream = torch.cuda.current_stream()
     for _ in range(args.warmup):
@@ -264,14 +281,27 @@ def run_b200(args):
     clocks = clk.stop()
     ms = statistics.mean(times)
     ms_max = max_over_ranks(ms, pg, dev)
-    value = world * nvox / (ms_max * 1e-3) / 1e9
+    value = nvox / (ms_max * 1e-3) / 1e9  # the whole volume, decoded by all ranks together
     info = cat.info
     alg_bytes = info.stream_bytes + 8 * info.palette_entries + 16 * n + 8 * int(sizes.sum())
+    if world > 1:  # this rank's share of the algorithmic bytes (its streams and palettes, its outputs)
+        E_all = np.concatenate([image_stats(img_left)[0], image_stats(img_right)[0]])
+        P_all = np.concatenate([image_stats(img_left)[1], image_stats(img_right)[1]])
+        alg_bytes = int(E_all[lo:hi].sum() + 8 * P_all[lo:hi].sum()) + 16 * (hi - lo) + 8 * int(sizes[lo:hi].sum())
     hbm, hbm_kind = peaks()
     achieved = alg_bytes / (ms * 1e-3) / 1e9
 
     # ---- end to end through the C ABI with host buffers: both images, open + seek index + decode + D2H
     per_img = [(img_left, bl, nl), (img_right, br, nr)]
+    first = [0, nl]  # global request index of each image's first brick here
+    if world > 1:  # this rank's bricks of each image (sub_image keeps header and model)
+        from csvb200.dist import sub_image
+        parts = [(sub_image(img_left, min(lo, nl), min(hi, nl)), bl, min(hi, nl) - min(lo, nl), min(lo, nl)),
+                 (sub_image(img_right, max(lo, nl) - nl, max(hi, nl) - nl), br, max(hi, nl) - max(lo, nl),
+                  max(lo, nl))]
+        parts = [p for p in parts if p[2] > 0]
+        per_img = [p[:3] for p in parts]
+        first = [p[3] for p in parts]
     h_outs = [torch.empty((nb_, b_ ** 3), dtype=torch.int64, pin_memory=True) for _, b_, nb_ in per_img]
     h_st = [np.zeros(nb_, np.uint32) for _, _, nb_ in per_img]
     host_imgs = [np.frombuffer(im, np.uint8) for im, _, _ in per_img]
@@ -298,9 +328,10 @@ def run_b200(args):
             if k > 0:
                 e2e_ms.append((t1 - t0) * 1e3)
     e2e_t = max_over_ranks(statistics.median(e2e_ms), pg, dev)
-    e2e_ok = bool(torch.equal(h_outs[0].view(-1).to(dev), out[: nl * bl ** 3]) and
-                  torch.equal(h_outs[1].view(-1).to(dev), out[nl * bl ** 3:]))
-    e2e = {"value": round(world * nvox / (e2e_t * 1e-3) / 1e9, 3), "unit": "Gvox/s",
+    e2e_ok = all(bool(torch.equal(h_outs[j].view(-1).to(dev),
+                                  out[int(dst[first[j]]): int(dst[first[j]]) + per_img[j][2] * per_img[j][1] ** 3]))
+                 for j in range(len(per_img)))
+    e2e = {"value": round(nvox / (e2e_t * 1e-3) / 1e9, 3), "unit": "Gvox/s",
            "h2d_bytes_per_step": len(img_left) + len(img_right), "d2h_bytes_per_step": 8 * nvox + 4 * n,
            "ms_per_step": round(e2e_t, 2), "ms_samples": [round(t, 1) for t in e2e_ms],
            "path": "csv_decode_image per image, the two images on two host threads and contexts: host .csbd -> "
@@ -325,14 +356,16 @@ def run_b200(args):
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "Gvox/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(ms_max, 4), "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": round(ms_max, 4), "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": workload_config(W, nl, nr, [img_left, img_right]),
             "decode": {"launch": "one CUDA graph (csv_decode_graph)", "decode_config": best.as_dict(),
+                       "ranks": world, "requests_rank0": [lo, hi],
                        "autotuned": not args.config, "autotune_ms": round(tune_ms, 4),
                        "device_stream_bytes": info.stream_bytes},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-                         "frac": round(achieved / hbm, 4), "traffic": load_traffic("decode_kernel", W["name"]),
+                         "frac": round(achieved / hbm, 4),
+                         "traffic": load_traffic("decode_kernel", W["name"]) if world == 1 else None,
                          "algorithmic_bytes": alg_bytes, "peak_kind": hbm_kind},
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -472,6 +505,70 @@ def orbit_path(n, center, seed, scale=1.0):
     return views
 
 
+def serve_mix(codec, ds, dev, S, views, admit=0):
+    """Continuous batching on the serving workload: four sessions share one server and one cache; they join
+    and leave mid-orbit (session 0 the whole orbit, session 1 frames 100-399, session 2 frames 200-499 on a
+    second orbit, session 3 from frame 300 on a third), every open session submits a frame each step.  Each
+    step is submitted, stepped and polled synchronously, so that the host wall time from the first submit to
+    the poll that returns the step's frames is the latency a viewer sees; per session: p50/p99 of the device
+    time of the steps it rendered in, and of that submit-to-poll latency."""
+    import math
+
+    import torch
+    from csvb200 import CONE_SCREEN, Server
+    Wp, Hp = S["width"], S["height"]
+    n = len(views)
+    c = [v / 2.0 for v in S["shape"][::-1]]
+    others = [orbit_path(n, c, S["seed"] + 11 * k, scale=0.8 + 0.2 * k) for k in (1, 2, 3)]
+    spans = [(0, n), (n // 6, 2 * n // 3), (n // 3, 5 * n // 6), (n // 2, n)]
+    paths = [views] + others
+    srv = Server(codec, ds, Wp, Hp, S["fov"], cache_bytes=S["cache_gib"] << 30, max_sessions=4, cone=CONE_SCREEN,
+                 admit=admit)
+    bufs = [(torch.empty(Wp * Hp, dtype=torch.int64, device=dev), torch.empty(Wp * Hp, dtype=torch.float32,
+                                                                              device=dev)) for _ in range(4)]
+    st = torch.cuda.current_stream()
+    dev_ms = {k: [] for k in range(4)}
+    lat_ms = {k: [] for k in range(4)}
+    joined, left, rebuilds, open_max = 0, 0, 0, 0
+    was_open = [False] * 4
+    torch.cuda.synchronize()
+    for f in range(n):
+        t0 = time.perf_counter()
+        now_open = [lo <= f < hi for lo, hi in spans]
+        for k in range(4):
+            if was_open[k] and not now_open[k]:
+                srv.leave(k)
+                left += 1
+            if now_open[k]:
+                joined += not was_open[k]
+                pos, d = paths[k][f]
+                srv.submit(k, pos, d, *bufs[k])
+        was_open = now_open
+        open_max = max(open_max, sum(now_open))
+        srv.step(st)
+        frames = srv.poll(wait=True)
+        t1 = time.perf_counter()
+        for fr in frames:
+            dev_ms[fr["session"]].append(fr["ms"])
+            lat_ms[fr["session"]].append((t1 - t0) * 1e3)
+        rebuilds += frames[0]["rebuilt"] if frames else 0
+    srv.close()
+
+    def pct(a, q):
+        return round(float(np.percentile(np.array(a), q)), 3) if a else None
+
+    per = {str(k): {"frames": len(dev_ms[k]), "span": list(spans[k]), "p50_ms": pct(dev_ms[k], 50),
+                    "p99_ms": pct(dev_ms[k], 99), "submit_to_poll_p50_ms": pct(lat_ms[k], 50),
+                    "submit_to_poll_p99_ms": pct(lat_ms[k], 99)} for k in range(4)}
+    every = [x for k in range(4) for x in dev_ms[k]]
+    lat = [x for k in range(4) for x in lat_ms[k]]
+    return {"sessions": per, "joins": joined, "leaves": left, "open_max": open_max, "rebuilds": rebuilds,
+            "admit": "rays" if admit else "cone",
+            "p99_ms_all": pct(every, 99), "submit_to_poll_p99_ms_all": pct(lat, 99),
+            "timing": "device time per step (CUDA events) and host wall time submit -> poll(wait), one step in "
+                      "flight"}
+
+
 def serve2048(codec, dev, args):
     """On-demand decode + render at 1920x1080 over a 2048^3 volume with a 24 GiB decoded-brick cache."""
     import math
@@ -542,6 +639,11 @@ def serve2048(codec, dev, args):
         srv.step(st)
     fr = srv.poll(wait=True, max_frames=len(views) + 8)
     ms2 = np.array([f["ms"] for f in fr])
+    srv.close()
+    # continuous batching: four sessions joining and leaving mid-orbit, cone admission and admission by rays
+    torch.cuda.empty_cache()
+    out["mix"] = serve_mix(codec, ds, dev, S, views, admit=0)
+    out["mix_rays"] = serve_mix(codec, ds, dev, S, views, admit=1)
     out["rgba"] = {"p50_ms": round(float(np.percentile(ms2, 50)), 3), "p99_ms": round(float(np.percentile(ms2, 99)), 3),
                    "max_ms": round(float(ms2.max()), 3), "mean_ms": round(float(ms2.mean()), 3),
                    "entered_bricks_mean": round(float(np.mean([f["entered"] for f in fr])), 1),

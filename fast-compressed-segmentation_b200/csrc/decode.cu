@@ -166,6 +166,74 @@ __device__ __forceinline__ uint32_t rans_step(uint32_t& x, uint32_t& pos, const 
 }
 
 // -------------------------------------------------------------- seek index
+// The rANS step of the serial pass.  Same arithmetic as rans_step; both bytes
+// a well-formed renormalisation can take are read before the state is known
+// (their addresses depend only on pos), so the loads overlap the table lookup
+// instead of following it on the chain.
+__device__ __forceinline__ uint32_t index_step(uint32_t& x, uint32_t& pos, const uint8_t* __restrict__ enc,
+                                               const uint32_t* lut) {
+    const uint32_t b1 = __ldg(enc + (pos > 0 ? pos - 1 : 0));
+    const uint32_t b2 = __ldg(enc + (pos > 1 ? pos - 2 : 0));
+    const uint32_t v = x & (kTot - 1);
+    const uint32_t e = lut[v];
+    x = ((e >> 4) & 0x1FFFu) * (x >> kTotBits) + v - (e >> 17);
+    if (x < kRansL && pos > 0) {
+        x = (x << 8) | b1;
+        --pos;
+        if (x < kRansL && pos > 0) {
+            x = (x << 8) | b2;
+            --pos;
+            while (x < kRansL && pos > 0) x = (x << 8) | __ldg(enc + (--pos));  // malformed streams only
+        }
+    }
+    return e & 15u;
+}
+
+// The serial pass over one brick's symbols.  The bookkeeping of each symbol
+// (Pd pairs, palette count, active children, ops per level) is computed with
+// selects rather than branches: one lane per warp runs this chain, so every
+// branch it waits on adds to every step.  Branches remain only for the rare
+// events (a checkpoint every S ops, the end of a level, truncation).
+__device__ __forceinline__ void index_chain(const BrickDesc& br, const uint8_t* __restrict__ enc, const uint32_t* lut,
+                                            Checkpoint* __restrict__ ck, uint32_t L, uint32_t S, uint32_t& x,
+                                            uint32_t& pos, uint32_t (&ls)[8], uint32_t& ops, uint32_t& n_ck,
+                                            uint32_t& flags) {
+    uint32_t sym = 1, ip = 0, need = 8, lvl = 0, act = 0, done = 0, until_ck = 0;
+    bool in_pd = false;
+    while (lvl + 1 < L && need > 0) {
+        if (!in_pd && until_ck == 0) {  // checkpoint before every S-th op
+            if (n_ck < br.ck_cap) ck[br.ck_off + n_ck] = Checkpoint{x, pos, sym, ip};
+            ++n_ck;
+            until_ck = S;
+        }
+        if (sym >= br.nsym) {
+            flags |= BF_TRUNCATED;
+            if (in_pd) ++ops;
+            break;
+        }
+        const uint32_t v = index_step(x, pos, enc, lut);
+        ++sym;
+        const uint32_t code = v >> 1;
+        const bool prim = !in_pd;                // a primary nibble (not a Pd op's delta)
+        const bool pd = prim && code == OP_PD;   // a Pd op's primary: the op ends with the next symbol
+        ip += (prim && code == OP_PA) ? 1u : 0u;
+        act += (prim && !(v & 1u)) ? 1u : 0u;
+        in_pd = pd;
+        const uint32_t fin = pd ? 0u : 1u;       // an op ends with this symbol
+        ops += fin;
+        until_ck -= fin;
+        done += fin;
+        if (fin && done == need) {
+            ++lvl;
+            ls[lvl] = ops;
+            need = 8 * act;
+            act = 0;
+            done = 0;
+        }
+    }
+    for (uint32_t k = lvl + 1; k < 8; ++k) ls[k] = ops;
+}
+
 // One thread per brick: the decoder's serial pass, recording a checkpoint
 // before every S-th op and the first op of every level.  Level l+1 has 8 ops
 // per op of level l with stop bit 0; level 1 has 8 unless the root's stop bit
@@ -189,7 +257,6 @@ __global__ void __launch_bounds__(128) build_index_kernel(BrickDesc* __restrict_
     BrickDesc br = bricks[bi];
     // a version-2 image names a shared table per brick; other tables are read through the cache
     const uint32_t model = min((br.flags >> BF_MODEL_SHIFT) & 255u, n_models - 1);
-    const uint32_t* lut = model == 0 ? lut0 : g_lut + (size_t)model * kTot;
     uint32_t ls[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) ls[k] = 0;
@@ -201,49 +268,19 @@ __global__ void __launch_bounds__(128) build_index_kernel(BrickDesc* __restrict_
         uint32_t pos = br.E - 4;
         uint32_t x = ((uint32_t)enc[br.E - 1] << 24) | ((uint32_t)enc[br.E - 2] << 16) |
                      ((uint32_t)enc[br.E - 3] << 8) | enc[br.E - 4];
-        uint32_t sym = 1;
-        uint32_t root = rans_step(x, pos, enc, lut);
+        // One symbol per iteration (a Pd op spans two), so the lanes of a warp
+        // never differ in the number of rANS steps an iteration takes.  Model 0's
+        // table is read from shared memory (the pointer is the shared array
+        // itself, so the loads are shared-memory loads), others through the cache.
+        const uint32_t root = model == 0 ? index_step(x, pos, enc, lut0)
+                                         : index_step(x, pos, enc, g_lut + (size_t)model * kTot);
         if (root & 1u) {
             flags = BF_UNIFORM;
         } else {
-            // One symbol per iteration (a Pd op spans two), so the lanes of a warp
-            // never differ in the number of rANS steps an iteration takes.
-            uint32_t ip = 0, need = 8, lvl = 0, act = 0, done = 0, until_ck = 0;
-            bool in_pd = false;
-            while (lvl + 1 < L && need > 0) {
-                if (!in_pd && until_ck == 0) {  // checkpoint before every S-th op
-                    if (n_ck < br.ck_cap) ck[br.ck_off + n_ck] = Checkpoint{x, pos, sym, ip};
-                    ++n_ck;
-                    until_ck = S;
-                }
-                if (sym >= br.nsym) {
-                    flags |= BF_TRUNCATED;
-                    if (in_pd) ++ops;
-                    break;
-                }
-                const uint32_t v = rans_step(x, pos, enc, lut);
-                ++sym;
-                if (!in_pd) {
-                    if ((v >> 1) == OP_PD) {
-                        in_pd = true;
-                        if (!(v & 1u)) ++act;
-                        continue;
-                    }
-                    if ((v >> 1) == OP_PA) ++ip;
-                    if (!(v & 1u)) ++act;
-                }
-                in_pd = false;
-                ++ops;
-                --until_ck;
-                if (++done == need) {
-                    ++lvl;
-                    ls[lvl] = ops;
-                    need = 8 * act;
-                    act = 0;
-                    done = 0;
-                }
-            }
-            for (uint32_t k = lvl + 1; k < 8; ++k) ls[k] = ops;
+            if (model == 0)
+                index_chain(br, enc, lut0, ck, L, S, x, pos, ls, ops, n_ck, flags);
+            else
+                index_chain(br, enc, g_lut + (size_t)model * kTot, ck, L, S, x, pos, ls, ops, n_ck, flags);
             if (n_ck > br.ck_cap) flags |= BF_TRUNCATED;
         }
     }
@@ -294,6 +331,10 @@ struct DecodeArgs {
 
 __device__ __forceinline__ void st_cs_v2(uint64_t* p, uint64_t a, uint64_t b) {
     asm volatile("st.global.cs.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(a), "l"(b) : "memory");
+}
+// One 32-byte store (sm_100's 256-bit global store; p 32-byte aligned), streaming.
+__device__ __forceinline__ void st_cs_v4(uint64_t* p, uint64_t a, uint64_t b, uint64_t c, uint64_t d) {
+    asm volatile("st.global.cs.v4.u64 [%0], {%1, %2, %3, %4};" ::"l"(p), "l"(a), "l"(b), "l"(c), "l"(d) : "memory");
 }
 
 // Writes `cnt` copies of `v` at out[0..cnt) (out 8-byte aligned).
@@ -406,6 +447,31 @@ __device__ __forceinline__ uint64_t label_of(const uint64_t* pal, uint32_t pidx,
 // Step 1: every thread decodes seek segments of the brick (S ops each) into op
 // records.  One rANS step per iteration; a Pd op's delta nibble is its own
 // iteration, so the lanes of a warp never differ in steps per iteration.
+// One op of a segment whose symbols are all in the stream: a Pd op reads its
+// delta nibble in the same call.  Returns the op's record.
+template <bool GLOBAL>
+__device__ __forceinline__ uint32_t decode_op(uint32_t& x, uint32_t& pos, uint32_t& ip, const uint8_t* enc,
+                                              const uint32_t* lut, uint32_t P, uint32_t& st, uint32_t LABEL0) {
+    const uint32_t v = rans_step<GLOBAL>(x, pos, enc, lut);
+    const uint32_t code = v >> 1, stop = (v & 1u) << 3;
+    uint32_t pidx;
+    if (code == OP_PD) {
+        pidx = ip - rans_step<GLOBAL>(x, pos, enc, lut) - 1;
+    } else {
+        ip += (code == OP_PA);
+        pidx = (code == OP_PA || code == OP_P0) ? ip : 0u;
+        if (code == 7) {
+            pidx = LABEL0;
+            st |= CSV_BRICK_BADOP;
+        }
+    }
+    if (code >= OP_PA && code <= OP_PD && pidx >= P) {  // past the palette: clamped as decode.wgsl:472-485
+        pidx = P - 1;
+        st |= CSV_BRICK_PALETTE;
+    }
+    return code | stop | (pidx << REC_PIDX_SHIFT);
+}
+
 template <bool GLOBAL>
 __device__ __forceinline__ void decode_segments(const DecodeArgs& A, const BrickDesc& br, const uint8_t* enc,
                                                 const uint32_t* lut, uint32_t n_need, uint32_t nseg,
@@ -415,6 +481,27 @@ __device__ __forceinline__ void decode_segments(const DecodeArgs& A, const Brick
         uint32_t x = c.state, pos = c.pos, sym = c.sym, ip = c.ip;
         uint32_t j = k * A.S;  // a multiple of 4 (S is)
         const uint32_t jend = min(j + A.S, n_need);
+        // Fast path: an op takes at most two symbols, so a segment whose ops cannot
+        // run past nSymbols needs no truncation test; four ops per iteration go to
+        // one 16-byte record group.  The general loop below takes what is left
+        // (a segment's last ops when fewer than four, or any segment near the end
+        // of a stream).
+        if (sym + 2 * (jend - j) <= br.nsym) {
+            const uint32_t sym0 = sym;
+            uint32_t n4 = (jend - j) & ~3u;
+            for (uint32_t e = j + n4; j < e; j += 4) {
+                const uint32_t r0 = decode_op<GLOBAL>(x, pos, ip, enc, lut, br.P, st, LABEL0);
+                const uint32_t r1 = decode_op<GLOBAL>(x, pos, ip, enc, lut, br.P, st, LABEL0);
+                const uint32_t r2 = decode_op<GLOBAL>(x, pos, ip, enc, lut, br.P, st, LABEL0);
+                const uint32_t r3 = decode_op<GLOBAL>(x, pos, ip, enc, lut, br.P, st, LABEL0);
+                reinterpret_cast<uint4*>(recs + j)[0] = make_uint4(r0, r1, r2, r3);
+                n4 += (r0 & 7u) == OP_PD;  // symbols: one per op plus one per Pd
+                n4 += (r1 & 7u) == OP_PD;
+                n4 += (r2 & 7u) == OP_PD;
+                n4 += (r3 & 7u) == OP_PD;
+            }
+            sym = sym0 + n4;
+        }
         uint32_t pd_stop = 0xFFFFFFFFu;  // != ~0: the primary nibble of a Pd op was read
         // records leave in 16-byte groups: lanes write different segments, so a
         // 4-byte store per op would cost one memory transaction per lane per op
@@ -615,6 +702,7 @@ __global__ void __launch_bounds__(dec_threads<KL>(), KL == kDecLevels ? 2 : 6) d
 
             // ---- 2./3. levels coarse to fine
             const bool vec = (((uintptr_t)out) & 15) == 0;
+            const bool vec32 = (((uintptr_t)out) & 31) == 0;
             uint32_t n_act = 1;
             for (uint32_t l = 0; l < t; ++l) {
                 const uint32_t lc = l + 1;
@@ -700,8 +788,49 @@ __global__ void __launch_bounds__(dec_threads<KL>(), KL == kDecLevels ? 2 : 6) d
                     }
                     n_act = n_act_c;
                     __syncthreads();
+                } else if (vec32) {
+                    // last level: labels to HBM with 32-byte stores, two lanes per
+                    // parent (four children each), so that a warp's store covers 1 KB
+                    // of contiguous output.  Stop-filled parents first: chunk q is
+                    // children 4(q&1) .. 4(q&1)+3 of parent q / 2.
+                    const uint32_t n_chunk = 2 * n_par;
+                    for (uint32_t q = tid; q < n_chunk; q += T) {
+                        const uint32_t p = q >> 1;
+                        if (!is_active(Vw, p)) {
+                            const uint64_t x = label_of(pal, Vw.val[p], LABEL0);
+                            st_cs_v4(out + 4ull * q, x, x, x, x);
+                        }
+                    }
+                    // active parents: two lanes per parent, four children each from
+                    // one 16-byte record load; the next parent's index and records
+                    // are fetched before this one is resolved.
+                    const uint32_t half = tid & 1u;
+                    auto fetch = [&](uint32_t g, uint32_t& p, uint4& r) {
+                        p = act_l[g];
+                        const uint32_t i0 = Vw.o + 8 * g + 4 * half;
+                        if ((i0 & 3u) == 0 && i0 + 4 <= Vw.n_rec) {
+                            r = *reinterpret_cast<const uint4*>(Vw.rec + i0);
+                        } else {
+                            r = make_uint4(get_rec(Vw, i0), get_rec(Vw, i0 + 1), get_rec(Vw, i0 + 2),
+                                           get_rec(Vw, i0 + 3));
+                        }
+                    };
+                    uint32_t g = tid >> 1, p_next = 0;
+                    uint4 r_next = make_uint4(0, 0, 0, 0);
+                    if (g < n_act) fetch(g, p_next, r_next);
+                    for (; g < n_act; g += T >> 1) {
+                        const uint32_t p = p_next;
+                        const uint4 r = r_next;
+                        if (g + (T >> 1) < n_act) fetch(g + (T >> 1), p_next, r_next);
+                        const uint32_t n0 = 8 * p + 4 * half;
+                        const uint64_t a = label_of(pal, resolve(Vw, r.x, n0, lc, &bad), LABEL0);
+                        const uint64_t b = label_of(pal, resolve(Vw, r.y, n0 + 1, lc, &bad), LABEL0);
+                        const uint64_t c = label_of(pal, resolve(Vw, r.z, n0 + 2, lc, &bad), LABEL0);
+                        const uint64_t d = label_of(pal, resolve(Vw, r.w, n0 + 3, lc, &bad), LABEL0);
+                        st_cs_v4(out + n0, a, b, c, d);
+                    }
                 } else {
-                    // last level: labels to HBM.  Each thread writes 16 bytes (two
+                    // last level, output not 32-byte aligned.  Each thread writes 16 bytes (two
                     // children) per step so that a warp's store covers 512
                     // contiguous bytes.  Stop-filled parents: chunk q is children
                     // 2q, 2q+1 of parent q / 4.

@@ -122,6 +122,15 @@ def brick_ranges(nb: int, world: int):
     return out
 
 
+def voxel_ranges(sizes, world: int):
+    """Contiguous request ranges [lo, hi) per rank with about equal output voxels (sizes: voxels per request,
+    in order).  Bricks are independent, so each rank decodes its range with no exchange."""
+    import numpy as np
+    c = np.concatenate([[0], np.cumsum(np.asarray(sizes, np.float64))])
+    cuts = [0] + [int(np.searchsorted(c, c[-1] * r / world)) for r in range(1, world)] + [len(c) - 1]
+    return [(cuts[r], max(cuts[r], cuts[r + 1])) for r in range(world)]
+
+
 def sub_image(image: bytes, lo: int, hi: int) -> bytes:
     """A version-1 .csbd image holding bricks [lo, hi) of `image` (same header and model; numBricks = hi - lo).
     Record layout: ID, P, palette[P], E, stream[E], nSymbols (fileIO.cpp:57-96)."""

@@ -44,3 +44,19 @@ def test_sharded_encode_and_decode_on_gloo_ranks(world):
         outs.append(out)
     for rank, (p, out) in enumerate(zip(procs, outs)):
         assert p.returncode == 0, f"rank {rank} exited {p.returncode}:\n{out[-3000:]}"
+
+
+def test_voxel_ranges_cover_and_balance():
+    """The bench's multi-GPU split: contiguous request ranges that cover every request once, each rank's
+    voxels within one request of an equal share."""
+    import numpy as np
+    from csvb200.dist import voxel_ranges
+    rng = np.random.default_rng(5)
+    for world in (1, 2, 3, 8):
+        sizes = np.concatenate([np.full(1000, 32 ** 3), np.full(130, 64 ** 3)])[rng.permutation(1130)]
+        r = voxel_ranges(sizes, world)
+        assert r[0][0] == 0 and r[-1][1] == len(sizes)
+        assert all(a[1] == b[0] for a, b in zip(r, r[1:]))
+        share = sizes.sum() / world
+        for lo, hi in r:
+            assert abs(sizes[lo:hi].sum() - share) <= sizes.max()
