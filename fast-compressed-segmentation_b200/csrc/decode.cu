@@ -33,6 +33,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <vector>
 
 #include "block_scan.cuh"
 #include "csv_internal.h"
@@ -189,78 +190,51 @@ __device__ __forceinline__ uint32_t index_step(uint32_t& x, uint32_t& pos, const
     return e & 15u;
 }
 
-// The serial pass over one brick's symbols.  The bookkeeping of each symbol
-// (Pd pairs, palette count, active children, ops per level) is computed with
-// selects rather than branches: one lane per warp runs this chain, so every
-// branch it waits on adds to every step.  Branches remain only for the rare
-// events (a checkpoint every S ops, the end of a level, truncation).
-__device__ __forceinline__ void index_chain(const BrickDesc& br, const uint8_t* __restrict__ enc, const uint32_t* lut,
-                                            Checkpoint* __restrict__ ck, uint32_t L, uint32_t S, uint32_t& x,
-                                            uint32_t& pos, uint32_t (&ls)[8], uint32_t& ops, uint32_t& n_ck,
-                                            uint32_t& flags) {
-    uint32_t sym = 1, ip = 0, need = 8, lvl = 0, act = 0, done = 0, until_ck = 0;
-    bool in_pd = false;
-    while (lvl + 1 < L && need > 0) {
-        if (!in_pd && until_ck == 0) {  // checkpoint before every S-th op
-            if (n_ck < br.ck_cap) ck[br.ck_off + n_ck] = Checkpoint{x, pos, sym, ip};
-            ++n_ck;
-            until_ck = S;
-        }
-        if (sym >= br.nsym) {
-            flags |= BF_TRUNCATED;
-            if (in_pd) ++ops;
-            break;
-        }
-        const uint32_t v = index_step(x, pos, enc, lut);
-        ++sym;
-        const uint32_t code = v >> 1;
-        const bool prim = !in_pd;                // a primary nibble (not a Pd op's delta)
-        const bool pd = prim && code == OP_PD;   // a Pd op's primary: the op ends with the next symbol
-        ip += (prim && code == OP_PA) ? 1u : 0u;
-        act += (prim && !(v & 1u)) ? 1u : 0u;
-        in_pd = pd;
-        const uint32_t fin = pd ? 0u : 1u;       // an op ends with this symbol
-        ops += fin;
-        until_ck -= fin;
-        done += fin;
-        if (fin && done == need) {
-            ++lvl;
-            ls[lvl] = ops;
-            need = 8 * act;
-            act = 0;
-            done = 0;
-        }
-    }
-    for (uint32_t k = lvl + 1; k < 8; ++k) ls[k] = ops;
-}
+// The seek index in three passes.  A brick's symbols form one dependent rANS
+// chain, and the longest brick sets the time, so the per-symbol bookkeeping
+// (Pd pairs, palette count, active children, ops per level, checkpoints) is
+// taken off that chain:
+//   1. index_symbols_kernel: one lane per brick runs the chain alone, writing
+//      every symbol (packed nibbles) and the state before every kSnap-th one;
+//   2. index_book_kernel: one warp per brick walks the nibbles 256 at a time:
+//      which nibbles start ops (a Pd op's delta does not) is a two-state
+//      automaton whose per-lane transfer functions compose in a warp scan; op,
+//      palette and active counts are warp prefix sums; level boundaries
+//      (level l+1 has 8 ops per active op of level l) are found by ballot; the
+//      checkpoints before every S-th op get their symbol and palette index;
+//   3. index_states_kernel: each checkpoint's (state, pos) is decoded again
+//      from the snapshot before it (fewer than kSnap steps), all in parallel.
+// The result equals the serial walk of the reference decoder
+// (brickDecoding.hpp:174-242): the same checkpoints, op count, level starts and
+// flags.
+constexpr uint32_t kSnap = 32;  // symbols between state snapshots
 
-// One thread per brick: the decoder's serial pass, recording a checkpoint
-// before every S-th op and the first op of every level.  Level l+1 has 8 ops
-// per op of level l with stop bit 0; level 1 has 8 unless the root's stop bit
-// is set (then the brick is one label).
-__global__ void __launch_bounds__(128) build_index_kernel(BrickDesc* __restrict__ bricks, uint32_t nb,
-                                                         const uint8_t* __restrict__ enc_pool,
-                                                         const uint32_t* __restrict__ g_lut,
-                                                         Checkpoint* __restrict__ ck, uint32_t L, uint32_t S,
-                                                         uint32_t n_models, uint32_t lanes) {
+__global__ void __launch_bounds__(128) index_symbols_kernel(BrickDesc* __restrict__ bricks, uint32_t nb,
+                                                           const uint8_t* __restrict__ enc_pool,
+                                                           const uint32_t* __restrict__ g_lut, uint32_t n_models,
+                                                           uint32_t lanes, const uint64_t* __restrict__ nib_off,
+                                                           const uint64_t* __restrict__ snap_off,
+                                                           uint32_t* __restrict__ nib, uint2* __restrict__ snap,
+                                                           uint8_t* __restrict__ chain, uint32_t L) {
+    // model 0's table in this pass's form: symbol | freq << 4 | (x - start) << 17,
+    // so that a step adds the offset within the symbol's range straight from the table
     __shared__ uint32_t lut0[kTot];
-    for (uint32_t i = threadIdx.x; i < kTot; i += blockDim.x) lut0[i] = g_lut[i];
+    for (uint32_t i = threadIdx.x; i < kTot; i += blockDim.x) {
+        const uint32_t e = g_lut[i];
+        lut0[i] = (e & 0x1FFFFu) | ((i - (e >> 17)) << 17);
+    }
     __syncthreads();
-    // The pass is one dependent chain per brick.  Lanes of one warp on
-    // different bricks run the union of their branch paths every step, so a
-    // warp works on only `lanes` bricks (lanes 0 .. lanes-1) when there are
-    // few enough bricks to give the SMs' schedulers many warps to interleave.
+    // Lanes of one warp on different bricks run the union of their branch paths
+    // every step, so a warp takes only `lanes` bricks when there are few enough
+    // bricks to give the schedulers many warps to interleave.
     const uint32_t lane = threadIdx.x & 31;
     if (lane >= lanes) return;
-    uint32_t bi = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * lanes + lane;
+    const uint32_t bi = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * lanes + lane;
     if (bi >= nb) return;
-    BrickDesc br = bricks[bi];
-    // a version-2 image names a shared table per brick; other tables are read through the cache
+    const BrickDesc br = bricks[bi];
     const uint32_t model = min((br.flags >> BF_MODEL_SHIFT) & 255u, n_models - 1);
-    uint32_t ls[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) ls[k] = 0;
-    uint32_t flags = 0, ops = 0, n_ck = 0;
+    uint32_t flags = 0;
+    bool go = false;
     if (br.E < 4 || br.nsym == 0) {
         flags = BF_TRUNCATED;
     } else {
@@ -268,44 +242,317 @@ __global__ void __launch_bounds__(128) build_index_kernel(BrickDesc* __restrict_
         uint32_t pos = br.E - 4;
         uint32_t x = ((uint32_t)enc[br.E - 1] << 24) | ((uint32_t)enc[br.E - 2] << 16) |
                      ((uint32_t)enc[br.E - 3] << 8) | enc[br.E - 4];
-        // One symbol per iteration (a Pd op spans two), so the lanes of a warp
-        // never differ in the number of rANS steps an iteration takes.  Model 0's
-        // table is read from shared memory (the pointer is the shared array
-        // itself, so the loads are shared-memory loads), others through the cache.
-        const uint32_t root = model == 0 ? index_step(x, pos, enc, lut0)
-                                         : index_step(x, pos, enc, g_lut + (size_t)model * kTot);
-        if (root & 1u) {
-            flags = BF_UNIFORM;
+        uint32_t* w = nib + nib_off[bi];
+        uint2* sn = snap + snap_off[bi];
+        sn[0] = make_uint2(x, pos);
+        // model 0's table from shared memory (the pointer is the shared array itself);
+        // a version-2 image's other tables in the usual form (rel: offsets stored)
+        auto run = [&](const uint32_t* lut, bool rel) {
+            // One rANS step: the stream is walked through a pointer to byte pos, so the
+            // two bytes a renormalisation can take are loads at fixed offsets, issued
+            // (predicated on pos) before the state is known.
+            const uint8_t* q = enc + pos;
+            auto step = [&]() -> uint32_t {
+                const uint32_t b1 = pos > 0 ? (uint32_t)__ldg(q - 1) : 0u;
+                const uint32_t b2 = pos > 1 ? (uint32_t)__ldg(q - 2) : 0u;
+                const uint32_t v = x & (kTot - 1);
+                const uint32_t e = lut[v];
+                x = ((e >> 4) & 0x1FFFu) * (x >> kTotBits) + (rel ? (e >> 17) : v - (e >> 17));
+                // the renormalisation's bytes in one choice: a second byte is taken
+                // exactly when x < 2^15, since (x << 8 | b1) < 2^23 then
+                const bool n1 = x < kRansL && pos > 0, n2 = n1 && x < (kRansL >> 8) && pos > 1;
+                const uint32_t c1 = (x << 8) | b1, c2 = (x << 16) | (b1 << 8) | b2;
+                x = n2 ? c2 : (n1 ? c1 : x);
+                const uint32_t nb = (n1 ? 1u : 0u) + (n2 ? 1u : 0u);
+                pos -= nb;
+                q -= nb;
+                while (x < kRansL && pos > 0) {  // malformed streams only
+                    x = (x << 8) | __ldg(--q);
+                    --pos;
+                }
+                return e & 15u;
+            };
+            const uint32_t root = step();
+            if (root & 1u) {
+                flags = BF_UNIFORM;  // the whole brick is palette[0]: nothing more to index
+                w[0] = root;
+                return;
+            }
+            go = L >= 2;
+            const uint32_t ns = br.nsym;
+            // word 0: the root and symbols 1..7
+            uint32_t word = root;
+            for (uint32_t i = 1; i < 8 && i < ns; ++i) word |= step() << (4 * i);
+            w[0] = word;
+            // whole words of 8 symbols (a snapshot before every 4th: symbol 32k)
+            uint32_t k = 1;
+            for (; 8 * k + 8 <= ns; ++k) {
+                if ((k & 3u) == 0) sn[k >> 2] = make_uint2(x, pos);
+                uint32_t wd = step();
+#pragma unroll
+                for (uint32_t j = 1; j < 8; ++j) wd |= step() << (4 * j);
+                w[k] = wd;
+            }
+            if (8 * k < ns) {  // the last, partial word
+                if ((k & 3u) == 0) sn[k >> 2] = make_uint2(x, pos);
+                uint32_t wd = 0;
+                for (uint32_t j = 0; 8 * k + j < ns; ++j) wd |= step() << (4 * j);
+                w[k] = wd;
+            }
+        };
+        if (model == 0) run(lut0, true);
+        else run(g_lut + (size_t)model * kTot, false);
+    }
+    chain[bi] = go ? 1 : 0;
+    if (!go) {
+        BrickDesc& o = bricks[bi];
+        o.n_ops = 0;
+        o.flags = (br.flags & ~BF_STATUS_MASK) | flags;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) o.level_start[k] = 0;
+    }
+}
+
+// Composition of the per-lane automaton transfers (bit 0: the state after, from
+// state 0; bit 1: from state 1): apply `first`, then `then`.
+__device__ __forceinline__ uint32_t compose2(uint32_t first, uint32_t then) {
+    const uint32_t a0 = (then >> (first & 1u)) & 1u, a1 = (then >> ((first >> 1) & 1u)) & 1u;
+    return a0 | (a1 << 1);
+}
+
+__global__ void __launch_bounds__(128) index_book_kernel(BrickDesc* __restrict__ bricks, uint32_t nb,
+                                                        const uint32_t* __restrict__ nib,
+                                                        const uint64_t* __restrict__ nib_off,
+                                                        const uint8_t* __restrict__ chain, Checkpoint* __restrict__ ck,
+                                                        uint32_t* __restrict__ n_ck_out, uint32_t L, uint32_t S) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t bi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (bi >= nb) return;
+    if (!chain[bi]) {
+        if (lane == 0) n_ck_out[bi] = 0;
+        return;
+    }
+    const uint32_t FULL = 0xFFFFFFFFu;
+    const BrickDesc br = bricks[bi];
+    const uint32_t* w = nib + nib_off[bi];
+    const uint32_t nsym = br.nsym;
+    // automaton state before the next chunk: 0 = the next nibble starts an op, 1 = it is a Pd op's delta
+    uint32_t st_in = 0;
+    uint32_t op_base = 0, ip_base = 0, act_base = 0;  // ops, Pa ops and active ops before the chunk
+    uint32_t lvl = 0, b_next = 8, act_cur = 0;        // level lvl+1 ends before op b_next; actives before its start
+    uint32_t ls[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t n_ck = 0, end_ops = 0xFFFFFFFFu;
+    bool done = false;
+    for (uint32_t c0 = 0; c0 < nsym && !done; c0 += 256) {
+        const uint32_t base = c0 + 8 * lane;
+        const uint32_t word = base < nsym ? w[base >> 3] : 0u;
+        // symbols of this lane: [max(base, 1), min(base + 8, nsym)) -- symbol 0 is the root
+        const uint32_t i0 = base == 0 ? 1u : base, i1 = min(base + 8, nsym);
+        auto step = [&](uint32_t st, uint32_t k) -> uint32_t {
+            const uint32_t v = (word >> (4 * k)) & 15u;
+            return (st == 0 && (v >> 1) == OP_PD) ? 1u : 0u;
+        };
+        uint32_t f0 = 0, f1 = 1;
+        for (uint32_t i = i0; i < i1; ++i) {
+            f0 = step(f0, i - base);
+            f1 = step(f1, i - base);
+        }
+        uint32_t inc = f0 | (f1 << 1);
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(FULL, inc, d);
+            if (lane >= (uint32_t)d) inc = compose2(y, inc);
+        }
+        uint32_t excl = __shfl_up_sync(FULL, inc, 1);
+        if (lane == 0) excl = 2u;  // identity
+        const uint32_t entry = (excl >> st_in) & 1u;
+        const uint32_t exit_all = (__shfl_sync(FULL, inc, 31) >> st_in) & 1u;
+        // this lane's op starts, Pa ops and active ops
+        uint32_t np = 0, npa = 0, nact = 0;
+        {
+            uint32_t st = entry;
+            for (uint32_t i = i0; i < i1; ++i) {
+                const uint32_t v = (word >> (4 * (i - base))) & 15u;
+                if (st == 0) {
+                    ++np;
+                    npa += (v >> 1) == OP_PA;
+                    nact += !(v & 1u);
+                }
+                st = step(st, i - base);
+            }
+        }
+        const uint32_t packed = np | (npa << 10) | (nact << 20);
+        uint32_t pin = packed;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(FULL, pin, d);
+            if (lane >= (uint32_t)d) pin += y;
+        }
+        const uint32_t pex = pin - packed, ptot = __shfl_sync(FULL, pin, 31);
+        const uint32_t my_op = op_base + (pex & 1023u), my_ip = ip_base + ((pex >> 10) & 1023u),
+                       my_act = act_base + (pex >> 20);
+        const uint32_t tot_np = ptot & 1023u;
+        // level boundaries among this chunk's op starts
+        while (!done && b_next < op_base + tot_np) {
+            const bool has = my_op <= b_next && b_next < my_op + np;
+            const uint32_t src = __ffs(__ballot_sync(FULL, has)) - 1;
+            uint32_t ap = 0;
+            if (has) {  // actives among the ops before b_next
+                ap = my_act;
+                uint32_t st = entry, j = my_op;
+                for (uint32_t i = i0; i < i1 && j < b_next; ++i) {
+                    const uint32_t v = (word >> (4 * (i - base))) & 15u;
+                    if (st == 0) {
+                        ap += !(v & 1u);
+                        ++j;
+                    }
+                    st = step(st, i - base);
+                }
+            }
+            ap = __shfl_sync(FULL, ap, src);
+            ++lvl;
+            ls[lvl] = b_next;
+            const uint32_t need = 8 * (ap - act_cur);
+            if (lvl + 1 >= L || need == 0) {
+                done = true;
+                end_ops = b_next;
+                break;
+            }
+            act_cur = ap;
+            b_next += need;
+        }
+        // checkpoints before every S-th op of the tree
+        {
+            uint32_t st = entry, j = my_op, ipr = my_ip, last = 0;
+            for (uint32_t i = i0; i < i1; ++i) {
+                const uint32_t v = (word >> (4 * (i - base))) & 15u;
+                if (st == 0) {
+                    if (j % S == 0 && j < end_ops) {
+                        const uint32_t c = j / S;
+                        if (c < br.ck_cap) ck[br.ck_off + c] = Checkpoint{0u, 0u, i, ipr};
+                        last = c + 1;
+                    }
+                    ipr += (v >> 1) == OP_PA;
+                    ++j;
+                }
+                st = step(st, i - base);
+            }
+#pragma unroll
+            for (int d = 16; d >= 1; d >>= 1) last = max(last, __shfl_xor_sync(FULL, last, d));
+            n_ck = max(n_ck, last);
+        }
+        op_base += tot_np;
+        ip_base += (ptot >> 10) & 1023u;
+        act_base += ptot >> 20;
+        st_in = exit_all;
+    }
+    uint32_t flags = 0, ops;
+    if (done) {
+        ops = end_ops;
+    } else {
+        // every symbol read: the level ending at the last op may still close the tree, unless that op is
+        // a Pd op without its delta nibble (the walk counts it, and stops there truncated)
+        ops = op_base;
+        if (b_next == op_base && st_in == 0) {
+            ++lvl;
+            ls[lvl] = b_next;
+            const uint32_t need = 8 * (act_base - act_cur);
+            if (!(lvl + 1 >= L || need == 0)) flags = BF_TRUNCATED;
         } else {
-            if (model == 0)
-                index_chain(br, enc, lut0, ck, L, S, x, pos, ls, ops, n_ck, flags);
-            else
-                index_chain(br, enc, g_lut + (size_t)model * kTot, ck, L, S, x, pos, ls, ops, n_ck, flags);
-            if (n_ck > br.ck_cap) flags |= BF_TRUNCATED;
+            flags = BF_TRUNCATED;  // the stream ends inside the level structure
         }
     }
-    BrickDesc& o = bricks[bi];
-    o.n_ops = ops;
-    o.flags = (br.flags & ~BF_STATUS_MASK) | flags;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) o.level_start[k] = ls[k];
+    if (lane == 0) {
+        BrickDesc& o = bricks[bi];
+        o.n_ops = ops;
+        if (n_ck > br.ck_cap) flags |= BF_TRUNCATED;
+        o.flags = (br.flags & ~BF_STATUS_MASK) | flags;
+        for (uint32_t k = 0; k < 8; ++k) o.level_start[k] = k <= lvl ? ls[k] : ops;
+        n_ck_out[bi] = min(n_ck, br.ck_cap);
+    }
+}
+
+__global__ void __launch_bounds__(128) index_states_kernel(const BrickDesc* __restrict__ bricks, uint32_t nb,
+                                                          const uint8_t* __restrict__ enc_pool,
+                                                          const uint32_t* __restrict__ g_lut, uint32_t n_models,
+                                                          const uint64_t* __restrict__ snap_off,
+                                                          const uint2* __restrict__ snap,
+                                                          const uint32_t* __restrict__ n_ck, Checkpoint* __restrict__ ck) {
+    __shared__ uint32_t lut0[kTot];
+    for (uint32_t i = threadIdx.x; i < kTot; i += blockDim.x) lut0[i] = g_lut[i];
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t bi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (bi >= nb) return;
+    const uint32_t n = n_ck[bi];
+    if (n == 0) return;
+    const BrickDesc br = bricks[bi];
+    const uint32_t model = min((br.flags >> BF_MODEL_SHIFT) & 255u, n_models - 1);
+    const uint8_t* enc = enc_pool + br.enc_off;
+    const uint2* sn = snap + snap_off[bi];
+    auto run = [&](const uint32_t* lut) {
+        for (uint32_t c = lane; c < n; c += 32) {
+            Checkpoint& k = ck[br.ck_off + c];
+            const uint32_t s = k.sym, j = s / kSnap;
+            const uint2 z = sn[j];
+            uint32_t x = z.x, pos = z.y;
+            for (uint32_t t = j * kSnap; t < s; ++t) index_step(x, pos, enc, lut);
+            k.state = x;
+            k.pos = pos;
+        }
+    };
+    if (model == 0) run(lut0);
+    else run(g_lut + (size_t)model * kTot);
 }
 
 cudaError_t launch_build_index(DeviceDataset& ds, cudaStream_t st) {
     if (ds.nb == 0) return cudaSuccess;
-    // bricks per warp: the fewest (a power of two) that keeps about 32 warps per SM
-    // or fewer (measured: one brick per warp pays for a few thousand 64^3 bricks,
-    // a few per warp for tens of thousands of 32^3 ones)
-    int sms = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ds.device);
-    const uint64_t warps_max = 32ull * (uint64_t)std::max(sms, 1);
-    uint32_t lanes = 1;
-    while (lanes < 32 && (ds.nb + lanes - 1) / lanes > warps_max) lanes <<= 1;
-    const uint32_t per_block = 4 * lanes;  // four warps per block share the LUT copy
-    const uint32_t blocks = (ds.nb + per_block - 1) / per_block;
-    build_index_kernel<<<blocks, 128, 0, st>>>(ds.d_bricks, ds.nb, ds.d_enc, ds.d_lut, ds.d_ck, ds.L, ds.S,
-                                              ds.n_models ? ds.n_models : 1u, lanes);
-    return cudaGetLastError();
+    const uint32_t nb = ds.nb;
+    // per brick: its nibble words and its snapshots
+    std::vector<uint64_t> off(2 * (size_t)nb);
+    uint64_t words = 0, snaps = 0;
+    for (uint32_t i = 0; i < nb; ++i) {
+        const uint64_t ns = ds.h_cost ? ds.h_cost[i] : ds.max_nsym;
+        off[i] = words;
+        off[nb + i] = snaps;
+        words += ns / 8 + 1;
+        snaps += ns / kSnap + 1;
+    }
+    uint32_t* d_nib = nullptr;
+    uint2* d_snap = nullptr;
+    uint64_t* d_off = nullptr;
+    uint8_t* d_chain = nullptr;
+    uint32_t* d_nck = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&d_nib, words * 4, st);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_snap, snaps * 8, st);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_off, off.size() * 8, st);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_chain, nb, st);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_nck, (size_t)nb * 4, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_off, off.data(), off.size() * 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // the host offsets are released on return
+    if (e == cudaSuccess) {
+        // pass 1: bricks per warp, the fewest (a power of two) that keeps about 32 warps per SM
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ds.device);
+        const uint64_t warps_max = 32ull * (uint64_t)std::max(sms, 1);
+        uint32_t lanes = 1;
+        while (lanes < 32 && (nb + lanes - 1) / lanes > warps_max) lanes <<= 1;
+        const uint32_t per_block = 4 * lanes;
+        const uint32_t nm = ds.n_models ? ds.n_models : 1u;
+        index_symbols_kernel<<<(nb + per_block - 1) / per_block, 128, 0, st>>>(
+            ds.d_bricks, nb, ds.d_enc, ds.d_lut, nm, lanes, d_off, d_off + nb, d_nib, d_snap, d_chain, ds.L);
+        index_book_kernel<<<(nb + 3) / 4, 128, 0, st>>>(ds.d_bricks, nb, d_nib, d_off, d_chain, ds.d_ck, d_nck, ds.L,
+                                                       ds.S);
+        index_states_kernel<<<(nb + 3) / 4, 128, 0, st>>>(ds.d_bricks, nb, ds.d_enc, ds.d_lut, nm, d_off + nb, d_snap,
+                                                         d_nck, ds.d_ck);
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(d_nib, st);
+    cudaFreeAsync(d_snap, st);
+    cudaFreeAsync(d_off, st);
+    cudaFreeAsync(d_chain, st);
+    cudaFreeAsync(d_nck, st);
+    return e;
 }
 
 // ------------------------------------------------------------ decode kernel
