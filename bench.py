@@ -472,14 +472,17 @@ def dense_leg(codec, dev, args):
     return res
 
 
-def selector1024(codec, dev, args):
-    """Learned mode / table selector: trained on ~20,000 64^3 bricks of seeded neurite-like volumes (512^3,
-    the neurite512 generator), evaluated on a held-out 1024^3 volume of the same kind against the exhaustive
-    search (every mode's statistics) and the plain encoder."""
+def selector_leg(codec, dev, args, train_vol, held_vol, train_desc, held_desc):
+    """Learned mode / table selector: trained on the 64^3 bricks of SELECTOR["train_volumes"] seeded volumes
+    (train_vol(k) fills and returns the k-th), evaluated on a held-out volume (held_vol()) against the
+    exhaustive search (every mode's statistics) and the plain encoder.  The trained tables and network go
+    through a selector file (csv_selector_write / csv_selector_read) and the learned encode runs as the one
+    call csv_encode_learned; its features / network / encode split is timed apart."""
+    import tempfile
+
     import torch
     from csvb200 import SelectorNet
     from csvb200.selector import exhaustive_choice, features, fit_tables, learned_choice, train
-    N = NEURITE
     st = torch.cuda.current_stream()
 
     def ev():
@@ -489,15 +492,13 @@ def selector1024(codec, dev, args):
 
     t0 = time.perf_counter()
     feats, hists = [], []
-    vol = torch.empty(N["shape"], dtype=torch.int64, device=dev)
     for k in range(SELECTOR["train_volumes"]):
-        codec.synth_volume(vol, N["kind"], N["n_cells"], N["n_tubes"], N["r_min"], N["r_max"], N["zero_frac"],
-                           SELECTOR["seed"] + k)
+        vol = train_vol(k)
         feats.append(features(codec, vol, 64))
         h = torch.empty((feats[-1].shape[0], 12, 16), dtype=torch.int32, device=dev)
         codec.encode_stats(vol, 64, h)
         hists.append(h)
-    del vol
+        del vol
     tables = fit_tables(torch.cat(hists).cpu().numpy().astype(np.uint64), 16, iters=8)
     labels = []
     for h in hists:
@@ -506,16 +507,21 @@ def selector1024(codec, dev, args):
         labels.append(sel)
     data_s = time.perf_counter() - t0
     e0 = ev()
-    net, losses = train(codec, torch.cat(feats), torch.cat(labels), steps=SELECTOR["steps"], batch=2048)
+    net0, losses = train(codec, torch.cat(feats), torch.cat(labels), steps=SELECTOR["steps"], batch=2048)
     e1 = ev()
     torch.cuda.synchronize()
     train_ms = e0.elapsed_time(e1)
-    # held-out 1024^3
-    held = torch.empty((1024, 1024, 1024), dtype=torch.int64, device=dev)
-    codec.synth_volume(held, N["kind"], N["n_cells"] * 8, N["n_tubes"] * 8, N["r_min"], N["r_max"], N["zero_frac"],
-                       SELECTOR["seed"] + 1000)
+    # the trained selector through a file: what a learned encode outside this process loads
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "selector.csvs")
+        net0.save(path, tables)
+        file_bytes = os.path.getsize(path)
+        net, tables_f = SelectorNet.load(codec, path)
+    net0.close()
+    assert np.array_equal(tables_f, tables)
+    held = held_vol()
     nvox = held.numel()
-    res = {}
+    res, split = {}, {}
     for rep in range(2):  # warm, then timed
         a = ev()
         codec.encode_device_sel(held, 64)
@@ -527,12 +533,21 @@ def selector1024(codec, dev, args):
         d = ev()
         exh = codec.encoded_image()[1]
         e = ev()
-        sel_l = learned_choice(net, features(codec, held, 64))
-        codec.encode_device_sel(held, 64, tables, sel_l)
+        codec.encode_learned(held, 64, net, tables)  # csv_encode_learned: the one call
         f = ev()
         learned = codec.encoded_image()[1]
+        # the same three steps apart: features, the network's choice, the version-2 encode
+        g = ev()
+        fe = features(codec, held, 64)
+        h_ = ev()
+        sel_l = learned_choice(net, fe)
+        i_ = ev()
+        codec.encode_device_sel(held, 64, tables, sel_l)
+        j_ = ev()
         torch.cuda.synchronize()
         res = {"plain_ms": a.elapsed_time(b), "exhaustive_ms": c.elapsed_time(d), "learned_ms": e.elapsed_time(f)}
+        split = {"features_ms": round(g.elapsed_time(h_), 3), "network_ms": round(h_.elapsed_time(i_), 3),
+                 "encode_v2_ms": round(i_.elapsed_time(j_), 3)}
     agree = float((sel_x == sel_l).float().mean())
     # the network alone on the tensor cores: one forward pass over 1 Mi feature rows
     rows = 1 << 20
@@ -550,17 +565,19 @@ def selector1024(codec, dev, args):
         os.path.join(ROOT, "MEASURED_PEAKS.json")) else 1590.0
     out = {
         "train": {"volumes": SELECTOR["train_volumes"], "bricks": int(sum(f.shape[0] for f in feats)),
-                  "volume": list(N["shape"][::-1]), "generator": "neurite512 (400 tubes r 2-12, 3000 cells, 15 % 0)",
-                  "tables": 16, "modes": 12, "steps": SELECTOR["steps"], "batch": 2048, "train_ms": round(train_ms, 1),
-                  "loss_first": round(losses[0], 4), "loss_last": round(float(np.mean(losses[-20:])), 4),
-                  "data_s": round(data_s, 2)},
-        "held_out": {"volume": [1024, 1024, 1024], "bricks": int(sel_x.numel()), "seed": SELECTOR["seed"] + 1000,
-                     "generator": "neurite512 scaled x8 (3200 tubes, 24000 cells)"},
+                  "generator": train_desc, "tables": 16, "modes": 12, "steps": SELECTOR["steps"], "batch": 2048,
+                  "train_ms": round(train_ms, 1), "loss_first": round(losses[0], 4),
+                  "loss_last": round(float(np.mean(losses[-20:])), 4), "data_s": round(data_s, 2),
+                  "selector_file_bytes": file_bytes},
+        "held_out": {"volume": list(held.shape[::-1]), "bricks": int(sel_x.numel()), "generator": held_desc},
         "bytes": {"plain": int(plain), "exhaustive": int(exh), "learned": int(learned)},
         "size_loss_vs_exhaustive": round(learned / exh - 1.0, 5),
         "size_vs_plain": round(learned / plain - 1.0, 5),
+        "exhaustive_vs_plain": round(exh / plain - 1.0, 5),
         "choice_agreement": round(agree, 4),
         "encode_ms": {k: round(v, 2) for k, v in res.items()},
+        "learned_split": split,
+        "learned_vs_plain_time": round(res["learned_ms"] / res["plain_ms"], 3),
         "encode_mvox_s": {k[:-3]: round(nvox / (v * 1e-3) / 1e6, 1) for k, v in res.items()},
         "speedup_vs_exhaustive": round(res["exhaustive_ms"] / res["learned_ms"], 2),
         "mlp_forward": {"rows": rows, "ms": round(fwd_ms, 3), "tflops": round(flops / (fwd_ms * 1e-3) / 1e12, 1),
@@ -570,6 +587,45 @@ def selector1024(codec, dev, args):
     net.close()
     del held
     torch.cuda.empty_cache()
+    return out
+
+
+def selector1024(codec, dev, args):
+    """The selector on two generators: the neurite-like volumes (trained on 40 x 512^3, held out 1024^3) and the
+    uneven batch's dense half (64^3 tube bricks: trained on the x >= 256 halves of 40 mixed512 volumes, held out
+    the x >= 512 half of the mixed1024 volume the decode headline uses)."""
+    import torch
+    N, M, M5 = NEURITE, MIXED, MIXED512
+
+    def neur_train(k):
+        v = torch.empty(N["shape"], dtype=torch.int64, device=dev)
+        codec.synth_volume(v, N["kind"], N["n_cells"], N["n_tubes"], N["r_min"], N["r_max"], N["zero_frac"],
+                           SELECTOR["seed"] + k)
+        return v
+
+    def neur_held():
+        v = torch.empty((1024, 1024, 1024), dtype=torch.int64, device=dev)
+        codec.synth_volume(v, N["kind"], N["n_cells"] * 8, N["n_tubes"] * 8, N["r_min"], N["r_max"], N["zero_frac"],
+                           SELECTOR["seed"] + 1000)
+        return v
+
+    def mixed_train(k):
+        v = torch.empty(M5["shape"], dtype=torch.int64, device=dev)
+        codec.synth_volume(v, M5["kind"], M5["n_cells"], M5["n_tubes"], M5["r_min"], M5["r_max"], M5["zero_frac"],
+                           SELECTOR["seed"] + 2000 + k)
+        return v[:, :, M5["split_x"]:].contiguous()
+
+    def mixed_held():
+        v = torch.empty(M["shape"], dtype=torch.int64, device=dev)
+        codec.synth_volume(v, M["kind"], M["n_cells"], M["n_tubes"], M["r_min"], M["r_max"], M["zero_frac"], M["seed"])
+        return v[:, :, M["split_x"]:].contiguous()
+
+    out = selector_leg(codec, dev, args, neur_train, neur_held,
+                       "neurite512 (400 tubes r 2-12, 3000 cells, 15 % 0), 40 seeds",
+                       "neurite512 scaled x8 (3200 tubes, 24000 cells), 1024^3")
+    out["mixed1024_tubes"] = selector_leg(codec, dev, args, mixed_train, mixed_held,
+                                          "mixed512 x >= 256 halves (625 tubes r 1-4 over 250 cells), 40 seeds",
+                                          "mixed1024 x >= 512 half (the decode headline's 64^3 image)")
     return out
 
 

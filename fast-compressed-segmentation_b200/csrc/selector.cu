@@ -170,11 +170,12 @@ __global__ void __launch_bounds__(kFThreads) features_kernel(const uint64_t* __r
         S.sorted[k] = v;
     }
     __syncthreads();
-    // full-resolution counts.  Warp w takes the rows y = w, w + 8, ... and walks
-    // z with rows z .. z+4 of its y in registers (the z-neighbours), loads rows
-    // (y+1, z) and (y+4, z) for the y-neighbours, and takes the x-neighbours and
-    // the run starts from other lanes (lane l holds x = l and x = l + 32): every
-    // voxel is read three times from the cache instead of eight.
+    // Counts over the rows of even y and even z (all x: a quarter of the voxels,
+    // every pair within such a row, and each such voxel's +1 / +4 neighbours in y
+    // and z).  Warp w takes the rows y = 2w, 2w + 16, ... and walks z in steps of
+    // two with planes z .. z+4 of its row in registers (the z-neighbours), loads
+    // rows (y+1, z) and (y+4, z) for the y-neighbours, and takes the x-neighbours
+    // and the run starts from other lanes (lane l holds x = l and x = l + 32).
     uint32_t c[15] = {};
     {
         const uint32_t nch = (b + 31) / 32;  // values per lane: 1 or 2
@@ -195,14 +196,14 @@ __global__ void __launch_bounds__(kFThreads) features_kernel(const uint64_t* __r
                 }
             }
         };
-        for (uint32_t y = warp; y < b; y += kFThreads / 32) {
+        for (uint32_t y = 2 * warp; y < b; y += 2 * (kFThreads / 32)) {
             uint64_t r[5][2];
 #pragma unroll
             for (uint32_t k = 0; k < 5; ++k) {
                 r[k][0] = r[k][1] = 0ull;
                 if (k < b) row(y, k, r[k]);
             }
-            for (uint32_t z = 0; z < b; ++z) {
+            for (uint32_t z = 0; z < b; z += 2) {
                 uint64_t ya[2] = {0ull, 0ull}, yd[2] = {0ull, 0ull};
                 if (y + 1 < b) row(y + 1, z, ya);
                 if (y + 4 < b) row(y + 4, z, yd);
@@ -253,12 +254,13 @@ __global__ void __launch_bounds__(kFThreads) features_kernel(const uint64_t* __r
                     }
                 }
 #pragma unroll
-                for (uint32_t k = 0; k < 4; ++k) {
-                    r[k][0] = r[k + 1][0];
-                    r[k][1] = r[k + 1][1];
+                for (uint32_t k = 0; k < 3; ++k) {  // planes z+2 .. z+6 for the next step
+                    r[k][0] = r[k + 2][0];
+                    r[k][1] = r[k + 2][1];
                 }
-                r[4][0] = r[4][1] = 0ull;
-                if (z + 5 < b) row(y, z + 5, r[4]);
+                r[3][0] = r[3][1] = r[4][0] = r[4][1] = 0ull;
+                if (z + 5 < b) row(y, z + 5, r[3]);
+                if (z + 6 < b) row(y, z + 6, r[4]);
             }
         }
     }
@@ -312,12 +314,18 @@ __global__ void __launch_bounds__(kFThreads) features_kernel(const uint64_t* __r
         uint32_t distinct = 1;
         for (uint32_t k = 1; k < 512; ++k) distinct += S.sorted[k] != S.sorted[k - 1];
         float* f = feat + (size_t)i * kFeat;
-        const float b3 = (float)b * (float)b * (float)b, pair1 = (float)b * (float)b * (float)(b - 1),
-                    pair4 = (float)b * (float)b * (float)(b > 4 ? b - 4 : 1);
+        // pairs tested: x within the sampled rows; y and z from the sampled rows outward
+        const float hb = (float)(b / 2), fb = (float)b;
+        const float px1 = hb * hb * (fb - 1.0f), px4 = hb * hb * (fb - 4.0f);
+        const float pyz1 = hb * hb * fb, pyz4 = (float)((b - 4) / 2) * hb * fb;
         f[0] = (float)bitlen(distinct) / 10.0f;
-        for (int k = 0; k < 3; ++k) f[1 + k] = (float)S.cnt[k] / pair1;
-        for (int k = 0; k < 3; ++k) f[4 + k] = (float)S.cnt[3 + k] / pair4;
-        f[7] = (float)S.cnt[6] / b3;
+        f[1] = (float)S.cnt[0] / px1;
+        f[2] = (float)S.cnt[1] / pyz1;
+        f[3] = (float)S.cnt[2] / pyz1;
+        f[4] = (float)S.cnt[3] / px4;
+        f[5] = (float)S.cnt[4] / pyz4;
+        f[6] = (float)S.cnt[5] / pyz4;
+        f[7] = (float)S.cnt[6] / (hb * hb * fb);
         const float runs = (float)max(S.cnt[14], 1u);
         for (int k = 0; k < 7; ++k) f[8 + k] = (float)S.cnt[7 + k] / runs;
         f[15] = (float)bitlen(S.cnt[14]) / 20.0f;

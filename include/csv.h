@@ -462,9 +462,10 @@ int csv_encode_device_sel(csv_ctx* ctx, const uint64_t* d_volume, uint32_t W, ui
                           uint32_t brick_size, const uint32_t* tables, uint32_t n_tables, const uint8_t* d_sel,
                           void* stream, size_t* image_len);
 /* 32 cheap statistics per brick (d_features: numBricks x 32 fp32): distinct
- * labels of an 8^3 sample, label equality of neighbours at distance 1 and 4
- * per axis, the fraction of label 0, the histogram of run lengths along x, the
- * run count, and the op-nibble histogram of the 8^3 sample encoded as a brick. */
+ * labels of an 8^3 sample; over the rows of even y and even z (all x), label
+ * equality of neighbours at distance 1 and 4 per axis, the fraction of label
+ * 0, the histogram of run lengths along x and the run count; and the
+ * op-nibble histogram of the 8^3 sample encoded as a brick. */
 int csv_brick_features(csv_ctx* ctx, const uint64_t* d_volume, uint32_t W, uint32_t H, uint32_t D,
                        uint32_t brick_size, float* d_features, void* stream);
 

@@ -208,8 +208,9 @@ int or_brick_features(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_
                     sorted[k] = v;
                 }
                 uint32_t c[15] = {0};
-                for (uint32_t z = 0; z < b; ++z)
-                    for (uint32_t y = 0; y < b; ++y) {
+                /* rows of even y and even z, all x */
+                for (uint32_t z = 0; z < b; z += 2)
+                    for (uint32_t y = 0; y < b; y += 2) {
                         uint32_t run = 0;
                         for (uint32_t x = 0; x < b; ++x) {
                             const size_t gx = x0 + x, gy = y0 + y, gz = z0 + z;
@@ -243,12 +244,17 @@ int or_brick_features(const uint64_t* vol, size_t W, size_t H, size_t D, uint32_
                 uint32_t nib[16] = {0};
                 mini_ops(samp, nib);
                 float* f = feat + i * NF;
-                const float b3 = (float)b * (float)b * (float)b, pair1 = (float)b * (float)b * (float)(b - 1),
-                            pair4 = (float)b * (float)b * (float)(b > 4 ? b - 4 : 1);
+                const float hb = (float)(b / 2), fb = (float)b;
+                const float px1 = hb * hb * (fb - 1.0f), px4 = hb * hb * (fb - 4.0f);
+                const float pyz1 = hb * hb * fb, pyz4 = (float)((b - 4) / 2) * hb * fb;
                 f[0] = (float)bitlen(distinct) / 10.0f;
-                for (int k = 0; k < 3; ++k) f[1 + k] = (float)c[k] / pair1;
-                for (int k = 0; k < 3; ++k) f[4 + k] = (float)c[3 + k] / pair4;
-                f[7] = (float)c[6] / b3;
+                f[1] = (float)c[0] / px1;
+                f[2] = (float)c[1] / pyz1;
+                f[3] = (float)c[2] / pyz1;
+                f[4] = (float)c[3] / px4;
+                f[5] = (float)c[4] / pyz4;
+                f[6] = (float)c[5] / pyz4;
+                f[7] = (float)c[6] / (hb * hb * fb);
                 const float runs = (float)(c[14] ? c[14] : 1u);
                 for (int k = 0; k < 7; ++k) f[8 + k] = (float)c[7 + k] / runs;
                 f[15] = (float)bitlen(c[14]) / 20.0f;
