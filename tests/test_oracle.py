@@ -247,3 +247,94 @@ def test_cpu_generator_is_deterministic(oracle, kind):
     assert len(np.unique(a)) > 10
     if kind == 0:
         assert 0.05 < float((a == 0).mean()) < 0.15
+
+
+def _full_res_cache(oracle, vol, b):
+    """Slots and labels of a volume decoded at full resolution, every brick resident (Morton-indexed slots)."""
+    from csvb200.camera import SLOT_DTYPE
+    D, H, W = vol.shape
+    nbx, nby, nbz = W // b, H // b, D // b
+    img = oracle.encode(vol, b)
+    dec, st = oracle.decode_image(img, b.bit_length() - 1)
+    n = b ** 3
+    ids = [oracle.morton3(bx, by, bz) for bx in range(nbx) for by in range(nby) for bz in range(nbz)]
+    n_slots = 1 << (3 * max(nbx, nby, nbz).bit_length())
+    slots = np.zeros(n_slots, SLOT_DTYPE)
+    slots["flags"] = 1
+    lab = np.zeros(n_slots * n, np.uint64)
+    for i, m in enumerate(ids):
+        lab[m * n:(m + 1) * n] = dec[i]
+        slots[m] = (m * n, b.bit_length() - 1, 0)
+    return slots, lab
+
+
+def _one_ray(oracle, vol, b, pos, direction, hidden=None):
+    """The label and depth of the single pixel of a 1x1 image (its ray is the camera's forward axis)."""
+    import math
+    from csvb200.camera import camera_uniform
+    slots, lab = _full_res_cache(oracle, vol, b)
+    bpa = vol.shape[0] // b
+    l, dep, _ = oracle.render(camera_uniform(pos, direction, math.pi / 3), 1, 1, float(bpa * b), b, bpa, slots, lab,
+                              hidden=hidden)
+    return int(l[0, 0]), float(dep[0, 0])
+
+
+def test_scalar_dda_known_answers(oracle):
+    """Rays whose first hit and entry distance follow by hand (rayTrace.wgsl:473-563, 647-892 restated): the
+    first non-zero, not hidden voxel along the ray, and the ray parameter t where the ray enters that cell
+    (the forward axis is a unit vector, so t is a distance in voxels).  The rays are tilted by 1e-3 off the
+    axes: the shader sets a zero direction component's inverse to sign(0) / 1e-6 = 0 (rayTrace.wgsl:613-617),
+    so a ray parallel to an axis plane never enters the volume -- also a known answer (case 0)."""
+    import math
+    e = 1e-3
+    vol = np.zeros((64, 64, 64), np.uint64)  # vol[z, y, x]
+    vol[30:, :, :] = 5
+    # 0. exactly along +z into a wall that fills the far half: no hit, infinite depth
+    lab, t = _one_ray(oracle, vol, 16, (8.5, 8.5, -10.0), (0.0, 0.0, 1.0))
+    assert lab == 0 and math.isinf(t)
+    # ... and the same ray tilted enters the wall at z = 30: t = 40 (x and y drift by 0.04)
+    lab, t = _one_ray(oracle, vol, 16, (8.5, 8.5, -10.0), (e, e, 1.0))
+    assert lab == 5 and t == pytest.approx(40.0, abs=1e-3)
+    # 1. along +z from (8.5, 8.5, -10): the voxel x = 8, y = 8, z = 20 is first; its z = 20 face is 30 away
+    vol = np.zeros((64, 64, 64), np.uint64)
+    vol[20, 8, 8] = 7
+    assert _one_ray(oracle, vol, 16, (8.5, 8.5, -10.0), (e, e, 1.0)) == (7, pytest.approx(30.0, abs=1e-3))
+    # 2. the same label hidden: the ray goes on to the voxel at z = 40 (t = 50)
+    vol[40, 8, 8] = 9
+    lab, t = _one_ray(oracle, vol, 16, (8.5, 8.5, -10.0), (e, e, 1.0), hidden=np.array([7], np.uint64))
+    assert lab == 9 and t == pytest.approx(50.0, abs=1e-3)
+    # 3. along +x from (-5, 8.5, 8.5): the voxel x = 30, y = 8, z = 8 is 35 away
+    vol2 = np.zeros((64, 64, 64), np.uint64)
+    vol2[8, 8, 30] = 3
+    assert _one_ray(oracle, vol2, 16, (-5.0, 8.5, 8.5), (1.0, e, e)) == (3, pytest.approx(35.0, abs=1e-3))
+    # 4. at 45 degrees in the x-z plane from (2.5, 8.5, -10) into a slab z >= 32 of label 5: the ray meets
+    #    z = 32 after 42 units of z, i.e. t = 42 * sqrt(2) = 59.397, at x = 2.5 + 42 = 44.5 (voxel x = 44)
+    vol3 = np.zeros((64, 64, 64), np.uint64)
+    vol3[32:, :, :] = 5
+    lab, t = _one_ray(oracle, vol3, 16, (2.5, 8.5, -10.0), (1.0, e, 1.0))
+    assert lab == 5 and t == pytest.approx(42.0 * math.sqrt(2.0), abs=2e-3)
+    # 5. looking away from the volume: nothing is hit, depth is infinite
+    lab, t = _one_ray(oracle, vol3, 16, (2.5, 8.5, -10.0), (e, e, -1.0))
+    assert lab == 0 and math.isinf(t)
+
+
+def test_brick_lod_known_answers(oracle):
+    """calculateBrickLOD (camera.js:103-137) worked out by hand for a 1920x1080 viewport at fov 60 degrees:
+    the screen size is min(W, H) = 1080, so focal = 540 / tan(30 deg) = 935.307; a 64^3 brick at LOD k has
+    voxels of 64 / 2^k, and the LOD is the finest k <= 6 with 935.307 * 64 / 2^k / max(d, 0.1) >= 1, i.e.
+    d <= 59859.7 / 2^k: thresholds 935.3 (k 6), 1870.6 (5), 3741.2 (4), 7482.5 (3), 14964.9 (2), 29929.8 (1);
+    beyond the last, LOD 0.  A 32^3 brick at its finest LOD (5) also has unit voxels, so its thresholds
+    are the same numbers one LOD lower: 935.3 (k 5), 1870.6 (4), ..., 14964.9 (1)."""
+    import math
+    from csvb200.camera import focal_length
+    f = focal_length(1080, math.pi / 3)
+    assert f == pytest.approx(935.307, abs=1e-3)
+    cases64 = [(0.05, 6), (935.0, 6), (936.0, 5), (1870.0, 5), (1871.0, 4), (3741.0, 4), (3742.0, 3), (7482.0, 3),
+               (7483.0, 2), (14964.0, 2), (14966.0, 1), (29929.0, 1), (29931.0, 0), (1e5, 0)]
+    for d, expect in cases64:
+        assert oracle.brick_lod((0.0, d, 0.0), 64.0, (0.0, 0.0, 0.0), f, 6) == expect, (d, expect)
+    cases32 = [(935.0, 5), (936.0, 4), (1870.0, 4), (1871.0, 3), (14964.0, 1), (14966.0, 0)]
+    for d, expect in cases32:
+        # the distance is measured between the brick centre and the camera, in any direction
+        assert oracle.brick_lod((d / math.sqrt(3), d / math.sqrt(3), d / math.sqrt(3)), 32.0, (0.0, 0.0, 0.0),
+                                f, 5) == expect, (d, expect)
