@@ -344,17 +344,35 @@ def run_b200(args):
 
     # ---- cold open: csv_open of each image from host bytes (H2D of the image + the seek-index pass, which a
     # file the reference encoder wrote needs; an image from the GPU encoder carries its index)
-    cold_open = {}
+    # index_ms: the device time of the seek-index passes inside that open (CUDA events around them); the
+    # sidecar figures open the same bytes with the image's index sidecar (csv_open_indexed)
+    cold_open = {"index_ms": {}, "sidecar_ms": {}, "sidecar_index_ms": {}, "sidecar_bytes": {}}
     for name_, im_ in (("32^3", img_left), ("64^3", img_right)):
-        ts_ = []
+        ts_, ix_ = [], []
         for _ in range(3):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             d_ = codec.open(im_)
             torch.cuda.synchronize()
             ts_.append((time.perf_counter() - t0) * 1e3)
+            ix_.append(d_.index_ms)
+            if _ == 0:
+                sc_ = d_.index_sidecar()
             d_.close()
         cold_open[name_] = round(min(ts_), 2)
+        cold_open["index_ms"][name_] = round(min(ix_), 3)
+        ts_, ix_ = [], []
+        for _ in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            d_ = codec.open(im_, sidecar=sc_)
+            torch.cuda.synchronize()
+            ts_.append((time.perf_counter() - t0) * 1e3)
+            ix_.append(d_.index_ms)
+            d_.close()
+        cold_open["sidecar_ms"][name_] = round(min(ts_), 2)
+        cold_open["sidecar_index_ms"][name_] = round(min(ix_), 3)
+        cold_open["sidecar_bytes"][name_] = len(sc_)
 
     # ---- neurite512: encode vs the reference encoder on this host, and its decode
     neur = neurite512(codec, dev, args, rank == 0 and world == 1 and not args.no_cpu)

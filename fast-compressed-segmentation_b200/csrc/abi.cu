@@ -263,6 +263,7 @@ int stage_dataset(csv_ctx* ctx, const uint8_t* img, const ImageView& v, DeviceDa
     }
     std::vector<uint32_t> lut((size_t)kTot * v.n_tables);
     for (uint32_t t = 0; t < v.n_tables; ++t) build_lut(v.freq[t], v.cum[t], &lut[(size_t)t * kTot]);
+    d.fast_models = lut_fast_mask(lut.data(), v.n_tables);
     cudaError_t e;
     if ((e = cudaMalloc(&d.d_bricks, sizeof(BrickDesc) * std::max<uint32_t>(1, v.nb))) != cudaSuccess ||
         (e = cudaMalloc(&d.d_pal, 8 * pal.size())) != cudaSuccess ||
@@ -279,6 +280,91 @@ int stage_dataset(csv_ctx* ctx, const uint8_t* img, const ImageView& v, DeviceDa
         return cuda_fail(ctx, e, "staging copy");
     // the host vectors go out of scope: finish the copies first
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "staging copy");
+    return CSV_OK;
+}
+
+// Seek-index sidecar (little endian): u32 magic "CSVX", u32 version 1, u32 bricks,
+// u32 symbols between states (kSeedSymbols), u64 states in all; per brick u32 E,
+// u32 nSymbols, u32 states (0, or one per kSeedSymbols symbols begun); then the
+// states {u32 x, u32 pos}, brick after brick.
+constexpr uint32_t kSidecarMagic = 0x58565343u;  // "CSVX"
+constexpr size_t kSidecarHead = 24;
+
+// The pieces of pass 1 a sidecar gives for image v, or an error naming the mismatch.
+int sidecar_pieces(csv_ctx* ctx, const ImageView& v, const uint8_t* sc, size_t len, IndexSeeds& out) {
+    if (!sc || len < kSidecarHead) return fail(ctx, CSV_EFORMAT, "index sidecar shorter than its header");
+    uint64_t total;
+    memcpy(&total, sc + 16, 8);
+    if (rd32(sc) != kSidecarMagic || rd32(sc + 4) != 1)
+        return fail(ctx, CSV_EFORMAT, "not a version-1 index sidecar");
+    if (rd32(sc + 8) != v.nb || rd32(sc + 12) != kSeedSymbols)
+        return fail(ctx, CSV_EFORMAT, "index sidecar does not match the image: brick count or state spacing");
+    if (total > 0xFFFFFFFFull || len != kSidecarHead + 12ull * v.nb + 8 * total)
+        return fail(ctx, CSV_EFORMAT, "index sidecar length does not match its header");
+    out.piece_base.assign((size_t)v.nb + 1, 0);
+    out.seed.clear();
+    out.seed.reserve((size_t)total + v.nb);
+    const uint8_t* states = sc + kSidecarHead + 12ull * v.nb;
+    uint64_t used = 0;
+    for (uint32_t i = 0; i < v.nb; ++i) {
+        const uint8_t* r = sc + kSidecarHead + 12ull * i;
+        const uint32_t E = rd32(r), ns = rd32(r + 4), n = rd32(r + 8);
+        const uint32_t full = (ns + kSeedSymbols - 1) / kSeedSymbols;
+        if (E != v.recs[i].E || ns != v.recs[i].nsym || (n != 0 && n != full) || used + n > total)
+            return fail(ctx, CSV_EFORMAT, "index sidecar does not match the image at brick " + std::to_string(i));
+        if (n == 0) {
+            out.seed.push_back(make_uint2(0, 0xFFFFFFFFu));  // one piece, from the stream header
+        } else {
+            for (uint32_t k = 0; k < n; ++k)
+                out.seed.push_back(make_uint2(rd32(states + 8 * (used + k)), rd32(states + 8 * (used + k) + 4)));
+        }
+        used += n;
+        out.piece_base[i + 1] = (uint32_t)out.seed.size();
+    }
+    if (used != total) return fail(ctx, CSV_EFORMAT, "index sidecar holds states for no brick");
+    return CSV_OK;
+}
+
+// csv_open and csv_open_indexed: stage the image, then the seek index from the
+// stream headers or from a sidecar's states.
+int open_dataset(csv_ctx* ctx, const uint8_t* image, size_t len, const uint8_t* sidecar, size_t sidecar_len,
+                 csv_dataset** out) {
+    if (!ctx || !out) return CSV_EINVAL;
+    *out = nullptr;
+    DeviceGuard g(ctx->device);
+    ImageView v;
+    int rc = parse_image(ctx, image, len, v);
+    if (rc) return rc;
+    IndexSeeds seeds;
+    if (sidecar && (rc = sidecar_pieces(ctx, v, sidecar, sidecar_len, seeds))) return rc;
+    csv_dataset* ds = new (std::nothrow) csv_dataset();
+    if (!ds) return fail(ctx, CSV_ENOMEM, "host allocation");
+    ds->ctx = ctx;
+    cudaStream_t st = 0;
+    rc = stage_dataset(ctx, image, v, ds->d, st);
+    if (rc == CSV_OK) {
+        // the passes' device time, from events on the stream around them
+        cudaEvent_t ev[2] = {nullptr, nullptr};
+        const bool timed = cudaEventCreate(&ev[0]) == cudaSuccess && cudaEventCreate(&ev[1]) == cudaSuccess;
+        if (timed) cudaEventRecord(ev[0], st);
+        bool rejected = false;
+        cudaError_t e = launch_build_index(ds->d, st, sidecar ? &seeds : nullptr, &rejected);
+        if (timed) cudaEventRecord(ev[1], st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "seek index");
+        else if (rejected)
+            rc = fail(ctx, CSV_EFORMAT, "index sidecar does not match the image: a stored rANS state differs");
+        float ms = 0;
+        if (rc == CSV_OK && timed && cudaEventElapsedTime(&ms, ev[0], ev[1]) == cudaSuccess) ds->d.index_ms = ms;
+        for (cudaEvent_t x : ev)
+            if (x) cudaEventDestroy(x);
+    }
+    if (rc) {
+        free_dataset(ds->d);
+        delete ds;
+        return rc;
+    }
+    *out = ds;
     return CSV_OK;
 }
 
@@ -328,28 +414,50 @@ void csv_destroy(csv_ctx* ctx) {
 const char* csv_last_error(const csv_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
 int csv_open(csv_ctx* ctx, const uint8_t* image, size_t len, csv_dataset** out) {
-    if (!ctx || !out) return CSV_EINVAL;
+    return open_dataset(ctx, image, len, nullptr, 0, out);
+}
+
+int csv_open_indexed(csv_ctx* ctx, const uint8_t* image, size_t len, const uint8_t* sidecar, size_t sidecar_len,
+                     csv_dataset** out) {
+    if (!sidecar) return ctx ? fail(ctx, CSV_EINVAL, "null index sidecar") : CSV_EINVAL;
+    return open_dataset(ctx, image, len, sidecar, sidecar_len, out);
+}
+
+int csv_index_save(csv_ctx* ctx, const csv_dataset* ds, uint8_t** out, size_t* out_len) {
+    if (!ctx || !ds || !out || !out_len) return CSV_EINVAL;
     *out = nullptr;
+    *out_len = 0;
     DeviceGuard g(ctx->device);
-    ImageView v;
-    int rc = parse_image(ctx, image, len, v);
-    if (rc) return rc;
-    csv_dataset* ds = new (std::nothrow) csv_dataset();
-    if (!ds) return fail(ctx, CSV_ENOMEM, "host allocation");
-    ds->ctx = ctx;
-    cudaStream_t st = 0;
-    rc = stage_dataset(ctx, image, v, ds->d, st);
-    if (rc == CSV_OK) {
-        cudaError_t e = launch_build_index(ds->d, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "seek index");
+    std::vector<uint32_t> n_seeds;
+    std::vector<uint2> seeds;
+    cudaError_t e = index_seeds_of(ds->d, 0, n_seeds, seeds);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "index sidecar");
+    const uint32_t nb = ds->d.nb;
+    std::vector<BrickDesc> desc(nb);
+    if (nb && (e = cudaMemcpy(desc.data(), ds->d.d_bricks, sizeof(BrickDesc) * nb, cudaMemcpyDeviceToHost)) !=
+                  cudaSuccess)
+        return cuda_fail(ctx, e, "index sidecar");
+    const size_t len = kSidecarHead + 12ull * nb + 8ull * seeds.size();
+    uint8_t* buf = (uint8_t*)malloc(len);
+    if (!buf) return fail(ctx, CSV_ENOMEM, "host allocation");
+    auto wr32 = [&](size_t at, uint32_t x) { memcpy(buf + at, &x, 4); };
+    wr32(0, kSidecarMagic);
+    wr32(4, 1);
+    wr32(8, nb);
+    wr32(12, kSeedSymbols);
+    const uint64_t total = seeds.size();
+    memcpy(buf + 16, &total, 8);
+    for (uint32_t i = 0; i < nb; ++i) {
+        wr32(kSidecarHead + 12ull * i, desc[i].E);
+        wr32(kSidecarHead + 12ull * i + 4, desc[i].nsym);
+        wr32(kSidecarHead + 12ull * i + 8, n_seeds[i]);
     }
-    if (rc) {
-        free_dataset(ds->d);
-        delete ds;
-        return rc;
+    for (size_t k = 0; k < seeds.size(); ++k) {
+        wr32(kSidecarHead + 12ull * nb + 8 * k, seeds[k].x);
+        wr32(kSidecarHead + 12ull * nb + 8 * k + 4, seeds[k].y);
     }
-    *out = ds;
+    *out = buf;
+    *out_len = len;
     return CSV_OK;
 }
 
@@ -363,6 +471,12 @@ int csv_dataset_info_get(const csv_dataset* ds, csv_dataset_info* info) {
     info->palette_entries = ds->d.palette_entries;
     memcpy(info->freq, ds->d.freq, sizeof info->freq);
     memcpy(info->cum, ds->d.cum, sizeof info->cum);
+    return CSV_OK;
+}
+
+int csv_dataset_index_ms(const csv_dataset* ds, float* ms) {
+    if (!ds || !ms) return CSV_EINVAL;
+    *ms = ds->d.index_ms;
     return CSV_OK;
 }
 
@@ -677,6 +791,7 @@ int csv_dataset_concat(csv_ctx* ctx, const csv_dataset* const* parts, uint32_t n
         pal_base += p.pal_pool_entries;
         enc_base += (p.enc_pool_bytes + 15) & ~15ull;
         ck_base += p.ck_entries;
+        if (model_base < 32) d.fast_models |= p.fast_models << model_base;
         model_base += p.n_models;
         id_base += p.nb;
     }

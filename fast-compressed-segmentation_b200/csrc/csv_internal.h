@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/csv.h"
 
@@ -76,6 +77,8 @@ struct DeviceDataset {
     uint64_t stream_bytes = 0, palette_entries = 0, ck_entries = 0;
     uint32_t max_nsym = 0, max_P = 0;
     uint32_t n_models = 1;  // LUTs at d_lut (a version-2 image's tables; a concatenation keeps each part's)
+    uint32_t fast_models = 0;  // bit m: model m's table is well formed (the seek index's fast step)
+    float index_ms = 0;        // device time of the seek-index passes csv_open ran (0: none ran)
     uint32_t mixed_b = 0;   // a concatenation of different brick sizes
     uint64_t enc_pool_bytes = 0, pal_pool_entries = 0;  // sizes of d_enc and d_pal
     uint32_t* h_cost = nullptr;  // per brick: decode work estimate (nSymbols), for scheduling
@@ -89,7 +92,30 @@ struct DeviceDataset {
 
 // Launch helpers implemented in decode.cu.
 cudaError_t build_lut(const uint32_t* freq, const uint32_t* cum, uint32_t* h_lut);
-cudaError_t launch_build_index(DeviceDataset& ds, cudaStream_t st);
+// Bit t set when table t (of n, the first 32) is well formed: every x in
+// [0, 4096) lies in its symbol's range [start, start + freq).
+uint32_t lut_fast_mask(const uint32_t* h_lut, uint32_t n);
+// A seek-index sidecar keeps the rANS state before every kSeedSymbols-th symbol.
+constexpr uint32_t kSeedSymbols = 512;
+// Pass 1 as pieces from given states: piece_base[i] .. piece_base[i + 1] are
+// brick i's pieces (piece_base has nb + 1 entries), seed[p] the state {x, pos}
+// before piece p's first symbol, or {0, 0xFFFFFFFF}: brick i's only piece,
+// run from its header.
+struct IndexSeeds {
+    std::vector<uint32_t> piece_base;
+    std::vector<uint2> seed;
+};
+// The seek index (checkpoints, op counts, level starts, flags) of every brick,
+// from the stream headers (seeds null) or from a sidecar's states; with seeds,
+// *rejected is set, and nothing is written past the chain pass, when a piece
+// did not end in the state given for the next (the dataset then needs a
+// rebuild from its headers).
+cudaError_t launch_build_index(DeviceDataset& ds, cudaStream_t st, const IndexSeeds* seeds = nullptr,
+                               bool* rejected = nullptr);
+// The states a sidecar keeps for ds (bricks whose chain the index walks; 0 for
+// the others), computed again from the stream headers.
+cudaError_t index_seeds_of(const DeviceDataset& ds, cudaStream_t st, std::vector<uint32_t>& n_seeds,
+                           std::vector<uint2>& seeds);
 
 struct DecodeScratch {
     uint8_t* base = nullptr;

@@ -143,6 +143,19 @@ cudaError_t build_lut(const uint32_t* freq, const uint32_t* cum, uint32_t* h_lut
     return cudaSuccess;
 }
 
+uint32_t lut_fast_mask(const uint32_t* h_lut, uint32_t n) {
+    uint32_t m = 0;
+    for (uint32_t t = 0; t < n && t < 32; ++t) {
+        bool ok = true;
+        for (uint32_t x = 0; x < kTot && ok; ++x) {
+            const uint32_t e = h_lut[(size_t)t * kTot + x], f = (e >> 4) & 0x1FFFu, start = e >> 17;
+            ok = start <= x && x - start < f;
+        }
+        if (ok) m |= 1u << t;
+    }
+    return m;
+}
+
 // One rANS decode step (ransDecodeSymbol, brickDecoding.cpp:137-151), totalFreq
 // 4096 so % and / are a mask and a shift.  GLOBAL: enc is global memory (read
 // through the non-coherent path); otherwise a generic pointer (shared staging).
@@ -208,29 +221,240 @@ __device__ __forceinline__ uint32_t index_step(uint32_t& x, uint32_t& pos, const
 // (brickDecoding.hpp:174-242): the same checkpoints, op count, level starts and
 // flags.
 constexpr uint32_t kSnap = 32;  // symbols between state snapshots
+static_assert(kSeedSymbols % kSnap == 0, "a sidecar's states fall on snapshots");
+
+// Pass 1's chain step in two forms.
+//
+// ChainRef: ransDecodeSymbol and the renormalisation loop as the reference
+// writes them (brickDecoding.cpp:137-151), for any table and start state.  The
+// two bytes a well-formed renormalisation can take are loads at fixed offsets
+// from a pointer to byte pos, issued (predicated on pos) before the state is
+// known.
+//
+// ChainFast: for a well-formed table (every x lies in its symbol's range, so a
+// step leaves x >= freq * 2^11 >= 2^11 when it began at x >= 2^23) and a chain
+// that began at x >= 2^23.  Then a renormalisation takes one byte below 2^23
+// and a second below 2^15 (x >= 2^27 after it), or stops at the stream's
+// start: the reference's loop never needs a third byte, and the bits to take
+// are min(want, 8 pos), shifted into x from a 64-bit buffer of the next stream
+// bytes (next byte on top) by one funnel shift.  The buffer is fed from
+// aligned 32-bit words walking down the stream (a stream starts 16-byte
+// aligned), one word ahead of need, so no step waits on a byte load; it holds
+// at least 32 bits at every second step.  Table form: (x - start) | symbol <<
+// 12 | freq << 19, one shift or mask per field.
+struct ChainRef {
+    const uint8_t* q;
+    uint32_t x, pos;
+    const uint32_t* lut;  // symbol | freq << 4 | start << 17
+    __device__ __forceinline__ void init(const uint8_t* enc, uint32_t x0, uint32_t pos0, const uint32_t* t) {
+        q = enc + pos0;
+        x = x0;
+        pos = pos0;
+        lut = t;
+    }
+    __device__ __forceinline__ uint32_t step() {
+        const uint32_t b1 = pos > 0 ? (uint32_t)__ldg(q - 1) : 0u;
+        const uint32_t b2 = pos > 1 ? (uint32_t)__ldg(q - 2) : 0u;
+        const uint32_t v = x & (kTot - 1);
+        const uint32_t e = lut[v];
+        x = ((e >> 4) & 0x1FFFu) * (x >> kTotBits) + v - (e >> 17);
+        // a second byte is taken exactly when x < 2^15, since (x << 8 | b1) < 2^23 then
+        const bool n1 = x < kRansL && pos > 0, n2 = n1 && x < (kRansL >> 8) && pos > 1;
+        const uint32_t c1 = (x << 8) | b1, c2 = (x << 16) | (b1 << 8) | b2;
+        x = n2 ? c2 : (n1 ? c1 : x);
+        const uint32_t nb = (n1 ? 1u : 0u) + (n2 ? 1u : 0u);
+        pos -= nb;
+        q -= nb;
+        while (x < kRansL && pos > 0) {  // malformed streams only
+            x = (x << 8) | __ldg(--q);
+            --pos;
+        }
+        return e & 15u;
+    }
+    __device__ __forceinline__ void refill() {}
+    __device__ __forceinline__ uint32_t where() const { return pos; }
+};
+
+struct ChainFast {
+    const uint32_t* encw;  // the stream as aligned words
+    uint32_t x, pos8;      // state and 8 x bytes left below the read position
+    int32_t lo;            // lowest stream byte in bb (below 0: zero padding)
+    uint64_t bb;           // the next bytes, next one in bits 63..56
+    uint32_t nw;           // the word just below lo (0 below the stream)
+    const uint32_t* lut;   // (x - start) | symbol << 12 | freq << 19
+    __device__ __forceinline__ void init(const uint8_t* enc, uint32_t x0, uint32_t pos0, const uint32_t* t) {
+        encw = reinterpret_cast<const uint32_t*>(enc);
+        x = x0;
+        pos8 = 8 * pos0;
+        lut = t;
+        bb = 0;
+        lo = 0;
+        nw = 0;
+        if (pos0 == 0) return;
+        // the word holding byte pos0 - 1 keeps its bytes below pos0 (c0 of them, on top), the word below follows
+        const uint32_t a0 = (pos0 - 1) & ~3u, c0 = pos0 - a0;
+        const uint32_t w0 = __ldg(encw + (a0 >> 2)) << (8 * (4 - c0));
+        const uint32_t w1 = a0 >= 4 ? __ldg(encw + (a0 >> 2) - 1) : 0u;
+        bb = ((uint64_t)w0 << 32) | ((uint64_t)w1 << (32 - 8 * c0));
+        lo = (int32_t)a0 - 4;
+        nw = lo >= 4 ? __ldg(encw + ((lo - 4) >> 2)) : 0u;
+    }
+    __device__ __forceinline__ uint32_t step() {
+        const uint32_t e = lut[x & (kTot - 1)];
+        x = (e >> 19) * (x >> kTotBits) + (e & (kTot - 1));
+        const uint32_t want = x < (kRansL >> 8) ? 16u : (x < kRansL ? 8u : 0u);
+        const uint32_t sh = min(want, pos8);
+        x = __funnelshift_lc((uint32_t)(bb >> 32), x, sh);
+        bb <<= sh;
+        pos8 -= sh;
+        return (e >> 12) & 15u;
+    }
+    // below 32 bits in the buffer: the prefetched word joins it, the next one is fetched
+    __device__ __forceinline__ void refill() {
+        const int32_t nbits = (int32_t)pos8 - 8 * lo;
+        if (nbits < 32) {
+            bb |= (uint64_t)nw << (32 - nbits);
+            lo -= 4;
+            nw = lo >= 4 ? __ldg(encw + ((lo - 4) >> 2)) : 0u;
+        }
+    }
+    __device__ __forceinline__ uint32_t where() const { return pos8 >> 3; }
+};
+
+// Symbols [s0, s1) of one brick's chain (s0 a multiple of kSnap): packed
+// nibbles to w (word s0 / 8 on), the state before every kSnap-th symbol to sn.
+// The brick's first piece (s0 == 0) also takes the root nibble; returns false
+// when the root's stop bit ends the brick there (its only nibble, the root, is
+// in w[0]).
+template <class Chain>
+__device__ __forceinline__ bool index_walk(Chain& c, uint32_t s0, uint32_t s1, uint32_t* __restrict__ w,
+                                           uint2* __restrict__ sn) {
+    uint32_t k = s0 / 8;
+    if (s0 == 0) {
+        sn[0] = make_uint2(c.x, c.where());
+        const uint32_t root = c.step();
+        c.refill();
+        if (root & 1u) {
+            w[0] = root;
+            return false;
+        }
+        // word 0: the root and symbols 1..7
+        uint32_t word = root;
+        for (uint32_t i = 1; i < 8 && i < s1; ++i) {
+            word |= c.step() << (4 * i);
+            c.refill();
+        }
+        w[0] = word;
+        k = 1;
+    }
+    // whole words of 8 symbols (a snapshot before every 4th: symbol 32m)
+    for (; 8 * k + 8 <= s1; ++k) {
+        if ((k & 3u) == 0) sn[k >> 2] = make_uint2(c.x, c.where());
+        uint32_t wd = 0;
+#pragma unroll
+        for (uint32_t j = 0; j < 8; ++j) {
+            wd |= c.step() << (4 * j);
+            if (j & 1u) c.refill();
+        }
+        w[k] = wd;
+    }
+    if (8 * k < s1) {  // the last, partial word
+        if ((k & 3u) == 0) sn[k >> 2] = make_uint2(c.x, c.where());
+        uint32_t wd = 0;
+        for (uint32_t j = 0; 8 * k + j < s1; ++j) {
+            wd |= c.step() << (4 * j);
+            c.refill();
+        }
+        w[k] = wd;
+    }
+    return true;
+}
+
+// A table in ChainFast's form from the usual one (symbol | freq << 4 | start << 17).
+__device__ __forceinline__ uint32_t fast_entry(uint32_t e, uint32_t i) {
+    return ((i - (e >> 17)) & (kTot - 1)) | ((e & 15u) << 12) | (((e >> 4) & 0x1FFFu) << 19);
+}
+
+__global__ void __launch_bounds__(256) index_fast_lut_kernel(const uint32_t* __restrict__ g_lut, uint32_t n,
+                                                            uint32_t* __restrict__ g_lutf) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) g_lutf[i] = fast_entry(g_lut[i], i & (kTot - 1));
+}
+
+// One brick's chain, or the piece [s0, s1) of it, from the state (x, pos);
+// ChainFast when `fast` (model 0's table from shared memory, the others' from
+// g_lutf), else ChainRef on the usual tables.  x and pos come back as the
+// state after the last symbol.
+__device__ __forceinline__ bool index_run(const uint8_t* enc, uint32_t& x, uint32_t& pos, const uint32_t* lut0f,
+                                          const uint32_t* __restrict__ g_lutf, const uint32_t* __restrict__ g_lut,
+                                          uint32_t model, bool fast, uint32_t s0, uint32_t s1, uint32_t* w,
+                                          uint2* sn) {
+    bool more;
+    if (fast && model == 0) {
+        ChainFast c;
+        c.init(enc, x, pos, lut0f);
+        more = index_walk(c, s0, s1, w, sn);
+        x = c.x;
+        pos = c.where();
+    } else if (fast) {
+        ChainFast c;
+        c.init(enc, x, pos, g_lutf + (size_t)model * kTot);
+        more = index_walk(c, s0, s1, w, sn);
+        x = c.x;
+        pos = c.where();
+    } else {
+        ChainRef c;
+        c.init(enc, x, pos, g_lut + (size_t)model * kTot);
+        more = index_walk(c, s0, s1, w, sn);
+        x = c.x;
+        pos = c.where();
+    }
+    return more;
+}
+
+// Model 0's table in ChainFast's form, in shared memory.
+__device__ __forceinline__ void load_fast_lut(uint32_t* lut0f, const uint32_t* __restrict__ g_lut) {
+    for (uint32_t i = threadIdx.x; i < kTot; i += blockDim.x) lut0f[i] = fast_entry(g_lut[i], i);
+}
+
+// The bricks' outcome of pass 1 that needs no bookkeeping: a brick with no
+// chain to index (header too short, no symbols, the root's stop bit, or one
+// level) gets no ops and its flags now; write_desc false leaves the
+// descriptors as they are (the chain alone is wanted).
+__device__ __forceinline__ void index_finish(BrickDesc* bricks, uint32_t bi, const BrickDesc& br, bool go,
+                                             uint32_t flags, uint8_t* chain, bool write_desc) {
+    chain[bi] = go ? 1 : 0;
+    if (!go && write_desc) {
+        BrickDesc& o = bricks[bi];
+        o.n_ops = 0;
+        o.flags = (br.flags & ~BF_STATUS_MASK) | flags;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) o.level_start[k] = 0;
+    }
+}
 
 __global__ void __launch_bounds__(128) index_symbols_kernel(BrickDesc* __restrict__ bricks, uint32_t nb,
                                                            const uint8_t* __restrict__ enc_pool,
-                                                           const uint32_t* __restrict__ g_lut, uint32_t n_models,
-                                                           uint32_t lanes, const uint64_t* __restrict__ nib_off,
+                                                           const uint32_t* __restrict__ g_lut,
+                                                           const uint32_t* __restrict__ g_lutf, uint32_t n_models,
+                                                           uint32_t fast_models, uint32_t lanes,
+                                                           const uint32_t* __restrict__ order,
+                                                           const uint64_t* __restrict__ nib_off,
                                                            const uint64_t* __restrict__ snap_off,
                                                            uint32_t* __restrict__ nib, uint2* __restrict__ snap,
-                                                           uint8_t* __restrict__ chain, uint32_t L) {
-    // model 0's table in this pass's form: symbol | freq << 4 | (x - start) << 17,
-    // so that a step adds the offset within the symbol's range straight from the table
+                                                           uint8_t* __restrict__ chain, uint32_t L, bool write_desc) {
     __shared__ uint32_t lut0[kTot];
-    for (uint32_t i = threadIdx.x; i < kTot; i += blockDim.x) {
-        const uint32_t e = g_lut[i];
-        lut0[i] = (e & 0x1FFFFu) | ((i - (e >> 17)) << 17);
-    }
+    load_fast_lut(lut0, g_lut);
     __syncthreads();
-    // Lanes of one warp on different bricks run the union of their branch paths
-    // every step, so a warp takes only `lanes` bricks when there are few enough
-    // bricks to give the schedulers many warps to interleave.
+    // The lanes of a warp take `lanes` bricks of similar length (order: longest
+    // first), so that a warp's chains end together, and one warp instruction
+    // steps them all: the longest chain then runs at its own latency instead of
+    // sharing a scheduler's issue slots with the other long chains.
     const uint32_t lane = threadIdx.x & 31;
     if (lane >= lanes) return;
-    const uint32_t bi = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * lanes + lane;
-    if (bi >= nb) return;
+    const uint32_t slot = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * lanes + lane;
+    if (slot >= nb) return;
+    const uint32_t bi = order[slot];
     const BrickDesc br = bricks[bi];
     const uint32_t model = min((br.flags >> BF_MODEL_SHIFT) & 255u, n_models - 1);
     uint32_t flags = 0;
@@ -242,75 +466,14 @@ __global__ void __launch_bounds__(128) index_symbols_kernel(BrickDesc* __restric
         uint32_t pos = br.E - 4;
         uint32_t x = ((uint32_t)enc[br.E - 1] << 24) | ((uint32_t)enc[br.E - 2] << 16) |
                      ((uint32_t)enc[br.E - 3] << 8) | enc[br.E - 4];
-        uint32_t* w = nib + nib_off[bi];
-        uint2* sn = snap + snap_off[bi];
-        sn[0] = make_uint2(x, pos);
-        // model 0's table from shared memory (the pointer is the shared array itself);
-        // a version-2 image's other tables in the usual form (rel: offsets stored)
-        auto run = [&](const uint32_t* lut, bool rel) {
-            // One rANS step: the stream is walked through a pointer to byte pos, so the
-            // two bytes a renormalisation can take are loads at fixed offsets, issued
-            // (predicated on pos) before the state is known.
-            const uint8_t* q = enc + pos;
-            auto step = [&]() -> uint32_t {
-                const uint32_t b1 = pos > 0 ? (uint32_t)__ldg(q - 1) : 0u;
-                const uint32_t b2 = pos > 1 ? (uint32_t)__ldg(q - 2) : 0u;
-                const uint32_t v = x & (kTot - 1);
-                const uint32_t e = lut[v];
-                x = ((e >> 4) & 0x1FFFu) * (x >> kTotBits) + (rel ? (e >> 17) : v - (e >> 17));
-                // the renormalisation's bytes in one choice: a second byte is taken
-                // exactly when x < 2^15, since (x << 8 | b1) < 2^23 then
-                const bool n1 = x < kRansL && pos > 0, n2 = n1 && x < (kRansL >> 8) && pos > 1;
-                const uint32_t c1 = (x << 8) | b1, c2 = (x << 16) | (b1 << 8) | b2;
-                x = n2 ? c2 : (n1 ? c1 : x);
-                const uint32_t nb = (n1 ? 1u : 0u) + (n2 ? 1u : 0u);
-                pos -= nb;
-                q -= nb;
-                while (x < kRansL && pos > 0) {  // malformed streams only
-                    x = (x << 8) | __ldg(--q);
-                    --pos;
-                }
-                return e & 15u;
-            };
-            const uint32_t root = step();
-            if (root & 1u) {
-                flags = BF_UNIFORM;  // the whole brick is palette[0]: nothing more to index
-                w[0] = root;
-                return;
-            }
+        const bool fast = x >= kRansL && model < 32 && ((fast_models >> model) & 1u);
+        if (index_run(enc, x, pos, lut0, g_lutf, g_lut, model, fast, 0, br.nsym, nib + nib_off[bi],
+                      snap + snap_off[bi]))
             go = L >= 2;
-            const uint32_t ns = br.nsym;
-            // word 0: the root and symbols 1..7
-            uint32_t word = root;
-            for (uint32_t i = 1; i < 8 && i < ns; ++i) word |= step() << (4 * i);
-            w[0] = word;
-            // whole words of 8 symbols (a snapshot before every 4th: symbol 32k)
-            uint32_t k = 1;
-            for (; 8 * k + 8 <= ns; ++k) {
-                if ((k & 3u) == 0) sn[k >> 2] = make_uint2(x, pos);
-                uint32_t wd = step();
-#pragma unroll
-                for (uint32_t j = 1; j < 8; ++j) wd |= step() << (4 * j);
-                w[k] = wd;
-            }
-            if (8 * k < ns) {  // the last, partial word
-                if ((k & 3u) == 0) sn[k >> 2] = make_uint2(x, pos);
-                uint32_t wd = 0;
-                for (uint32_t j = 0; 8 * k + j < ns; ++j) wd |= step() << (4 * j);
-                w[k] = wd;
-            }
-        };
-        if (model == 0) run(lut0, true);
-        else run(g_lut + (size_t)model * kTot, false);
+        else
+            flags = BF_UNIFORM;  // the whole brick is palette[0]: nothing more to index
     }
-    chain[bi] = go ? 1 : 0;
-    if (!go) {
-        BrickDesc& o = bricks[bi];
-        o.n_ops = 0;
-        o.flags = (br.flags & ~BF_STATUS_MASK) | flags;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) o.level_start[k] = 0;
-    }
+    index_finish(bricks, bi, br, go, flags, chain, write_desc);
 }
 
 // Composition of the per-lane automaton transfers (bit 0: the state after, from
@@ -505,10 +668,108 @@ __global__ void __launch_bounds__(128) index_states_kernel(const BrickDesc* __re
     else run(g_lut + (size_t)model * kTot);
 }
 
-cudaError_t launch_build_index(DeviceDataset& ds, cudaStream_t st) {
-    if (ds.nb == 0) return cudaSuccess;
+// Pass 1 from a seek-index sidecar: the state before every kSeedSymbols-th
+// symbol of each brick is given, so the chain runs as independent pieces, one
+// lane per piece.  A piece checks that it ends in the state given for the next
+// one, and the first piece that its state is the stream header's: by induction
+// every piece then ran from the true state, and the nibbles and snapshots are
+// the serial pass's.  Any difference (a sidecar of another image, or damaged)
+// counts in *bad and the host discards the result.  A brick the sidecar gives
+// no states for (seed.y == kFromHeader) is one piece, run from its header.
+constexpr uint32_t kFromHeader = 0xFFFFFFFFu;
+__global__ void __launch_bounds__(128) index_seeded_kernel(BrickDesc* __restrict__ bricks, uint32_t nb,
+                                                          const uint8_t* __restrict__ enc_pool,
+                                                          const uint32_t* __restrict__ g_lut,
+                                                          const uint32_t* __restrict__ g_lutf, uint32_t n_models,
+                                                          uint32_t fast_models, const uint32_t* __restrict__ piece_base,
+                                                          const uint2* __restrict__ seed, uint32_t n_pieces,
+                                                          const uint64_t* __restrict__ nib_off,
+                                                          const uint64_t* __restrict__ snap_off,
+                                                          uint32_t* __restrict__ nib, uint2* __restrict__ snap,
+                                                          uint8_t* __restrict__ chain, uint32_t L,
+                                                          uint32_t* __restrict__ bad) {
+    __shared__ uint32_t lut0[kTot];
+    load_fast_lut(lut0, g_lut);
+    __syncthreads();
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n_pieces) return;
+    // the piece's brick: the last bi with piece_base[bi] <= p (piece_base[0] = 0, piece_base[nb] = n_pieces)
+    uint32_t lo = 0, hi = nb;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (piece_base[mid] <= p) lo = mid;
+        else hi = mid;
+    }
+    const uint32_t bi = lo, k = p - piece_base[bi], n_here = piece_base[bi + 1] - piece_base[bi];
+    const BrickDesc br = bricks[bi];
+    if (br.E < 4 || br.nsym == 0) {
+        if (k == 0) index_finish(bricks, bi, br, false, BF_TRUNCATED, chain, true);
+        return;
+    }
+    const uint32_t model = min((br.flags >> BF_MODEL_SHIFT) & 255u, n_models - 1);
+    const uint8_t* enc = enc_pool + br.enc_off;
+    const uint32_t x0 = ((uint32_t)enc[br.E - 1] << 24) | ((uint32_t)enc[br.E - 2] << 16) |
+                        ((uint32_t)enc[br.E - 3] << 8) | enc[br.E - 4];
+    // FAST depends on the chain's true start (the header), as in the serial pass
+    const bool fast = x0 >= kRansL && model < 32 && ((fast_models >> model) & 1u);
+    const uint2 sd = seed[p];
+    uint32_t x = x0, pos = br.E - 4, s0 = 0, s1 = br.nsym;
+    if (sd.y == kFromHeader) {
+        if (k != 0 || n_here != 1) {
+            atomicAdd(bad, 1u);
+            return;
+        }
+    } else {
+        s0 = k * kSeedSymbols;
+        s1 = min(s0 + kSeedSymbols, br.nsym);
+        // a state past the stream's end would read outside it: refused before any step
+        if (s0 >= br.nsym || sd.y > br.E - 4 || (k == 0 && (sd.x != x0 || sd.y != br.E - 4))) {
+            atomicAdd(bad, 1u);
+            return;
+        }
+        x = sd.x;
+        pos = sd.y;
+    }
+    const bool more =
+        index_run(enc, x, pos, lut0, g_lutf, g_lut, model, fast, s0, s1, nib + nib_off[bi], snap + snap_off[bi]);
+    if (k == 0) index_finish(bricks, bi, br, more && L >= 2, more ? 0u : BF_UNIFORM, chain, true);
+    if (more && k + 1 < n_here) {
+        const uint2 nx = seed[p + 1];
+        if (nx.x != x || nx.y != pos) atomicAdd(bad, 1u);
+    }
+}
+
+// The states a sidecar keeps, from pass 1's snapshots: for a brick with a chain,
+// the state before symbols 0, kSeedSymbols, 2 kSeedSymbols, ... (one warp per brick).
+__global__ void __launch_bounds__(128) index_seeds_gather_kernel(const BrickDesc* __restrict__ bricks, uint32_t nb,
+                                                                const uint8_t* __restrict__ chain,
+                                                                const uint32_t* __restrict__ seed_base,
+                                                                const uint64_t* __restrict__ snap_off,
+                                                                const uint2* __restrict__ snap,
+                                                                uint2* __restrict__ seeds) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t bi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (bi >= nb || !chain[bi]) return;
+    const uint32_t n = seed_base[bi + 1] - seed_base[bi];
+    for (uint32_t k = lane; k < n; k += 32)
+        seeds[seed_base[bi] + k] = snap[snap_off[bi] + (uint64_t)k * (kSeedSymbols / kSnap)];
+}
+
+namespace {
+// Device temporaries of the index passes: per brick its nibble words and its snapshots.
+struct IndexTemps {
+    uint32_t* nib = nullptr;
+    uint2* snap = nullptr;
+    uint64_t* off = nullptr;  // nib_off[nb] | snap_off[nb]
+    uint32_t* order = nullptr;  // bricks by nSymbols, longest first
+    uint8_t* chain = nullptr;
+    uint32_t* nck = nullptr;
+    uint32_t* bad = nullptr;
+    uint32_t* lutf = nullptr;  // every model's table in ChainFast's form
+};
+
+cudaError_t index_alloc(const DeviceDataset& ds, cudaStream_t st, IndexTemps& t) {
     const uint32_t nb = ds.nb;
-    // per brick: its nibble words and its snapshots
     std::vector<uint64_t> off(2 * (size_t)nb);
     uint64_t words = 0, snaps = 0;
     for (uint32_t i = 0; i < nb; ++i) {
@@ -518,40 +779,155 @@ cudaError_t launch_build_index(DeviceDataset& ds, cudaStream_t st) {
         words += ns / 8 + 1;
         snaps += ns / kSnap + 1;
     }
-    uint32_t* d_nib = nullptr;
-    uint2* d_snap = nullptr;
-    uint64_t* d_off = nullptr;
-    uint8_t* d_chain = nullptr;
-    uint32_t* d_nck = nullptr;
-    cudaError_t e = cudaMallocAsync((void**)&d_nib, words * 4, st);
-    if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_snap, snaps * 8, st);
-    if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_off, off.size() * 8, st);
-    if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_chain, nb, st);
-    if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_nck, (size_t)nb * 4, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_off, off.data(), off.size() * 8, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // the host offsets are released on return
+    std::vector<uint32_t> order(nb);
+    for (uint32_t i = 0; i < nb; ++i) order[i] = i;
+    if (ds.h_cost)
+        std::stable_sort(order.begin(), order.end(),
+                         [&](uint32_t a, uint32_t b) { return ds.h_cost[a] > ds.h_cost[b]; });
+    cudaError_t e = cudaMallocAsync((void**)&t.nib, words * 4, st);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&t.snap, snaps * 8, st);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&t.off, off.size() * 8, st);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&t.order, (size_t)nb * 4, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(t.order, order.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&t.chain, nb, st);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&t.nck, (size_t)nb * 4, st);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&t.bad, 4, st);
+    const uint32_t nm = ds.n_models ? ds.n_models : 1u;
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&t.lutf, (size_t)nm * kTot * 4, st);
     if (e == cudaSuccess) {
-        // pass 1: bricks per warp, the fewest (a power of two) that keeps about 32 warps per SM
-        int sms = 0;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ds.device);
-        const uint64_t warps_max = 32ull * (uint64_t)std::max(sms, 1);
-        uint32_t lanes = 1;
-        while (lanes < 32 && (nb + lanes - 1) / lanes > warps_max) lanes <<= 1;
-        const uint32_t per_block = 4 * lanes;
-        const uint32_t nm = ds.n_models ? ds.n_models : 1u;
-        index_symbols_kernel<<<(nb + per_block - 1) / per_block, 128, 0, st>>>(
-            ds.d_bricks, nb, ds.d_enc, ds.d_lut, nm, lanes, d_off, d_off + nb, d_nib, d_snap, d_chain, ds.L);
-        index_book_kernel<<<(nb + 3) / 4, 128, 0, st>>>(ds.d_bricks, nb, d_nib, d_off, d_chain, ds.d_ck, d_nck, ds.L,
-                                                       ds.S);
-        index_states_kernel<<<(nb + 3) / 4, 128, 0, st>>>(ds.d_bricks, nb, ds.d_enc, ds.d_lut, nm, d_off + nb, d_snap,
-                                                         d_nck, ds.d_ck);
+        index_fast_lut_kernel<<<(nm * kTot + 255) / 256, 256, 0, st>>>(ds.d_lut, nm * kTot, t.lutf);
         e = cudaGetLastError();
     }
-    cudaFreeAsync(d_nib, st);
-    cudaFreeAsync(d_snap, st);
-    cudaFreeAsync(d_off, st);
-    cudaFreeAsync(d_chain, st);
-    cudaFreeAsync(d_nck, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(t.bad, 0, 4, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(t.off, off.data(), off.size() * 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // the host offsets are released on return
+    return e;
+}
+
+void index_free(IndexTemps& t, cudaStream_t st) {
+    cudaFreeAsync(t.nib, st);
+    cudaFreeAsync(t.snap, st);
+    cudaFreeAsync(t.off, st);
+    cudaFreeAsync(t.order, st);
+    cudaFreeAsync(t.chain, st);
+    cudaFreeAsync(t.nck, st);
+    cudaFreeAsync(t.bad, st);
+    cudaFreeAsync(t.lutf, st);
+    t = IndexTemps();
+}
+
+// pass 1 from the stream headers: four bricks per warp, four warps per block.
+// (Measured on the 2048 bricks of a 1024 x 1024 x 512 volume of 64^3 bricks,
+// longest 126k symbols: one brick per warp 10.4 ms, its warps sharing the
+// schedulers' issue slots; 32 per warp 15.8 ms, each step slowed by 32 lanes'
+// scattered byte loads and table bank conflicts.)
+void index_pass1_serial(const DeviceDataset& ds, const IndexTemps& t, cudaStream_t st, bool write_desc) {
+    const uint32_t nb = ds.nb;
+    constexpr uint32_t lanes = 4;
+    const uint32_t per_block = 4 * lanes;
+    const uint32_t nm = ds.n_models ? ds.n_models : 1u;
+    index_symbols_kernel<<<(nb + per_block - 1) / per_block, 128, 0, st>>>(
+        ds.d_bricks, nb, ds.d_enc, ds.d_lut, t.lutf, nm, ds.fast_models, lanes, t.order, t.off, t.off + nb, t.nib,
+        t.snap, t.chain, ds.L, write_desc);
+}
+}  // namespace
+
+cudaError_t launch_build_index(DeviceDataset& ds, cudaStream_t st, const IndexSeeds* seeds, bool* rejected) {
+    if (rejected) *rejected = false;
+    if (ds.nb == 0) return cudaSuccess;
+    const uint32_t nb = ds.nb;
+    const uint32_t nm = ds.n_models ? ds.n_models : 1u;
+    IndexTemps t;
+    uint32_t* d_base = nullptr;
+    uint2* d_seed = nullptr;
+    cudaError_t e = index_alloc(ds, st, t);
+    if (e == cudaSuccess && seeds) {
+        const uint32_t n_pieces = seeds->piece_base.back();
+        e = cudaMallocAsync((void**)&d_base, 4 * seeds->piece_base.size(), st);
+        if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_seed, 8 * std::max<size_t>(1, seeds->seed.size()), st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_base, seeds->piece_base.data(), 4 * seeds->piece_base.size(),
+                                cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess && !seeds->seed.empty())
+            e = cudaMemcpyAsync(d_seed, seeds->seed.data(), 8 * seeds->seed.size(), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) {
+            index_seeded_kernel<<<(n_pieces + 127) / 128, 128, 0, st>>>(
+                ds.d_bricks, nb, ds.d_enc, ds.d_lut, t.lutf, nm, ds.fast_models, d_base, d_seed, n_pieces, t.off,
+                t.off + nb, t.nib, t.snap, t.chain, ds.L, t.bad);
+            e = cudaGetLastError();
+        }
+        // the bookkeeping passes run only on a chain every piece confirmed (an unconfirmed
+        // piece may have left snapshots that the states pass would follow outside a stream)
+        uint32_t h_bad = 0;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&h_bad, t.bad, 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e == cudaSuccess && h_bad) {
+            if (rejected) *rejected = true;
+            cudaFreeAsync(d_base, st);
+            cudaFreeAsync(d_seed, st);
+            index_free(t, st);
+            return cudaSuccess;
+        }
+    } else if (e == cudaSuccess) {
+        index_pass1_serial(ds, t, st, true);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        index_book_kernel<<<(nb + 3) / 4, 128, 0, st>>>(ds.d_bricks, nb, t.nib, t.off, t.chain, ds.d_ck, t.nck, ds.L,
+                                                       ds.S);
+        index_states_kernel<<<(nb + 3) / 4, 128, 0, st>>>(ds.d_bricks, nb, ds.d_enc, ds.d_lut, nm, t.off + nb,
+                                                         t.snap, t.nck, ds.d_ck);
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(d_base, st);
+    cudaFreeAsync(d_seed, st);
+    index_free(t, st);
+    return e;
+}
+
+cudaError_t index_seeds_of(const DeviceDataset& ds, cudaStream_t st, std::vector<uint32_t>& n_seeds,
+                           std::vector<uint2>& seeds) {
+    n_seeds.assign(ds.nb, 0);
+    seeds.clear();
+    if (ds.nb == 0) return cudaSuccess;
+    const uint32_t nb = ds.nb;
+    IndexTemps t;
+    uint32_t* d_base = nullptr;
+    uint2* d_seeds = nullptr;
+    std::vector<uint8_t> chain(nb);
+    std::vector<BrickDesc> desc(nb);
+    cudaError_t e = index_alloc(ds, st, t);
+    if (e == cudaSuccess) {
+        index_pass1_serial(ds, t, st, false);  // the dataset's descriptors stay as they are
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(chain.data(), t.chain, nb, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(desc.data(), ds.d_bricks, sizeof(BrickDesc) * nb, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    std::vector<uint32_t> base(nb + 1, 0);
+    if (e == cudaSuccess) {
+        for (uint32_t i = 0; i < nb; ++i) {
+            n_seeds[i] = chain[i] ? (desc[i].nsym + kSeedSymbols - 1) / kSeedSymbols : 0u;
+            base[i + 1] = base[i] + n_seeds[i];
+        }
+        seeds.resize(base[nb]);
+        e = cudaMallocAsync((void**)&d_base, 4ull * (nb + 1), st);
+        if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_seeds, 8ull * std::max<uint32_t>(1, base[nb]), st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d_base, base.data(), 4ull * (nb + 1), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) {
+            index_seeds_gather_kernel<<<(nb + 3) / 4, 128, 0, st>>>(ds.d_bricks, nb, t.chain, d_base, t.off + nb,
+                                                                   t.snap, d_seeds);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess && base[nb])
+            e = cudaMemcpyAsync(seeds.data(), d_seeds, 8ull * base[nb], cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    cudaFreeAsync(d_base, st);
+    cudaFreeAsync(d_seeds, st);
+    index_free(t, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     return e;
 }
 

@@ -1122,6 +1122,7 @@ int encoder_to_dataset(EncoderState* s, DeviceDataset& d, std::string& err) {
     d.n_models = s->n_tables;
     std::vector<uint32_t> lut((size_t)kTot * s->n_tables);
     for (uint32_t t = 0; t < s->n_tables; ++t) build_lut(s->tab_freq[t], s->tab_cum[t], &lut[(size_t)t * kTot]);
+    d.fast_models = lut_fast_mask(lut.data(), s->n_tables);
     cudaError_t e;
     if ((e = cudaMalloc(&d.d_bricks, sizeof(BrickDesc) * std::max<uint32_t>(1, nb))) != cudaSuccess ||
         (e = cudaMalloc(&d.d_pal, 8 * std::max<uint64_t>(1, pal_n))) != cudaSuccess ||

@@ -133,6 +133,9 @@ def load_library() -> C.CDLL:
     L.csv_open_encoded.argtypes = [vp, C.POINTER(vp)]
     L.csv_dataset_info_get.argtypes = [vp, C.POINTER(_Info)]
     L.csv_dataset_ids.argtypes = [vp, u32p, C.c_uint32]
+    L.csv_dataset_index_ms.argtypes = [vp, C.POINTER(C.c_float)]
+    L.csv_index_save.argtypes = [vp, vp, C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(C.c_size_t)]
+    L.csv_open_indexed.argtypes = [vp, u8p, C.c_size_t, u8p, C.c_size_t, C.POINTER(vp)]
     L.csv_close.argtypes = [vp]
     L.csv_decode_batch.argtypes = [vp, vp, vp, C.c_uint32, vp, vp, vp]
     L.csv_decode_image.argtypes = [vp, u8p, C.c_size_t, C.c_uint32, u64p, u32p]
@@ -238,6 +241,22 @@ class Dataset:
     @property
     def brick_size(self) -> int:
         return self.info.brick_size
+
+    @property
+    def index_ms(self) -> float:
+        """Device time of the seek-index passes csv_open ran (0.0 when none ran)."""
+        ms = C.c_float()
+        self.codec._check(self.codec.lib.csv_dataset_index_ms(self.handle, C.byref(ms)))
+        return ms.value
+
+    def index_sidecar(self) -> bytes:
+        """csv_index_save: the seek-index sidecar of this dataset's image (give it to Codec.open)."""
+        out = C.POINTER(C.c_uint8)()
+        n = C.c_size_t()
+        self.codec._check(self.codec.lib.csv_index_save(self.codec.handle, self.handle, C.byref(out), C.byref(n)))
+        data = C.string_at(out, n.value)
+        self.codec.lib.csv_free(out)
+        return data
 
     def ids(self) -> np.ndarray:
         out = np.zeros(max(1, self.num_bricks), np.uint32)
@@ -371,10 +390,18 @@ class Codec:
         return torch.as_tensor(_View(), device=f"cuda:{self.device}")
 
     # ---- datasets ------------------------------------------------------
-    def open(self, image: bytes) -> Dataset:
+    def open(self, image: bytes, sidecar: bytes | None = None) -> Dataset:
+        """csv_open, or csv_open_indexed with a seek-index sidecar (Dataset.index_sidecar of the same image)."""
         a = np.frombuffer(image, np.uint8)
         h = C.c_void_p()
-        self._check(self.lib.csv_open(self.handle, a.ctypes.data_as(C.POINTER(C.c_uint8)), len(image), C.byref(h)))
+        if sidecar is None:
+            self._check(self.lib.csv_open(self.handle, a.ctypes.data_as(C.POINTER(C.c_uint8)), len(image),
+                                          C.byref(h)))
+        else:
+            sc = np.frombuffer(sidecar, np.uint8)
+            self._check(self.lib.csv_open_indexed(self.handle, a.ctypes.data_as(C.POINTER(C.c_uint8)), len(image),
+                                                  sc.ctypes.data_as(C.POINTER(C.c_uint8)), len(sidecar),
+                                                  C.byref(h)))
         return Dataset(self, h.value)
 
     def concat(self, parts) -> Dataset:

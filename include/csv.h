@@ -130,6 +130,23 @@ int csv_open(csv_ctx* ctx, const uint8_t* image, size_t len, csv_dataset** out);
  * index from the encoder instead of rebuilding it. */
 int csv_open_encoded(csv_ctx* ctx, csv_dataset** out);
 int csv_dataset_info_get(const csv_dataset* ds, csv_dataset_info* info);
+/* Device time in ms of the seek-index passes csv_open ran for this dataset
+ * (CUDA events on its stream around them); 0 when none ran (csv_open_encoded,
+ * csv_dataset_concat).  No reference counterpart: the reference's index is the
+ * serial walk inside decodeRansStream (brickDecoding.cpp:153-188). */
+int csv_dataset_index_ms(const csv_dataset* ds, float* ms);
+/* Seek-index sidecar.  csv_index_save writes, for the dataset's image, the
+ * rANS state before every 512th symbol of each brick (8 bytes per 512
+ * symbols; the buffer is this library's, free it with csv_free).
+ * csv_open_indexed opens the image as csv_open does, with pass 1 of the index
+ * run as independent 512-symbol pieces from those states: each piece checks
+ * that it ends in the next stored state, so the index equals csv_open's, and a
+ * sidecar of another image, or a damaged one, fails with CSV_EFORMAT (open
+ * without it then).  No reference counterpart: the reference rebuilds the walk
+ * on every load (brickDecoding.cpp:153-188). */
+int csv_index_save(csv_ctx* ctx, const csv_dataset* ds, uint8_t** out, size_t* out_len);
+int csv_open_indexed(csv_ctx* ctx, const uint8_t* image, size_t len, const uint8_t* sidecar, size_t sidecar_len,
+                     csv_dataset** out);
 /* Morton brick IDs (datasetLoader.js:113-123) in file order, host array. */
 int csv_dataset_ids(const csv_dataset* ds, uint32_t* ids, uint32_t n);
 void csv_close(csv_dataset* ds);

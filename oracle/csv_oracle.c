@@ -547,6 +547,30 @@ int or_rans_decode(const uint32_t* freq, const uint32_t* cum, uint32_t total_fre
     return 0;
 }
 
+/* The chain of decodeRansStream (brickDecoding.cpp:153-188) sampled: the
+ * state {x, pos} before symbol k * every, for every k with k * every < nsym,
+ * to states[2k], states[2k + 1] (a seek-index sidecar's contents).  Returns
+ * the number of states, or -1 for a stream shorter than its header. */
+int or_rans_states(const uint32_t* freq, const uint32_t* cum, const uint8_t* enc, uint32_t E, uint32_t nsym,
+                   uint32_t every, uint32_t* states) {
+    if (E < 4 || every == 0) return -1;
+    uint32_t pos = E - 4;
+    uint32_t x = ((uint32_t)enc[E - 1] << 24) | ((uint32_t)enc[E - 2] << 16) | ((uint32_t)enc[E - 3] << 8) | enc[E - 4];
+    int n = 0;
+    for (uint32_t i = 0; i < nsym; ++i) {
+        if (i % every == 0) {
+            states[2 * n] = x;
+            states[2 * n + 1] = pos;
+            ++n;
+        }
+        uint32_t v = x % TOT;
+        uint32_t s = find_sym(v, cum);
+        x = freq[s] * (x / TOT) + (v - cum[s]);
+        while (x < RANS_L && pos > 0) x = (x << 8) | enc[--pos];
+    }
+    return n;
+}
+
 /* decode.wgsl:344-509 in label space (the RGBA transfer function of
  * decode.wgsl:135-172 is not applied), which equals brickDecoding.hpp:174-242
  * at full resolution.  Slot of node m at level l is m << 3(t-l)

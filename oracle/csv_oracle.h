@@ -40,6 +40,9 @@ int or_decode_brick(const uint64_t* palette, uint32_t P, const uint8_t* nib, uin
 int or_decode_image(const uint8_t* img, size_t len, uint32_t t, uint64_t* out, uint32_t* status);
 
 /* Seek index of one brick (the project's sidecar format; see csv.h). */
+/* The rANS state {x, pos} before every `every`-th symbol of a brick's chain. */
+int or_rans_states(const uint32_t* freq16, const uint32_t* cum16, const uint8_t* enc, uint32_t enc_len, uint32_t nsym,
+                   uint32_t every, uint32_t* states);
 int or_seek_index(const uint32_t* freq16, const uint32_t* cum16, const uint8_t* enc, uint32_t enc_len,
                   uint32_t nsym, uint32_t P, uint32_t b, uint32_t ops_per_ckpt,
                   uint32_t* n_ops, uint32_t* level_start /* [8] */, uint32_t* ckpt /* 4 per */,

@@ -72,6 +72,7 @@ class Oracle:
         L.or_rans_decode.argtypes = [_u32p, _u32p, C.c_uint32, _u8p, C.c_uint32, C.c_uint32, _u8p]
         L.or_decode_brick.argtypes = [_u64p, C.c_uint32, _u8p, C.c_uint32, C.c_uint32, C.c_uint32, _u64p]
         L.or_decode_image.argtypes = [_u8p, C.c_size_t, C.c_uint32, _u64p, _u32p]
+        L.or_rans_states.argtypes = [_u32p, _u32p, _u8p, C.c_uint32, C.c_uint32, C.c_uint32, _u32p]
         L.or_seek_index.argtypes = [_u32p, _u32p, _u8p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                     C.c_uint32, _u32p, _u32p, _u32p, C.c_uint32, _u32p]
         L.or_free.argtypes = [C.c_void_p]
@@ -348,6 +349,18 @@ class Oracle:
         st = self.lib.or_decode_brick(_ptr(p, _u64p), len(p), _ptr(n, _u8p), len(nib), brick, lod,
                                       _ptr(out, _u64p))
         return out, st
+
+    def rans_states(self, freq, cum16, enc: bytes, nsym: int, every: int) -> np.ndarray:
+        """(n, 2) uint32: the chain's state {x, pos} before symbols 0, every, 2 every, ... (or_rans_states)."""
+        f = np.ascontiguousarray(freq, np.uint32)
+        c = np.ascontiguousarray(cum16, np.uint32)
+        e = np.frombuffer(enc, np.uint8) if len(enc) else np.zeros(1, np.uint8)
+        out = np.zeros(2 * (nsym // every + 1), np.uint32)
+        n = self.lib.or_rans_states(_ptr(f, _u32p), _ptr(c, _u32p), _ptr(e, _u8p), len(enc), nsym, every,
+                                    _ptr(out, _u32p))
+        if n < 0:
+            raise ValueError("stream shorter than its header")
+        return out[: 2 * n].reshape(-1, 2)
 
     def seek_index(self, freq, cum16, enc: bytes, nsym: int, P: int, brick: int, S: int):
         f = np.ascontiguousarray(freq, np.uint32)

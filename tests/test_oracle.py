@@ -135,6 +135,60 @@ def test_golden_encode_roundtrip(oracle, golden, name):
         assert [sha(d[k]) for k in range(d.shape[0])] == g["lod"][str(t)]
 
 
+def _shipped_bricks():
+    """(freq, cum, [(E, enc, nsym)]) of the shipped 8-brick subset (v1 layout: fileIO.cpp:25-96)."""
+    import struct
+    img = read_golden("shipped_subset")
+    freq = np.frombuffer(img[24:88], np.uint32)
+    cum = np.frombuffer(img[88:152], np.uint32)
+    nb = struct.unpack_from("<I", img, 8)[0]
+    o, out = 152, []
+    for _ in range(nb):
+        ID, P = struct.unpack_from("<2I", img, o)
+        o += 8 + 8 * P
+        E = struct.unpack_from("<I", img, o)[0]
+        enc = img[o + 4:o + 4 + E]
+        o += 4 + E
+        ns = struct.unpack_from("<I", img, o)[0]
+        o += 4
+        out.append((E, enc, ns))
+    return img, freq, cum, out
+
+
+def test_rans_states_resume_the_reference_chain(oracle, reference):
+    """or_rans_states, the content of a seek-index sidecar, on the shipped bricks: the state before symbol 0 is
+    the stream header; after the last nibble of the packed bytes (nSymbols rounded up to even: the encoder
+    codes the pad nibble too) the state is the encoder's initial one, 2^23, with every byte read; and 64 symbols decoded from every state sampled each 512 symbols equal the compiled reference decoder's
+    nibbles there."""
+    img, freq, cum, bricks = _shipped_bricks()
+    lut = []
+    for x in range(4096):
+        s = 0
+        while s + 1 < 16 and x >= cum[s + 1]:
+            s += 1
+        lut.append(s)
+    for i, (E, enc, ns) in enumerate(bricks):
+        n_all = ns + (ns & 1)  # nibbles of the packed bytes
+        st = oracle.rans_states(freq, cum, enc, n_all + 1, 1)  # + 1: the state after the last one too
+        assert st.shape == (n_all + 1, 2)
+        assert tuple(st[0]) == (int.from_bytes(enc[E - 4:E], "little"), E - 4)
+        assert tuple(st[-1]) == (1 << 23, 0)
+        sampled = oracle.rans_states(freq, cum, enc, ns, 512)
+        assert np.array_equal(sampled, st[:ns:512])
+        ref = reference.rans_decode(img, i, ns)
+        ref_sym = [(ref[j // 2] >> (4 * (1 - j % 2))) & 15 for j in range(ns)]
+        for k, (x, pos) in enumerate(sampled):
+            x, pos = int(x), int(pos)
+            for j in range(512 * k, min(512 * k + 64, ns)):
+                v = x & 4095
+                sym = lut[v]
+                assert sym == ref_sym[j], (i, k, j)
+                x = int(freq[sym]) * (x >> 12) + v - int(cum[sym])
+                while x < (1 << 23) and pos > 0:
+                    pos -= 1
+                    x = (x << 8) | enc[pos]
+
+
 def test_seek_index_checkpoints_resume_decode(oracle):
     """Each checkpoint (state, byte position, nibble index, palette index) lets the rANS decoder resume."""
     import struct
