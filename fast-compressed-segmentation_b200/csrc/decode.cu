@@ -180,7 +180,8 @@ __device__ __forceinline__ uint32_t rans_step(uint32_t& x, uint32_t& pos, const 
 }
 
 // -------------------------------------------------------------- seek index
-// The rANS step of the serial pass.  Same arithmetic as rans_step; both bytes
+// The rANS step of the states pass (a checkpoint's state decoded again from the
+// snapshot before it).  Same arithmetic as rans_step; both bytes
 // a well-formed renormalisation can take are read before the state is known
 // (their addresses depend only on pos), so the loads overlap the table lookup
 // instead of following it on the chain.
@@ -189,7 +190,7 @@ __device__ __forceinline__ uint32_t index_step(uint32_t& x, uint32_t& pos, const
     const uint32_t b1 = __ldg(enc + (pos > 0 ? pos - 1 : 0));
     const uint32_t b2 = __ldg(enc + (pos > 1 ? pos - 2 : 0));
     const uint32_t v = x & (kTot - 1);
-    const uint32_t e = lut[v];
+    const uint32_t e = __ldg(lut + v);
     x = ((e >> 4) & 0x1FFFu) * (x >> kTotBits) + v - (e >> 17);
     if (x < kRansL && pos > 0) {
         x = (x << 8) | b1;
@@ -506,9 +507,12 @@ __global__ void __launch_bounds__(128) index_book_kernel(BrickDesc* __restrict__
     uint32_t ls[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     uint32_t n_ck = 0, end_ops = 0xFFFFFFFFu;
     bool done = false;
+    // each chunk's nibble word is loaded one chunk ahead
+    uint32_t word_next = 8 * lane < nsym ? w[lane] : 0u;
     for (uint32_t c0 = 0; c0 < nsym && !done; c0 += 256) {
         const uint32_t base = c0 + 8 * lane;
-        const uint32_t word = base < nsym ? w[base >> 3] : 0u;
+        const uint32_t word = word_next;
+        word_next = base + 256 < nsym ? w[(base + 256) >> 3] : 0u;
         // symbols of this lane: [max(base, 1), min(base + 8, nsym)) -- symbol 0 is the root
         const uint32_t i0 = base == 0 ? 1u : base, i1 = min(base + 8, nsym);
         auto step = [&](uint32_t st, uint32_t k) -> uint32_t {
@@ -635,17 +639,16 @@ __global__ void __launch_bounds__(128) index_book_kernel(BrickDesc* __restrict__
     }
 }
 
+// One block per brick: its threads share the brick's checkpoints, so a long
+// brick's re-decodes spread over the block instead of one warp (the table is
+// read through L1: the decodes are short).
 __global__ void __launch_bounds__(128) index_states_kernel(const BrickDesc* __restrict__ bricks, uint32_t nb,
                                                           const uint8_t* __restrict__ enc_pool,
                                                           const uint32_t* __restrict__ g_lut, uint32_t n_models,
                                                           const uint64_t* __restrict__ snap_off,
                                                           const uint2* __restrict__ snap,
                                                           const uint32_t* __restrict__ n_ck, Checkpoint* __restrict__ ck) {
-    __shared__ uint32_t lut0[kTot];
-    for (uint32_t i = threadIdx.x; i < kTot; i += blockDim.x) lut0[i] = g_lut[i];
-    __syncthreads();
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t bi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const uint32_t bi = blockIdx.x;
     if (bi >= nb) return;
     const uint32_t n = n_ck[bi];
     if (n == 0) return;
@@ -653,19 +656,16 @@ __global__ void __launch_bounds__(128) index_states_kernel(const BrickDesc* __re
     const uint32_t model = min((br.flags >> BF_MODEL_SHIFT) & 255u, n_models - 1);
     const uint8_t* enc = enc_pool + br.enc_off;
     const uint2* sn = snap + snap_off[bi];
-    auto run = [&](const uint32_t* lut) {
-        for (uint32_t c = lane; c < n; c += 32) {
-            Checkpoint& k = ck[br.ck_off + c];
-            const uint32_t s = k.sym, j = s / kSnap;
-            const uint2 z = sn[j];
-            uint32_t x = z.x, pos = z.y;
-            for (uint32_t t = j * kSnap; t < s; ++t) index_step(x, pos, enc, lut);
-            k.state = x;
-            k.pos = pos;
-        }
-    };
-    if (model == 0) run(lut0);
-    else run(g_lut + (size_t)model * kTot);
+    const uint32_t* lut = g_lut + (size_t)model * kTot;
+    for (uint32_t c = threadIdx.x; c < n; c += blockDim.x) {
+        Checkpoint& k = ck[br.ck_off + c];
+        const uint32_t s = k.sym, j = s / kSnap;
+        const uint2 z = sn[j];
+        uint32_t x = z.x, pos = z.y;
+        for (uint32_t t = j * kSnap; t < s; ++t) index_step(x, pos, enc, lut);
+        k.state = x;
+        k.pos = pos;
+    }
 }
 
 // Pass 1 from a seek-index sidecar: the state before every kSeedSymbols-th
@@ -875,7 +875,7 @@ cudaError_t launch_build_index(DeviceDataset& ds, cudaStream_t st, const IndexSe
     if (e == cudaSuccess) {
         index_book_kernel<<<(nb + 3) / 4, 128, 0, st>>>(ds.d_bricks, nb, t.nib, t.off, t.chain, ds.d_ck, t.nck, ds.L,
                                                        ds.S);
-        index_states_kernel<<<(nb + 3) / 4, 128, 0, st>>>(ds.d_bricks, nb, ds.d_enc, ds.d_lut, nm, t.off + nb,
+        index_states_kernel<<<nb, 128, 0, st>>>(ds.d_bricks, nb, ds.d_enc, ds.d_lut, nm, t.off + nb,
                                                          t.snap, t.nck, ds.d_ck);
         e = cudaGetLastError();
     }
