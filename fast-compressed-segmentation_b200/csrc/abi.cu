@@ -109,6 +109,27 @@ int abi_ensure_scratch_small(csv_ctx* ctx) {
     return CSV_OK;
 }
 
+int abi_ensure_scratch_wide(csv_ctx* ctx, uint32_t b) {
+    if (ctx->scr_wide.base && ctx->scr_wide_b >= b) return CSV_OK;
+    cudaFree(ctx->scr_wide.base);
+    cudaFree(ctx->scr_wide.d_queue);
+    ctx->scr_wide = DecodeScratch();
+    ctx->scr_wide_b = 0;
+    const size_t bytes = decode_scratch_wide_bytes(ctx->device, b);
+    cudaError_t e = cudaMalloc(&ctx->scr_wide.base, bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->scr_wide.d_queue, 64);
+    if (e != cudaSuccess) {
+        cudaFree(ctx->scr_wide.base);
+        ctx->scr_wide = DecodeScratch();
+        return abi_fail(ctx, CSV_ENOMEM, std::string("decode scratch: ") + cudaGetErrorString(e));
+    }
+    ctx->scr_wide.per_cta = decode_scratch_per_cta(b);  // the 64^3 variant's layout
+    ctx->scr_wide.ctas = (uint32_t)(bytes / ctx->scr_wide.per_cta);
+    ctx->scr_wide.bytes = bytes;
+    ctx->scr_wide_b = b;
+    return CSV_OK;
+}
+
 }  // namespace csv
 
 namespace {
@@ -401,6 +422,8 @@ void csv_destroy(csv_ctx* ctx) {
     cudaFree(ctx->scr.d_queue);
     cudaFree(ctx->scr_small.base);
     cudaFree(ctx->scr_small.d_queue);
+    cudaFree(ctx->scr_wide.base);
+    cudaFree(ctx->scr_wide.d_queue);
     for (int i = 0; i < 2; ++i) {
         cudaFree(ctx->chunk_buf[i]);
         if (ctx->pipe_stream[i]) cudaStreamDestroy(ctx->pipe_stream[i]);
@@ -824,11 +847,21 @@ namespace {
 // times the CTAs per SM; each part keeps the request order, or with `lpt` runs
 // largest first (estimated work = nSymbols of the brick, rANS + replay, plus a
 // quarter of the labels written).  ord = [large part | small part].
+// The requests in launch order: outputs above 32^3 whose brick has fewer than 255 palette entries (when
+// narrow8: the 8-bit variant's part, n8 of them), the other outputs above 32^3 (n_large in all, with the
+// first part), then the rest; each part longest first when lpt.
 int graph_schedule(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_reqs, uint32_t n, bool lpt,
-                   std::vector<uint32_t>& ord, uint32_t& n_large) {
+                   bool narrow8, std::vector<uint32_t>& ord, uint32_t& n8, uint32_t& n_large) {
     std::vector<csv_request> h(n);
     cudaError_t e = cudaMemcpy(h.data(), d_reqs, sizeof(csv_request) * n, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "request copy");
+    std::vector<uint8_t> small_pal(ds->d.nb, 0);
+    if (narrow8 && ds->d.nb) {
+        std::vector<BrickDesc> desc(ds->d.nb);
+        e = cudaMemcpy(desc.data(), ds->d.d_bricks, sizeof(BrickDesc) * ds->d.nb, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "brick table copy");
+        for (uint32_t i = 0; i < ds->d.nb; ++i) small_pal[i] = desc[i].P < 0xFFu;
+    }
     std::vector<uint64_t> cost(n);
     for (uint32_t i = 0; i < n; ++i) {
         uint64_t c = 0;
@@ -836,14 +869,19 @@ int graph_schedule(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_req
         cost[i] = c;
     }
     ord.clear();
+    auto narrow_req = [&](uint32_t i) { return h[i].brick < ds->d.nb && small_pal[h[i].brick]; };
     for (uint32_t i = 0; i < n; ++i)
-        if (h[i].lod > kSmallLod) ord.push_back(i);
+        if (h[i].lod > kSmallLod && narrow_req(i)) ord.push_back(i);
+    n8 = (uint32_t)ord.size();
+    for (uint32_t i = 0; i < n; ++i)
+        if (h[i].lod > kSmallLod && !narrow_req(i)) ord.push_back(i);
     n_large = (uint32_t)ord.size();
     for (uint32_t i = 0; i < n; ++i)
         if (h[i].lod <= kSmallLod) ord.push_back(i);
     if (lpt) {
         auto by_cost = [&](uint32_t a, uint32_t b) { return cost[a] > cost[b]; };
-        std::stable_sort(ord.begin(), ord.begin() + n_large, by_cost);
+        std::stable_sort(ord.begin(), ord.begin() + n8, by_cost);
+        std::stable_sort(ord.begin() + n8, ord.begin() + n_large, by_cost);
         std::stable_sort(ord.begin() + n_large, ord.end(), by_cost);
     }
     return CSV_OK;
@@ -862,7 +900,9 @@ int csv_decode_graph_create(csv_ctx* ctx, const csv_dataset* ds, const csv_reque
     int rc = ensure_scratch(ctx, ds->d.b);
     if (rc) return rc;
     decode_grid(ctx->device, 1);  // occupancy queries happen outside the capture
-    const bool split = ds->d.L > kSmallLod + 1 && n && !(cfg && cfg->layout != 0);
+    const uint32_t layout = cfg ? cfg->layout : 0;
+    if (layout > 2) return fail(ctx, CSV_EINVAL, "layout is 0, 1 or 2");
+    const bool split = ds->d.L > kSmallLod + 1 && n && layout != 1;
     if (split && (rc = abi_ensure_scratch_small(ctx))) return rc;
     csv_graph* gr = new (std::nothrow) csv_graph();
     if (!gr) return fail(ctx, CSV_ENOMEM, "host allocation");
@@ -873,12 +913,15 @@ int csv_decode_graph_create(csv_ctx* ctx, const csv_dataset* ds, const csv_reque
         dc.stage = cfg->stage;
         dc.layout = cfg->layout;
     }
-    // a dataset with 64^3 bricks: split the requests by output size (two launches), else one launch
-    uint32_t n_large = n;
+    // a dataset with 64^3 bricks: split the requests by output size and, for the outputs above 32^3, by
+    // palette size (up to three launches), else one launch
+    uint32_t n_large = n, n8 = 0;
     if (split || (cfg && cfg->lpt && n)) {
         std::vector<uint32_t> ord;
-        rc = graph_schedule(ctx, ds, d_reqs, n, cfg && cfg->lpt, ord, n_large);
-        if (!rc && !split) n_large = n;  // one part: all of them, in the scheduled order
+        rc = graph_schedule(ctx, ds, d_reqs, n, cfg && cfg->lpt, split && layout == 0, ord, n8, n_large);
+        if (!rc && !split) n_large = n, n8 = 0;  // one part: all of them, in the scheduled order
+        // the wide 64^3 part beside the 8-bit one needs scratch of its own
+        if (!rc && n8 && n_large > n8) rc = abi_ensure_scratch_wide(ctx, ds->d.b);
         cudaError_t e = rc ? cudaSuccess : cudaMalloc(&gr->d_order, sizeof(uint32_t) * n);
         if (!rc && e != cudaSuccess) rc = fail(ctx, CSV_ENOMEM, "order allocation");
         if (!rc && (e = cudaMemcpy(gr->d_order, ord.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice)) != cudaSuccess)
@@ -902,25 +945,38 @@ int csv_decode_graph_create(csv_ctx* ctx, const csv_dataset* ds, const csv_reque
             le = launch_decode(ds->d, d_reqs, n, d_out, d_status, ctx->scr, s, &dc);
             gr->kernels = n ? 1u : 0u;
         } else {
-            // the large outputs first (longest bricks), then the small ones at three times the
-            // occupancy.  With both parts present the second is a programmatic dependent of the
-            // first, with its own scratch and queue (reset before the first launch): its CTAs
-            // fill the SMs that the first launch's CTAs leave once its queue has run dry.
-            DecodeConfig part = dc;
-            part.n_order = n_large;
-            const bool both = n_large && n > n_large;
-            if (both) le = cudaMemsetAsync(ctx->scr_small.d_queue, 0, sizeof(uint32_t), s);
-            if (le == cudaSuccess && n_large) {
-                le = launch_decode(ds->d, d_reqs, n, d_out, d_status, ctx->scr, s, &part);
+            // the large outputs first (longest bricks; those with palettes below 255 entries in
+            // the 8-bit variant, three CTAs per SM, then the others), then the small ones at three
+            // times the occupancy.  Each launch after the first is a programmatic dependent of the
+            // one before, with its own scratch and queue (all reset before the first launch): its
+            // CTAs fill the SMs that the earlier launches' CTAs leave once their queues run dry.
+            struct Part {
+                uint32_t first, count;
+                bool narrow8, small;
+            };
+            const Part parts[3] = {{0, n8, true, false}, {n8, n_large - n8, false, false},
+                                   {n_large, n - n_large, false, true}};
+            const csv::DecodeScratch* scrs[3] = {&ctx->scr, n8 ? &ctx->scr_wide : &ctx->scr, &ctx->scr_small};
+            uint32_t n_parts = 0;
+            for (const Part& p : parts) n_parts += p.count > 0;
+            // each launch's queue: the first one's is reset by launch_decode, the others here
+            bool first = true;
+            for (int k = 0; k < 3 && le == cudaSuccess; ++k)
+                if (parts[k].count && !first) le = cudaMemsetAsync(scrs[k]->d_queue, 0, sizeof(uint32_t), s);
+                else if (parts[k].count) first = false;
+            first = true;
+            for (int k = 0; k < 3 && le == cudaSuccess; ++k) {
+                if (!parts[k].count) continue;
+                DecodeConfig part = dc;
+                part.order = gr->d_order + parts[k].first;
+                part.n_order = parts[k].count;
+                part.narrow8 = parts[k].narrow8;
+                part.small_only = parts[k].small;
+                part.pdl = !first;
+                // a part alone uses the context's main scratch
+                le = launch_decode(ds->d, d_reqs, n, d_out, d_status, n_parts == 1 ? ctx->scr : *scrs[k], s, &part);
                 ++gr->kernels;
-            }
-            part.order = gr->d_order + n_large;
-            part.n_order = n - n_large;
-            part.small_only = true;
-            part.pdl = both;
-            if (le == cudaSuccess && n > n_large) {
-                le = launch_decode(ds->d, d_reqs, n, d_out, d_status, both ? ctx->scr_small : ctx->scr, s, &part);
-                ++gr->kernels;
+                first = false;
             }
         }
         e = cudaStreamEndCapture(s, &gr->graph);
@@ -973,7 +1029,7 @@ int csv_decode_autotune(csv_ctx* ctx, const csv_dataset* ds, const csv_request* 
     csv_decode_config bestc{0, 1, 0, 0};
     int rc = CSV_OK;
     const uint32_t per_sm_options[] = {0, 2, 1};  // 0: as many CTAs as fit
-    const uint32_t n_layouts = ds->d.L > kSmallLod + 1 ? 2 : 1;  // layout matters with 64^3 bricks only
+    const uint32_t n_layouts = ds->d.L > kSmallLod + 1 ? 3 : 1;  // layout matters with 64^3 bricks only
     for (uint32_t layout = 0; layout < n_layouts && rc == CSV_OK; ++layout)
     for (uint32_t ps : per_sm_options) {
         for (uint32_t stage = 0; stage <= 1 && rc == CSV_OK; ++stage) {

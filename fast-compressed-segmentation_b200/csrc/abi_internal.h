@@ -17,6 +17,10 @@ struct csv_ctx {
     // the second launch of a split graph (outputs of 32^3 and smaller) runs beside the first
     // one's last CTAs, so it has scratch and a queue counter of its own; created on first use
     csv::DecodeScratch scr_small;
+    // the 64^3 outputs of bricks with 255 or more palette entries, when a split graph gives the
+    // others to the 8-bit variant: a third launch, beside the first; created on first use
+    csv::DecodeScratch scr_wide;
+    uint32_t scr_wide_b = 0;
     csv::EncoderState* enc = nullptr;
     // csv_decode_image's pipeline: two chunk buffers (decode one while the
     // other drains to the host), its streams and events; created on first use
@@ -40,6 +44,7 @@ int abi_cuda_fail(csv_ctx* ctx, cudaError_t e, const char* where);
 int abi_ensure_scratch(csv_ctx* ctx, uint32_t b);
 // Allocate the context's scratch for the small variant's part of a split schedule.
 int abi_ensure_scratch_small(csv_ctx* ctx);
+int abi_ensure_scratch_wide(csv_ctx* ctx, uint32_t b);
 // buildTransferFunctionBuffers (webgpuSetup.js:389-465) on a dataset: its distinct
 // non-zero palette labels ascending and their RGBA8, hidden labels transparent.
 cudaError_t transfer_function(const DeviceDataset& d, const uint64_t* hidden, uint32_t n_hidden,

@@ -128,6 +128,9 @@ size_t decode_scratch_per_cta(uint32_t b, uint32_t kl = 6);
 size_t decode_scratch_bytes(int device, uint32_t b);
 // Scratch for the small variant's CTAs at 32^3 outputs (the second part of a split schedule).
 size_t decode_scratch_small_bytes(int device);
+// Scratch for the 64^3 variant with 16- or 32-bit node values at its occupancy (the part of a split
+// schedule with the 64^3 bricks of 255 or more palette entries).
+size_t decode_scratch_wide_bytes(int device, uint32_t b);
 uint32_t decode_grid(int device, uint32_t n);
 // Requests at this LOD (32^3 labels) or coarser can run in the decode kernel's
 // small-footprint variant (six CTAs per SM instead of two).
@@ -140,7 +143,8 @@ struct DecodeConfig {
     uint32_t n_order = 0;             // entries of order (0: n)
     const uint32_t* n_dev = nullptr;  // device-resident queue length (<= n or n_order), or null
     bool small_only = false;          // every queued request is at LOD 5 (32^3) or coarser
-    uint32_t layout = 0;              // 1: every request in the small (six-CTA-per-SM) kernel
+    uint32_t layout = 0;              // 1: every request in the small (six-CTA-per-SM) kernel; 2: no 8-bit values
+    bool narrow8 = false;             // every queued request's brick has fewer than 255 palette entries
     // launched as a programmatic dependent of the previous kernel in the stream: its CTAs
     // start on the SMs that kernel's CTAs leave; the caller has reset scr.d_queue
     bool pdl = false;

@@ -46,12 +46,20 @@ namespace csv {
 // of a brick wait at each phase barrier, more bricks are in flight per SM)
 constexpr int kDecThreads = 320;      // the 32^3 variant: up to six CTAs per SM
 constexpr int kDecThreadsBig = 768;   // the 64^3 variant: two CTAs per SM
-template <uint32_t KL>
-__host__ __device__ constexpr int dec_threads() { return KL == 6 ? kDecThreadsBig : kDecThreads; }
+constexpr int kDecThreadsNarrow = 512;  // the 64^3 variant with 8-bit node values: three CTAs per SM
+// (8-bit node values halve the level arrays, so a third 64^3 brick fits per SM: mixed1024 replay
+// 2.385 -> 2.28 ms with its 64^3 bricks in it; four CTAs of 384 threads, the rANS table read through
+// L1 to make room, measured no faster than two of 768)
+template <class V, uint32_t KL>
+__host__ __device__ constexpr int dec_threads() {
+    return KL == 6 ? (sizeof(V) == 1 ? kDecThreadsNarrow : kDecThreadsBig) : kDecThreads;
+}
+template <class V, uint32_t KL>
+__host__ __device__ constexpr int dec_ctas_per_sm() { return KL == 6 ? (sizeof(V) == 1 ? 3 : 2) : 6; }
 constexpr uint32_t kDecLevels = 6;       // parent levels 0..5 (a 64^3 brick has 7 levels)
 constexpr uint32_t kPalCache = 1024;     // palettes up to this size are copied to shared memory
-template <uint32_t KL>
-__host__ __device__ constexpr uint32_t pal_cache() { return KL == 6 ? kPalCache : 512u; }
+template <class V, uint32_t KL>
+__host__ __device__ constexpr uint32_t pal_cache() { return sizeof(V) == 1 ? 256u : (KL == 6 ? kPalCache : 512u); }
 constexpr uint32_t REC_MISSING = OP_RP | 8u;
 
 // Node values of level l at val + voff(l): lvl_off rounded up to 8 entries (16 bytes for u16).
@@ -81,7 +89,7 @@ struct DecShared {
     alignas(16) V val[LevelDims<KL>::val];
     uint32_t mask[LevelDims<KL>::mask];
     uint16_t pre[LevelDims<KL>::mask];
-    uint64_t pal[pal_cache<KL>()];
+    uint64_t pal[pal_cache<V, KL>()];
     uint32_t warp_sums[1024 / 32 + 1];
     BrickDesc br;
     csv_request req;
@@ -95,6 +103,7 @@ template <class V, uint32_t KL>
 __host__ __device__ constexpr uint32_t stage_cap() {
     return (uint32_t)(sizeof(V) * LevelDims<KL>::val + 6 * LevelDims<KL>::mask) & ~15u;
 }
+static_assert((sizeof(uint8_t) * LevelDims<kDecLevels>::val) % 16 == 0, "mask follows val without padding");
 static_assert((sizeof(uint16_t) * LevelDims<kDecLevels>::val) % 16 == 0, "mask follows val without padding");
 static_assert((sizeof(uint16_t) * LevelDims<kSmallLevels>::val) % 16 == 0, "mask follows val without padding");
 
@@ -1178,10 +1187,11 @@ __device__ __forceinline__ void decode_segments(const DecodeArgs& A, const Brick
     }
 }
 
-// V = uint16_t when every palette of the dataset has fewer than 65535 entries
-// (value 0xFFFF stands for "label 0"), else uint32_t (one CTA per SM).
+// V = uint8_t when every requested brick's palette has fewer than 255 entries
+// (value 0xFF stands for "label 0"; 64^3 variant only), uint16_t when every
+// palette of the dataset has fewer than 65535 entries (0xFFFF), else uint32_t.
 template <class V, uint32_t KL>
-__global__ void __launch_bounds__(dec_threads<KL>(), KL == kDecLevels ? 2 : 6) decode_kernel(DecodeArgs A) {
+__global__ void __launch_bounds__(dec_threads<V, KL>(), dec_ctas_per_sm<V, KL>()) decode_kernel(DecodeArgs A) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     DecShared<V, KL>& S = *reinterpret_cast<DecShared<V, KL>*>(smem_raw);
     const uint32_t tid = threadIdx.x, T = blockDim.x;
@@ -1189,7 +1199,7 @@ __global__ void __launch_bounds__(dec_threads<KL>(), KL == kDecLevels ? 2 : 6) d
     // split schedule: other requests, other scratch) may start on the SMs this
     // grid's CTAs leave; without one this is a no-op.
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    constexpr uint32_t LABEL0 = sizeof(V) == 2 ? 0xFFFFu : PIDX_LABEL0;
+    constexpr uint32_t LABEL0 = sizeof(V) == 1 ? 0xFFu : (sizeof(V) == 2 ? 0xFFFFu : PIDX_LABEL0);
 
     for (uint32_t i = tid; i < kTot; i += T) S.lut[i] = A.lut[i];
     if (tid == 0) {
@@ -1264,7 +1274,7 @@ __global__ void __launch_bounds__(dec_threads<KL>(), KL == kDecLevels ? 2 : 6) d
         uint64_t* out = A.out + req.dst;
         const uint64_t* gpal = A.pal + br.pal_off;
         const uint64_t* pal = gpal;
-        if (br.P <= pal_cache<KL>()) {
+        if (br.P <= pal_cache<V, KL>()) {
             for (uint32_t i = tid; i < br.P; i += T) S.pal[i] = gpal[i];
             pal = S.pal;
         }
@@ -1341,11 +1351,14 @@ __global__ void __launch_bounds__(dec_threads<KL>(), KL == kDecLevels ? 2 : 6) d
                 if (lc < t) {
                     V* val_c = lc < KL ? S.val + voff(lc) : spill;
                     uint32_t* mask_c = S.mask + moff(lc);
-                    // children of stop-filled parents inherit (16 bytes of u16 or 2 x 16 of u32)
+                    // children of stop-filled parents inherit (8 bytes of u8, 16 of u16 or 2 x 16 of u32)
                     for (uint32_t p = tid; p < n_par; p += T) {
                         if (!is_active(Vw, p)) {
                             const uint32_t v = Vw.val[p];
-                            if (sizeof(V) == 2) {
+                            if (sizeof(V) == 1) {
+                                const uint32_t vv = v * 0x01010101u;
+                                reinterpret_cast<uint2*>(val_c + 8 * p)[0] = make_uint2(vv, vv);
+                            } else if (sizeof(V) == 2) {
                                 const uint32_t vv = v | (v << 16);
                                 reinterpret_cast<uint4*>(val_c + 8 * p)[0] = make_uint4(vv, vv, vv, vv);
                             } else {
@@ -1528,16 +1541,16 @@ size_t decode_scratch_per_cta(uint32_t b, uint32_t kl) {
     return (size_t)(rec_bytes + act_bytes + spill_bytes);
 }
 
-static int g_dec_occ[4][64] = {{0}};
+static int g_dec_occ[6][64] = {{0}};
 
 template <class V, uint32_t KL>
 static int occupancy(int device) {
-    int& occ = g_dec_occ[(sizeof(V) == 2 ? 0 : 1) + (KL == kDecLevels ? 0 : 2)][device & 63];
+    int& occ = g_dec_occ[(sizeof(V) == 1 ? 4 : sizeof(V) == 2 ? 0 : 1) + (KL == kDecLevels ? 0 : 2)][device & 63];
     if (occ == 0) {
         cudaFuncSetAttribute(decode_kernel<V, KL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(DecShared<V, KL>));
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, decode_kernel<V, KL>, dec_threads<KL>(),
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, decode_kernel<V, KL>, dec_threads<V, KL>(),
                                                       sizeof(DecShared<V, KL>));
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -1547,7 +1560,8 @@ static int occupancy(int device) {
 }
 
 uint32_t decode_grid(int device, uint32_t n) {
-    uint32_t occ = (uint32_t)std::max(occupancy<uint16_t, kDecLevels>(device), occupancy<uint32_t, kDecLevels>(device));
+    uint32_t occ = (uint32_t)std::max({occupancy<uint8_t, kDecLevels>(device), occupancy<uint16_t, kDecLevels>(device),
+                                       occupancy<uint32_t, kDecLevels>(device)});
     return n < occ ? n : occ;
 }
 
@@ -1559,6 +1573,11 @@ size_t decode_scratch_bytes(int device, uint32_t b) {
                          (size_t)std::max(occupancy<uint16_t, kSmallLevels>(device),
                                           occupancy<uint32_t, kSmallLevels>(device));
     return std::max(big, small);
+}
+
+size_t decode_scratch_wide_bytes(int device, uint32_t b) {
+    return decode_scratch_per_cta(b, kDecLevels) *
+           (size_t)std::max(occupancy<uint16_t, kDecLevels>(device), occupancy<uint32_t, kDecLevels>(device));
 }
 
 size_t decode_scratch_small_bytes(int device) {
@@ -1586,7 +1605,7 @@ static cudaError_t launch_variant(const DecodeArgs& A0, const DecodeScratch& scr
     if (cfg && cfg->pdl) {
         cudaLaunchConfig_t lc = {};
         lc.gridDim = dim3(grid);
-        lc.blockDim = dim3(dec_threads<KL>());
+        lc.blockDim = dim3(dec_threads<V, KL>());
         lc.dynamicSmemBytes = sizeof(DecShared<V, KL>);
         lc.stream = st;
         cudaLaunchAttribute at[1];
@@ -1596,7 +1615,7 @@ static cudaError_t launch_variant(const DecodeArgs& A0, const DecodeScratch& scr
         lc.numAttrs = 1;
         return cudaLaunchKernelEx(&lc, decode_kernel<V, KL>, A);
     }
-    decode_kernel<V, KL><<<grid, dec_threads<KL>(), sizeof(DecShared<V, KL>), st>>>(A);
+    decode_kernel<V, KL><<<grid, dec_threads<V, KL>(), sizeof(DecShared<V, KL>), st>>>(A);
     return cudaGetLastError();
 }
 
@@ -1605,6 +1624,9 @@ cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, ui
     if (n == 0) return cudaSuccess;
     if (ds.L > kDecLevels + 1) return cudaErrorInvalidValue;  // bricks up to 64^3
     const bool narrow = ds.max_P < 0xFFFFu;
+    // 8-bit node values (64^3 variant): every palette of the dataset, or of the requested bricks (the
+    // caller's word, from a schedule that split the requests by palette size), below 255 entries
+    const bool narrow8 = (ds.max_P < 0xFFu || (cfg && cfg->narrow8)) && !(cfg && cfg->layout == 2);
     // the small variant when the dataset's bricks are 32^3 or smaller, when the caller
     // says every request is at LOD 5 or coarser, or when asked to take every request
     const bool small = ds.L <= kSmallLevels + 1 || (cfg && (cfg->small_only || cfg->layout == 1));
@@ -1639,6 +1661,7 @@ cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, ui
         if (narrow) return launch_variant<uint16_t, kSmallLevels>(A, scr, st, cfg, ds.device);
         return launch_variant<uint32_t, kSmallLevels>(A, scr, st, cfg, ds.device);
     }
+    if (narrow8) return launch_variant<uint8_t, kDecLevels>(A, scr, st, cfg, ds.device);
     if (narrow) return launch_variant<uint16_t, kDecLevels>(A, scr, st, cfg, ds.device);
     return launch_variant<uint32_t, kDecLevels>(A, scr, st, cfg, ds.device);
 }

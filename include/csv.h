@@ -198,10 +198,12 @@ int csv_dataset_concat(csv_ctx* ctx, const csv_dataset* const* parts, uint32_t n
  * stage each brick's compressed stream in shared memory by a bulk copy), lpt
  * (1 = hand out the largest bricks first: a request permutation computed at
  * creation), layout (for datasets with 64^3 bricks: 0 = requests above LOD 5
- * in the decode kernel that holds every level in shared memory, two CTAs per
- * SM, then the rest in the six-CTA-per-SM kernel, as two launches; 1 = every
- * request in the six-CTA kernel, which keeps a 64^3 brick's last parent
- * level in its global scratch). */
+ * in the decode kernel that holds every level in shared memory -- those whose
+ * brick has fewer than 255 palette entries with 8-bit node values, three CTAs
+ * per SM, the others with 16- or 32-bit values, two CTAs per SM -- then the
+ * rest in the six-CTA-per-SM kernel, up to three launches; 1 = every request
+ * in the six-CTA kernel, which keeps a 64^3 brick's last parent level in its
+ * global scratch; 2 = as 0 without the 8-bit part). */
 typedef struct csv_decode_config {
     uint32_t ctas_per_sm;
     uint32_t stage;
@@ -214,12 +216,13 @@ typedef struct csv_graph csv_graph;
 int csv_decode_graph_create(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_reqs, uint32_t n,
                             uint64_t* d_out, uint32_t* d_status, const csv_decode_config* cfg, csv_graph** out);
 int csv_graph_launch(csv_graph* g, void* stream);
-/* Decode kernels one replay of the graph launches (1, or 2 when it splits the
- * requests by output size; 0 for an empty batch).  In a split replay the second
- * kernel may start while the first one's last bricks are still decoding; the
- * replay as a whole still completes in stream order like any other graph launch.
- * A split graph uses a second decode scratch of the context (allocated on the
- * first split graph's creation), so graphs of one context replay one at a time. */
+/* Decode kernels one replay of the graph launches (1; 2 or 3 when it splits the
+ * requests by output size and palette size; 0 for an empty batch).  In a split
+ * replay each kernel may start while the one before still has bricks decoding;
+ * the replay as a whole still completes in stream order like any other graph
+ * launch.  A split graph uses further decode scratch of the context (allocated
+ * on the first split graph's creation that needs it), so graphs of one context
+ * replay one at a time. */
 int csv_graph_kernels(const csv_graph* g, uint32_t* n);
 void csv_graph_destroy(csv_graph* g);
 /* Times every candidate configuration on this batch (a captured graph each,
