@@ -46,10 +46,10 @@ namespace csv {
 // of a brick wait at each phase barrier, more bricks are in flight per SM)
 constexpr int kDecThreads = 320;      // the 32^3 variant: up to six CTAs per SM
 constexpr int kDecThreadsBig = 768;   // the 64^3 variant: two CTAs per SM
-constexpr int kDecThreadsNarrow = 512;  // the 64^3 variant with 8-bit node values: three CTAs per SM
+constexpr int kDecThreadsNarrow = 640;  // the 64^3 variant with 8-bit node values: three CTAs per SM
 // (8-bit node values halve the level arrays, so a third 64^3 brick fits per SM: mixed1024 replay
-// 2.385 -> 2.28 ms with its 64^3 bricks in it; four CTAs of 384 threads, the rANS table read through
-// L1 to make room, measured no faster than two of 768)
+// 2.385 -> 2.29 ms with its 64^3 bricks in it at 512 threads, 2.27 at 640; four CTAs of 384 threads,
+// the rANS table read through L1 to make room, measured no faster than two of 768)
 template <class V, uint32_t KL>
 __host__ __device__ constexpr int dec_threads() {
     return KL == 6 ? (sizeof(V) == 1 ? kDecThreadsNarrow : kDecThreadsBig) : kDecThreads;
