@@ -849,9 +849,10 @@ namespace {
 // quarter of the labels written).  ord = [large part | small part].
 // The requests in launch order: outputs above 32^3 whose brick has fewer than 255 palette entries (when
 // narrow8: the 8-bit variant's part, n8 of them), the other outputs above 32^3 (n_large in all, with the
-// first part), then the rest; each part longest first when lpt.
+// first part), then the rest (small8: every one of them with fewer than 255 palette entries, when
+// narrow8); each part longest first when lpt.
 int graph_schedule(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_reqs, uint32_t n, bool lpt,
-                   bool narrow8, std::vector<uint32_t>& ord, uint32_t& n8, uint32_t& n_large) {
+                   bool narrow8, std::vector<uint32_t>& ord, uint32_t& n8, uint32_t& n_large, bool& small8) {
     std::vector<csv_request> h(n);
     cudaError_t e = cudaMemcpy(h.data(), d_reqs, sizeof(csv_request) * n, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "request copy");
@@ -876,8 +877,12 @@ int graph_schedule(csv_ctx* ctx, const csv_dataset* ds, const csv_request* d_req
     for (uint32_t i = 0; i < n; ++i)
         if (h[i].lod > kSmallLod && !narrow_req(i)) ord.push_back(i);
     n_large = (uint32_t)ord.size();
+    small8 = narrow8;
     for (uint32_t i = 0; i < n; ++i)
-        if (h[i].lod <= kSmallLod) ord.push_back(i);
+        if (h[i].lod <= kSmallLod) {
+            ord.push_back(i);
+            small8 = small8 && narrow_req(i);
+        }
     if (lpt) {
         auto by_cost = [&](uint32_t a, uint32_t b) { return cost[a] > cost[b]; };
         std::stable_sort(ord.begin(), ord.begin() + n8, by_cost);
@@ -916,10 +921,11 @@ int csv_decode_graph_create(csv_ctx* ctx, const csv_dataset* ds, const csv_reque
     // a dataset with 64^3 bricks: split the requests by output size and, for the outputs above 32^3, by
     // palette size (up to three launches), else one launch
     uint32_t n_large = n, n8 = 0;
+    bool small8 = false;
     if (split || (cfg && cfg->lpt && n)) {
         std::vector<uint32_t> ord;
-        rc = graph_schedule(ctx, ds, d_reqs, n, cfg && cfg->lpt, split && layout == 0, ord, n8, n_large);
-        if (!rc && !split) n_large = n, n8 = 0;  // one part: all of them, in the scheduled order
+        rc = graph_schedule(ctx, ds, d_reqs, n, cfg && cfg->lpt, split && layout == 0, ord, n8, n_large, small8);
+        if (!rc && !split) n_large = n, n8 = 0, small8 = false;  // one part: all of them, in the scheduled order
         // the wide 64^3 part beside the 8-bit one needs scratch of its own
         if (!rc && n8 && n_large > n8) rc = abi_ensure_scratch_wide(ctx, ds->d.b);
         cudaError_t e = rc ? cudaSuccess : cudaMalloc(&gr->d_order, sizeof(uint32_t) * n);
@@ -955,7 +961,7 @@ int csv_decode_graph_create(csv_ctx* ctx, const csv_dataset* ds, const csv_reque
                 bool narrow8, small;
             };
             const Part parts[3] = {{0, n8, true, false}, {n8, n_large - n8, false, false},
-                                   {n_large, n - n_large, false, true}};
+                                   {n_large, n - n_large, small8, true}};
             const csv::DecodeScratch* scrs[3] = {&ctx->scr, n8 ? &ctx->scr_wide : &ctx->scr, &ctx->scr_small};
             uint32_t n_parts = 0;
             for (const Part& p : parts) n_parts += p.count > 0;

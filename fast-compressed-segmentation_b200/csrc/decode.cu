@@ -50,12 +50,17 @@ constexpr int kDecThreadsNarrow = 640;  // the 64^3 variant with 8-bit node valu
 // (8-bit node values halve the level arrays, so a third 64^3 brick fits per SM: mixed1024 replay
 // 2.385 -> 2.29 ms with its 64^3 bricks in it at 512 threads, 2.27 at 640; four CTAs of 384 threads,
 // the rANS table read through L1 to make room, measured no faster than two of 768)
+// the 32^3 variant with 8-bit node values: seven CTAs per SM (mixed1024 replay 2.27 -> 2.19 ms)
+constexpr int kDecThreadsSmallNarrow = 288;
 template <class V, uint32_t KL>
 __host__ __device__ constexpr int dec_threads() {
-    return KL == 6 ? (sizeof(V) == 1 ? kDecThreadsNarrow : kDecThreadsBig) : kDecThreads;
+    return KL == 6 ? (sizeof(V) == 1 ? kDecThreadsNarrow : kDecThreadsBig)
+                   : (sizeof(V) == 1 ? kDecThreadsSmallNarrow : kDecThreads);
 }
 template <class V, uint32_t KL>
-__host__ __device__ constexpr int dec_ctas_per_sm() { return KL == 6 ? (sizeof(V) == 1 ? 3 : 2) : 6; }
+__host__ __device__ constexpr int dec_ctas_per_sm() {
+    return KL == 6 ? (sizeof(V) == 1 ? 3 : 2) : (sizeof(V) == 1 ? 7 : 6);
+}
 constexpr uint32_t kDecLevels = 6;       // parent levels 0..5 (a 64^3 brick has 7 levels)
 constexpr uint32_t kPalCache = 1024;     // palettes up to this size are copied to shared memory
 template <class V, uint32_t KL>
@@ -1188,7 +1193,7 @@ __device__ __forceinline__ void decode_segments(const DecodeArgs& A, const Brick
 }
 
 // V = uint8_t when every requested brick's palette has fewer than 255 entries
-// (value 0xFF stands for "label 0"; 64^3 variant only), uint16_t when every
+// (value 0xFF stands for "label 0"), uint16_t when every
 // palette of the dataset has fewer than 65535 entries (0xFFFF), else uint32_t.
 template <class V, uint32_t KL>
 __global__ void __launch_bounds__(dec_threads<V, KL>(), dec_ctas_per_sm<V, KL>()) decode_kernel(DecodeArgs A) {
@@ -1545,7 +1550,7 @@ static int g_dec_occ[6][64] = {{0}};
 
 template <class V, uint32_t KL>
 static int occupancy(int device) {
-    int& occ = g_dec_occ[(sizeof(V) == 1 ? 4 : sizeof(V) == 2 ? 0 : 1) + (KL == kDecLevels ? 0 : 2)][device & 63];
+    int& occ = g_dec_occ[2 * (sizeof(V) == 1 ? 2 : sizeof(V) == 2 ? 0 : 1) + (KL == kDecLevels ? 0 : 1)][device & 63];
     if (occ == 0) {
         cudaFuncSetAttribute(decode_kernel<V, KL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(DecShared<V, KL>));
@@ -1570,8 +1575,9 @@ uint32_t decode_grid(int device, uint32_t n) {
 size_t decode_scratch_bytes(int device, uint32_t b) {
     const size_t big = decode_scratch_per_cta(b, kDecLevels) * (size_t)decode_grid(device, 0xFFFFFFFFu);
     const size_t small = decode_scratch_per_cta(b, kSmallLevels) *
-                         (size_t)std::max(occupancy<uint16_t, kSmallLevels>(device),
-                                          occupancy<uint32_t, kSmallLevels>(device));
+                         (size_t)std::max({occupancy<uint8_t, kSmallLevels>(device),
+                                           occupancy<uint16_t, kSmallLevels>(device),
+                                           occupancy<uint32_t, kSmallLevels>(device)});
     return std::max(big, small);
 }
 
@@ -1582,7 +1588,8 @@ size_t decode_scratch_wide_bytes(int device, uint32_t b) {
 
 size_t decode_scratch_small_bytes(int device) {
     return decode_scratch_per_cta(1u << kSmallLevels, kSmallLevels) *
-           (size_t)std::max(occupancy<uint16_t, kSmallLevels>(device), occupancy<uint32_t, kSmallLevels>(device));
+           (size_t)std::max({occupancy<uint8_t, kSmallLevels>(device), occupancy<uint16_t, kSmallLevels>(device),
+                             occupancy<uint32_t, kSmallLevels>(device)});
 }
 
 template <class V, uint32_t KL>
@@ -1624,8 +1631,8 @@ cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, ui
     if (n == 0) return cudaSuccess;
     if (ds.L > kDecLevels + 1) return cudaErrorInvalidValue;  // bricks up to 64^3
     const bool narrow = ds.max_P < 0xFFFFu;
-    // 8-bit node values (64^3 variant): every palette of the dataset, or of the requested bricks (the
-    // caller's word, from a schedule that split the requests by palette size), below 255 entries
+    // 8-bit node values: every palette of the dataset, or of the requested bricks (the caller's word,
+    // from a schedule that split the requests by palette size), below 255 entries
     const bool narrow8 = (ds.max_P < 0xFFu || (cfg && cfg->narrow8)) && !(cfg && cfg->layout == 2);
     // the small variant when the dataset's bricks are 32^3 or smaller, when the caller
     // says every request is at LOD 5 or coarser, or when asked to take every request
@@ -1658,6 +1665,7 @@ cudaError_t launch_decode(const DeviceDataset& ds, const csv_request* d_reqs, ui
     A.stage_cap = 0;
     A.n_models = ds.n_models ? ds.n_models : 1u;
     if (small) {
+        if (narrow8) return launch_variant<uint8_t, kSmallLevels>(A, scr, st, cfg, ds.device);
         if (narrow) return launch_variant<uint16_t, kSmallLevels>(A, scr, st, cfg, ds.device);
         return launch_variant<uint32_t, kSmallLevels>(A, scr, st, cfg, ds.device);
     }

@@ -258,9 +258,10 @@ def test_graph_reports_its_kernels(codec, mixed):
 
 def test_graph_three_parts_by_palette_size(codec, oracle):
     """64^3 outputs of bricks with fewer than 255 palette entries go to the 8-bit variant (three CTAs per SM),
-    the other 64^3 outputs to the 16-bit one, and 32^3 and coarser outputs to the six-CTA kernel: three
-    launches (layout 0), two without the 8-bit part (layout 2), one with layout 1; every output equals the
-    oracle's, and so does one csv_decode_batch of the same requests."""
+    the other 64^3 outputs to the 16-bit one, and 32^3 and coarser outputs to the small kernel (8-bit values,
+    seven CTAs per SM, when all of them have small palettes; else 16-bit, six): three launches (layout 0),
+    two without the 8-bit part (layout 2), one with layout 1; every output equals the oracle's, and so does
+    one csv_decode_batch of the same requests."""
     import torch
     from csvb200 import requests, requests_tensor
     imgs = []
@@ -319,6 +320,22 @@ def test_graph_three_parts_by_palette_size(codec, oracle):
     codec.decode_batch(cat, requests_tensor(reqs), out, st)
     torch.cuda.synchronize()
     check(out.cpu().numpy().view(np.uint64), st.cpu().numpy())
+    # requests of the small-palette bricks only: both launches (64^3 outputs, then 32^3 and coarser) take
+    # 8-bit node values
+    bricks = np.concatenate([np.arange(3), rng.integers(0, 3, 30)])
+    lods = np.concatenate([np.full(3, 6), rng.integers(0, 6, 30)])
+    sizes = 8 ** lods.astype(np.uint64)
+    dst = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.uint64)
+    reqs = requests(bricks, lods, dst)
+    total = int(sizes.sum())
+    out = torch.full((total,), -3, dtype=torch.int64, device="cuda")
+    st = torch.full((len(reqs),), -1, dtype=torch.int32, device="cuda")
+    g = codec.decode_graph(cat, requests_tensor(reqs), out, st, DecodeConfig(0, 1, 0, 0))
+    assert g.kernels == 2
+    g.launch()
+    torch.cuda.synchronize()
+    check(out.cpu().numpy().view(np.uint64), st.cpu().numpy())
+    g.close()
     cat.close()
     for d in dss:
         d.close()
