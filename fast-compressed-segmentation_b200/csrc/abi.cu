@@ -150,6 +150,7 @@ uint32_t rd32(const uint8_t* p) {
 // brick's table (bits 4..7) and encoding mode (bits 0..3).
 struct ImageView {
     uint32_t version = 1, nb = 0, b = 0, total = 0, n_tables = 1;
+    size_t image_len = 0;  // bytes up to the end of the last brick record
     uint32_t freq[16][16], cum[16][16];
     struct Rec {
         size_t pal_at, enc_at;
@@ -218,6 +219,7 @@ int parse_image(csv_ctx* ctx, const uint8_t* img, size_t len, ImageView& v) {
         r.nsym = rd32(img + o);
         o += 4;
     }
+    v.image_len = o;
     return CSV_OK;
 }
 
@@ -232,6 +234,26 @@ void free_dataset(DeviceDataset& d) {
     d = DeviceDataset();
 }
 
+
+// The image's palettes and streams into their device pools: one block per brick, from a device copy of
+// the image (records are byte-aligned there: a palette entry is read a byte at a time).
+__global__ void __launch_bounds__(128) stage_gather_kernel(const uint8_t* __restrict__ img,
+                                                          const uint64_t* __restrict__ src,
+                                                          const BrickDesc* __restrict__ bricks, uint32_t nb,
+                                                          uint64_t* __restrict__ pal, uint8_t* __restrict__ enc) {
+    const uint32_t i = blockIdx.x;
+    if (i >= nb) return;
+    const BrickDesc& b = bricks[i];
+    const uint8_t* ps = img + src[2 * i];
+    for (uint32_t k = threadIdx.x; k < b.P; k += blockDim.x) {
+        uint64_t x = 0;
+#pragma unroll
+        for (int j = 7; j >= 0; --j) x = (x << 8) | ps[8ull * k + j];
+        pal[b.pal_off + k] = x;
+    }
+    const uint8_t* es = img + src[2 * i + 1];
+    for (uint32_t j = threadIdx.x; j < b.E; j += blockDim.x) enc[b.enc_off + j] = es[j];
+}
 
 int stage_dataset(csv_ctx* ctx, const uint8_t* img, const ImageView& v, DeviceDataset& d, cudaStream_t st) {
     d.device = ctx->device;
@@ -275,32 +297,47 @@ int stage_dataset(csv_ctx* ctx, const uint8_t* img, const ImageView& v, DeviceDa
     d.ck_entries = ck_n;
     d.enc_pool_bytes = std::max<uint64_t>(16, enc_n);
     d.pal_pool_entries = std::max<uint64_t>(1, pal_n);
-    std::vector<uint64_t> pal(std::max<uint64_t>(1, pal_n));
-    std::vector<uint8_t> enc(std::max<uint64_t>(16, enc_n), 0);
+    // where each brick's palette and stream start in the image (the pools are gathered on the device
+    // from one copy of the image, instead of repacked on the host)
+    std::vector<uint64_t> src(2 * (size_t)std::max<uint32_t>(1, v.nb));
     for (uint32_t i = 0; i < v.nb; ++i) {
-        const auto& r = v.recs[i];
-        memcpy(pal.data() + desc[i].pal_off, img + r.pal_at, 8ull * r.P);
-        memcpy(enc.data() + desc[i].enc_off, img + r.enc_at, r.E);
+        src[2 * i] = v.recs[i].pal_at;
+        src[2 * i + 1] = v.recs[i].enc_at;
     }
     std::vector<uint32_t> lut((size_t)kTot * v.n_tables);
     for (uint32_t t = 0; t < v.n_tables; ++t) build_lut(v.freq[t], v.cum[t], &lut[(size_t)t * kTot]);
     d.fast_models = lut_fast_mask(lut.data(), v.n_tables);
     cudaError_t e;
     if ((e = cudaMalloc(&d.d_bricks, sizeof(BrickDesc) * std::max<uint32_t>(1, v.nb))) != cudaSuccess ||
-        (e = cudaMalloc(&d.d_pal, 8 * pal.size())) != cudaSuccess ||
-        (e = cudaMalloc(&d.d_enc, enc.size())) != cudaSuccess ||
+        (e = cudaMalloc(&d.d_pal, 8 * d.pal_pool_entries)) != cudaSuccess ||
+        (e = cudaMalloc(&d.d_enc, d.enc_pool_bytes)) != cudaSuccess ||
         (e = cudaMalloc(&d.d_ck, sizeof(Checkpoint) * std::max<uint64_t>(1, ck_n))) != cudaSuccess ||
         (e = cudaMalloc(&d.d_lut, sizeof(uint32_t) * lut.size())) != cudaSuccess)
         return fail(ctx, CSV_ENOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
-    if ((e = cudaMemcpyAsync(d.d_bricks, desc.data(), sizeof(BrickDesc) * v.nb, cudaMemcpyHostToDevice, st)) !=
-            cudaSuccess ||
-        (e = cudaMemcpyAsync(d.d_pal, pal.data(), 8 * pal.size(), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(d.d_enc, enc.data(), enc.size(), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(d.d_lut, lut.data(), sizeof(uint32_t) * lut.size(), cudaMemcpyHostToDevice, st)) !=
-            cudaSuccess)
-        return cuda_fail(ctx, e, "staging copy");
+    uint8_t* d_img = nullptr;
+    uint64_t* d_src = nullptr;
+    if ((e = cudaMallocAsync((void**)&d_img, std::max<size_t>(1, v.image_len), st)) != cudaSuccess ||
+        (e = cudaMallocAsync((void**)&d_src, 8 * src.size(), st)) != cudaSuccess) {
+        cudaFreeAsync(d_img, st);
+        cudaStreamSynchronize(st);
+        return fail(ctx, CSV_ENOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
+    }
+    if ((e = cudaMemcpyAsync(d.d_bricks, desc.data(), sizeof(BrickDesc) * v.nb, cudaMemcpyHostToDevice, st)) ==
+            cudaSuccess &&
+        (e = cudaMemcpyAsync(d_img, img, v.image_len, cudaMemcpyHostToDevice, st)) == cudaSuccess &&
+        (e = cudaMemcpyAsync(d_src, src.data(), 8 * src.size(), cudaMemcpyHostToDevice, st)) == cudaSuccess &&
+        (e = cudaMemcpyAsync(d.d_lut, lut.data(), sizeof(uint32_t) * lut.size(), cudaMemcpyHostToDevice, st)) ==
+            cudaSuccess &&
+        (e = cudaMemsetAsync(d.d_enc, 0, d.enc_pool_bytes, st)) == cudaSuccess && v.nb) {
+        stage_gather_kernel<<<v.nb, 128, 0, st>>>(d_img, d_src, d.d_bricks, v.nb, d.d_pal, d.d_enc);
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(d_img, st);
+    cudaFreeAsync(d_src, st);
     // the host vectors go out of scope: finish the copies first
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "staging copy");
+    const cudaError_t e2 = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "staging copy");
     return CSV_OK;
 }
 
