@@ -46,12 +46,14 @@ namespace csv {
 // of a brick wait at each phase barrier, more bricks are in flight per SM)
 constexpr int kDecThreads = 320;      // the 32^3 variant: up to six CTAs per SM
 constexpr int kDecThreadsBig = 768;   // the 64^3 variant: two CTAs per SM
-constexpr int kDecThreadsNarrow = 640;  // the 64^3 variant with 8-bit node values: three CTAs per SM
-// (8-bit node values halve the level arrays, so a third 64^3 brick fits per SM: mixed1024 replay
-// 2.385 -> 2.29 ms with its 64^3 bricks in it at 512 threads, 2.27 at 640; four CTAs of 384 threads,
-// the rANS table read through L1 to make room, measured no faster than two of 768)
-// the 32^3 variant with 8-bit node values: seven CTAs per SM (mixed1024 replay 2.27 -> 2.19 ms)
-constexpr int kDecThreadsSmallNarrow = 288;
+constexpr int kDecThreadsNarrow = 512;  // the 64^3 variant with 8-bit node values: four CTAs per SM
+// (8-bit node values halve the level arrays, so more 64^3 bricks fit per SM: mixed1024 replay 2.385 ->
+// 2.29 ms at three CTAs of 512 threads, 2.27 at three of 640; with the compact rANS table below, four
+// of 512 and the 32^3 variant at nine of 224: 2.196 -> 2.144 ms.  Four CTAs of 384 threads with the
+// full table read through L1 instead measured no faster than two of 768)
+// the 32^3 variant with 8-bit node values: nine CTAs per SM (seven of 288 threads with the full rANS
+// table: mixed1024 replay 2.27 -> 2.19 ms)
+constexpr int kDecThreadsSmallNarrow = 224;
 template <class V, uint32_t KL>
 __host__ __device__ constexpr int dec_threads() {
     return KL == 6 ? (sizeof(V) == 1 ? kDecThreadsNarrow : kDecThreadsBig)
@@ -59,7 +61,7 @@ __host__ __device__ constexpr int dec_threads() {
 }
 template <class V, uint32_t KL>
 __host__ __device__ constexpr int dec_ctas_per_sm() {
-    return KL == 6 ? (sizeof(V) == 1 ? 3 : 2) : (sizeof(V) == 1 ? 7 : 6);
+    return KL == 6 ? (sizeof(V) == 1 ? 4 : 2) : (sizeof(V) == 1 ? 9 : 6);
 }
 constexpr uint32_t kDecLevels = 6;       // parent levels 0..5 (a 64^3 brick has 7 levels)
 constexpr uint32_t kPalCache = 1024;     // palettes up to this size are copied to shared memory
@@ -85,9 +87,16 @@ struct LevelDims {
     static constexpr uint32_t mask = moff(kDecLevels);   // 1172
 };
 
+// The 8-bit variants keep the rANS table compact in shared memory: a symbol byte per x (4 KB) and
+// the 16 symbols' entries after it (an entry, symbol | freq << 4 | start << 17, depends only on the
+// symbol, so this is exact for every table), one more dependent load per step for 12 KB less per CTA.
+template <class V>
+__host__ __device__ constexpr bool compact_lut() { return sizeof(V) == 1; }
+constexpr uint32_t kLutCompactWords = kTot / 4 + 16;
+
 template <class V, uint32_t KL>
 struct DecShared {
-    uint32_t lut[kTot];
+    uint32_t lut[compact_lut<V>() ? kLutCompactWords : kTot];
     // During the rANS phase the level arrays (val, mask, pre: contiguous) are
     // idle: the brick's compressed stream is staged over them by one bulk
     // (TMA) copy when it fits (stage_cap bytes).
@@ -173,11 +182,12 @@ uint32_t lut_fast_mask(const uint32_t* h_lut, uint32_t n) {
 // One rANS decode step (ransDecodeSymbol, brickDecoding.cpp:137-151), totalFreq
 // 4096 so % and / are a mask and a shift.  GLOBAL: enc is global memory (read
 // through the non-coherent path); otherwise a generic pointer (shared staging).
-template <bool GLOBAL = true>
+template <bool GLOBAL = true, bool CLUT = false>
 __device__ __forceinline__ uint32_t rans_step(uint32_t& x, uint32_t& pos, const uint8_t* __restrict__ enc,
                                               const uint32_t* __restrict__ lut) {
     uint32_t v = x & (kTot - 1);
-    uint32_t e = lut[v];
+    // CLUT: the compact table (symbol bytes, then the 16 entries)
+    uint32_t e = CLUT ? lut[kTot / 4 + reinterpret_cast<const uint8_t*>(lut)[v]] : lut[v];
     uint32_t f = (e >> 4) & 0x1FFFu, st = e >> 17;
     x = f * (x >> kTotBits) + v - st;
     // renormalisation (the reference's while loop): in a well-formed stream it
@@ -1086,14 +1096,14 @@ __device__ __forceinline__ uint64_t label_of(const uint64_t* pal, uint32_t pidx,
 // iteration, so the lanes of a warp never differ in steps per iteration.
 // One op of a segment whose symbols are all in the stream: a Pd op reads its
 // delta nibble in the same call.  Returns the op's record.
-template <bool GLOBAL>
+template <bool GLOBAL, bool CLUT>
 __device__ __forceinline__ uint32_t decode_op(uint32_t& x, uint32_t& pos, uint32_t& ip, const uint8_t* enc,
                                               const uint32_t* lut, uint32_t P, uint32_t& st, uint32_t LABEL0) {
-    const uint32_t v = rans_step<GLOBAL>(x, pos, enc, lut);
+    const uint32_t v = rans_step<GLOBAL, CLUT>(x, pos, enc, lut);
     const uint32_t code = v >> 1, stop = (v & 1u) << 3;
     uint32_t pidx;
     if (code == OP_PD) {
-        pidx = ip - rans_step<GLOBAL>(x, pos, enc, lut) - 1;
+        pidx = ip - rans_step<GLOBAL, CLUT>(x, pos, enc, lut) - 1;
     } else {
         ip += (code == OP_PA);
         pidx = (code == OP_PA || code == OP_P0) ? ip : 0u;
@@ -1109,7 +1119,7 @@ __device__ __forceinline__ uint32_t decode_op(uint32_t& x, uint32_t& pos, uint32
     return code | stop | (pidx << REC_PIDX_SHIFT);
 }
 
-template <bool GLOBAL>
+template <bool GLOBAL, bool CLUT>
 __device__ __forceinline__ void decode_segments(const DecodeArgs& A, const BrickDesc& br, const uint8_t* enc,
                                                 const uint32_t* lut, uint32_t n_need, uint32_t nseg,
                                                 uint32_t* __restrict__ recs, uint32_t& st, uint32_t LABEL0) {
@@ -1127,10 +1137,10 @@ __device__ __forceinline__ void decode_segments(const DecodeArgs& A, const Brick
             const uint32_t sym0 = sym;
             uint32_t n4 = (jend - j) & ~3u;
             for (uint32_t e = j + n4; j < e; j += 4) {
-                const uint32_t r0 = decode_op<GLOBAL>(x, pos, ip, enc, lut, br.P, st, LABEL0);
-                const uint32_t r1 = decode_op<GLOBAL>(x, pos, ip, enc, lut, br.P, st, LABEL0);
-                const uint32_t r2 = decode_op<GLOBAL>(x, pos, ip, enc, lut, br.P, st, LABEL0);
-                const uint32_t r3 = decode_op<GLOBAL>(x, pos, ip, enc, lut, br.P, st, LABEL0);
+                const uint32_t r0 = decode_op<GLOBAL, CLUT>(x, pos, ip, enc, lut, br.P, st, LABEL0);
+                const uint32_t r1 = decode_op<GLOBAL, CLUT>(x, pos, ip, enc, lut, br.P, st, LABEL0);
+                const uint32_t r2 = decode_op<GLOBAL, CLUT>(x, pos, ip, enc, lut, br.P, st, LABEL0);
+                const uint32_t r3 = decode_op<GLOBAL, CLUT>(x, pos, ip, enc, lut, br.P, st, LABEL0);
                 reinterpret_cast<uint4*>(recs + j)[0] = make_uint4(r0, r1, r2, r3);
                 n4 += (r0 & 7u) == OP_PD;  // symbols: one per op plus one per Pd
                 n4 += (r1 & 7u) == OP_PD;
@@ -1155,7 +1165,7 @@ __device__ __forceinline__ void decode_segments(const DecodeArgs& A, const Brick
                 }
                 break;
             }
-            const uint32_t v = rans_step<GLOBAL>(x, pos, enc, lut);
+            const uint32_t v = rans_step<GLOBAL, CLUT>(x, pos, enc, lut);
             ++sym;
             uint32_t rec;
             if (pd_stop != 0xFFFFFFFFu) {
@@ -1192,6 +1202,20 @@ __device__ __forceinline__ void decode_segments(const DecodeArgs& A, const Brick
     }
 }
 
+// One model's rANS table into shared memory, full or compact (compact_lut).
+template <class V>
+__device__ __forceinline__ void load_lut(uint32_t* lut, const uint32_t* __restrict__ g, uint32_t tid, uint32_t T) {
+    if (compact_lut<V>()) {
+        for (uint32_t i = tid; i < kTot; i += T) {
+            const uint32_t e = g[i];
+            reinterpret_cast<uint8_t*>(lut)[i] = (uint8_t)(e & 15u);
+            lut[kTot / 4 + (e & 15u)] = e;  // every x of a symbol stores the same entry
+        }
+    } else {
+        for (uint32_t i = tid; i < kTot; i += T) lut[i] = g[i];
+    }
+}
+
 // V = uint8_t when every requested brick's palette has fewer than 255 entries
 // (value 0xFF stands for "label 0"), uint16_t when every
 // palette of the dataset has fewer than 65535 entries (0xFFFF), else uint32_t.
@@ -1206,7 +1230,7 @@ __global__ void __launch_bounds__(dec_threads<V, KL>(), dec_ctas_per_sm<V, KL>()
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     constexpr uint32_t LABEL0 = sizeof(V) == 1 ? 0xFFu : (sizeof(V) == 2 ? 0xFFFFu : PIDX_LABEL0);
 
-    for (uint32_t i = tid; i < kTot; i += T) S.lut[i] = A.lut[i];
+    load_lut<V>(S.lut, A.lut, tid, T);
     if (tid == 0) {
         mbar_init(&S.bar);
         S.rewait = 0;
@@ -1268,7 +1292,7 @@ __global__ void __launch_bounds__(dec_threads<V, KL>(), dec_ctas_per_sm<V, KL>()
             continue;
         }
         if (model != cur_model) {  // made visible by the barrier after the palette copy
-            for (uint32_t i = tid; i < kTot; i += T) S.lut[i] = A.lut[(size_t)model * kTot + i];
+            load_lut<V>(S.lut, A.lut + (size_t)model * kTot, tid, T);
             cur_model = model;
         }
         const BrickDesc br = S.br;
@@ -1308,10 +1332,10 @@ __global__ void __launch_bounds__(dec_threads<V, KL>(), dec_ctas_per_sm<V, KL>()
                 }
             }
             if (staged)
-                decode_segments<false>(A, br, reinterpret_cast<const uint8_t*>(S.val), S.lut, n_need, nseg, recs,
+                decode_segments<false, compact_lut<V>()>(A, br, reinterpret_cast<const uint8_t*>(S.val), S.lut, n_need, nseg, recs,
                                        st, LABEL0);
             else
-                decode_segments<true>(A, br, A.enc + br.enc_off, S.lut, n_need, nseg, recs, st, LABEL0);
+                decode_segments<true, compact_lut<V>()>(A, br, A.enc + br.enc_off, S.lut, n_need, nseg, recs, st, LABEL0);
             __syncthreads();  // the staged stream is dead: its space becomes the level arrays
             if (S.rewait) {
                 // The late copy must land before the staging region is written: a second
