@@ -529,7 +529,7 @@ __global__ void __launch_bounds__(128) index_book_kernel(BrickDesc* __restrict__
     uint32_t op_base = 0, ip_base = 0, act_base = 0;  // ops, Pa ops and active ops before the chunk
     uint32_t lvl = 0, b_next = 8, act_cur = 0;        // level lvl+1 ends before op b_next; actives before its start
     uint32_t ls[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    uint32_t n_ck = 0, end_ops = 0xFFFFFFFFu;
+    uint32_t end_ops = 0xFFFFFFFFu;
     bool done = false;
     // each chunk's nibble word is loaded one chunk ahead
     uint32_t word_next = 8 * lane < nsym ? w[lane] : 0u;
@@ -537,18 +537,29 @@ __global__ void __launch_bounds__(128) index_book_kernel(BrickDesc* __restrict__
         const uint32_t base = c0 + 8 * lane;
         const uint32_t word = word_next;
         word_next = base + 256 < nsym ? w[(base + 256) >> 3] : 0u;
-        // symbols of this lane: [max(base, 1), min(base + 8, nsym)) -- symbol 0 is the root
-        const uint32_t i0 = base == 0 ? 1u : base, i1 = min(base + 8, nsym);
-        auto step = [&](uint32_t st, uint32_t k) -> uint32_t {
-            const uint32_t v = (word >> (4 * k)) & 15u;
-            return (st == 0 && (v >> 1) == OP_PD) ? 1u : 0u;
+        // The lane's eight nibbles as nibble-spaced masks (bit 4k: symbol base + k): V its symbols,
+        // [max(base, 1), min(base + 8, nsym)) -- symbol 0 is the root; PD the Pd codes, PA the Pa
+        // codes, ACT the nibbles whose stop bit is clear (an op there leaves its node active).
+        const uint32_t hi = nsym > base ? min(nsym - base, 8u) : 0u;
+        const uint32_t V = (hi == 8 ? 0x11111111u : (0x11111111u & ((1u << (4 * hi)) - 1u))) & (base == 0 ? ~1u : ~0u);
+        const uint32_t codes = (word >> 1) & 0x77777777u;
+        auto eq = [&](uint32_t K) {  // nibbles whose 3-bit code is K
+            const uint32_t x = codes ^ (K * 0x11111111u);
+            return ~(x | (x >> 1) | (x >> 2)) & 0x11111111u;
         };
-        uint32_t f0 = 0, f1 = 1;
-        for (uint32_t i = i0; i < i1; ++i) {
-            f0 = step(f0, i - base);
-            f1 = step(f1, i - base);
+        const uint32_t PD = eq(OP_PD) & V, PA = eq(OP_PA) & V, ACT = ~word & 0x11111111u & V;
+        // which nibbles start ops, from entry state 0 and from entry state 1 (1: the first nibble is
+        // a Pd op's delta), and the state after the lane's nibbles: the automaton unrolled
+        uint32_t s0 = 0, s1 = 1, S0 = 0, S1 = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t valid = (V >> (4 * k)) & 1u, pd = (PD >> (4 * k)) & 1u;
+            S0 |= (valid & (s0 ^ 1u)) << (4 * k);
+            S1 |= (valid & (s1 ^ 1u)) << (4 * k);
+            s0 = valid ? ((s0 ^ 1u) & pd) : s0;
+            s1 = valid ? ((s1 ^ 1u) & pd) : s1;
         }
-        uint32_t inc = f0 | (f1 << 1);
+        uint32_t inc = s0 | (s1 << 1);
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
             const uint32_t y = __shfl_up_sync(FULL, inc, d);
@@ -559,19 +570,8 @@ __global__ void __launch_bounds__(128) index_book_kernel(BrickDesc* __restrict__
         const uint32_t entry = (excl >> st_in) & 1u;
         const uint32_t exit_all = (__shfl_sync(FULL, inc, 31) >> st_in) & 1u;
         // this lane's op starts, Pa ops and active ops
-        uint32_t np = 0, npa = 0, nact = 0;
-        {
-            uint32_t st = entry;
-            for (uint32_t i = i0; i < i1; ++i) {
-                const uint32_t v = (word >> (4 * (i - base))) & 15u;
-                if (st == 0) {
-                    ++np;
-                    npa += (v >> 1) == OP_PA;
-                    nact += !(v & 1u);
-                }
-                st = step(st, i - base);
-            }
-        }
+        const uint32_t starts = entry ? S1 : S0;
+        const uint32_t np = __popc(starts), npa = __popc(starts & PA), nact = __popc(starts & ACT);
         const uint32_t packed = np | (npa << 10) | (nact << 20);
         uint32_t pin = packed;
 #pragma unroll
@@ -588,17 +588,10 @@ __global__ void __launch_bounds__(128) index_book_kernel(BrickDesc* __restrict__
             const bool has = my_op <= b_next && b_next < my_op + np;
             const uint32_t src = __ffs(__ballot_sync(FULL, has)) - 1;
             uint32_t ap = 0;
-            if (has) {  // actives among the ops before b_next
-                ap = my_act;
-                uint32_t st = entry, j = my_op;
-                for (uint32_t i = i0; i < i1 && j < b_next; ++i) {
-                    const uint32_t v = (word >> (4 * (i - base))) & 15u;
-                    if (st == 0) {
-                        ap += !(v & 1u);
-                        ++j;
-                    }
-                    st = step(st, i - base);
-                }
+            if (has) {  // actives among the ops before b_next: the lane's first b_next - my_op starts
+                uint32_t rest = starts;
+                for (uint32_t t = my_op; t < b_next; ++t) rest &= rest - 1u;
+                ap = my_act + __popc((starts ^ rest) & ACT);
             }
             ap = __shfl_sync(FULL, ap, src);
             ++lvl;
@@ -612,25 +605,14 @@ __global__ void __launch_bounds__(128) index_book_kernel(BrickDesc* __restrict__
             act_cur = ap;
             b_next += need;
         }
-        // checkpoints before every S-th op of the tree
-        {
-            uint32_t st = entry, j = my_op, ipr = my_ip, last = 0;
-            for (uint32_t i = i0; i < i1; ++i) {
-                const uint32_t v = (word >> (4 * (i - base))) & 15u;
-                if (st == 0) {
-                    if (j % S == 0 && j < end_ops) {
-                        const uint32_t c = j / S;
-                        if (c < br.ck_cap) ck[br.ck_off + c] = Checkpoint{0u, 0u, i, ipr};
-                        last = c + 1;
-                    }
-                    ipr += (v >> 1) == OP_PA;
-                    ++j;
-                }
-                st = step(st, i - base);
-            }
-#pragma unroll
-            for (int d = 16; d >= 1; d >>= 1) last = max(last, __shfl_xor_sync(FULL, last, d));
-            n_ck = max(n_ck, last);
+        // checkpoints before every S-th op of the tree (at most one per lane when S > 8)
+        for (uint32_t j = (my_op + S - 1) / S * S; j < my_op + np && j < end_ops; j += S) {
+            uint32_t rest = starts;  // the (j - my_op)-th start of the lane is rest's lowest bit
+            for (uint32_t t = my_op; t < j; ++t) rest &= rest - 1u;
+            const uint32_t p = __ffs(rest) - 1;
+            const uint32_t ipr = my_ip + __popc(starts & PA & ((1u << p) - 1u));
+            const uint32_t c = j / S;
+            if (c < br.ck_cap) ck[br.ck_off + c] = Checkpoint{0u, 0u, base + (p >> 2), ipr};
         }
         op_base += tot_np;
         ip_base += (ptot >> 10) & 1023u;
@@ -653,6 +635,8 @@ __global__ void __launch_bounds__(128) index_book_kernel(BrickDesc* __restrict__
             flags = BF_TRUNCATED;  // the stream ends inside the level structure
         }
     }
+    // a checkpoint before every S-th op below ops (those past ck_cap are not stored)
+    const uint32_t n_ck = (ops + S - 1) / S;
     if (lane == 0) {
         BrickDesc& o = bricks[bi];
         o.n_ops = ops;
