@@ -257,6 +257,7 @@ __global__ void __launch_bounds__(128) stage_gather_kernel(const uint8_t* __rest
 
 int stage_dataset(csv_ctx* ctx, const uint8_t* img, const ImageView& v, DeviceDataset& d, cudaStream_t st) {
     d.device = ctx->device;
+    d.pool = ctx->pool;
     d.nb = v.nb;
     d.b = v.b;
     d.L = levels_of(v.b);
@@ -316,8 +317,8 @@ int stage_dataset(csv_ctx* ctx, const uint8_t* img, const ImageView& v, DeviceDa
         return fail(ctx, CSV_ENOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
     uint8_t* d_img = nullptr;
     uint64_t* d_src = nullptr;
-    if ((e = cudaMallocAsync((void**)&d_img, std::max<size_t>(1, v.image_len), st)) != cudaSuccess ||
-        (e = cudaMallocAsync((void**)&d_src, 8 * src.size(), st)) != cudaSuccess) {
+    if ((e = tmp_alloc((void**)&d_img, std::max<size_t>(1, v.image_len), d.pool, st)) != cudaSuccess ||
+        (e = tmp_alloc((void**)&d_src, 8 * src.size(), d.pool, st)) != cudaSuccess) {
         cudaFreeAsync(d_img, st);
         cudaStreamSynchronize(st);
         return fail(ctx, CSV_ENOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
@@ -448,6 +449,20 @@ int csv_create(int device, csv_ctx** out) {
         delete c;
         return CSV_ECUDA;
     }
+    // The temporaries of each open (the image copy, the seek index's nibbles and snapshots: ~130 MB for
+    // a 27.9 MB image) come from a pool of the context that keeps up to 1 GiB of freed memory, so that
+    // the next open does not map it again; without a pool, the device's default one.
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if (cudaMemPoolCreate(&c->pool, &props) == cudaSuccess) {
+        uint64_t keep = 1ull << 30;
+        cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    } else {
+        c->pool = nullptr;
+        cudaGetLastError();
+    }
     *out = c;
     return CSV_OK;
 }
@@ -468,6 +483,7 @@ void csv_destroy(csv_ctx* ctx) {
     for (cudaEvent_t ev : ctx->pipe_event)
         if (ev) cudaEventDestroy(ev);
     encoder_state_free(ctx->enc);
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     delete ctx;
 }
 

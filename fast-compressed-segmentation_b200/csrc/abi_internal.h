@@ -20,6 +20,7 @@ struct csv_ctx {
     // the 64^3 outputs of bricks with 255 or more palette entries, when a split graph gives the
     // others to the 8-bit variant: a third launch, beside the first; created on first use
     csv::DecodeScratch scr_wide;
+    cudaMemPool_t pool = nullptr;  // stream-ordered temporaries of opens (keeps freed memory)
     uint32_t scr_wide_b = 0;
     csv::EncoderState* enc = nullptr;
     // csv_decode_image's pipeline: two chunk buffers (decode one while the

@@ -79,6 +79,9 @@ struct DeviceDataset {
     uint32_t n_models = 1;  // LUTs at d_lut (a version-2 image's tables; a concatenation keeps each part's)
     uint32_t fast_models = 0;  // bit m: model m's table is well formed (the seek index's fast step)
     float index_ms = 0;        // device time of the seek-index passes csv_open ran (0: none ran)
+    // pool for the stream-ordered temporaries of staging and the seek index (the opening context's;
+    // null: the device's default pool)
+    cudaMemPool_t pool = nullptr;
     uint32_t mixed_b = 0;   // a concatenation of different brick sizes
     uint64_t enc_pool_bytes = 0, pal_pool_entries = 0;  // sizes of d_enc and d_pal
     uint32_t* h_cost = nullptr;  // per brick: decode work estimate (nSymbols), for scheduling
@@ -89,6 +92,11 @@ struct DeviceDataset {
     uint32_t* d_lut = nullptr; // 4096 packed entries: sym | freq << 4 | start << 17
     uint32_t* h_ids = nullptr;
 };
+
+// A stream-ordered temporary from `pool`, or from the device's default pool when it is null.
+inline cudaError_t tmp_alloc(void** p, size_t bytes, cudaMemPool_t pool, cudaStream_t st) {
+    return pool ? cudaMallocFromPoolAsync(p, bytes, pool, st) : cudaMallocAsync(p, bytes, st);
+}
 
 // Launch helpers implemented in decode.cu.
 cudaError_t build_lut(const uint32_t* freq, const uint32_t* cum, uint32_t* h_lut);

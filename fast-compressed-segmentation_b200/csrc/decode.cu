@@ -792,16 +792,16 @@ cudaError_t index_alloc(const DeviceDataset& ds, cudaStream_t st, IndexTemps& t)
     if (ds.h_cost)
         std::stable_sort(order.begin(), order.end(),
                          [&](uint32_t a, uint32_t b) { return ds.h_cost[a] > ds.h_cost[b]; });
-    cudaError_t e = cudaMallocAsync((void**)&t.nib, words * 4, st);
-    if (e == cudaSuccess) e = cudaMallocAsync((void**)&t.snap, snaps * 8, st);
-    if (e == cudaSuccess) e = cudaMallocAsync((void**)&t.off, off.size() * 8, st);
-    if (e == cudaSuccess) e = cudaMallocAsync((void**)&t.order, (size_t)nb * 4, st);
+    cudaError_t e = tmp_alloc((void**)&t.nib, words * 4, ds.pool, st);
+    if (e == cudaSuccess) e = tmp_alloc((void**)&t.snap, snaps * 8, ds.pool, st);
+    if (e == cudaSuccess) e = tmp_alloc((void**)&t.off, off.size() * 8, ds.pool, st);
+    if (e == cudaSuccess) e = tmp_alloc((void**)&t.order, (size_t)nb * 4, ds.pool, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(t.order, order.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMallocAsync((void**)&t.chain, nb, st);
-    if (e == cudaSuccess) e = cudaMallocAsync((void**)&t.nck, (size_t)nb * 4, st);
-    if (e == cudaSuccess) e = cudaMallocAsync((void**)&t.bad, 4, st);
+    if (e == cudaSuccess) e = tmp_alloc((void**)&t.chain, nb, ds.pool, st);
+    if (e == cudaSuccess) e = tmp_alloc((void**)&t.nck, (size_t)nb * 4, ds.pool, st);
+    if (e == cudaSuccess) e = tmp_alloc((void**)&t.bad, 4, ds.pool, st);
     const uint32_t nm = ds.n_models ? ds.n_models : 1u;
-    if (e == cudaSuccess) e = cudaMallocAsync((void**)&t.lutf, (size_t)nm * kTot * 4, st);
+    if (e == cudaSuccess) e = tmp_alloc((void**)&t.lutf, (size_t)nm * kTot * 4, ds.pool, st);
     if (e == cudaSuccess) {
         index_fast_lut_kernel<<<(nm * kTot + 255) / 256, 256, 0, st>>>(ds.d_lut, nm * kTot, t.lutf);
         e = cudaGetLastError();
@@ -851,8 +851,8 @@ cudaError_t launch_build_index(DeviceDataset& ds, cudaStream_t st, const IndexSe
     cudaError_t e = index_alloc(ds, st, t);
     if (e == cudaSuccess && seeds) {
         const uint32_t n_pieces = seeds->piece_base.back();
-        e = cudaMallocAsync((void**)&d_base, 4 * seeds->piece_base.size(), st);
-        if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_seed, 8 * std::max<size_t>(1, seeds->seed.size()), st);
+        e = tmp_alloc((void**)&d_base, 4 * seeds->piece_base.size(), ds.pool, st);
+        if (e == cudaSuccess) e = tmp_alloc((void**)&d_seed, 8 * std::max<size_t>(1, seeds->seed.size()), ds.pool, st);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(d_base, seeds->piece_base.data(), 4 * seeds->piece_base.size(),
                                 cudaMemcpyHostToDevice, st);
@@ -920,8 +920,8 @@ cudaError_t index_seeds_of(const DeviceDataset& ds, cudaStream_t st, std::vector
             base[i + 1] = base[i] + n_seeds[i];
         }
         seeds.resize(base[nb]);
-        e = cudaMallocAsync((void**)&d_base, 4ull * (nb + 1), st);
-        if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_seeds, 8ull * std::max<uint32_t>(1, base[nb]), st);
+        e = tmp_alloc((void**)&d_base, 4ull * (nb + 1), ds.pool, st);
+        if (e == cudaSuccess) e = tmp_alloc((void**)&d_seeds, 8ull * std::max<uint32_t>(1, base[nb]), ds.pool, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(d_base, base.data(), 4ull * (nb + 1), cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess) {
             index_seeds_gather_kernel<<<(nb + 3) / 4, 128, 0, st>>>(ds.d_bricks, nb, t.chain, d_base, t.off + nb,
