@@ -77,7 +77,10 @@ typedef struct csv_dataset_info {
     uint32_t cum[16];
 } csv_dataset_info;
 
-/* ---- context -------------------------------------------------------- */
+/* ---- context --------------------------------------------------------
+ * A context keeps its decode scratch (grown to the largest brick size seen)
+ * and a stream-ordered memory pool for the temporaries of csv_open that holds
+ * up to 1 GiB of freed memory between opens; csv_destroy releases both. */
 int csv_create(int device, csv_ctx** out);
 void csv_destroy(csv_ctx* ctx);
 const char* csv_last_error(const csv_ctx* ctx);
