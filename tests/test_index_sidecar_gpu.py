@@ -213,3 +213,33 @@ def test_sidecar_mismatch_is_refused(codec, golden):
     assert st.max() == 0
     assert [sha(out[k]) for k in range(out.shape[0])] == golden["shipped_subset"]["lod"]["6"]
     ds.close()
+
+
+def test_repeated_opens_hold_steady_memory(codec):
+    """The temporaries of csv_open (the image copy, the seek index's nibbles and snapshots) come from the
+    context's pool, which keeps freed memory for the next open: after the first opens, more opens of the same
+    image (with and without its sidecar) take no further device memory, and the index is the same each time."""
+    import torch
+    vol = torch.empty((128, 128, 192), dtype=torch.int64, device="cuda")
+    codec.synth_volume(vol, 1, 400, 80, 1.0, 5.0, 0.1, 21)
+    codec.encode_device(vol, 64)
+    img = bytes(codec.encoded_image_tensor().cpu().numpy())
+    del vol
+    torch.cuda.synchronize()
+    first = codec.open(img)
+    sc = first.index_sidecar()
+    ref, _ = decode_all(codec, first, 6)
+    first.close()
+    for s in (None, sc):  # warm the pool for both paths
+        codec.open(img, sidecar=s).close()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for k in range(12):
+        ds = codec.open(img, sidecar=sc if k % 2 else None)
+        if k in (5, 10):
+            out, st = decode_all(codec, ds, 6)
+            assert st.max() == 0 and np.array_equal(out, ref)
+        ds.close()
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free0 - free1 < (64 << 20), (free0, free1)
