@@ -339,3 +339,64 @@ def test_graph_three_parts_by_palette_size(codec, oracle):
     cat.close()
     for d in dss:
         d.close()
+
+
+def test_palette_size_boundary_254_255(codec, oracle):
+    """The 8-bit node values stop at palettes of 254 entries (0xFF is kept for label 0): a brick with 254
+    distinct labels and one with 255, decoded at every LOD by csv_decode_batch (the dataset as a whole takes
+    16 bits), by a split graph (the first brick's 64^3 output in the 8-bit kernel, the second's in the
+    16-bit one), and alone (the 254-label image takes 8 bits in both variants), all equal to the oracle."""
+    import torch
+    from csvb200 import DecodeConfig, requests, requests_tensor
+    # one label per x-row of 4^3 blocks (the rows past n - 1 keep the last one); n = 158 and 159 give the
+    # encoder's palettes of exactly 254 and 255 entries (its coarse levels add entries of their own)
+    def brick(n):
+        labels = np.random.default_rng(5).integers(1, 1 << 62, n, dtype=np.uint64)
+        sub = np.zeros((16, 16, 16), np.uint64)
+        for bz in range(16):
+            for by in range(16):
+                sub[bz, by, :] = labels[min(16 * bz + by, n - 1)]
+        return np.repeat(np.repeat(np.repeat(sub, 4, 0), 4, 1), 4, 2)
+    vol = np.zeros((64, 64, 128), np.uint64)
+    vol[:, :, :64] = brick(158)
+    vol[:, :, 64:] = brick(159)
+    img_both = codec.encode(vol, 64)
+    img_254 = codec.encode(np.ascontiguousarray(vol[:, :, :64]), 64)
+    for img, pals in ((img_both, (254, 255)), (img_254, (254,))):
+        o, got = 152, []
+        for _ in pals:
+            P = int(np.frombuffer(img[o + 4:o + 8], np.uint32)[0])
+            got.append(P)
+            o += 8 + 8 * P
+            E = int(np.frombuffer(img[o:o + 4], np.uint32)[0])
+            o += 4 + E + 4
+        assert tuple(got) == pals
+        ref = {t: oracle.decode_image(img, t)[0] for t in range(7)}
+        ds = codec.open(img)
+        nb = len(pals)
+        bricks = np.concatenate([np.arange(nb)] * 7)
+        lods = np.repeat(np.arange(7), nb)
+        sizes = 8 ** lods.astype(np.uint64)
+        dst = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.uint64)
+        reqs = requests(bricks, lods, dst)
+        total = int(sizes.sum())
+        outs = []
+        out = torch.full((total,), -3, dtype=torch.int64, device="cuda")
+        st = torch.full((len(reqs),), -1, dtype=torch.int32, device="cuda")
+        codec.decode_batch(ds, requests_tensor(reqs), out, st)
+        torch.cuda.synchronize()
+        outs.append((out.cpu().numpy().view(np.uint64), st.cpu().numpy()))
+        for layout in (0, 1, 2):
+            out = torch.full((total,), -3, dtype=torch.int64, device="cuda")
+            st = torch.full((len(reqs),), -1, dtype=torch.int32, device="cuda")
+            g = codec.decode_graph(ds, requests_tensor(reqs), out, st, DecodeConfig(0, 1, 0, layout))
+            g.launch()
+            torch.cuda.synchronize()
+            g.close()
+            outs.append((out.cpu().numpy().view(np.uint64), st.cpu().numpy()))
+        for o_, s_ in outs:
+            assert int(np.abs(s_).max()) == 0
+            for k in range(len(bricks)):
+                r = ref[int(lods[k])][int(bricks[k])]
+                assert np.array_equal(o_[int(dst[k]):int(dst[k]) + len(r)], r), (pals, k)
+        ds.close()
