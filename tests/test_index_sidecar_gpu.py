@@ -243,3 +243,36 @@ def test_repeated_opens_hold_steady_memory(codec):
     torch.cuda.synchronize()
     free1 = torch.cuda.mem_get_info()[0]
     assert free0 - free1 < (64 << 20), (free0, free1)
+
+
+@pytest.mark.parametrize("b", [32, 64])
+def test_sidecar_of_a_version2_image(codec, b):
+    """A version-2 image (each brick names its mode and one of several shared rANS tables): the seeded pieces
+    of the bricks on tables other than the first read those tables from global memory.  The sidecar of the
+    image opened from its bytes equals the encoder's dataset's, and opening with it decodes every LOD like
+    csv_open."""
+    import torch
+    from csvb200.selector import fit_tables
+    v = torch.empty((64, 128, 128), dtype=torch.int64, device="cuda")
+    codec.synth_volume(v, 1, 120, 30, 1.5, 5.0, 0.2, 31 + b)
+    nb = (64 // b) * (128 // b) * (128 // b)
+    hist = torch.empty((nb, 12, 16), dtype=torch.int32, device="cuda")
+    codec.encode_stats(v, b, hist)
+    tables = fit_tables(hist.cpu().numpy().astype(np.uint64), 6, iters=4)
+    rng = np.random.default_rng(b)
+    choice = torch.from_numpy(rng.integers(0, 12, nb) | (rng.integers(0, len(tables), nb) << 4)).to(torch.uint8)
+    codec.encode_device_sel(v, b, tables, choice.cuda())
+    img = bytes(codec.encoded_image_tensor().cpu().numpy())
+    del v
+    assert struct.unpack_from("<I", img, 4)[0] == 2
+    dse = codec.open_encoded()
+    ds = codec.open(img)
+    sc = ds.index_sidecar()
+    assert dse.index_sidecar() == sc
+    ds2 = codec.open(img, sidecar=sc)
+    for t in range(b.bit_length()):
+        a, sa = decode_all(codec, ds, t)
+        c, sc2 = decode_all(codec, ds2, t)
+        assert sa.max() == 0 and np.array_equal(sa, sc2) and np.array_equal(a, c), t
+    for d in (dse, ds, ds2):
+        d.close()
