@@ -647,10 +647,10 @@ __global__ void __launch_bounds__(128) index_book_kernel(BrickDesc* __restrict__
     }
 }
 
-// One block per brick: its threads share the brick's checkpoints, so a long
-// brick's re-decodes spread over the block instead of one warp (the table is
-// read through L1: the decodes are short).
-__global__ void __launch_bounds__(128) index_states_kernel(const BrickDesc* __restrict__ bricks, uint32_t nb,
+// One block of 512 threads per brick: its threads share the brick's checkpoints,
+// so a long brick's re-decodes spread over the block instead of one warp (the
+// table is read through L1: the decodes are short).
+__global__ void __launch_bounds__(512) index_states_kernel(const BrickDesc* __restrict__ bricks, uint32_t nb,
                                                           const uint8_t* __restrict__ enc_pool,
                                                           const uint32_t* __restrict__ g_lut, uint32_t n_models,
                                                           const uint64_t* __restrict__ snap_off,
@@ -883,7 +883,7 @@ cudaError_t launch_build_index(DeviceDataset& ds, cudaStream_t st, const IndexSe
     if (e == cudaSuccess) {
         index_book_kernel<<<(nb + 3) / 4, 128, 0, st>>>(ds.d_bricks, nb, t.nib, t.off, t.chain, ds.d_ck, t.nck, ds.L,
                                                        ds.S);
-        index_states_kernel<<<nb, 128, 0, st>>>(ds.d_bricks, nb, ds.d_enc, ds.d_lut, nm, t.off + nb,
+        index_states_kernel<<<nb, 512, 0, st>>>(ds.d_bricks, nb, ds.d_enc, ds.d_lut, nm, t.off + nb,
                                                          t.snap, t.nck, ds.d_ck);
         e = cudaGetLastError();
     }
